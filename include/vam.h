@@ -1,0 +1,262 @@
+/*
+ * vam.h -- C ABI of the B200 (sm_100a) tomographic projection core.
+ *
+ * Every entry point takes plain pointers, sizes and a CUDA stream, returns an
+ * int status (VAM_OK == 0) and is stream-ordered: nothing blocks the host, no
+ * entry point allocates device memory after plan creation, so every compute
+ * call may be captured in a CUDA graph.  Device pointers are marked `_dev`;
+ * everything else is host memory.  `vam_stream_t` is ABI-compatible with
+ * `cudaStream_t` (pass 0 for the legacy default stream).
+ *
+ * Array layouts follow the reference toolbox (C order, last index fastest):
+ *   target volume      x[nY][nX][nZ]        (vamtoolbox/geometry.py:224)
+ *   parallel sinogram  b[nR][nA][nZ], nR=nY (vamtoolbox/projector/Projector3DParallel.py:129-131)
+ *   ray-traced grid    f[nX][nY][nZ]        (vamtoolbox/medium.py:37-40, xg shape)
+ *   ray sinogram       g[nR*nA*nZr]         (vamtoolbox/projector/pyTorchRayTrace.py:1629-1632)
+ */
+#ifndef VAM_H
+#define VAM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* vam_stream_t;
+
+enum vam_status {
+    VAM_OK = 0,
+    VAM_ERR_ARG = 1,      /* null pointer, bad enum, non-finite parameter      */
+    VAM_ERR_SHAPE = 2,    /* inconsistent or unsupported sizes                  */
+    VAM_ERR_CUDA = 3,     /* a CUDA runtime call failed (message has the name)  */
+    VAM_ERR_TIMEOUT = 4,  /* a bounded device wait ran out                      */
+    VAM_ERR_NOTSUP = 5,   /* option combination not implemented                 */
+    VAM_ERR_NOMEM = 6     /* plan-time allocation failed                        */
+};
+
+/* Message of the last failing call on the calling host thread ("" if none). */
+const char* vam_last_error_string(void);
+/* Library version string, e.g. "vamcore 1.0 sm_100a". */
+const char* vam_version(void);
+
+/* ======================================================================= */
+/* Parallel-beam projector family                                          */
+/* ======================================================================= */
+
+typedef struct vam_parallel_plan vam_parallel_plan;
+
+typedef struct {
+    int32_t n_y, n_x, n_z;     /* target array shape; the reference requires n_x == n_y */
+    int32_t n_angles;
+    const double* angles_deg;  /* host, n_angles projection angles in degrees */
+    int32_t device;            /* CUDA device ordinal the plan lives on */
+} vam_parallel_geom;
+
+/* Builds per-angle tables (cos, sin, warp offsets), the inscribed-circle mask
+ * and the workspace.  Replaces the constructor of
+ * Projector3DParallelPython (vamtoolbox/projector/Projector3DParallel.py:57-75)
+ * and Projector2DParallelPython (Projector2DParallel.py:47-68). */
+int vam_parallel_plan_create(const vam_parallel_geom* geom, vam_parallel_plan** out);
+int vam_parallel_plan_destroy(vam_parallel_plan* plan);
+
+enum vam_absorption_mode {
+    VAM_ABS_NONE = 0,
+    VAM_ABS_MASK = 1,  /* radial mask exp(-a(R-r)): vamtoolbox/geometry.py:161-193,
+                          applied as in Projector3DParallel.py:28-29,51-52          */
+    VAM_ABS_RAY = 2    /* per-sample exp(-a*max(0, s - s_entry(t))), s_entry = -sqrt(R^2-t^2),
+                          zero for |t|>R: the ray model of astra3Dabsorption.py:129-145
+                          expressed in the projector's own (t, s) frame               */
+};
+
+/* Absorption weighting used by forward / backward_ref / adjoint.
+ * MASK: mask_dev is an [nY][nX] device array (broadcast over z), copied.
+ * RAY : alpha_per_px (1/pixel) and radius_px (container radius in pixels). */
+int vam_parallel_set_absorption(vam_parallel_plan* plan, int mode, const float* mask_dev,
+                                float alpha_per_px, float radius_px, vam_stream_t stream);
+
+/* Occlusion from an attenuation field / insert: insert_dev is [nY][nX][nZ];
+ * voxels > 0 are opaque.  Builds the occlusion sinogram of
+ * Projector3DParallelPython.generateOccSinogram (Projector3DParallel.py:77-111)
+ * on the device; later forward/backward_ref/adjoint calls apply the shadow
+ * (Projector3DParallel.py:147-153, 192-201, 209-216). */
+int vam_parallel_set_occlusion(vam_parallel_plan* plan, const float* insert_dev, vam_stream_t stream);
+int vam_parallel_clear_occlusion(vam_parallel_plan* plan);
+/* Copies the occlusion sinogram ([nR][nA][nZ], NaN where a column has no
+ * occluder) into out_dev.  VAM_ERR_ARG if no occlusion is set. */
+int vam_parallel_get_occlusion_sinogram(vam_parallel_plan* plan, float* out_dev, vam_stream_t stream);
+
+/* R1 forward: rotate-and-sum Radon transform with bilinear sampling, zero
+ * outside the image, detector width nY.  Replaces
+ * Projector3DParallelPython.forward (Projector3DParallel.py:113-156). */
+int vam_parallel_forward(vam_parallel_plan* plan, const float* vol_dev, float* sino_dev,
+                         vam_stream_t stream);
+
+/* R2 reference-parity backprojection: pixel-driven, linear interpolation
+ * along the detector with zero outside (np.interp left=right=0), then the
+ * inscribed-circle clip.  Replaces Projector3DParallelPython.backward
+ * (Projector3DParallel.py:158-207).  Not the transpose of R1. */
+int vam_parallel_backward_ref(vam_parallel_plan* plan, const float* sino_dev, float* vol_dev,
+                              vam_stream_t stream);
+
+/* Matched transpose of R1 (<A x, y> == <x, A^T y>), gather form, no atomics.
+ * No counterpart in the reference (its backward is R2); used for autograd. */
+int vam_parallel_adjoint(vam_parallel_plan* plan, const float* sino_dev, float* vol_dev,
+                         vam_stream_t stream);
+
+/* ======================================================================= */
+/* Curved-ray tracer (graded-index medium)                                 */
+/* ======================================================================= */
+
+typedef struct vam_ray_plan vam_ray_plan;
+
+enum vam_ray_param { VAM_PARAM_PHYSICAL = 0, VAM_PARAM_CANONICAL = 1, VAM_PARAM_OPTICAL = 2 };
+enum vam_ray_solver { VAM_ODE_SYMPLECTIC_EULER = 0, VAM_ODE_EULER = 1, VAM_ODE_LEAPFROG = 2 };
+enum vam_index_kind { VAM_INDEX_HOMOGENEOUS = 0, VAM_INDEX_GRID = 1, VAM_INDEX_LUNEBURG = 2 };
+enum vam_alpha_kind { VAM_ALPHA_ZERO = 0, VAM_ALPHA_CYLINDER = 1, VAM_ALPHA_BALL = 2, VAM_ALPHA_GRID = 3 };
+
+typedef struct {
+    int32_t n_x, n_y, n_z;      /* grid shape (nZ == 1 for a 2D problem) */
+    double coord_min[3];        /* xv[0], yv[0], zv[0]   (vamtoolbox/medium.py:44-51) */
+    double coord_max[3];        /* xv[-1], yv[-1], zv[-1] */
+    double voxel[3];            /* xv[1]-xv[0] ...; voxel[2] = +inf in 2D (medium.py:52-56) */
+    double step_size;           /* parameter step h (pyTorchRayTrace.py:44-46) */
+    int32_t max_num_step;       /* step cap (pyTorchRayTrace.py:47-49) */
+    int32_t num_step_per_exit_check; /* exit test cadence (pyTorchRayTrace.py:233) */
+    int32_t parametrization;    /* enum vam_ray_param */
+    int32_t ode_solver;         /* enum vam_ray_solver */
+    int64_t num_rays;
+    int32_t device;
+} vam_ray_geom;
+
+typedef struct {
+    int32_t index_kind;         /* enum vam_index_kind (vamtoolbox/medium.py:276-473) */
+    float n_sur;                /* homogeneous / Luneburg surround index */
+    float lune_R, lune_p;       /* Luneburg radius (physical) and power */
+    const float* n_grid_dev;    /* [nX][nY][nZ] index samples (GRID) */
+    const float* grad_n_grid_dev; /* [nX][nY][nZ][3] gradient samples (GRID) */
+    int32_t atten_kind;         /* enum vam_alpha_kind (medium.py:753-915) */
+    float atten_value;          /* alpha_internal for CYLINDER / BALL */
+    float atten_R;              /* physical radius for CYLINDER / BALL */
+    const float* atten_grid_dev;/* [nX][nY][nZ] (GRID, zero padding) */
+    const float* absorb_at_grid_dev; /* [nX][nY][nZ] absorption coefficient at the grid
+                                        points: pyTorchRayTrace.py:458-462, 515-519 */
+} vam_ray_medium;
+
+/* Ray starting states: x0_dev, v0_dev are [num_rays][3] float32 (the
+ * RayState.setupRaysParallel layout, pyTorchRayTrace.py:1515-1666), copied
+ * into the plan; energy0 is the per-ray initial energy of the forward
+ * (ray_density^-1 in 2D or ^-2 in 3D, :1682-1686).  The plan owns a grid-sized
+ * scratch buffer and a float4 texel copy of the index field. */
+int vam_ray_plan_create(const vam_ray_geom* geom, const float* x0_dev, const float* v0_dev,
+                        float energy0, vam_ray_plan** out);
+int vam_ray_plan_destroy(vam_ray_plan* plan);
+
+/* Binds the medium (IndexModel / AttenuationModel / absorption at the grid
+ * points, vamtoolbox/medium.py:276-915) to the plan: grid fields are copied
+ * into the plan's packed layout, so later calls read the plan, not the
+ * caller's buffers.  Call again after changing a field. */
+int vam_ray_set_medium(vam_ray_plan* plan, const vam_ray_medium* medium, vam_stream_t stream);
+
+/* R6 forward (integrate): g[r] = sum over steps and trilinear corners of
+ * f[corner] * alpha_abs[corner] * (h/voxel_x) * w_corner * E(s).  Replaces
+ * PyTorchRayTracingPropagator.forward (pyTorchRayTrace.py:87-107) ->
+ * integrateEnergyUntilExit (:471-571).  f is not modified (the reference
+ * multiplies its input in place, :515-519). */
+int vam_ray_integrate(vam_ray_plan* plan, const float* f_dev, float* g_dev, vam_stream_t stream);
+
+/* R5 adjoint (deposit): dose = alpha_abs * sum over rays/steps/corners of
+ * g[r] * (h/voxel_x) * w_corner * E(s), accumulated with float32 atomics.
+ * Replaces PyTorchRayTracingPropagator.backward (pyTorchRayTrace.py:109-133)
+ * -> depositEnergyUntilExit (:378-469).  dose_dev is overwritten. */
+int vam_ray_deposit(vam_ray_plan* plan, const float* g_dev, float* dose_dev, vam_stream_t stream);
+
+/* Gradients of L = sum_r w[r] * integrate(f)[r]:
+ *   grad_att_dev[v] += dL/d alpha_att[v]  (GRID attenuation only), through the
+ *                      exp(-integral alpha ds) energy decay, each ray's path
+ *                      traced twice (total, then suffix sums) instead of stored;
+ *   grad_abs_dev[v] += dL/d alpha_abs[v] = f[v] * sum of the deposit of w at v.
+ * Either output may be null.  No counterpart in the reference (it has no
+ * differentiable ray tracer). */
+int vam_ray_grad_alpha(vam_ray_plan* plan, const float* f_dev, const float* w_dev,
+                       float* grad_att_dev, float* grad_abs_dev, vam_stream_t stream);
+
+/* Number of rays still active when the step cap was reached in the last
+ * integrate/deposit call (the reference logs an ERROR for this,
+ * pyTorchRayTrace.py:464-467).  Synchronises the device. */
+int vam_ray_active_at_cap(vam_ray_plan* plan, int64_t* out_count);
+
+/* ======================================================================= */
+/* Optimizer iteration bodies (vamtoolbox/optimizer/*.py)                   */
+/* ======================================================================= */
+
+/* Workspace for the reductions below, in bytes, for arrays of n elements. */
+size_t vam_reduce_workspace_bytes(int64_t n);
+
+enum vam_reduce_op { VAM_RED_MAX = 0, VAM_RED_MIN = 1, VAM_RED_SUM = 2 };
+
+/* out_dev[0] = op over x[0..n) (float, deterministic two-level tree). */
+int vam_reduce(const float* x_dev, int64_t n, int op, float* out_dev, void* work_dev,
+               size_t work_bytes, vam_stream_t stream);
+
+/* Volumetric error rate (vamtoolbox/metrics.py:47-87): out_dev[0] =
+ * #(void >= min(gel)) / (#gel + #void).  mask_dev: 1 = gel, 2 = void, 0 = outside. */
+int vam_metric_ver(const float* x_dev, const uint8_t* mask_dev, int64_t n, float* out_dev,
+                   void* work_dev, size_t work_bytes, vam_stream_t stream);
+
+/* BCLP state update, one pass over the dose (vamtoolbox/optimizer/BCLP.py:277-437):
+ * mapped = response(dose) (interpolation table), e = mapped - f_T,
+ * eb = |e| - eps, v = eb > 0, operand = v*w*|eb|^(p-1)*sign(e)*dresponse(dose).
+ * stats_dev[0..8] = { sum v*w*|eb|^p, l0, l0_eps0, l1, l1_eps0, l2^2, l2_eps0^2, lf, lf_eps0 }.
+ * Scalars: eps / weight are arrays when eps_dev / weight_dev are non-null. */
+typedef struct {
+    const float* table_f;       /* device, n_table sample points (uniformly spaced) */
+    const float* table_map;     /* device, response at the sample points */
+    const float* table_dmap;    /* device, derivative at the sample points */
+    int32_t n_table;
+    float table_f0;             /* table_f[0] (host copy, seeds the bin search) */
+    float table_inv_step;       /* (n_table - 1) / (table_f[n-1] - table_f[0]) */
+    float eps, weight, p;
+    const float* eps_dev;       /* optional per-voxel eps */
+    const float* weight_dev;    /* optional per-voxel weight */
+} vam_bclp_params;
+
+int vam_bclp_dose_pass(const float* dose_dev, const float* target_dev, int64_t n,
+                       const vam_bclp_params* prm, float* mapped_dev, float* operand_dev,
+                       float* stats_dev, void* work_dev, size_t work_bytes, vam_stream_t stream);
+
+/* g = clip(g - lr * pref * grad, lo, hi) with pref = q*L^((q-p)/q), L =
+ * stats_dev[0]^(q/p), and pref = 1 when L == 0 (BCLP.py:370-375, 477-534).
+ * has_hi == 0 means no upper bound. */
+int vam_bclp_sino_update(float* g_dev, const float* grad_dev, int64_t n, float lr, float p,
+                         float q, float lo, float hi, int has_hi, const float* stats_dev,
+                         vam_stream_t stream);
+
+/* Elementwise helpers used by CAL / OSMO / PM iteration bodies. */
+/* y = 1/(1+exp(-(x*scale_dev[0]^-1 - d)/g)) - t   (CAL.py:147-175 with x normalised by a device max) */
+int vam_cal_threshold(const float* x_dev, const float* xmax_dev, const float* target_dev, int64_t n,
+                      float d_h, float g, float* out_dev, vam_stream_t stream);
+/* b = clip(b - lr*(db*(1-m) + db_prev*m/(1-m^(it+1))), 0)   (CAL.py:177-186) */
+int vam_cal_sino_update(float* b_dev, const float* db_dev, const float* db_prev_dev, int64_t n,
+                        float lr, float momentum, int32_t iter, vam_stream_t stream);
+/* x = max(x/scale_dev[0], floor_val) when apply_floor, else x/scale_dev[0] */
+int vam_scale_by_device(float* x_dev, const float* scale_dev, int64_t n, int apply_floor,
+                        float floor_val, vam_stream_t stream);
+/* OSMO model update (OSMO.py:36-109), with xn = x / xmax_dev[0] (xmax_dev may be
+ * null when x is already normalised): gel voxels (mask == 1, gel != 0)
+ * xm += max(d_h - xn, 0); void voxels (mask == 2, gel == 0) xm -= max(xn - d_l, 0). */
+int vam_osmo_model_update(float* xm_dev, const float* x_dev, const float* xmax_dev,
+                          const uint8_t* mask_dev, int64_t n, int gel, float d, vam_stream_t stream);
+
+/* Graph-friendly log append: row = counter_dev[0]; if row < cap_rows,
+ * arr_dev[row*n + i] = src_dev[i] for i < n; then counter_dev[0] += 1.  Lets a
+ * captured iteration record per-iteration scalars (loss, norms, VER) without
+ * per-iteration kernel arguments (BCLP.py LogPerf :14-135, CAL.py / OSMO.py error arrays). */
+int vam_append(const float* src_dev, int32_t n, float* arr_dev, int32_t* counter_dev, int32_t cap_rows,
+               vam_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VAM_H */

@@ -1,0 +1,244 @@
+"""Generate the golden vectors under tests/golden/ by running the reference.
+
+Run in a checkout that has the reference tree (default /root/reference, or
+VAM_REFERENCE_ROOT):
+
+    python tests/golden/make_golden.py
+
+Every array stored here is produced by the reference's own Python code
+(Projector3DParallelPython, Projector2DParallelPython, the PyTorch ray tracer
+on the CPU, the CAL / OSMO / BCLP optimizers), loaded through
+oracle/refload.py.  The only restated routine on that path is
+skimage.transform.warp (absent here), see oracle/refload.py.  Inputs are
+seeded synthetic targets; sizes are small so the fixtures stay a few hundred KB.
+"""
+from __future__ import annotations
+
+import sys
+import warnings
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+from oracle import refload  # noqa: E402
+
+OUT = Path(__file__).resolve().parent
+
+
+def ellipses_target(n, nz, rng, n_ell=4):
+    y, x = np.mgrid[:n, :n] - (n - 1) / 2
+    t = np.zeros((n, n, nz))
+    for z in range(nz):
+        img = np.zeros((n, n))
+        for _ in range(n_ell):
+            cy, cx = rng.uniform(-n / 4, n / 4, 2)
+            a, b = rng.uniform(n / 10, n / 3, 2)
+            th = rng.uniform(0, np.pi)
+            xr = (x - cx) * np.cos(th) + (y - cy) * np.sin(th)
+            yr = -(x - cx) * np.sin(th) + (y - cy) * np.cos(th)
+            img[(xr / a) ** 2 + (yr / b) ** 2 <= 1] = 1.0
+        t[:, :, z] = img
+    return t
+
+
+def parallel_cases(vam):
+    geo = vam.geometry
+    P3 = vam.projector.Projector3DParallel.Projector3DParallelPython
+    out = {}
+    rng = np.random.default_rng(1234)
+    for tag, n, nz, na, full in (("even", 24, 3, 16, 360.0), ("odd", 25, 2, 13, 180.0)):
+        x = rng.uniform(0, 1, (n, n, nz))
+        ang = np.linspace(0, full, na, endpoint=False)
+        tg = geo.TargetGeometry(target=x.copy(), clip_to_circle=False)
+        pg = geo.ProjectionGeometry(ang, "parallel", CUDA=False, attenuation_field=np.zeros((n, n, nz)))
+        A = P3(tg, pg)
+        b = A.forward(x.copy())
+        bb = rng.uniform(0, 1, b.shape)
+        xb = A.backward(bb.copy())
+        out[f"{tag}_x"] = x
+        out[f"{tag}_angles"] = ang
+        out[f"{tag}_fwd"] = b
+        out[f"{tag}_b"] = bb
+        out[f"{tag}_bwd"] = xb
+    # occlusion: an opaque insert (attenuation_field > 0)
+    n, nz, na = 24, 2, 12
+    x = ellipses_target(n, nz, rng)
+    ins = np.zeros((n, n, nz))
+    ins[9:13, 14:18, :] = 1.0
+    ins[4:6, 6:9, 1] = 1.0
+    ang = np.linspace(0, 360, na, endpoint=False)
+    tg = geo.TargetGeometry(target=x.copy(), clip_to_circle=False)
+    pg = geo.ProjectionGeometry(ang, "parallel", CUDA=False, attenuation_field=ins.copy())
+    A = P3(tg, pg)
+    b = A.forward(x.copy())
+    bb = rng.uniform(0, 1, b.shape)
+    out["occ_x"] = x
+    out["occ_insert"] = ins
+    out["occ_angles"] = ang
+    out["occ_sino"] = A.occ_sinogram
+    out["occ_fwd"] = b
+    out["occ_b"] = bb
+    out["occ_bwd"] = A.backward(bb.copy())
+    # 2D class (reachable after segmentZ(int)): forward clips its input
+    P2 = vam.projector.Projector2DParallel.Projector2DParallelPython
+    n, na = 20, 10
+    x2 = rng.uniform(0, 1, (n, n))
+    ang = np.linspace(0, 360, na, endpoint=False)
+    tg = geo.TargetGeometry(target=x2.copy(), clip_to_circle=False)
+    tg.segmentZ(0)
+    # Projector2DParallel.py:205 reads target_geo.target, which TargetGeometry
+    # never sets (AttributeError in the reference); alias it to the array.
+    tg.target = tg.array
+    pg = geo.ProjectionGeometry(ang, "parallel", CUDA=False)
+    A2 = P2(tg, pg)
+    out["p2_x"] = x2
+    out["p2_angles"] = ang
+    out["p2_fwd"] = A2.forward(x2.copy())
+    bb = rng.uniform(0, 1, (n, na))
+    out["p2_b"] = bb
+    out["p2_bwd"] = A2.backward(bb.copy())
+    # absorption mask (geometry.py:161-193) for a 3-D target
+    n = 24
+    tg = geo.TargetGeometry(target=np.ones((n, n, 2)))
+    pg = geo.ProjectionGeometry(np.array([0.0]), "parallel", projector_pixel_size=0.01,
+                                absorption_coeff=2.0, container_radius=0.15)
+    pg.calcAbsorptionMask(tg)
+    out["mask"] = np.ascontiguousarray(pg.absorption_mask[:, :, 0])
+    out["mask_params"] = np.array([0.01, 2.0, 0.15])
+    np.savez_compressed(OUT / "parallel.npz", **out)
+
+
+def ray_cases(vam):
+    import torch
+
+    geo, med = vam.geometry, vam.medium
+    RT = vam.projector.pyTorchRayTrace
+    out = {}
+    rng = np.random.default_rng(99)
+    for tag, (n, nz) in (("r3", (12, 6)), ("r2", (14, 1))):
+        t = rng.uniform(0, 1, (n, n, nz))
+        tg = geo.TargetGeometry(target=t if nz > 1 else t[:, :, 0])
+        cv = tg.constructCoordVec()
+        xg, yg, zg = np.meshgrid(*cv, indexing="ij")
+        R = np.amax(cv[0])
+        r2 = (xg ** 2 + yg ** 2) / R ** 2
+        n_x = 1.30 + 0.05 * r2 + 0.01 * rng.uniform(-1, 1, xg.shape)
+        alpha_x = 20.0 * (1 + 0.3 * rng.uniform(-1, 1, xg.shape))
+        im = med.IndexModel(cv, type="interpolation", form="freeform", n_x=torch.as_tensor(n_x))
+        am = med.AttenuationModel(cv, type="interpolation", form="freeform", alpha_x=torch.as_tensor(alpha_x))
+        ang = np.linspace(0, 360, 5, endpoint=False)
+        pg = geo.ProjectionGeometry(ang, "ray_trace", CUDA=False, index_model=im, attenuation_model=am,
+                                    absorption_model=am, ray_trace_method="eikonal",
+                                    eikonal_parametrization="physical_path_length",
+                                    ray_trace_ode_solver="forward_symplectic_euler",
+                                    ray_trace_ray_config="parallel", inclination_angle=0.0, ray_density=1)
+        P = RT.PyTorchRayTracingPropagator(tg, pg)
+        f = rng.uniform(0, 1, tg.array.shape)
+        g = P.forward(f.copy())
+        gin = rng.uniform(0, 1, g.shape).astype(np.float32)
+        dose = P.backward(gin.copy())
+        out[f"{tag}_xv"], out[f"{tag}_yv"], out[f"{tag}_zv"] = cv
+        out[f"{tag}_n"] = n_x
+        out[f"{tag}_alpha"] = alpha_x
+        out[f"{tag}_angles"] = ang
+        out[f"{tag}_x0"] = P.ray_state.x_0.numpy()
+        out[f"{tag}_v0"] = P.ray_state.v_0.numpy()
+        out[f"{tag}_f"] = f
+        out[f"{tag}_fwd"] = g
+        out[f"{tag}_g"] = gin
+        out[f"{tag}_bwd"] = dose
+        out[f"{tag}_step"] = np.array([P.tracing_step_size, P.max_num_step])
+    # analytic media: homogeneous index (n_sur = 1) and absorbing cylinder
+    n, nz = 12, 4
+    tg = geo.TargetGeometry(target=np.ones((n, n, nz)))
+    cv = tg.constructCoordVec()
+    im = med.IndexModel(cv, type="analytical", form="homogeneous", n_sur=1.0)
+    am = med.AttenuationModel(cv, type="analytical", form="homogeneous_cylinder", R=1, alpha_internal=30.0)
+    ang = np.linspace(0, 360, 4, endpoint=False)
+    pg = geo.ProjectionGeometry(ang, "ray_trace", CUDA=False, index_model=im, attenuation_model=am,
+                                absorption_model=am, ray_trace_method="eikonal",
+                                eikonal_parametrization="physical_path_length",
+                                ray_trace_ode_solver="forward_symplectic_euler",
+                                ray_trace_ray_config="parallel", inclination_angle=0.0, ray_density=1)
+    P = RT.PyTorchRayTracingPropagator(tg, pg)
+    f = rng.uniform(0, 1, tg.array.shape)
+    out["ha_xv"], out["ha_yv"], out["ha_zv"] = cv
+    out["ha_angles"] = ang
+    out["ha_f"] = f
+    out["ha_fwd"] = P.forward(f.copy())
+    gin = rng.uniform(0, 1, out["ha_fwd"].shape).astype(np.float32)
+    out["ha_g"] = gin
+    out["ha_bwd"] = P.backward(gin.copy())
+    out["ha_params"] = np.array([1.0, 30.0, np.amax(cv[0]) - np.amin(cv[0])])
+    np.savez_compressed(OUT / "raytrace.npz", **out)
+
+
+def optimizer_cases(vam):
+    geo = vam.geometry
+    out = {}
+    rng = np.random.default_rng(7)
+    n, nz = 24, 2
+    t = ellipses_target(n, nz, rng)
+    ang = np.linspace(0, 360, 18, endpoint=False)
+    out["target"] = t
+    out["angles"] = ang
+
+    def run(method, **kw):
+        tg = geo.TargetGeometry(target=t.copy())
+        pg = geo.ProjectionGeometry(ang, "parallel", CUDA=False, attenuation_field=np.zeros((n, n, nz)))
+        opts = refload.fresh_options(vam, method=method, **kw)
+        return vam.optimize.optimize(tg, pg, opts)
+
+    s, r, e = run("CAL", n_iter=5, learning_rate=0.4, d_h=0.5, sigmoid=0.01)
+    out["cal_sino"], out["cal_recon"], out["cal_err"] = s.array, r.array, e
+    s, r, e = run("OSMO", n_iter=4, d_h=0.8, d_l=0.7, filter="ram-lak")
+    out["osmo_sino"], out["osmo_recon"], out["osmo_err"] = s.array, r.array, e
+    s, r, e = run("FBP", n_iter=1, filter="ram-lak")
+    out["fbp_sino"], out["fbp_recon"], out["fbp_err"] = s.array, r.array, e
+    # BCLP grayscale with a generalised-logistic response model
+    tgray = np.clip(t * 0.8 + 0.1 * rng.uniform(0, 1, t.shape), 0, 1)
+    out["bclp_target"] = tgray
+    rm = vam.response.ResponseModel(B=12, M=0.6)
+    tg = geo.TargetGeometry(target=tgray.copy())
+    pg = geo.ProjectionGeometry(ang, "parallel", CUDA=False, attenuation_field=np.zeros((n, n, nz)))
+    opts = refload.fresh_options(vam, method="BCLP", n_iter=4, p=2, q=1, eps=0.05, learning_rate=0.002,
+                                 response_model=rm, filter="ram-lak")
+    sino, dose, mapped, logs = vam.optimize.optimize(tg, pg, opts, output="full")
+    out["bclp_sino"], out["bclp_dose"], out["bclp_mapped"] = sino.array, dose.array, mapped.array
+    out["bclp_loss"] = logs.loss
+    out["bclp_norms"] = np.stack([logs.l0, logs.l1, logs.l2, logs.lf, logs.l0_eps0, logs.l1_eps0,
+                                  logs.l2_eps0, logs.lf_eps0])
+    # response model tables
+    out["resp_f"], out["resp_map"], out["resp_dmap"] = rm.interp_f_0, rm.interp_map_0, rm.interp_dmapdf_0
+    out["resp_inv_probe"] = rm.map_inv(np.linspace(-0.1, 1.1, 37))
+    # PM (L-BFGS-B) few iterations
+    tg = geo.TargetGeometry(target=t.copy())
+    pg = geo.ProjectionGeometry(ang, "parallel", CUDA=False, attenuation_field=np.zeros((n, n, nz)))
+    opts = refload.fresh_options(vam, method="PM", n_iter=3, d_h=0.8, d_l=0.6, rho_1=1, rho_2=1, p=2)
+    s, r, e = vam.optimize.optimize(tg, pg, opts)
+    out["pm_sino"], out["pm_recon"], out["pm_err"] = s.array, r.array, e
+    # filters
+    for name in ("ram-lak", "shepp-logan", "cosine", "hamming", "hanning"):
+        out["filt_" + name] = vam.util.data._get_fourier_filter(64, name)[:, 0]
+    sino = rng.uniform(0, 1, (24, 5, 2))
+    out["filt_sino_in"] = sino
+    out["filt_sino_ramlak"] = vam.util.data.filterSinogram(sino.copy(), "ram-lak")
+    out["filt_osmo"] = vam.util.data.filterTargetOSMO(t.copy(), "ram-lak")
+    np.savez_compressed(OUT / "optim.npz", **out)
+
+
+def main():
+    warnings.simplefilter("ignore")
+    vam = refload.load()
+    parallel_cases(vam)
+    ray_cases(vam)
+    optimizer_cases(vam)
+    for p in sorted(OUT.glob("*.npz")):
+        print(p.name, p.stat().st_size)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,105 @@
+"""Pins the CPU oracle (oracle/vamoracle.c) against golden vectors produced by
+the reference's own code (tests/golden/make_golden.py).  CPU only."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.conftest import relL2
+
+
+@pytest.mark.parametrize("tag", ["even", "odd"])
+def test_parallel_forward_backward_match_reference(golden, tag):
+    P = golden["parallel"]
+    b = O.parallel_forward(P[f"{tag}_x"], P[f"{tag}_angles"])
+    assert np.array_equal(b, P[f"{tag}_fwd"]) or relL2(b, P[f"{tag}_fwd"]) < 1e-14
+    x = O.parallel_backward_ref(P[f"{tag}_b"], P[f"{tag}_angles"])
+    assert relL2(x, P[f"{tag}_bwd"]) < 1e-14
+
+
+def test_occlusion_matches_reference(golden):
+    P = golden["parallel"]
+    occ, flag = O.occlusion_sinogram(P["occ_insert"], P["occ_angles"])
+    ref = P["occ_sino"]
+    assert np.array_equal(np.isnan(occ), np.isnan(ref))
+    assert np.nanmax(np.abs(occ - ref)) == 0.0
+    b = O.parallel_forward(P["occ_x"], P["occ_angles"], occlusion=(occ, flag))
+    assert relL2(b, P["occ_fwd"]) < 1e-14
+    x = O.parallel_backward_ref(P["occ_b"], P["occ_angles"], occlusion=(occ, flag))
+    assert relL2(x, P["occ_bwd"]) < 1e-14
+
+
+def test_2d_class_matches_3d_discretisation(golden):
+    """The 2D class (Projector2DParallel.py:145-233) clips its input first and
+    otherwise uses the same discretisation as the 3D class with nZ = 1."""
+    P = golden["parallel"]
+    x = O.clip_to_circle(P["p2_x"])
+    b = O.parallel_forward(x[:, :, None], P["p2_angles"])[:, :, 0]
+    assert relL2(b, P["p2_fwd"]) < 1e-14
+    xb = O.parallel_backward_ref(P["p2_b"][:, :, None], P["p2_angles"])[:, :, 0]
+    assert relL2(xb, P["p2_bwd"]) < 1e-14
+
+
+def test_adjoint_is_transpose():
+    rng = np.random.default_rng(0)
+    ang = np.linspace(0, 360, 11, endpoint=False)
+    x = rng.uniform(size=(20, 20, 2))
+    y = rng.uniform(size=(20, 11, 2))
+    for absn in (None, ("ray", 0.05, 8.0)):
+        lhs = np.sum(O.parallel_forward(x, ang, absorption=absn) * y)
+        rhs = np.sum(x * O.parallel_adjoint(y, ang, absorption=absn))
+        assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
+
+
+def test_disk_sinogram_known_answer():
+    """Sinogram of a centred uniform disk of radius rho is 2 sqrt(rho^2 - t^2)."""
+    n, rho = 64, 20.0
+    yy, xx = np.mgrid[:n, :n] - n // 2
+    # supersampled disk so that bilinear sampling sees a smooth edge
+    disk = np.zeros((n, n))
+    for dy in np.linspace(-0.5, 0.5, 8, endpoint=False) + 1 / 16:
+        for dx in np.linspace(-0.5, 0.5, 8, endpoint=False) + 1 / 16:
+            disk += ((xx + dx) ** 2 + (yy + dy) ** 2 <= rho ** 2)
+    disk /= 64
+    b = O.parallel_forward(disk[:, :, None], np.array([0.0, 37.0, 90.0]))[:, :, 0]
+    t = np.arange(n) - n // 2
+    chord = 2 * np.sqrt(np.clip(rho ** 2 - t ** 2, 0, None))
+    inner = np.abs(t) < rho - 2
+    # pixelised disk vs the continuous chord: well under 1 % inside the disk
+    assert np.max(np.abs(b[inner] - chord[inner, None]) / chord[inner, None]) < 0.01
+    # 0 and 90 degrees sample mirror-image lattices of a symmetric disk
+    assert np.allclose(b[:, 0], b[:, 2], rtol=0, atol=1e-12)
+
+
+def test_ray_oracle_matches_reference(golden):
+    R = golden["raytrace"]
+    for tag in ("r3", "r2"):
+        xv, yv, zv = R[f"{tag}_xv"], R[f"{tag}_yv"], R[f"{tag}_zv"]
+        x0, v0, _ = O.setup_rays_parallel(xv, yv, zv, R[f"{tag}_angles"])
+        assert np.array_equal(x0, R[f"{tag}_x0"]) and np.array_equal(v0, R[f"{tag}_v0"])
+        h, ms = R[f"{tag}_step"]
+        grid = dict(xv=xv, yv=yv, zv=zv)
+        a = R[f"{tag}_alpha"]
+        kw = dict(step_size=h, max_num_step=int(ms), n_kind=1, n_grid=R[f"{tag}_n"], a_kind=3, a_grid=a, absorb=a)
+        g, _ = O.ray_trace("integrate", grid, x0, v0, 1.0, f=R[f"{tag}_f"], **kw)
+        assert relL2(g, R[f"{tag}_fwd"]) < 1e-6
+        d, _ = O.ray_trace("deposit", grid, x0, v0, 1.0, g=R[f"{tag}_g"], **kw)
+        assert relL2(d.squeeze(), R[f"{tag}_bwd"]) < 1e-6
+
+
+def test_ray_oracle_analytic_medium(golden):
+    import torch
+
+    R = golden["raytrace"]
+    xv, yv, zv = R["ha_xv"], R["ha_yv"], R["ha_zv"]
+    x0, v0, _ = O.setup_rays_parallel(xv, yv, zv, R["ha_angles"])
+    nsur, aval, _ = R["ha_params"]
+    Rc = min((xv.max() - xv.min()) / 2, (yv.max() - yv.min()) / 2, (zv.max() - zv.min()) / 2)
+    xg, yg, zg = np.meshgrid(xv, yv, zv, indexing="ij")
+    r = torch.linalg.norm(torch.as_tensor(np.stack([xg.ravel(), yg.ravel()], 1)), dim=1).numpy()
+    absorb = np.where(r < Rc, aval, 0.0).reshape(xg.shape)
+    kw = dict(step_size=(xv[1] - xv[0]) / 2, max_num_step=3 * xv.size, n_kind=0, n_sur=nsur, a_kind=1,
+              a_val=aval, a_R=Rc, absorb=absorb)
+    g, _ = O.ray_trace("integrate", dict(xv=xv, yv=yv, zv=zv), x0, v0, 1.0, f=R["ha_f"], **kw)
+    assert relL2(g, R["ha_fwd"]) < 1e-6
+    d, _ = O.ray_trace("deposit", dict(xv=xv, yv=yv, zv=zv), x0, v0, 1.0, g=R["ha_g"], **kw)
+    assert relL2(d, R["ha_bwd"]) < 1e-6

@@ -1,0 +1,165 @@
+"""Parallel-beam kernels (through the C ABI) against the oracle and the
+reference's golden vectors.  Tolerance: relative L2 <= 1e-5 (float32 kernels
+vs the reference's float64), dot test <= 1e-6 relative."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from tests.conftest import relL2
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+def plan_for(shape, angles):
+    from vamtoolbox_b200.projector.Projector3DParallel import ParallelPlan
+
+    return ParallelPlan(shape[0], shape[1], shape[2], angles)
+
+
+def dev(a):
+    return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float32), device="cuda")
+
+
+@pytest.mark.parametrize("tag", ["even", "odd"])
+def test_forward_backward_match_reference_golden(golden, tag):
+    P = golden["parallel"]
+    x, ang = P[f"{tag}_x"], P[f"{tag}_angles"]
+    p = plan_for(x.shape, ang)
+    b = p.forward(dev(x)).cpu().numpy()
+    assert relL2(b, P[f"{tag}_fwd"]) < TOL
+    xb = p.backward_ref(dev(P[f"{tag}_b"])).cpu().numpy()
+    assert relL2(xb, P[f"{tag}_bwd"]) < TOL
+
+
+def test_occlusion_matches_reference_golden(golden):
+    P = golden["parallel"]
+    p = plan_for(P["occ_x"].shape, P["occ_angles"])
+    p.set_occlusion(P["occ_insert"])
+    occ = p.occlusion_sinogram().cpu().numpy()
+    ref = P["occ_sino"]
+    assert np.array_equal(np.isnan(occ), np.isnan(ref))
+    assert np.nanmax(np.abs(occ - ref)) == 0.0
+    assert relL2(p.forward(dev(P["occ_x"])).cpu().numpy(), P["occ_fwd"]) < TOL
+    assert relL2(p.backward_ref(dev(P["occ_b"])).cpu().numpy(), P["occ_bwd"]) < TOL
+
+
+@pytest.mark.parametrize("shape,na", [((32, 32, 8), 24), ((33, 33, 5), 17), ((40, 40, 1), 30),
+                                      ((24, 24, 12), 9), ((48, 48, 64), 12), ((20, 20, 3), 360)])
+def test_against_oracle_shapes(shape, na):
+    rng = np.random.default_rng(sum(shape) + na)
+    ang = np.sort(rng.uniform(0, 360, na))
+    ang[0] = 0.0
+    x = rng.uniform(0, 1, shape)
+    b = rng.uniform(0, 1, (shape[0], na, shape[2]))
+    p = plan_for(shape, ang)
+    assert relL2(p.forward(dev(x)).cpu().numpy(), O.parallel_forward(x, ang)) < TOL
+    assert relL2(p.backward_ref(dev(b)).cpu().numpy(), O.parallel_backward_ref(b, ang)) < TOL
+    assert relL2(p.adjoint(dev(b)).cpu().numpy(), O.parallel_adjoint(b, ang)) < TOL
+
+
+def test_exact_angles_and_binary_target():
+    """Multiples of 90 degrees put samples on integer coordinates (floor == ceil)."""
+    n = 64
+    yy, xx = np.mgrid[:n, :n] - n / 2
+    x = ((xx ** 2 + yy ** 2) < 20 ** 2).astype(float)[:, :, None] * np.ones((1, 1, 4))
+    ang = np.array([0.0, 45.0, 90.0, 180.0, 270.0, 359.5])
+    p = plan_for(x.shape, ang)
+    assert relL2(p.forward(dev(x)).cpu().numpy(), O.parallel_forward(x, ang)) < TOL
+    bb = O.parallel_forward(x, ang)
+    assert relL2(p.backward_ref(dev(bb)).cpu().numpy(), O.parallel_backward_ref(bb, ang)) < TOL
+
+
+@pytest.mark.parametrize("absn", [None, "ray", "mask"])
+def test_adjoint_dot_product(absn):
+    rng = np.random.default_rng(3)
+    shape, na = (36, 36, 8), 20
+    ang = np.linspace(0, 360, na, endpoint=False) + 0.3
+    p = plan_for(shape, ang)
+    mask = None
+    if absn == "ray":
+        p.set_absorption("ray", alpha_per_px=0.03, radius_px=15.0)
+        oabs = ("ray", 0.03, 15.0)
+    elif absn == "mask":
+        mask = rng.uniform(0.2, 1.0, shape[:2])
+        p.set_absorption("mask", mask=mask)
+        oabs = ("mask", mask)
+    else:
+        oabs = None
+    x = rng.uniform(0, 1, shape)
+    y = rng.uniform(0, 1, (shape[0], na, shape[2]))
+    Ax = p.forward(dev(x)).double()
+    Aty = p.adjoint(dev(y)).double()
+    lhs = float((Ax * dev(y).double()).sum())
+    rhs = float((dev(x).double() * Aty).sum())
+    assert abs(lhs - rhs) <= 1e-6 * abs(lhs)
+    # signed inputs: error relative to the sum of magnitudes
+    xs, ys = dev(rng.standard_normal(shape)), dev(rng.standard_normal((shape[0], na, shape[2])))
+    a1 = p.forward(xs).double() * ys.double()
+    a2 = xs.double() * p.adjoint(ys).double()
+    assert abs(float(a1.sum() - a2.sum())) <= 1e-6 * float(a1.abs().sum())
+    assert relL2(Ax.cpu().numpy(), O.parallel_forward(x, ang, absorption=oabs)) < TOL
+    assert relL2(p.backward_ref(dev(y)).cpu().numpy(), O.parallel_backward_ref(y, ang, absorption=oabs)) < TOL
+
+
+def test_occlusion_adjoint_is_transpose(golden):
+    P = golden["parallel"]
+    p = plan_for(P["occ_x"].shape, P["occ_angles"])
+    p.set_occlusion(P["occ_insert"])
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal(P["occ_x"].shape)
+    y = rng.standard_normal(P["occ_fwd"].shape)
+    lhs = float((p.forward(dev(x)).double() * dev(y).double()).sum())
+    rhs = float((dev(x).double() * p.adjoint(dev(y)).double()).sum())
+    assert abs(lhs - rhs) <= 1e-5 * abs(lhs)
+
+
+def test_mask_matches_reference_mask(golden):
+    from vamtoolbox_b200 import geometry
+
+    P = golden["parallel"]
+    px, a, R = P["mask_params"]
+    tg = geometry.TargetGeometry(target=np.ones((24, 24, 2)))
+    pg = geometry.ProjectionGeometry(np.array([0.0]), "parallel", projector_pixel_size=px, absorption_coeff=a,
+                                     container_radius=R)
+    pg.calcAbsorptionMask(tg)
+    assert np.array_equal(pg.absorption_mask[:, :, 0], P["mask"])
+
+
+def test_projector_class_numpy_roundtrip(golden):
+    from vamtoolbox_b200 import geometry
+    from vamtoolbox_b200.projector.Projector3DParallel import Projector3DParallel
+
+    P = golden["parallel"]
+    x, ang = P["even_x"], P["even_angles"]
+    tg = geometry.TargetGeometry(target=x.copy(), clip_to_circle=False)
+    pg = geometry.ProjectionGeometry(ang, "parallel", CUDA=True)
+    A = Projector3DParallel(tg, pg)
+    b = A.forward(x)
+    assert isinstance(b, np.ndarray) and b.dtype == np.float64 and b.shape == P["even_fwd"].shape
+    assert relL2(b, P["even_fwd"]) < TOL
+    assert relL2(A.backward(P["even_b"]), P["even_bwd"]) < TOL
+    t = A.forward(torch.as_tensor(x, device="cuda", dtype=torch.float32))
+    assert t.is_cuda and t.dtype == torch.float32
+
+
+def test_deterministic_gather_kernels():
+    rng = np.random.default_rng(11)
+    shape, ang = (40, 40, 16), np.linspace(0, 180, 33)
+    x, y = dev(rng.uniform(size=shape)), dev(rng.uniform(size=(40, 33, 16)))
+    p = plan_for(shape, ang)
+    for f, a in ((p.forward, x), (p.backward_ref, y), (p.adjoint, y)):
+        assert torch.equal(f(a), f(a))
+
+
+def test_bad_inputs_raise():
+    from vamtoolbox_b200._lib import VamError
+
+    p = plan_for((16, 16, 4), np.linspace(0, 180, 8))
+    with pytest.raises(ValueError):
+        p.forward(torch.zeros((16, 16, 5), device="cuda"))
+    with pytest.raises(TypeError):
+        p.forward(torch.zeros((16, 16, 4), device="cuda", dtype=torch.float64))
+    with pytest.raises(VamError):
+        p.set_absorption("ray", alpha_per_px=float("nan"), radius_px=3.0)

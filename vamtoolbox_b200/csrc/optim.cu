@@ -1,0 +1,431 @@
+// optim.cu -- fused bodies of the optimizer iterations (vamtoolbox/optimizer/*.py).
+//
+// Every reduction is a fixed two-level tree (per-block partials in the caller's
+// workspace, then one block), so results are deterministic run to run and no
+// value ever returns to the host: scalars such as max(x) or the BCLP loss stay
+// in device memory and the consuming kernel reads them, which keeps a whole
+// optimizer iteration capturable in one CUDA graph.
+#include <float.h>
+#include <math.h>
+
+#include <cmath>
+
+#include "vam_internal.cuh"
+
+namespace vam {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kMaxBlocks = 1184;    // 148 SMs x 8
+constexpr int kStats = 9;
+constexpr size_t kWorkBytes = (size_t)kMaxBlocks * kStats * sizeof(double) + 1024;
+
+int blocks_for(int64_t n) {
+    int64_t b = (n + (int64_t)kThreads * 8 - 1) / ((int64_t)kThreads * 8);
+    if (b < 1) b = 1;
+    if (b > kMaxBlocks) b = kMaxBlocks;
+    return (int)b;
+}
+
+template <typename T, int OP>
+__device__ __forceinline__ T red_op(T a, T b) {
+    if (OP == VAM_RED_MAX) return a > b ? a : (b != b ? b : a);  // NaN propagates like np.max
+    if (OP == VAM_RED_MIN) return a < b ? a : (b != b ? b : a);
+    return a + b;
+}
+
+template <typename T, int OP>
+__device__ __forceinline__ T red_identity() {
+    if (OP == VAM_RED_MAX) return (T)-INFINITY;
+    if (OP == VAM_RED_MIN) return (T)INFINITY;
+    return (T)0;
+}
+
+// Block-wide reduction of one value per thread; result valid in thread 0.
+template <typename T, int OP>
+__device__ T block_reduce(T v) {
+    __shared__ T sh[kThreads / 32];
+    for (int off = 16; off > 0; off >>= 1) v = red_op<T, OP>(v, __shfl_xor_sync(0xffffffffu, v, off));
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        v = l < (int)(blockDim.x >> 5) ? sh[l] : red_identity<T, OP>();
+        for (int off = 16; off > 0; off >>= 1) v = red_op<T, OP>(v, __shfl_xor_sync(0xffffffffu, v, off));
+    }
+    return v;
+}
+
+// ---------------------------------------------------------------------------
+// generic reduce
+// ---------------------------------------------------------------------------
+template <int OP>
+__global__ void __launch_bounds__(kThreads) k_reduce_partial(const float* __restrict__ x, int64_t n,
+                                                             double* __restrict__ part) {
+    double acc = red_identity<double, OP>();
+    for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads)
+        acc = red_op<double, OP>(acc, (double)x[i]);
+    acc = block_reduce<double, OP>(acc);
+    if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
+template <int OP>
+__global__ void __launch_bounds__(kThreads) k_reduce_final(const double* __restrict__ part, int nb,
+                                                           float* __restrict__ out) {
+    double acc = red_identity<double, OP>();
+    for (int i = threadIdx.x; i < nb; i += kThreads) acc = red_op<double, OP>(acc, part[i]);
+    acc = block_reduce<double, OP>(acc);
+    if (threadIdx.x == 0) out[0] = (float)acc;
+}
+
+// ---------------------------------------------------------------------------
+// VER (metrics.py:47-76): min over gel, then count void >= min
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_ver_min(const float* __restrict__ x, const uint8_t* __restrict__ m,
+                                                      int64_t n, double* __restrict__ part) {
+    double mn = INFINITY;
+    double cnt = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads) {
+        const uint8_t t = m[i];
+        if (t == 1) mn = fmin(mn, (double)x[i]);
+        cnt += (t != 0);
+    }
+    mn = block_reduce<double, VAM_RED_MIN>(mn);
+    cnt = block_reduce<double, VAM_RED_SUM>(cnt);
+    if (threadIdx.x == 0) { part[blockIdx.x] = mn; part[kMaxBlocks + blockIdx.x] = cnt; }
+}
+
+__global__ void __launch_bounds__(kThreads) k_ver_min_final(double* __restrict__ part, int nb) {
+    double mn = INFINITY, cnt = 0.0;
+    for (int i = threadIdx.x; i < nb; i += kThreads) { mn = fmin(mn, part[i]); cnt += part[kMaxBlocks + i]; }
+    mn = block_reduce<double, VAM_RED_MIN>(mn);
+    cnt = block_reduce<double, VAM_RED_SUM>(cnt);
+    if (threadIdx.x == 0) { part[2 * kMaxBlocks] = mn; part[2 * kMaxBlocks + 1] = cnt; }
+}
+
+__global__ void __launch_bounds__(kThreads) k_ver_count(const float* __restrict__ x, const uint8_t* __restrict__ m,
+                                                        int64_t n, double* __restrict__ part) {
+    const float mn = (float)part[2 * kMaxBlocks];
+    double cnt = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads)
+        cnt += (m[i] == 2 && x[i] >= mn);
+    cnt = block_reduce<double, VAM_RED_SUM>(cnt);
+    if (threadIdx.x == 0) part[blockIdx.x] = cnt;
+}
+
+__global__ void __launch_bounds__(kThreads) k_ver_final(const double* __restrict__ part, int nb, float* __restrict__ out) {
+    double cnt = 0.0;
+    for (int i = threadIdx.x; i < nb; i += kThreads) cnt += part[i];
+    cnt = block_reduce<double, VAM_RED_SUM>(cnt);
+    if (threadIdx.x == 0) out[0] = (float)(cnt / part[2 * kMaxBlocks + 1]);
+}
+
+// ---------------------------------------------------------------------------
+// BCLP dose pass (BCLP.py:293-437)
+// ---------------------------------------------------------------------------
+struct TableRef {
+    const float* f;
+    const float* m;
+    const float* dm;
+    int n;
+    float f0, inv_step;
+};
+
+// np.interp(d, f, y, left=y[0], right=y[-1]) on a uniformly spaced table
+__device__ __forceinline__ void table_interp(const TableRef& t, float d, float& out_m, float& out_dm) {
+    if (!(d > t.f[0])) {
+        if (d == t.f[0] || !(d == d)) { out_m = d == d ? t.m[0] : d; out_dm = d == d ? t.dm[0] : d; return; }
+        out_m = t.m[0]; out_dm = t.dm[0]; return;
+    }
+    if (!(d < t.f[t.n - 1])) { out_m = t.m[t.n - 1]; out_dm = t.dm[t.n - 1]; return; }
+    int j = (int)((d - t.f0) * t.inv_step);
+    j = min(max(j, 0), t.n - 2);
+    while (j > 0 && t.f[j] > d) --j;
+    while (j < t.n - 2 && t.f[j + 1] <= d) ++j;
+    const float fj = t.f[j], fj1 = t.f[j + 1];
+    if (fj == d) { out_m = t.m[j]; out_dm = t.dm[j]; return; }
+    const float w = (d - fj) / (fj1 - fj);
+    out_m = fmaf(w, t.m[j + 1] - t.m[j], t.m[j]);
+    out_dm = fmaf(w, t.dm[j + 1] - t.dm[j], t.dm[j]);
+}
+
+__device__ __forceinline__ float powabs(float a, float p) {
+    if (p == 2.f) return a * a;
+    if (p == 1.f) return a;
+    if (p == 4.f) { float b = a * a; return b * b; }
+    if (p == 3.f) return a * a * a;
+    if (p == 0.f) return 1.f;
+    return powf(a, p);
+}
+
+__global__ void __launch_bounds__(kThreads) k_bclp_dose(const float* __restrict__ dose, const float* __restrict__ target,
+                                                        int64_t n, TableRef tab, float eps, float weight, float p,
+                                                        const float* __restrict__ eps_arr,
+                                                        const float* __restrict__ w_arr, float* __restrict__ mapped,
+                                                        float* __restrict__ operand, double* __restrict__ part) {
+    double s_loss = 0, s_l0 = 0, s_l0e = 0, s_l1 = 0, s_l1e = 0, s_l2 = 0, s_l2e = 0;
+    double m_lf = 0, m_lfe = 0;
+    for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads) {
+        const float d = dose[i];
+        float mp, dmp;
+        table_interp(tab, d, mp, dmp);
+        const float e = mp - target[i];
+        const float ae = fabsf(e);
+        const float ep = eps_arr ? eps_arr[i] : eps;
+        const float w = w_arr ? w_arr[i] : weight;
+        const float eb = ae - ep;
+        const bool v = eb > 0.f;
+        const float aeb = fabsf(eb);
+        float op = 0.f;
+        if (v) {
+            const float sgn = (e > 0.f) ? 1.f : ((e < 0.f) ? -1.f : 0.f);
+            op = w * powabs(aeb, p - 1.f) * sgn * dmp;
+            s_loss += (double)(w * powabs(aeb, p));
+            s_l0 += 1.0;
+            s_l1 += aeb;
+            s_l2 += (double)eb * eb;
+            m_lf = fmax(m_lf, (double)aeb);
+        }
+        s_l0e += (ae > 0.f);
+        s_l1e += ae;
+        s_l2e += (double)e * e;
+        if (ae > 0.f) m_lfe = fmax(m_lfe, (double)ae);
+        if (mapped) mapped[i] = mp;
+        operand[i] = op;
+    }
+    double vals[kStats] = {s_loss, s_l0, s_l0e, s_l1, s_l1e, s_l2, s_l2e, m_lf, m_lfe};
+#pragma unroll
+    for (int k = 0; k < kStats; ++k) {
+        double r = (k >= 7) ? block_reduce<double, VAM_RED_MAX>(vals[k]) : block_reduce<double, VAM_RED_SUM>(vals[k]);
+        if (threadIdx.x == 0) part[(size_t)k * kMaxBlocks + blockIdx.x] = r;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_bclp_stats_final(const double* __restrict__ part, int nb,
+                                                               float* __restrict__ stats) {
+#pragma unroll
+    for (int k = 0; k < kStats; ++k) {
+        double acc = (k >= 7) ? 0.0 : 0.0;
+        for (int i = threadIdx.x; i < nb; i += kThreads) {
+            const double v = part[(size_t)k * kMaxBlocks + i];
+            acc = (k >= 7) ? fmax(acc, v) : acc + v;
+        }
+        acc = (k >= 7) ? block_reduce<double, VAM_RED_MAX>(acc) : block_reduce<double, VAM_RED_SUM>(acc);
+        if (threadIdx.x == 0) stats[k] = (float)acc;
+    }
+}
+
+// g = clip(g - lr * pref * grad, lo, hi); pref from the device loss (BCLP.py:370-375)
+__global__ void __launch_bounds__(kThreads) k_bclp_update(float* __restrict__ g, const float* __restrict__ grad,
+                                                          int64_t n, float lr, float p, float q, float lo, float hi,
+                                                          int has_hi, const float* __restrict__ stats) {
+    const double S = (double)stats[0];
+    const double L = pow(S, (double)q / (double)p);
+    const float pref = (L != 0.0) ? (float)((double)q * pow(L, ((double)q - (double)p) / (double)q)) : 1.f;
+    const float step = lr * pref;
+    for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads) {
+        float v = g[i] - step * grad[i];
+        v = fmaxf(v, lo);
+        if (has_hi) v = fminf(v, hi);
+        g[i] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// CAL / OSMO helpers
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_cal_threshold(const float* __restrict__ x, const float* __restrict__ xmax,
+                                                            const float* __restrict__ t, int64_t n, float d_h, float g,
+                                                            float* __restrict__ out) {
+    const float inv = 1.f / xmax[0];
+    const float ig = 1.f / g;
+    for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads) {
+        const float y = x[i] * inv - d_h;
+        out[i] = 1.f / (1.f + expf(-y * ig)) - t[i];
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_cal_update(float* __restrict__ b, const float* __restrict__ db,
+                                                         const float* __restrict__ dbp, int64_t n, float lr, float m,
+                                                         float mscale) {
+    for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads) {
+        const float grad = db[i] * (1.f - m) + (dbp ? dbp[i] * mscale : 0.f);
+        b[i] = fmaxf(b[i] - lr * grad, 0.f);
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_scale(float* __restrict__ x, const float* __restrict__ s, int64_t n,
+                                                    int floor_on, float floor_val) {
+    const float inv = 1.f / s[0];
+    for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads) {
+        float v = x[i] * inv;
+        if (floor_on) v = fmaxf(v, floor_val);
+        x[i] = v;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_osmo_model(float* __restrict__ xm, const float* __restrict__ x,
+                                                         const float* __restrict__ xmax, const uint8_t* __restrict__ m,
+                                                         int64_t n, int gel, float d) {
+    const float inv = xmax ? 1.f / xmax[0] : 1.f;
+    const uint8_t sel = gel ? 1 : 2;
+    for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads) {
+        if (m[i] != sel) continue;
+        const float xv = x[i] * inv;
+        if (gel) xm[i] += fmaxf(d - xv, 0.f);
+        else xm[i] -= fmaxf(xv - d, 0.f);
+    }
+}
+
+__global__ void k_append(const float* __restrict__ src, int n, float* __restrict__ arr, int* __restrict__ counter,
+                         int cap) {
+    const int row = counter[0];
+    if (row < cap)
+        for (int i = threadIdx.x; i < n; i += blockDim.x) arr[(size_t)row * n + i] = src[i];
+    __syncthreads();
+    if (threadIdx.x == 0) counter[0] = row + 1;
+}
+
+}  // namespace
+}  // namespace vam
+
+using namespace vam;
+
+extern "C" int vam_append(const float* src, int32_t n, float* arr, int32_t* counter, int32_t cap, vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(src && arr && counter, VAM_ERR_ARG, "vam_append: null argument");
+    VAM_REQUIRE(n > 0 && cap > 0, VAM_ERR_SHAPE, "vam_append: n and cap_rows must be positive");
+    k_append<<<1, 32, 0, (cudaStream_t)stream>>>(src, n, arr, counter, cap);
+    VAM_CHECK_LAUNCH("vam_append");
+    return VAM_OK;
+}
+
+extern "C" size_t vam_reduce_workspace_bytes(int64_t n) {
+    (void)n;
+    return kWorkBytes;
+}
+
+extern "C" int vam_reduce(const float* x, int64_t n, int op, float* out, void* work, size_t work_bytes,
+                          vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(x && out && work, VAM_ERR_ARG, "vam_reduce: null argument");
+    VAM_REQUIRE(n > 0, VAM_ERR_SHAPE, "vam_reduce: empty input");
+    VAM_REQUIRE(work_bytes >= kWorkBytes, VAM_ERR_ARG, "vam_reduce: workspace too small");
+    const int nb = blocks_for(n);
+    cudaStream_t st = (cudaStream_t)stream;
+    double* part = (double*)work;
+    switch (op) {
+        case VAM_RED_MAX:
+            k_reduce_partial<VAM_RED_MAX><<<nb, kThreads, 0, st>>>(x, n, part);
+            k_reduce_final<VAM_RED_MAX><<<1, kThreads, 0, st>>>(part, nb, out);
+            break;
+        case VAM_RED_MIN:
+            k_reduce_partial<VAM_RED_MIN><<<nb, kThreads, 0, st>>>(x, n, part);
+            k_reduce_final<VAM_RED_MIN><<<1, kThreads, 0, st>>>(part, nb, out);
+            break;
+        case VAM_RED_SUM:
+            k_reduce_partial<VAM_RED_SUM><<<nb, kThreads, 0, st>>>(x, n, part);
+            k_reduce_final<VAM_RED_SUM><<<1, kThreads, 0, st>>>(part, nb, out);
+            break;
+        default:
+            return set_error(VAM_ERR_ARG, "vam_reduce: unknown op");
+    }
+    VAM_CHECK_LAUNCH("vam_reduce");
+    return VAM_OK;
+}
+
+extern "C" int vam_metric_ver(const float* x, const uint8_t* mask, int64_t n, float* out, void* work,
+                              size_t work_bytes, vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(x && mask && out && work, VAM_ERR_ARG, "vam_metric_ver: null argument");
+    VAM_REQUIRE(n > 0, VAM_ERR_SHAPE, "vam_metric_ver: empty input");
+    VAM_REQUIRE(work_bytes >= kWorkBytes, VAM_ERR_ARG, "vam_metric_ver: workspace too small");
+    const int nb = blocks_for(n);
+    cudaStream_t st = (cudaStream_t)stream;
+    double* part = (double*)work;
+    k_ver_min<<<nb, kThreads, 0, st>>>(x, mask, n, part);
+    k_ver_min_final<<<1, kThreads, 0, st>>>(part, nb);
+    k_ver_count<<<nb, kThreads, 0, st>>>(x, mask, n, part);
+    k_ver_final<<<1, kThreads, 0, st>>>(part, nb, out);
+    VAM_CHECK_LAUNCH("vam_metric_ver");
+    return VAM_OK;
+}
+
+extern "C" int vam_bclp_dose_pass(const float* dose, const float* target, int64_t n, const vam_bclp_params* prm,
+                                  float* mapped, float* operand, float* stats, void* work, size_t work_bytes,
+                                  vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(dose && target && prm && operand && stats && work, VAM_ERR_ARG, "vam_bclp_dose_pass: null argument");
+    VAM_REQUIRE(prm->table_f && prm->table_map && prm->table_dmap && prm->n_table >= 2, VAM_ERR_ARG,
+                "vam_bclp_dose_pass: response table needs >= 2 points");
+    VAM_REQUIRE(n > 0, VAM_ERR_SHAPE, "vam_bclp_dose_pass: empty input");
+    VAM_REQUIRE(work_bytes >= kWorkBytes, VAM_ERR_ARG, "vam_bclp_dose_pass: workspace too small");
+    VAM_REQUIRE(std::isfinite(prm->p) && prm->p > 0.f, VAM_ERR_ARG, "vam_bclp_dose_pass: p must be > 0");
+    // The table is uniform (np.linspace): table_f0 / table_inv_step seed the bin
+    // search, which is then corrected against the table values themselves.
+    TableRef t;
+    t.f = prm->table_f; t.m = prm->table_map; t.dm = prm->table_dmap; t.n = prm->n_table;
+    t.f0 = prm->table_f0; t.inv_step = prm->table_inv_step;
+    const int nb = blocks_for(n);
+    cudaStream_t st = (cudaStream_t)stream;
+    double* part = (double*)work;
+    k_bclp_dose<<<nb, kThreads, 0, st>>>(dose, target, n, t, prm->eps, prm->weight, prm->p, prm->eps_dev,
+                                         prm->weight_dev, mapped, operand, part);
+    k_bclp_stats_final<<<1, kThreads, 0, st>>>(part, nb, stats);
+    VAM_CHECK_LAUNCH("vam_bclp_dose_pass");
+    return VAM_OK;
+}
+
+extern "C" int vam_bclp_sino_update(float* g, const float* grad, int64_t n, float lr, float p, float q, float lo,
+                                    float hi, int has_hi, const float* stats, vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(g && grad && stats, VAM_ERR_ARG, "vam_bclp_sino_update: null argument");
+    VAM_REQUIRE(n > 0, VAM_ERR_SHAPE, "vam_bclp_sino_update: empty input");
+    k_bclp_update<<<blocks_for(n), kThreads, 0, (cudaStream_t)stream>>>(g, grad, n, lr, p, q, lo, hi, has_hi, stats);
+    VAM_CHECK_LAUNCH("vam_bclp_sino_update");
+    return VAM_OK;
+}
+
+extern "C" int vam_cal_threshold(const float* x, const float* xmax, const float* target, int64_t n, float d_h,
+                                 float g, float* out, vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(x && xmax && target && out, VAM_ERR_ARG, "vam_cal_threshold: null argument");
+    VAM_REQUIRE(n > 0, VAM_ERR_SHAPE, "vam_cal_threshold: empty input");
+    k_cal_threshold<<<blocks_for(n), kThreads, 0, (cudaStream_t)stream>>>(x, xmax, target, n, d_h, g, out);
+    VAM_CHECK_LAUNCH("vam_cal_threshold");
+    return VAM_OK;
+}
+
+extern "C" int vam_cal_sino_update(float* b, const float* db, const float* db_prev, int64_t n, float lr,
+                                   float momentum, int32_t iter, vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(b && db, VAM_ERR_ARG, "vam_cal_sino_update: null argument");
+    VAM_REQUIRE(n > 0, VAM_ERR_SHAPE, "vam_cal_sino_update: empty input");
+    const double m = momentum;
+    const float mscale = (float)(m / (1.0 - std::pow(m, (double)iter + 1.0)));
+    k_cal_update<<<blocks_for(n), kThreads, 0, (cudaStream_t)stream>>>(b, db, momentum != 0.f ? db_prev : nullptr, n,
+                                                                       lr, momentum, mscale);
+    VAM_CHECK_LAUNCH("vam_cal_sino_update");
+    return VAM_OK;
+}
+
+extern "C" int vam_scale_by_device(float* x, const float* s, int64_t n, int apply_floor, float floor_val,
+                                   vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(x && s, VAM_ERR_ARG, "vam_scale_by_device: null argument");
+    VAM_REQUIRE(n > 0, VAM_ERR_SHAPE, "vam_scale_by_device: empty input");
+    k_scale<<<blocks_for(n), kThreads, 0, (cudaStream_t)stream>>>(x, s, n, apply_floor, floor_val);
+    VAM_CHECK_LAUNCH("vam_scale_by_device");
+    return VAM_OK;
+}
+
+extern "C" int vam_osmo_model_update(float* xm, const float* x, const float* xmax, const uint8_t* mask, int64_t n,
+                                     int gel, float d, vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(xm && x && mask, VAM_ERR_ARG, "vam_osmo_model_update: null argument");
+    VAM_REQUIRE(n > 0, VAM_ERR_SHAPE, "vam_osmo_model_update: empty input");
+    k_osmo_model<<<blocks_for(n), kThreads, 0, (cudaStream_t)stream>>>(xm, x, xmax, mask, n, gel, d);
+    VAM_CHECK_LAUNCH("vam_osmo_model_update");
+    return VAM_OK;
+}

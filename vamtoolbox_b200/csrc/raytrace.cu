@@ -1,0 +1,614 @@
+// raytrace.cu -- curved-ray tracer in a graded-index medium, sm_100a.
+//
+// One thread per ray; every thread runs the reference's step loop
+// (vamtoolbox/projector/pyTorchRayTrace.py:378-571 with the step of :738-832)
+// to the step cap with the exit test every `check` steps, so the host never
+// polls an active count and a whole forward or adjoint is one launch.
+//
+// Fields live in L2-resident device buffers owned by the plan: the index and
+// its gradient packed as float4 texels (n, dn/dx, dn/dy, dn/dz) so one trilinear
+// corner is one 16-byte load, the attenuation as float.  Rays are numbered
+// (detector, angle, z) with z fastest (:1629-1632), so the 32 rays of a warp are
+// 32 neighbouring z rows at one detector position and angle: their corner loads
+// hit consecutive addresses of the [x][y][z] fields.
+//
+// Precision: ray state, field sampling and the deposited energy are float32;
+// the voxel-index coordinates of the deposit / integrate step are float64 as
+// in the reference (:1253-1260), because the floor/ceil neighbour rule counts a
+// voxel twice at an exactly integral coordinate (:1262-1280) and float32
+// rounding would create such coordinates where the reference has none.
+#include <math.h>
+
+#include <cmath>
+#include <cstring>
+
+#include "vam_internal.cuh"
+
+struct vam_ray_plan {
+    vam_ray_geom g;
+    float energy0;
+    float* d_x0;         // [nr][3]
+    float* d_v0;         // [nr][3]
+    float4* d_nfield;    // [nX][nY][nZ] (n, gx, gy, gz)
+    float* d_afield;     // [nX][nY][nZ] attenuation (GRID)
+    float* d_absorb;     // [nX][nY][nZ] absorption at the grid points
+    float* d_scratch;    // [nX][nY][nZ] f * absorb, or the raw deposit
+    unsigned long long* d_active;  // rays active at the cap (last call)
+    vam_ray_medium med;  // kinds and analytic parameters (pointers unused after bind)
+    int has_medium;
+};
+
+namespace vam {
+namespace {
+
+struct RayArgs {
+    const float* x0;
+    const float* v0;
+    const float4* nfield;
+    const float* afield;
+    int64_t nr;
+    int nx, ny, nz;
+    float norm[3];        // 2/span (0 for a 2D z axis)
+    double half_span[3];  // span/2
+    double inv_voxel[3];  // 1/voxel (0 for a 2D z axis)
+    double bmax[3], bmin[3];  // exit bounds: max + voxel, min - voxel
+    float h;              // parameter step, float32 as the reference multiplies it
+    float h_idx;          // step / voxel_x
+    int max_steps, check, twod;
+    int param, solver;
+    int n_kind;
+    float n_sur, lune_R, lune_p;
+    int a_kind;
+    float a_val, a_R;
+    float energy0;
+    unsigned long long* active;
+};
+
+constexpr int kRayThreads = 128;
+
+// grid_sample(align_corners=True) unnormalised coordinate of axis d
+__device__ __forceinline__ float unnorm(float x, float nrm, int size, bool border) {
+    float u = x * nrm;
+    float ix = ((u + 1.f) * 0.5f) * (float)(size - 1);
+    if (border) ix = fminf((float)(size - 1), fmaxf(ix, 0.f));
+    return ix;
+}
+
+// Trilinear sample of the packed index texels with border padding.
+__device__ __forceinline__ float4 sample_n(const RayArgs& a, const float* x) {
+    const float ix = unnorm(x[0], a.norm[0], a.nx, true);
+    const float iy = unnorm(x[1], a.norm[1], a.ny, true);
+    const float iz = unnorm(x[2], a.norm[2], a.nz, true);
+    const int x0 = (int)floorf(ix), y0 = (int)floorf(iy), z0 = (int)floorf(iz);
+    const float wx1 = ix - (float)x0, wy1 = iy - (float)y0, wz1 = iz - (float)z0;
+    const float wx0 = 1.f - wx1, wy0 = 1.f - wy1, wz0 = 1.f - wz1;
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int cz = 0; cz < 2; ++cz) {
+        const int Z = z0 + cz;
+        if (Z >= a.nz) continue;
+        const float wz = cz ? wz1 : wz0;
+#pragma unroll
+        for (int cy = 0; cy < 2; ++cy) {
+            const int Y = y0 + cy;
+            if (Y >= a.ny) continue;
+            const float wyz = (cy ? wy1 : wy0) * wz;
+#pragma unroll
+            for (int cx = 0; cx < 2; ++cx) {
+                const int X = x0 + cx;
+                if (X >= a.nx) continue;
+                const float w = (cx ? wx1 : wx0) * wyz;
+                const float4 t = __ldg(a.nfield + ((size_t)X * a.ny + Y) * a.nz + Z);
+                acc.x = fmaf(w, t.x, acc.x);
+                acc.y = fmaf(w, t.y, acc.y);
+                acc.z = fmaf(w, t.z, acc.z);
+                acc.w = fmaf(w, t.w, acc.w);
+            }
+        }
+    }
+    return acc;
+}
+
+// (n, grad n) at x for the configured index kind (medium.py:276-473)
+__device__ __forceinline__ void index_at(const RayArgs& a, const float* x, float& n, float* gn) {
+    if (a.n_kind == VAM_INDEX_GRID) {
+        const float4 t = sample_n(a, x);
+        n = t.x; gn[0] = t.y; gn[1] = t.z; gn[2] = t.w;
+    } else if (a.n_kind == VAM_INDEX_LUNEBURG) {
+        const float r = sqrtf(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+        if (r < a.lune_R) {
+            n = a.n_sur * powf(2.f - powf(r / a.lune_R, a.lune_p), 1.f / a.lune_p);
+            const float k = -powf(a.n_sur / a.lune_R, a.lune_p) * powf(n, 1.f - a.lune_p) * powf(r, a.lune_p - 2.f);
+            gn[0] = k * x[0]; gn[1] = k * x[1]; gn[2] = k * x[2];
+        } else {
+            n = (a.n_sur != 1.f) ? a.n_sur : 1.f;
+            gn[0] = gn[1] = gn[2] = 0.f;
+        }
+    } else {
+        n = a.n_sur;
+        gn[0] = gn[1] = gn[2] = 0.f;
+    }
+}
+
+// attenuation coefficient at x (medium.py:753-915; GRID uses zero padding)
+__device__ __forceinline__ float alpha_at(const RayArgs& a, const float* x) {
+    if (a.a_kind == VAM_ALPHA_CYLINDER || a.a_kind == VAM_ALPHA_BALL) {
+        float r2 = x[0] * x[0] + x[1] * x[1];
+        if (a.a_kind == VAM_ALPHA_BALL) r2 += x[2] * x[2];
+        return sqrtf(r2) < a.a_R ? a.a_val : 0.f;
+    }
+    if (a.a_kind != VAM_ALPHA_GRID) return 0.f;
+    const float ix = unnorm(x[0], a.norm[0], a.nx, false);
+    const float iy = unnorm(x[1], a.norm[1], a.ny, false);
+    const float iz = unnorm(x[2], a.norm[2], a.nz, false);
+    const float fx = floorf(ix), fy = floorf(iy), fz = floorf(iz);
+    const int x0 = (int)fx, y0 = (int)fy, z0 = (int)fz;
+    const float wx1 = ix - fx, wy1 = iy - fy, wz1 = iz - fz;
+    float acc = 0.f;
+#pragma unroll
+    for (int cz = 0; cz < 2; ++cz) {
+        const int Z = z0 + cz;
+        if ((unsigned)Z >= (unsigned)a.nz) continue;
+        const float wz = cz ? wz1 : 1.f - wz1;
+#pragma unroll
+        for (int cy = 0; cy < 2; ++cy) {
+            const int Y = y0 + cy;
+            if ((unsigned)Y >= (unsigned)a.ny) continue;
+            const float wyz = (cy ? wy1 : 1.f - wy1) * wz;
+#pragma unroll
+            for (int cx = 0; cx < 2; ++cx) {
+                const int X = x0 + cx;
+                if ((unsigned)X >= (unsigned)a.nx) continue;
+                acc = fmaf((cx ? wx1 : 1.f - wx1) * wyz, __ldg(a.afield + ((size_t)X * a.ny + Y) * a.nz + Z), acc);
+            }
+        }
+    }
+    return acc;
+}
+
+// dv/dstep and dx/dstep of the three parametrisations (pyTorchRayTrace.py:694-735)
+__device__ __forceinline__ void dv_dstep(const RayArgs& a, float n, const float* gn, float* dv) {
+    if (a.param == VAM_PARAM_CANONICAL) { dv[0] = n * gn[0]; dv[1] = n * gn[1]; dv[2] = n * gn[2]; }
+    else if (a.param == VAM_PARAM_OPTICAL) { dv[0] = gn[0] / n; dv[1] = gn[1] / n; dv[2] = gn[2] / n; }
+    else { dv[0] = gn[0]; dv[1] = gn[1]; dv[2] = gn[2]; }
+}
+
+__device__ __forceinline__ void dx_dstep(const RayArgs& a, float n, const float* v, float* dx) {
+    if (a.param == VAM_PARAM_CANONICAL) { dx[0] = v[0]; dx[1] = v[1]; dx[2] = v[2]; }
+    else if (a.param == VAM_PARAM_OPTICAL) {
+        const float in2 = 1.f / (n * n);
+        dx[0] = v[0] * in2; dx[1] = v[1] * in2; dx[2] = v[2] * in2;
+    } else { dx[0] = v[0] / n; dx[1] = v[1] / n; dx[2] = v[2] / n; }
+}
+
+struct RayState {
+    float xi[3], xp[3], vi[3], vp[3];
+    float att, E, E0;
+    bool active;
+};
+
+__device__ __forceinline__ void ray_init(const RayArgs& a, int64_t r, float E0, RayState& st) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        st.xi[d] = st.xp[d] = a.x0[r * 3 + d];
+        st.vi[d] = st.vp[d] = a.v0[r * 3 + d];
+    }
+    st.att = 0.f;
+    st.E0 = E0;
+    st.E = E0;
+    st.active = true;
+    if (a.solver == VAM_ODE_LEAPFROG) {  // half step back in v (pyTorchRayTrace.py:816-828)
+        float n, gn[3], dv[3];
+        index_at(a, st.xp, n, gn);
+        dv_dstep(a, n, gn, dv);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) st.vp[d] = st.vp[d] - dv[d] * a.h / 2.f;
+    }
+}
+
+// One step of the configured ODE solver; returns the physical length ds and
+// the attenuation alpha(x_i) used for the energy update.
+__device__ __forceinline__ void ray_step(const RayArgs& a, RayState& st, float& ds, float& alpha) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { st.xi[d] = st.xp[d]; st.vi[d] = st.vp[d]; }
+    float n, gn[3], dv[3], dx[3];
+    index_at(a, st.xi, n, gn);
+    dv_dstep(a, n, gn, dv);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) st.vp[d] = st.vi[d] + dv[d] * a.h;
+    if (a.solver == VAM_ODE_EULER) dx_dstep(a, n, st.vi, dx);
+    else dx_dstep(a, n, st.vp, dx);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { dx[d] = dx[d] * a.h; st.xp[d] = st.xi[d] + dx[d]; }
+    ds = sqrtf(dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2]);
+    alpha = alpha_at(a, st.xi);
+    st.att = st.att + alpha * ds;
+    st.E = st.E0 * expf(-st.att);
+}
+
+// Exit test of pyTorchRayTrace.py:1343-1424 (position past max+voxel moving
+// outward, or below min-voxel moving inward's opposite), float64 bounds.
+__device__ __forceinline__ bool exited(const RayArgs& a, const RayState& st) {
+    bool ex = false;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const double x = (double)st.xp[d];
+        ex |= (x > a.bmax[d] && st.vp[d] > 0.f) || (x < a.bmin[d] && st.vp[d] < 0.f);
+    }
+    return ex;
+}
+
+// Trilinear corners of the deposit / integrate step at x_ip1, with the
+// reference's floor / ceil neighbours (a voxel at an integral coordinate is
+// visited twice, each time with weight 1 along that axis).
+struct Corners {
+    int lo[3], hi[3];
+    float wlo[3], whi[3];
+};
+
+__device__ __forceinline__ void corners_at(const RayArgs& a, const float* x, Corners& c) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const double idx = ((double)x[d] + a.half_span[d]) * a.inv_voxel[d];
+        const double fl = floor(idx), ce = ceil(idx);
+        c.lo[d] = (int)fmax(fmin(fl, 2.0e9), -2.0e9);
+        c.hi[d] = (int)fmax(fmin(ce, 2.0e9), -2.0e9);
+        c.wlo[d] = (float)(1.0 - (idx - fl));
+        c.whi[d] = (float)(1.0 - (ce - idx));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// integrate (forward)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kRayThreads) k_ray_integrate(RayArgs a, const float* __restrict__ fa,
+                                                               float* __restrict__ g) {
+    const int64_t r = (int64_t)blockIdx.x * kRayThreads + threadIdx.x;
+    if (r >= a.nr) return;
+    RayState st;
+    ray_init(a, r, a.energy0, st);
+    float integral = 0.f;
+    const int ncorner = a.twod ? 4 : 8;
+    for (int step = 0; step < a.max_steps; ++step) {
+        if (st.active) {
+            float ds, alpha;
+            ray_step(a, st, ds, alpha);
+            Corners c;
+            corners_at(a, st.xp, c);
+            const float eh = a.h_idx * st.E;
+            for (int cn = 0; cn < ncorner; ++cn) {
+                const int X = (cn & 1) ? c.hi[0] : c.lo[0];
+                const int Y = (cn & 2) ? c.hi[1] : c.lo[1];
+                const int Z = (cn & 4) ? c.hi[2] : c.lo[2];
+                if ((unsigned)X >= (unsigned)a.nx || (unsigned)Y >= (unsigned)a.ny || (unsigned)Z >= (unsigned)a.nz)
+                    continue;
+                const float w = ((cn & 1) ? c.whi[0] : c.wlo[0]) * ((cn & 2) ? c.whi[1] : c.wlo[1]) *
+                                ((cn & 4) ? c.whi[2] : c.wlo[2]);
+                integral = fmaf(__ldg(fa + ((size_t)X * a.ny + Y) * a.nz + Z), w * eh, integral);
+            }
+            if (step % a.check == 0 && exited(a, st)) st.active = false;
+        }
+    }
+    g[r] = integral;
+    if (st.active) atomicAdd(a.active, 1ULL);
+}
+
+// ---------------------------------------------------------------------------
+// deposit (adjoint)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kRayThreads) k_ray_deposit(RayArgs a, const float* __restrict__ gin,
+                                                             float* __restrict__ dose) {
+    const int64_t r = (int64_t)blockIdx.x * kRayThreads + threadIdx.x;
+    if (r >= a.nr) return;
+    RayState st;
+    ray_init(a, r, gin[r], st);
+    const int ncorner = a.twod ? 4 : 8;
+    const bool zero = st.E0 == 0.f;  // a zero-energy ray deposits nothing; still traced for the cap count
+    for (int step = 0; step < a.max_steps; ++step) {
+        if (st.active) {
+            float ds, alpha;
+            ray_step(a, st, ds, alpha);
+            if (!zero) {
+                Corners c;
+                corners_at(a, st.xp, c);
+                const float eh = a.h_idx * st.E;
+                for (int cn = 0; cn < ncorner; ++cn) {
+                    const int X = (cn & 1) ? c.hi[0] : c.lo[0];
+                    const int Y = (cn & 2) ? c.hi[1] : c.lo[1];
+                    const int Z = (cn & 4) ? c.hi[2] : c.lo[2];
+                    if ((unsigned)X >= (unsigned)a.nx || (unsigned)Y >= (unsigned)a.ny ||
+                        (unsigned)Z >= (unsigned)a.nz)
+                        continue;
+                    const float w = ((cn & 1) ? c.whi[0] : c.wlo[0]) * ((cn & 2) ? c.whi[1] : c.wlo[1]) *
+                                    ((cn & 4) ? c.whi[2] : c.wlo[2]);
+                    atomicAdd(dose + ((size_t)X * a.ny + Y) * a.nz + Z, w * eh);
+                }
+            }
+            if (step % a.check == 0 && exited(a, st)) st.active = false;
+        }
+    }
+    if (st.active) atomicAdd(a.active, 1ULL);
+}
+
+// ---------------------------------------------------------------------------
+// d<w, integrate(f)>/d alpha_att: pass 1 totals, pass 2 suffix sums
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kRayThreads) k_ray_grad_att(RayArgs a, const float* __restrict__ fa,
+                                                              const float* __restrict__ w, float* __restrict__ grad) {
+    const int64_t r = (int64_t)blockIdx.x * kRayThreads + threadIdx.x;
+    if (r >= a.nr) return;
+    const float wr = w[r];
+    if (wr == 0.f) return;
+    const int ncorner = a.twod ? 4 : 8;
+    float total = 0.f;
+    for (int pass = 0; pass < 2; ++pass) {
+        RayState st;
+        ray_init(a, r, a.energy0, st);
+        float prefix = 0.f;
+        for (int step = 0; step < a.max_steps; ++step) {
+            if (!st.active) break;
+            float ds, alpha;
+            ray_step(a, st, ds, alpha);
+            Corners c;
+            corners_at(a, st.xp, c);
+            const float eh = a.h_idx * st.E;
+            float contrib = 0.f;
+            for (int cn = 0; cn < ncorner; ++cn) {
+                const int X = (cn & 1) ? c.hi[0] : c.lo[0];
+                const int Y = (cn & 2) ? c.hi[1] : c.lo[1];
+                const int Z = (cn & 4) ? c.hi[2] : c.lo[2];
+                if ((unsigned)X >= (unsigned)a.nx || (unsigned)Y >= (unsigned)a.ny || (unsigned)Z >= (unsigned)a.nz)
+                    continue;
+                const float wt = ((cn & 1) ? c.whi[0] : c.wlo[0]) * ((cn & 2) ? c.whi[1] : c.wlo[1]) *
+                                 ((cn & 4) ? c.whi[2] : c.wlo[2]);
+                contrib = fmaf(__ldg(fa + ((size_t)X * a.ny + Y) * a.nz + Z), wt * eh, contrib);
+            }
+            if (pass == 1 && ds > 0.f) {
+                // att(step) = sum alpha(x_i) ds  ->  d integral / d alpha(x_i at this step)
+                //   = -ds * (contributions of this and all later steps)
+                const float suffix = total - prefix;
+                const float coef = -wr * ds * suffix;
+                if (coef != 0.f) {
+                    const float ix = unnorm(st.xi[0], a.norm[0], a.nx, false);
+                    const float iy = unnorm(st.xi[1], a.norm[1], a.ny, false);
+                    const float iz = unnorm(st.xi[2], a.norm[2], a.nz, false);
+                    const float fx = floorf(ix), fy = floorf(iy), fz = floorf(iz);
+                    const int x0 = (int)fx, y0 = (int)fy, z0 = (int)fz;
+                    const float wx1 = ix - fx, wy1 = iy - fy, wz1 = iz - fz;
+                    for (int cz = 0; cz < 2; ++cz) {
+                        const int Z = z0 + cz;
+                        if ((unsigned)Z >= (unsigned)a.nz) continue;
+                        for (int cy = 0; cy < 2; ++cy) {
+                            const int Y = y0 + cy;
+                            if ((unsigned)Y >= (unsigned)a.ny) continue;
+                            for (int cx = 0; cx < 2; ++cx) {
+                                const int X = x0 + cx;
+                                if ((unsigned)X >= (unsigned)a.nx) continue;
+                                const float tw = (cx ? wx1 : 1.f - wx1) * (cy ? wy1 : 1.f - wy1) * (cz ? wz1 : 1.f - wz1);
+                                atomicAdd(grad + ((size_t)X * a.ny + Y) * a.nz + Z, coef * tw);
+                            }
+                        }
+                    }
+                }
+            }
+            prefix += contrib;
+            if (step % a.check == 0 && exited(a, st)) st.active = false;
+        }
+        total = prefix;
+    }
+}
+
+__global__ void k_mul(const float* __restrict__ a, const float* __restrict__ b, float* __restrict__ out, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = a[i] * b[i];
+}
+
+__global__ void k_mul_acc(const float* __restrict__ a, const float* __restrict__ b, float scale, float* __restrict__ out,
+                          int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] += scale * (a[i] * b[i]);
+}
+
+__global__ void k_pack_n(const float* __restrict__ n, const float* __restrict__ g, float4* __restrict__ out, int64_t nv) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = make_float4(n[i], g[3 * i], g[3 * i + 1], g[3 * i + 2]);
+}
+
+RayArgs make_args(const vam_ray_plan* p) {
+    RayArgs a;
+    std::memset(&a, 0, sizeof(a));
+    const vam_ray_geom& g = p->g;
+    a.x0 = p->d_x0; a.v0 = p->d_v0; a.nfield = p->d_nfield; a.afield = p->d_afield;
+    a.nr = g.num_rays;
+    a.nx = g.n_x; a.ny = g.n_y; a.nz = g.n_z;
+    a.twod = g.n_z == 1;
+    for (int d = 0; d < 3; ++d) {
+        const double span = g.coord_max[d] - g.coord_min[d];
+        const double nrm = 2.0 / span;
+        a.norm[d] = std::isfinite(nrm) ? (float)nrm : 0.f;
+        a.half_span[d] = span / 2.0;
+        const double iv = 1.0 / g.voxel[d];
+        a.inv_voxel[d] = std::isfinite(iv) ? iv : 0.0;
+        a.bmax[d] = g.coord_max[d] + g.voxel[d];
+        a.bmin[d] = g.coord_min[d] - g.voxel[d];
+    }
+    a.h = (float)g.step_size;
+    a.h_idx = (float)(g.step_size / g.voxel[0]);
+    a.max_steps = g.max_num_step;
+    a.check = g.num_step_per_exit_check;
+    a.param = g.parametrization;
+    a.solver = g.ode_solver;
+    a.n_kind = p->med.index_kind;
+    a.n_sur = p->med.n_sur; a.lune_R = p->med.lune_R; a.lune_p = p->med.lune_p;
+    a.a_kind = p->med.atten_kind;
+    a.a_val = p->med.atten_value; a.a_R = p->med.atten_R;
+    a.energy0 = p->energy0;
+    a.active = p->d_active;
+    return a;
+}
+
+int ew_blocks(int64_t n) {
+    int64_t b = (n + 255) / 256;
+    return (int)(b > 4736 ? 4736 : (b < 1 ? 1 : b));
+}
+
+}  // namespace
+}  // namespace vam
+
+using namespace vam;
+
+extern "C" int vam_ray_plan_create(const vam_ray_geom* geom, const float* x0, const float* v0, float energy0,
+                                   vam_ray_plan** out) {
+    clear_error();
+    VAM_REQUIRE(geom && x0 && v0 && out, VAM_ERR_ARG, "vam_ray_plan_create: null argument");
+    *out = nullptr;
+    const vam_ray_geom& g = *geom;
+    VAM_REQUIRE(g.n_x > 1 && g.n_y > 1 && g.n_z >= 1 && g.num_rays > 0, VAM_ERR_SHAPE,
+                "vam_ray_plan_create: grid needs n_x, n_y >= 2, n_z >= 1 and num_rays > 0");
+    VAM_REQUIRE(g.max_num_step >= 0 && g.num_step_per_exit_check >= 1, VAM_ERR_ARG,
+                "vam_ray_plan_create: max_num_step >= 0 and num_step_per_exit_check >= 1 required");
+    VAM_REQUIRE(g.parametrization >= 0 && g.parametrization <= 2 && g.ode_solver >= 0 && g.ode_solver <= 2, VAM_ERR_ARG,
+                "vam_ray_plan_create: unknown parametrization or ode_solver");
+    VAM_REQUIRE(std::isfinite(g.step_size) && g.step_size > 0.0 && g.voxel[0] > 0.0 && g.voxel[1] > 0.0,
+                VAM_ERR_ARG, "vam_ray_plan_create: step size and voxel must be positive");
+    VAM_REQUIRE(g.n_z > 1 ? (std::isfinite(g.voxel[2]) && g.voxel[2] > 0.0) : true, VAM_ERR_ARG,
+                "vam_ray_plan_create: 3D grid needs a finite voxel[2]");
+    DeviceGuard dg(g.device);
+    VAM_REQUIRE(dg.ok, VAM_ERR_CUDA, "vam_ray_plan_create: cannot select device");
+    auto* p = new vam_ray_plan();
+    std::memset(p, 0, sizeof(*p));
+    p->g = g;
+    p->energy0 = energy0;
+    const size_t nv = (size_t)g.n_x * g.n_y * g.n_z;
+    cudaError_t e = cudaMalloc(&p->d_x0, sizeof(float) * 3 * g.num_rays);
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_v0, sizeof(float) * 3 * g.num_rays);
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_scratch, sizeof(float) * nv);
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_absorb, sizeof(float) * nv);
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_active, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemcpy(p->d_x0, x0, sizeof(float) * 3 * g.num_rays, cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(p->d_v0, v0, sizeof(float) * 3 * g.num_rays, cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) e = cudaMemset(p->d_active, 0, sizeof(unsigned long long));
+    if (e != cudaSuccess) {
+        vam_ray_plan_destroy(p);
+        return set_error(VAM_ERR_NOMEM, std::string("vam_ray_plan_create: ") + cudaGetErrorString(e));
+    }
+    *out = p;
+    return VAM_OK;
+}
+
+extern "C" int vam_ray_plan_destroy(vam_ray_plan* p) {
+    if (!p) return VAM_OK;
+    DeviceGuard dg(p->g.device);
+    cudaFree(p->d_x0);
+    cudaFree(p->d_v0);
+    cudaFree(p->d_nfield);
+    cudaFree(p->d_afield);
+    cudaFree(p->d_absorb);
+    cudaFree(p->d_scratch);
+    cudaFree(p->d_active);
+    delete p;
+    return VAM_OK;
+}
+
+extern "C" int vam_ray_set_medium(vam_ray_plan* p, const vam_ray_medium* m, vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(p && m, VAM_ERR_ARG, "vam_ray_set_medium: null argument");
+    VAM_REQUIRE(m->index_kind >= 0 && m->index_kind <= 2 && m->atten_kind >= 0 && m->atten_kind <= 3, VAM_ERR_ARG,
+                "vam_ray_set_medium: unknown index or attenuation kind");
+    VAM_REQUIRE(m->absorb_at_grid_dev, VAM_ERR_ARG, "vam_ray_set_medium: absorb_at_grid_dev is required");
+    DeviceGuard dg(p->g.device);
+    cudaStream_t st = (cudaStream_t)stream;
+    const int64_t nv = (int64_t)p->g.n_x * p->g.n_y * p->g.n_z;
+    if (m->index_kind == VAM_INDEX_GRID) {
+        VAM_REQUIRE(m->n_grid_dev && m->grad_n_grid_dev, VAM_ERR_ARG, "vam_ray_set_medium: GRID index needs n and grad n");
+        if (!p->d_nfield) VAM_TRY_CUDA(cudaMalloc(&p->d_nfield, sizeof(float4) * nv));
+        k_pack_n<<<ew_blocks(nv), 256, 0, st>>>(m->n_grid_dev, m->grad_n_grid_dev, p->d_nfield, nv);
+        VAM_CHECK_LAUNCH("k_pack_n");
+    } else {
+        VAM_REQUIRE(std::isfinite(m->n_sur) && m->n_sur > 0.f, VAM_ERR_ARG, "vam_ray_set_medium: n_sur must be > 0");
+    }
+    if (m->atten_kind == VAM_ALPHA_GRID) {
+        VAM_REQUIRE(m->atten_grid_dev, VAM_ERR_ARG, "vam_ray_set_medium: GRID attenuation needs atten_grid_dev");
+        if (!p->d_afield) VAM_TRY_CUDA(cudaMalloc(&p->d_afield, sizeof(float) * nv));
+        VAM_TRY_CUDA(cudaMemcpyAsync(p->d_afield, m->atten_grid_dev, sizeof(float) * nv, cudaMemcpyDeviceToDevice, st));
+    }
+    VAM_TRY_CUDA(cudaMemcpyAsync(p->d_absorb, m->absorb_at_grid_dev, sizeof(float) * nv, cudaMemcpyDeviceToDevice, st));
+    p->med = *m;
+    p->med.n_grid_dev = p->med.grad_n_grid_dev = p->med.atten_grid_dev = p->med.absorb_at_grid_dev = nullptr;
+    p->has_medium = 1;
+    return VAM_OK;
+}
+
+extern "C" int vam_ray_integrate(vam_ray_plan* p, const float* f, float* g, vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(p && f && g, VAM_ERR_ARG, "vam_ray_integrate: null argument");
+    VAM_REQUIRE(p->has_medium, VAM_ERR_ARG, "vam_ray_integrate: no medium bound (vam_ray_set_medium)");
+    DeviceGuard dg(p->g.device);
+    cudaStream_t st = (cudaStream_t)stream;
+    const int64_t nv = (int64_t)p->g.n_x * p->g.n_y * p->g.n_z;
+    k_mul<<<ew_blocks(nv), 256, 0, st>>>(f, p->d_absorb, p->d_scratch, nv);
+    VAM_TRY_CUDA(cudaMemsetAsync(p->d_active, 0, sizeof(unsigned long long), st));
+    RayArgs a = make_args(p);
+    const unsigned nb = (unsigned)((p->g.num_rays + kRayThreads - 1) / kRayThreads);
+    k_ray_integrate<<<nb, kRayThreads, 0, st>>>(a, p->d_scratch, g);
+    VAM_CHECK_LAUNCH("k_ray_integrate");
+    return VAM_OK;
+}
+
+extern "C" int vam_ray_deposit(vam_ray_plan* p, const float* gin, float* dose, vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(p && gin && dose, VAM_ERR_ARG, "vam_ray_deposit: null argument");
+    VAM_REQUIRE(p->has_medium, VAM_ERR_ARG, "vam_ray_deposit: no medium bound (vam_ray_set_medium)");
+    DeviceGuard dg(p->g.device);
+    cudaStream_t st = (cudaStream_t)stream;
+    const int64_t nv = (int64_t)p->g.n_x * p->g.n_y * p->g.n_z;
+    VAM_TRY_CUDA(cudaMemsetAsync(p->d_scratch, 0, sizeof(float) * nv, st));
+    VAM_TRY_CUDA(cudaMemsetAsync(p->d_active, 0, sizeof(unsigned long long), st));
+    RayArgs a = make_args(p);
+    const unsigned nb = (unsigned)((p->g.num_rays + kRayThreads - 1) / kRayThreads);
+    k_ray_deposit<<<nb, kRayThreads, 0, st>>>(a, gin, p->d_scratch);
+    VAM_CHECK_LAUNCH("k_ray_deposit");
+    k_mul<<<ew_blocks(nv), 256, 0, st>>>(p->d_scratch, p->d_absorb, dose, nv);
+    VAM_CHECK_LAUNCH("k_mul");
+    return VAM_OK;
+}
+
+extern "C" int vam_ray_grad_alpha(vam_ray_plan* p, const float* f, const float* w, float* grad_att, float* grad_abs,
+                                  vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(p && f && w, VAM_ERR_ARG, "vam_ray_grad_alpha: null argument");
+    VAM_REQUIRE(p->has_medium, VAM_ERR_ARG, "vam_ray_grad_alpha: no medium bound (vam_ray_set_medium)");
+    VAM_REQUIRE(!grad_att || p->med.atten_kind == VAM_ALPHA_GRID, VAM_ERR_NOTSUP,
+                "vam_ray_grad_alpha: grad_att needs a GRID attenuation");
+    DeviceGuard dg(p->g.device);
+    cudaStream_t st = (cudaStream_t)stream;
+    const int64_t nv = (int64_t)p->g.n_x * p->g.n_y * p->g.n_z;
+    RayArgs a = make_args(p);
+    const unsigned nb = (unsigned)((p->g.num_rays + kRayThreads - 1) / kRayThreads);
+    if (grad_att) {
+        k_mul<<<ew_blocks(nv), 256, 0, st>>>(f, p->d_absorb, p->d_scratch, nv);
+        k_ray_grad_att<<<nb, kRayThreads, 0, st>>>(a, p->d_scratch, w, grad_att);
+        VAM_CHECK_LAUNCH("k_ray_grad_att");
+    }
+    if (grad_abs) {
+        VAM_TRY_CUDA(cudaMemsetAsync(p->d_scratch, 0, sizeof(float) * nv, st));
+        VAM_TRY_CUDA(cudaMemsetAsync(p->d_active, 0, sizeof(unsigned long long), st));
+        // deposit of w with unit start energy, times the forward's energy0:
+        // sum_r w_r * energy0 * exp(-att) * (h/voxel) * w_corner at every voxel
+        k_ray_deposit<<<nb, kRayThreads, 0, st>>>(a, w, p->d_scratch);
+        VAM_CHECK_LAUNCH("k_ray_deposit");
+        k_mul_acc<<<ew_blocks(nv), 256, 0, st>>>(p->d_scratch, f, p->energy0, grad_abs, nv);
+        VAM_CHECK_LAUNCH("k_mul_acc");
+    }
+    return VAM_OK;
+}
+
+extern "C" int vam_ray_active_at_cap(vam_ray_plan* p, int64_t* out) {
+    clear_error();
+    VAM_REQUIRE(p && out, VAM_ERR_ARG, "vam_ray_active_at_cap: null argument");
+    DeviceGuard dg(p->g.device);
+    unsigned long long v = 0;
+    VAM_TRY_CUDA(cudaMemcpy(&v, p->d_active, sizeof(v), cudaMemcpyDeviceToHost));
+    *out = (int64_t)v;
+    return VAM_OK;
+}

@@ -1,0 +1,72 @@
+// vam_internal.cuh -- shared definitions of the sm_100a projection core.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/vam.h"
+
+namespace vam {
+
+// Records the message of the failing call (thread-local) and returns code.
+int set_error(int code, const std::string& msg);
+void clear_error();
+
+#define VAM_TRY_CUDA(call)                                                                     \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return ::vam::set_error(VAM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define VAM_CHECK_LAUNCH(name)                                                                 \
+    do {                                                                                       \
+        cudaError_t e_ = cudaGetLastError();                                                   \
+        if (e_ != cudaSuccess)                                                                 \
+            return ::vam::set_error(VAM_ERR_CUDA, std::string(name) + " launch: " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define VAM_REQUIRE(cond, code, msg)                                                           \
+    do {                                                                                       \
+        if (!(cond)) return ::vam::set_error((code), (msg));                                   \
+    } while (0)
+
+// Makes `device` current for the scope of an entry point and restores the
+// caller's device on exit.
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = true;
+    explicit DeviceGuard(int device) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != device) ok = cudaSetDevice(device) == cudaSuccess;
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+constexpr int kWarp = 32;
+
+__host__ __device__ inline int ilog2_pow2(int v) {
+    int r = 0;
+    while ((1 << r) < v) ++r;
+    return r;
+}
+
+}  // namespace vam
+
+// Plan of the parallel-beam projector family (lives on one device).
+struct vam_parallel_plan {
+    int nY, nX, nZ, nA, C, device;
+    double4* d_trig;        // per angle: cos, sin, m02, m12 (skimage warp matrix offsets)
+    uint8_t* d_circle;      // [nY][nX], 1 inside the inscribed circle (util/data.py:14-40)
+    int abs_mode;           // vam_absorption_mode
+    float abs_alpha, abs_R;
+    float* d_mask;          // [nY][nX] for VAM_ABS_MASK
+    float* d_occ;           // [nR][nA][nZ] occlusion sinogram, NaN = none
+    uint8_t* d_occ_flag;    // [nA][nZ] forward shadow gate
+    int has_occ;
+};

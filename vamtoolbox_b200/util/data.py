@@ -1,0 +1,155 @@
+"""Array helpers of the reference's ``vamtoolbox.util.data`` (vamtoolbox/util/data.py).
+
+Host (numpy) versions keep the reference's semantics, including its in-place
+writes (``clipToCircle`` modifies and returns its argument); ``*_t`` variants
+operate on torch tensors on the device.  The Fourier filters run once per
+optimisation at initialisation; the sinogram filter has a device version
+(batched FFT along the detector axis, ``filterSinogram_t``).
+"""
+from __future__ import annotations
+
+import numpy as np
+import scipy.fft
+from scipy.fft import fft, fft2, ifft, ifft2
+
+
+def sigmoid(x, g):
+    """1 / (1 + exp(-x / g)) (util/data.py:9-11)."""
+    return (1 / (1 + np.exp(-x * (1 / g)))).astype(float)
+
+
+def _circle_outside(ny, nx):
+    cy, cx = np.meshgrid(np.linspace(-1, 1, ny), np.linspace(-1, 1, nx))
+    return cx ** 2 + cy ** 2 > 1
+
+
+def clipToCircle(x):
+    """Zero everything outside the inscribed circle, in place (util/data.py:14-40)."""
+    out = _circle_outside(x.shape[0], x.shape[1])
+    if x.ndim == 2:
+        x[out] = 0
+    else:
+        x[np.broadcast_to(out[..., np.newaxis], x.shape)] = 0
+    return x
+
+
+def circle_inside_mask(ny, nx):
+    """Boolean [ny, nx] mask of the pixels clipToCircle keeps."""
+    return ~_circle_outside(ny, nx)
+
+
+def filterTargetOSMO(x, filter_name):
+    """Radial 2-D Fourier filter of each z slice (util/data.py:43-113)."""
+    filter_types = ("ram-lak", "shepp-logan", "cosine", "hamming", "hanning", None)
+    if filter_name not in filter_types:
+        raise ValueError("Unknown filter: %s" % filter_name)
+    if filter_name is None or filter_name.lower() == "none":
+        return x
+    n_y, n_x = x.shape[0], x.shape[1]
+    f_y, f_x = np.meshgrid(np.linspace(-1, 1, n_y), np.linspace(-1, 1, n_x), indexing="ij")
+    f = np.sqrt(f_x ** 2 + f_y ** 2)
+    filt = np.real(f)
+    if filter_name == "shepp-logan":
+        omega = np.pi / 2 * f
+        nz = omega != 0
+        filt[nz] *= np.sin(omega[nz]) / omega[nz]
+    elif filter_name == "cosine":
+        filt *= np.cos(np.pi / 2 * f)
+    elif filter_name == "hamming":
+        w = np.abs(np.hamming(n_x))
+        filt *= np.abs(np.sqrt(np.outer(w, w)))
+    elif filter_name == "hanning":
+        w = np.abs(np.hanning(n_x))
+        filt *= np.abs(np.sqrt(np.outer(w, w)))
+    X = scipy.fft.fftshift(fft2(x, axes=(0, 1)), axes=(0, 1))
+    if x.ndim == 2:
+        out = ifft2(scipy.fft.ifftshift(X * filt, axes=(0, 1)), axes=(0, 1))
+    else:
+        out = ifft2(scipy.fft.ifftshift(X * filt[:, :, np.newaxis], axes=(0, 1)), axes=(0, 1))
+    return out.astype(float)
+
+
+def _get_fourier_filter(size, filter_name):
+    """Ram-Lak family filter built from its spatial form (util/data.py:373-438; Kak & Slaney ch. 3 eq. 61)."""
+    n = np.concatenate((np.arange(1, size / 2 + 1, 2, dtype=int), np.arange(size / 2 - 1, 0, -2, dtype=int)))
+    f = np.zeros(size)
+    f[0] = 0.25
+    f[1::2] = -1 / (np.pi * n) ** 2
+    filt = 2 * np.real(fft(f))
+    if filter_name == "shepp-logan":
+        omega = np.pi * scipy.fft.fftfreq(size)[1:]
+        filt[1:] *= np.sin(omega) / omega
+    elif filter_name == "cosine":
+        filt *= scipy.fft.fftshift(np.sin(np.linspace(0, np.pi, size, endpoint=False)))
+    elif filter_name == "hamming":
+        filt *= scipy.fft.fftshift(np.hamming(size))
+    elif filter_name == "hanning":
+        filt *= scipy.fft.fftshift(np.hanning(size))
+    elif filter_name == "ram-lak_freq":
+        filt /= (np.pi / 4) ** 2
+    elif filter_name == "ram-lak_scikit":
+        filt *= np.pi / 2
+    elif filter_name is None or filter_name.lower() == "none":
+        filt[:] = 1
+    return filt[:, np.newaxis]
+
+
+_SINO_FILTERS = ("ram-lak", "shepp-logan", "cosine", "hamming", "hanning", "ram-lak_freq", "ram-lak_scikit", None)
+
+
+def filterSinogram(sinogram, filter_name):
+    """Filter along the detector axis, zero-padded to a power of two >= 2 nR (util/data.py:302-370)."""
+    if filter_name is None or filter_name.lower() == "none":
+        return sinogram
+    if filter_name.lower() not in _SINO_FILTERS:
+        raise ValueError("Unknown filter: %s" % filter_name)
+    if sinogram.ndim not in (2, 3):
+        raise Exception("The sinogram provided does not have compatible number of dimension (2 or 3).")
+    pX = sinogram.shape[0]
+    size = max(64, int(2 ** np.ceil(np.log2(2 * pX))))
+    filt = _get_fourier_filter(size, filter_name)
+    if sinogram.ndim == 2:
+        img = np.pad(sinogram, ((0, size - pX), (0, 0)))
+        return np.real(ifft(fft(img, axis=0) * filt, axis=0)[:pX, :])
+    out = np.zeros(sinogram.shape, dtype=float)
+    for z in range(sinogram.shape[2]):
+        img = np.pad(sinogram[:, :, z], ((0, size - pX), (0, 0)))
+        out[:, :, z] = np.real(ifft(fft(img, axis=0) * filt, axis=0)[:pX, :])
+    return out
+
+
+def filterSinogram_t(sino, filter_name):
+    """Device version of filterSinogram for a [nR, nA, nZ] (or [nR, nA]) torch tensor."""
+    import torch
+
+    if filter_name is None or filter_name.lower() == "none":
+        return sino
+    if filter_name.lower() not in _SINO_FILTERS:
+        raise ValueError("Unknown filter: %s" % filter_name)
+    pX = sino.shape[0]
+    size = max(64, int(2 ** np.ceil(np.log2(2 * pX))))
+    filt = torch.as_tensor(_get_fourier_filter(size, filter_name)[:, 0], device=sino.device, dtype=torch.float64)
+    shape = (size,) + (1,) * (sino.ndim - 1)
+    spec = torch.fft.fft(sino.to(torch.float64), n=size, dim=0) * filt.reshape(shape)
+    return torch.fft.ifft(spec, dim=0).real[:pX].to(sino.dtype).contiguous()
+
+
+def discretize(x, bit_depth, range, output_dtype=float):
+    """Quantise to 2**bit_depth levels of np.linspace(range) (util/data.py:495-523)."""
+    assert len(range) == 2, "range argument should have 2 elements [min,max]"
+    bins = np.linspace(range[0], range[1], 2 ** bit_depth, endpoint=True)
+    return bins[np.digitize(x, bins=bins) - 1].astype(output_dtype)
+
+
+def discretize_t(x, bit_depth, lo, hi):
+    """Device version of discretize for a torch tensor (lo / hi python or 0-d tensors)."""
+    import torch
+
+    n = 2 ** bit_depth
+    t = torch.linspace(0.0, 1.0, n, device=x.device, dtype=torch.float64)
+    lo = torch.as_tensor(lo, device=x.device, dtype=torch.float64)
+    hi = torch.as_tensor(hi, device=x.device, dtype=torch.float64)
+    bins = lo + (hi - lo) * t
+    idx = torch.bucketize(x.to(torch.float64), bins, right=True) - 1
+    idx = idx % n  # np.digitize below the first bin gives -1 -> last bin (numpy wraps)
+    return bins[idx].to(x.dtype)
