@@ -1,0 +1,459 @@
+#!/usr/bin/env python
+"""Benchmark: fused BCLP iterations/s at 256^3 x 360 angles with absorption.
+
+One step = one BCLP iteration (vamtoolbox/optimizer/BCLP.py:277-534) on the
+3-D parallel-beam absorbing target (seeded union of ellipsoids / cylinders in
+a radius-120 vial, 256^3 float32, 360 angles over [0, 360), radial
+absorption mask with e^-1 transmission across the container): reference-parity
+backprojection, fused dose pass, forward projection, clamped update, all on
+the device, replayed from one CUDA graph.  With N GPUs every rank owns a
+256-slice z-slab of a 256 x 256 x 256N target (weak scaling); slices are
+independent in both projectors, so the only exchange is an all-reduce of the
+9 loss / norm sums per iteration.
+
+Reported beside the headline:
+  e2e         the same iteration driven with host buffers: pinned-host g -> device,
+              iteration, g and the loss sums -> pinned host, every step;
+  plain       the reference's numpy loop calling the projector per step with host
+              arrays (engine="host"), the plain per-call GPU path;
+  fwd_adj     forward + reference-parity backprojection pairs per second;
+  roofline    of the dominant kernel (forward projector), HBM bytes it must move;
+  cpu_baseline the reference's algorithm (oracle/vamoracle.c, OpenMP) on a bounded
+              z-slab sample on this host's cores, extrapolated to the full volume.
+`--impl reference` prints the CPU reference arm's line instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "BCLP iter/s & fwd+adj proj/s, 256³×360 ang: fused vs plain GPU, relL2≤1e-4"
+UNIT = "iter/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--angles", type=int, default=360)
+    ap.add_argument("--plain-steps", type=int, default=2)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+PIXEL_CM = 0.002          # 500 voxels / cm
+
+
+def build_problem(n, n_angles, seed):
+    from vamtoolbox_b200 import geometry, synthetic
+
+    target = synthetic.ellipsoids_3d(n, seed=seed, radius=120.0 * n / 256)
+    angles = np.linspace(0, 360, n_angles, endpoint=False)
+    R = n / 2 * PIXEL_CM                       # container radius = grid radius
+    alpha = 1.0 / (2 * R)                      # e^-1 transmission across the diameter
+    tg = geometry.TargetGeometry(target=target)
+    pg = geometry.ProjectionGeometry(angles, "parallel", CUDA=True, projector_pixel_size=PIXEL_CM,
+                                     absorption_coeff=alpha, container_radius=R)
+    pg.calcAbsorptionMask(tg)
+    return tg, pg
+
+
+def bclp_options(n_iter):
+    from vamtoolbox_b200.optimize import Options
+
+    return Options(method="BCLP", n_iter=n_iter, p=2, q=1, eps=0.1, learning_rate=1e-5, filter="ram-lak")
+
+
+def count_angle_pairs(angles):
+    """Pairs (a, a + 180 deg) the forward kernel samples from one lattice (same rule as the plan)."""
+    used = np.zeros(len(angles), bool)
+    pairs = 0
+    for i in range(len(angles)):
+        if used[i]:
+            continue
+        used[i] = True
+        for k in range(i + 1, len(angles)):
+            if used[k]:
+                continue
+            d = np.fmod(angles[k] - angles[i] - 180.0, 360.0)
+            d = d + 360.0 if d < 0 else d
+            if d < 1e-9 or 360.0 - d < 1e-9:
+                used[k] = True
+                pairs += 1
+                break
+    return pairs
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    def __init__(self, index):
+        self.path = Path(tempfile.mkstemp(suffix=".csv")[1])
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in self.path.read_text().splitlines():
+            p = [x.strip() for x in line.split(",")]
+            if len(p) >= 9:
+                rows.append(p)
+        self.path.unlink(missing_ok=True)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# CPU reference algorithm (oracle) on a z-slab sample
+# ---------------------------------------------------------------------------
+def cpu_bclp_sample(tg, pg, g0, opts, n_slices, steps=1):
+    """Time `steps` BCLP iterations of the reference's algorithm on n_slices z-slices."""
+    from oracle import oracle as O
+
+    rm = opts.response_model
+    f_T = np.asarray(tg.array[:, :, :n_slices], dtype=np.float64)
+    g = np.asarray(g0[:, :, :n_slices], dtype=np.float64).copy()
+    mask = np.asarray(pg.absorption_mask)[:, :, 0]
+    ang = np.asarray(pg.angles, dtype=np.float64)
+    absn = ("mask", mask)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        dose = O.parallel_backward_ref(g, ang, absorption=absn)
+        mapped = rm.map(dose)
+        e = mapped - f_T
+        eb = np.abs(e) - opts.eps
+        v = eb > 0
+        loss = np.sum(v * opts.weight * np.abs(eb) ** opts.p) ** (opts.q / opts.p)
+        operand = v * opts.weight * np.abs(eb) ** (opts.p - 1) * np.sign(e) * rm.dmapdf(dose)
+        fwd = O.parallel_forward(operand, ang, absorption=absn)
+        grad = (opts.q * loss ** ((opts.q - opts.p) / opts.q)) * fwd if loss != 0 else fwd
+        g = np.clip(g - opts.learning_rate * grad, opts.blb, opts.bub)
+    return (time.perf_counter() - t0) / steps
+
+
+def cpu_baseline(tg, pg, g0, opts, n_total, budget_s):
+    from oracle import oracle as O
+
+    cores = O.num_threads()
+    t1 = cpu_bclp_sample(tg, pg, g0, opts, 1)
+    n = int(max(1, min(n_total, budget_s / max(t1, 1e-6))))
+    n = max(1, min(n, 64))
+    t = cpu_bclp_sample(tg, pg, g0, opts, n)
+    per_iter = t * n_total / n
+    return {"value": 1.0 / per_iter, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{n} of {n_total} z-slices x {pg.n_angles} angles, 1 BCLP iteration (float64 C oracle, "
+                      f"OpenMP {cores} threads), extrapolated linearly over z-slices ({t:.2f} s measured)"}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+
+    ws_, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if ws_ > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    from vamtoolbox_b200 import _lib
+    from vamtoolbox_b200.optimizer.BCLP import BCLPNorm
+
+    _lib.load()
+    n, na = args.size, args.angles
+    tg, pg = build_problem(n, na, seed=1000 + rank)
+    n_iter = args.warmup + args.steps + 4
+    opts = bclp_options(n_iter)
+    bclp = BCLPNorm(tg, pg, opts)
+
+    reduce_stats = None
+    if dist is not None:
+        def reduce_stats(stats):
+            dist.all_reduce(stats[:7], op=dist.ReduceOp.SUM)
+            dist.all_reduce(stats[7:], op=dist.ReduceOp.MAX)
+
+    it = bclp.device_iteration(reduce_stats=reduce_stats)
+    st = torch.cuda.current_stream(dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    # ---- fused iteration: graph when single GPU, eager stream-ordered otherwise
+    if dist is None:
+        graph = it.capture()
+        run_step = graph.replay
+    else:
+        graph = None
+        run_step = it.step
+    for _ in range(args.warmup):
+        run_step()
+    barrier()
+    clocks = ClockSampler(local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record(st)
+    for _ in range(args.steps):
+        run_step()
+    e1.record(st)
+    barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    ms_max = ms
+    if dist is not None:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = ws_ * 1000.0 / ms_max
+
+    # ---- per-kernel timing over an eager pass (same kernels, events on the stream)
+    plan = bclp.P.plan
+    kt = {"forward": [], "backward_ref": [], "dose_pass+update": []}
+    for _ in range(args.steps):
+        a, b_, c, d = (torch.cuda.Event(enable_timing=True) for _ in range(4))
+        a.record(st)
+        it.back(it.g, it.dose)
+        b_.record(st)
+        it.ws.bclp_dose_pass(it.dose, it.fT, it.prm, it.mapped, it.operand, it.stats)
+        c.record(st)
+        it.fwd(it.operand, it.grad)
+        d.record(st)
+        torch.cuda.synchronize(dev)
+        kt["backward_ref"].append(a.elapsed_time(b_))
+        kt["dose_pass+update"].append(b_.elapsed_time(c))
+        kt["forward"].append(c.elapsed_time(d))
+    kmean = {k: float(np.mean(v)) for k, v in kt.items()}
+
+    # ---- fwd + adj projection pairs / s
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(st)
+    for _ in range(args.steps):
+        plan.forward(it.operand, it.grad)
+        plan.backward_ref(it.g, it.dose)
+    e3.record(st)
+    torch.cuda.synchronize(dev)
+    fwd_adj = 1000.0 / (e2.elapsed_time(e3) / args.steps)
+    e2.record(st)
+    for _ in range(args.steps):
+        plan.forward(it.operand, it.grad)
+        plan.adjoint(it.g, it.dose)
+    e3.record(st)
+    torch.cuda.synchronize(dev)
+    fwd_matched = 1000.0 / (e2.elapsed_time(e3) / args.steps)
+
+    # ---- end to end with host buffers (pinned), every step
+    g_host = it.g.detach().cpu().pin_memory()
+    g_out = torch.empty_like(g_host).pin_memory()
+    s_out = torch.empty(9, dtype=torch.float32).pin_memory()
+    for _ in range(2):
+        it.g.copy_(g_host, non_blocking=True)
+        run_step()
+        g_out.copy_(it.g, non_blocking=True)
+        s_out.copy_(it.stats, non_blocking=True)
+    barrier()
+    e2.record(st)
+    for _ in range(args.steps):
+        it.g.copy_(g_host, non_blocking=True)
+        run_step()
+        g_out.copy_(it.g, non_blocking=True)
+        s_out.copy_(it.stats, non_blocking=True)
+    e3.record(st)
+    barrier()
+    e2e_ms = e2.elapsed_time(e3) / args.steps
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    h2d = g_host.numel() * 4
+    d2h = g_out.numel() * 4 + s_out.numel() * 4
+
+    # ---- plain per-call GPU path (reference numpy loop, host arrays)
+    plain = None
+    if rank == 0 and args.plain_steps > 0:
+        from vamtoolbox_b200.optimize import Options
+
+        o2 = Options(method="BCLP", n_iter=args.plain_steps, p=2, q=1, eps=0.1, learning_rate=1e-5, engine="host")
+        b2 = BCLPNorm.__new__(BCLPNorm)
+        b2.__dict__.update(bclp.__dict__)
+        b2.logs = type(bclp.logs)(o2)
+        b2.logs.startTiming()
+        b2.exit_param = None
+        t0 = time.perf_counter()
+        b2.gradientDescentHost()
+        torch.cuda.synchronize(dev)
+        plain = args.plain_steps / (time.perf_counter() - t0 - 0.0)
+
+    # ---- roofline of the dominant kernel (forward projector)
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        pass
+    hbm_peak = peaks.get("hbm_gbs")
+    peak_src = "measured" if hbm_peak else "fallback"
+    hbm_peak = hbm_peak or 6650.0
+    ny = nx = n
+    vol_bytes = ny * nx * n * 4
+    sino_bytes = ny * na * n * 4
+    fwd_ms = kmean["forward"]
+    achieved = (vol_bytes + sino_bytes) / (fwd_ms * 1e-3) / 1e9
+    # taps the kernel gathers: 4 x 4 B per lattice sample and slice; angle pairs (a, a+180) share one
+    # lattice of (N+1)^2 samples (even N), unpaired angles use N^2
+    pairs = count_angle_pairs(np.linspace(0, 360, na, endpoint=False))
+    lattice = pairs * (n + 1 - n % 2) ** 2 + (na - 2 * pairs) * n * n
+    tap_bytes = 16.0 * lattice * n
+    onchip_peak = 148 * 128 * 1.965e9 / 1e9     # L1/shared load bandwidth, nominal
+    traffic = None
+    tf = ROOT / "profiles" / "forward_traffic.json"
+    if tf.exists():
+        try:
+            tr = json.loads(tf.read_text())
+            traffic = tr.get("bytes_per_launch_scaled")
+        except Exception:
+            traffic = None
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        try:
+            cpu = cpu_baseline(tg, pg, bclp.g0, opts, n, args.cpu_seconds)
+        except Exception as exc:  # report, never fail the GPU number on it
+            cpu = {"value": None, "unit": UNIT, "error": str(exc)}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": ws_, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_max, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ellipsoid/cylinder target, "
+            "shapes of the 256^3 x 360 absorbing OSMO/BCLP configuration)",
+            "config": {"workload": f"BCLP iteration, parallel beam, {n}^3 x {na} angles per GPU, radial absorption "
+                                   f"mask e^-1, z-slab per rank", "global_batch": ws_, "target": [n, n, n * ws_],
+                       "angles": na, "parallelism": f"z-slab x{ws_}" if ws_ > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (working set ~450 MB per iteration)",
+                       "graph": dist is None},
+            "e2e": {"value": round(1000.0 * ws_ / e2e_ms, 4), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "plain_gpu": {"value": plain, "unit": UNIT, "path": "reference numpy BCLP loop, projector per call with "
+                                                                 "host arrays"},
+            "fused_vs_plain": (value / ws_ / plain) if plain else None,
+            "fwd_adj_proj_per_s": round(fwd_adj, 3),
+            "fwd_matched_adj_proj_per_s": round(fwd_matched, 3),
+            "kernel_ms": {k: round(v, 4) for k, v in kmean.items()},
+            "gpu_launches": it.launches_per_step * args.steps,
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm_peak, "unit": "GB/s",
+                         "frac": round(achieved / hbm_peak, 5), "traffic": traffic, "peak_source": peak_src,
+                         "kernel": "forward projector (R1)",
+                         "onchip": {"gathered_tap_bytes": tap_bytes, "reference_tap_bytes": 16.0 * n * n * na * n,
+                                    "achieved_GBs": round(tap_bytes / (fwd_ms * 1e-3) / 1e9, 1),
+                                    "nominal_peak_GBs": round(onchip_peak, 1),
+                                    "frac": round(tap_bytes / (fwd_ms * 1e-3) / 1e9 / onchip_peak, 4)}},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    del graph
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    ws_, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import oracle as O
+
+    n, na = args.size, args.angles
+    tg, pg = build_problem(n, na, seed=1000)
+    opts = bclp_options(4)
+    # initial sinogram as the reference builds it: forward of map_inv(target), filter, scale (CPU oracle, sample)
+    n_s = 1
+    f0 = opts.response_model.map_inv(tg.array[:, :, :n_s])
+    absn = ("mask", np.asarray(pg.absorption_mask)[:, :, 0])
+    from vamtoolbox_b200.util.data import filterSinogram
+
+    g_s = filterSinogram(O.parallel_forward(f0, pg.angles, absorption=absn), "ram-lak") * np.pi / (2 * na)
+    g_s = np.clip(g_s, 0, None)
+    t1 = cpu_bclp_sample(tg, pg, g_s, opts, n_s)
+    n_slice = int(max(1, min(n, args.cpu_seconds / max(t1, 1e-6))))
+    f0 = opts.response_model.map_inv(tg.array[:, :, :n_slice])
+    g_s = np.clip(filterSinogram(O.parallel_forward(f0, pg.angles, absorption=absn), "ram-lak") * np.pi / (2 * na), 0,
+                  None)
+    for _ in range(max(0, min(args.warmup, 1))):
+        cpu_bclp_sample(tg, pg, g_s, opts, n_slice)
+    ts = [cpu_bclp_sample(tg, pg, g_s, opts, n_slice) for _ in range(max(1, min(args.steps, 3)))]
+    per = float(np.mean(ts)) * n / n_slice
+    value = 1.0 / per
+    cores = O.num_threads()
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws_, "steps": len(ts), "warmup": args.warmup,
+            "ms_per_step": per * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"BCLP iteration, parallel beam, {n}^3 x {na} angles, radial absorption mask"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{n_slice} of {n} z-slices per step, float64 C restatement of the reference's "
+                                       f"projectors + numpy BCLP body, extrapolated over z"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,114 @@
+"""Optimizers through the public API vs the reference's own optimizer runs
+(tests/golden/optim.npz, float64 numpy) and device engine vs host engine."""
+import numpy as np
+import pytest
+
+from tests.conftest import relL2
+
+pytestmark = pytest.mark.gpu
+
+
+def geo(target, angles):
+    from vamtoolbox_b200 import geometry
+
+    return geometry.TargetGeometry(target=target.copy()), geometry.ProjectionGeometry(angles, "parallel", CUDA=True)
+
+
+def opts(**kw):
+    from vamtoolbox_b200.optimize import Options
+
+    return Options(**kw)
+
+
+def counts_close(a, b, tg):
+    n = np.sum(tg.gel_inds) + np.sum(tg.void_inds)
+    return np.all(np.abs(np.asarray(a) - np.asarray(b)) * n <= 1.0 + 1e-9)
+
+
+@pytest.mark.parametrize("engine", ["device", "host"])
+def test_cal_matches_reference(golden, engine):
+    from vamtoolbox_b200.optimize import optimize
+
+    O = golden["optim"]
+    tg, pg = geo(O["target"], O["angles"])
+    s, r, e = optimize(tg, pg, opts(method="CAL", n_iter=5, learning_rate=0.4, d_h=0.5, sigmoid=0.01, engine=engine))
+    assert relL2(s.array, O["cal_sino"]) < 1e-4
+    assert relL2(r.array, O["cal_recon"]) < 1e-4
+    assert counts_close(e, O["cal_err"], tg)
+
+
+@pytest.mark.parametrize("engine", ["device", "host"])
+def test_osmo_matches_reference(golden, engine):
+    from vamtoolbox_b200.optimize import optimize
+
+    O = golden["optim"]
+    tg, pg = geo(O["target"], O["angles"])
+    s, r, e = optimize(tg, pg, opts(method="OSMO", n_iter=4, d_h=0.8, d_l=0.7, filter="ram-lak", engine=engine))
+    assert relL2(s.array, O["osmo_sino"]) < 1e-4
+    assert relL2(r.array, O["osmo_recon"]) < 1e-4
+    assert counts_close(e, O["osmo_err"], tg)
+
+
+def test_fbp_matches_reference(golden):
+    from vamtoolbox_b200.optimize import optimize
+
+    O = golden["optim"]
+    tg, pg = geo(O["target"], O["angles"])
+    s, r, e = optimize(tg, pg, opts(method="FBP", n_iter=1, filter="ram-lak"))
+    assert relL2(s.array, O["fbp_sino"]) < 1e-5
+    assert relL2(r.array, O["fbp_recon"]) < 1e-5
+    assert counts_close(e[:1], O["fbp_err"][:1], tg)
+
+
+@pytest.mark.parametrize("engine", ["device", "host"])
+def test_bclp_matches_reference(golden, engine):
+    from vamtoolbox_b200.optimize import optimize
+    from vamtoolbox_b200.response import ResponseModel
+
+    O = golden["optim"]
+    tg, pg = geo(O["bclp_target"], O["angles"])
+    rm = ResponseModel(B=12, M=0.6)
+    assert np.array_equal(rm.interp_map_0, O["resp_map"]) and np.array_equal(rm.interp_dmapdf_0, O["resp_dmap"])
+    sino, dose, mapped, logs = optimize(tg, pg, opts(method="BCLP", n_iter=4, p=2, q=1, eps=0.05, learning_rate=0.002,
+                                                     response_model=rm, filter="ram-lak", engine=engine), output="full")
+    assert relL2(sino.array, O["bclp_sino"]) < 1e-4
+    assert relL2(dose.array, O["bclp_dose"]) < 1e-4
+    assert relL2(mapped.array, O["bclp_mapped"]) < 1e-4
+    assert np.allclose(logs.loss, O["bclp_loss"], rtol=1e-4)
+    norms = np.stack([logs.l0, logs.l1, logs.l2, logs.lf, logs.l0_eps0, logs.l1_eps0, logs.l2_eps0, logs.lf_eps0])
+    assert np.all(np.abs(norms[0] - O["bclp_norms"][0]) <= 1)  # voxel counts
+    assert np.allclose(norms[1:4], O["bclp_norms"][1:4], rtol=1e-3, atol=1e-5)
+    assert np.allclose(norms[5:], O["bclp_norms"][5:], rtol=1e-3, atol=1e-5)
+
+
+def test_pm_runs_and_tracks_reference(golden):
+    from vamtoolbox_b200.optimize import optimize
+
+    O = golden["optim"]
+    tg, pg = geo(O["target"], O["angles"])
+    s, r, e = optimize(tg, pg, opts(method="PM", n_iter=3, d_h=0.8, d_l=0.6, rho_1=1, rho_2=1, p=2))
+    assert relL2(s.array, O["pm_sino"]) < 1e-3
+    assert np.isfinite(e[0])
+
+
+def test_bclp_graph_equals_eager():
+    from vamtoolbox_b200.optimize import Options
+    from vamtoolbox_b200.optimizer import BCLP
+    from vamtoolbox_b200 import geometry
+
+    rng = np.random.default_rng(1)
+    t = np.clip(rng.uniform(size=(32, 32, 8)), 0, 1)
+    out = []
+    for graph in (True, False):
+        tg = geometry.TargetGeometry(target=t.copy())
+        pg = geometry.ProjectionGeometry(np.linspace(0, 360, 24, endpoint=False), "parallel")
+        b = BCLP.BCLPNorm(tg, pg, Options(method="BCLP", n_iter=6, learning_rate=1e-3))
+        out.append((b.gradientDescentDevice(graph=graph), b.logs.loss.copy()))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+
+
+def test_options_do_not_leak_between_instances():
+    a = opts(method="CAL", learning_rate=0.4)
+    b = opts(method="CAL")
+    assert a.learning_rate == 0.4 and b.learning_rate == 0.01

@@ -163,3 +163,38 @@ def test_bad_inputs_raise():
         p.forward(torch.zeros((16, 16, 4), device="cuda", dtype=torch.float64))
     with pytest.raises(VamError):
         p.set_absorption("ray", alpha_per_px=float("nan"), radius_px=3.0)
+
+
+FAST_CASES = [
+    ((32, 32, 128), np.linspace(0, 360, 24, endpoint=False)),     # even N, all angles paired, VZ=4
+    ((33, 33, 256), np.linspace(0, 360, 20, endpoint=False)),     # odd N, paired, VZ=8
+    ((30, 30, 128), None),                                        # unpaired random angles
+    ((28, 28, 192), np.concatenate([np.linspace(0, 180, 7, endpoint=False), [200.0, 380.0]])),  # mixed
+]
+
+
+@pytest.mark.parametrize("shape,ang", FAST_CASES)
+@pytest.mark.parametrize("absn", [None, "mask", "ray"])
+def test_fast_paths_against_oracle(shape, ang, absn):
+    rng = np.random.default_rng(shape[2] + shape[0])
+    if ang is None:
+        ang = np.sort(rng.uniform(0, 360, 17))
+    x = rng.uniform(0, 1, shape)
+    b = rng.uniform(0, 1, (shape[0], ang.size, shape[2]))
+    p = plan_for(shape, ang)
+    oabs = None
+    if absn == "mask":
+        m = rng.uniform(0.3, 1.0, shape[:2])
+        p.set_absorption("mask", mask=m)
+        oabs = ("mask", m)
+    elif absn == "ray":
+        p.set_absorption("ray", alpha_per_px=0.04, radius_px=shape[0] / 2 - 1.5)
+        oabs = ("ray", 0.04, shape[0] / 2 - 1.5)
+    assert relL2(p.forward(dev(x)).cpu().numpy(), O.parallel_forward(x, ang, absorption=oabs)) < TOL
+    assert relL2(p.backward_ref(dev(b)).cpu().numpy(), O.parallel_backward_ref(b, ang, absorption=oabs)) < TOL
+    assert relL2(p.adjoint(dev(b)).cpu().numpy(), O.parallel_adjoint(b, ang, absorption=oabs)) < TOL
+    # dot test <Ax, y> = <x, A^T y>
+    Ax = p.forward(dev(x)).double()
+    lhs = float((Ax * dev(b).double()).sum())
+    rhs = float((dev(x).double() * p.adjoint(dev(b)).double()).sum())
+    assert abs(lhs - rhs) <= 1e-6 * abs(lhs)

@@ -29,8 +29,9 @@ int blocks_for(int64_t n) {
 
 template <typename T, int OP>
 __device__ __forceinline__ T red_op(T a, T b) {
-    if (OP == VAM_RED_MAX) return a > b ? a : (b != b ? b : a);  // NaN propagates like np.max
-    if (OP == VAM_RED_MIN) return a < b ? a : (b != b ? b : a);
+    // NaN propagates like np.max / np.min: a NaN operand wins
+    if (OP == VAM_RED_MAX) return (b != b) ? b : ((a > b || a != a) ? a : b);
+    if (OP == VAM_RED_MIN) return (b != b) ? b : ((a < b || a != a) ? a : b);
     return a + b;
 }
 

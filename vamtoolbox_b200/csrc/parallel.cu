@@ -73,6 +73,7 @@ struct Args {
 
 template <int VZ>
 __device__ __forceinline__ void load_vec(const float* p, float (&d)[VZ]) {
+    static_assert(VZ == 1 || VZ == 4, "load_vec handles 1 or 4 floats; use load_vz for multiples of 4");
     if constexpr (VZ == 4) {
         float4 t = __ldg(reinterpret_cast<const float4*>(p));
         d[0] = t.x; d[1] = t.y; d[2] = t.z; d[3] = t.w;
@@ -230,6 +231,332 @@ __global__ void __launch_bounds__(256) k_forward(Args a) {
     for (int e = 0; e < VZ; ++e)
         for (int off = LZ; off < 32; off <<= 1) acc[e] += __shfl_xor_sync(kFull, acc[e], off);
     if (kl == 0 && zok) store_vec<VZ>(a.out + ((size_t)j * a.nA + theta) * a.nZ + z0, acc);
+}
+
+// ---------------------------------------------------------------------------
+// R1 forward, fast path: 32 lanes along z (VZ floats each), one lattice row
+// (angle, detector) per warp, angle pairs (a, a+180) sampled from one lattice.
+//
+// The sample points of angle a+180 are those of angle a mirrored through the
+// rotation centre: sample (j', k') of a+180 is lattice point (2C-j', 2C-k') of
+// a (the warp matrices of Projector3DParallel.py:137-143 satisfy this
+// identically), so one pass over a's lattice row gives both rays.  For odd N
+// the k ranges coincide; for even N (2C = N) angle a sums k in [0, N-1] and
+// a+180 sums k in [1, N] on the row j in [0, N]; the shared part k in [1, N-1]
+// is accumulated once and the two end samples are added separately.
+// ---------------------------------------------------------------------------
+struct FastArgs {
+    const float* vol;
+    float* sino;
+    const double4* trig;
+    const int2* tasks;
+    int nY, nX, nZ, nA, C;
+    int RS;          // row stride of the volume in floats (nX * nZ)
+    int zchunks;     // ceil(nZ / (32 * VZ))
+    int even;        // N even
+    float alpha, R;  // RAY absorption (tasks are unpaired then)
+};
+
+template <int VZ>
+struct Acc {
+    float v[VZ];
+};
+
+// One bilinear sample (all taps checked), added with weight f into acc.
+template <int VZ>
+__device__ __forceinline__ void load_vz(const float* __restrict__ p, float* d) {
+#pragma unroll
+    for (int q = 0; q < VZ / 4; ++q) {
+        const float4 t = __ldg(reinterpret_cast<const float4*>(p) + q);
+        d[4 * q] = t.x; d[4 * q + 1] = t.y; d[4 * q + 2] = t.z; d[4 * q + 3] = t.w;
+    }
+}
+
+template <int VZ>
+__device__ __forceinline__ void sample_checked(const FastArgs& a, const float* __restrict__ volz, double row,
+                                               double col, float f, float (&acc)[VZ]) {
+    const double fr = floor(row), fc = floor(col);
+    const int r0 = (int)fr, c0 = (int)fc;
+    const bool rc = row > fr, cc = col > fc;
+    const float dr = (float)(row - fr), dc = (float)(col - fc);
+    const bool vr0 = (unsigned)r0 < (unsigned)a.nY, vr1 = rc && (unsigned)(r0 + 1) < (unsigned)a.nY;
+    const bool vc0 = (unsigned)c0 < (unsigned)a.nX, vc1 = cc && (unsigned)(c0 + 1) < (unsigned)a.nX;
+    const float w00 = (1.f - dr) * (1.f - dc) * f, w01 = (1.f - dr) * dc * f;
+    const float w10 = dr * (1.f - dc) * f, w11 = dr * dc * f;
+    float t[VZ];
+    if (vr0 && vc0) {
+        load_vz<VZ>(volz + (size_t)r0 * a.RS + (size_t)c0 * a.nZ, t);
+#pragma unroll
+        for (int e = 0; e < VZ; ++e) acc[e] = fmaf(w00, t[e], acc[e]);
+    }
+    if (vr0 && vc1) {
+        load_vz<VZ>(volz + (size_t)r0 * a.RS + (size_t)(c0 + 1) * a.nZ, t);
+#pragma unroll
+        for (int e = 0; e < VZ; ++e) acc[e] = fmaf(w01, t[e], acc[e]);
+    }
+    if (vr1 && vc0) {
+        load_vz<VZ>(volz + (size_t)(r0 + 1) * a.RS + (size_t)c0 * a.nZ, t);
+#pragma unroll
+        for (int e = 0; e < VZ; ++e) acc[e] = fmaf(w10, t[e], acc[e]);
+    }
+    if (vr1 && vc1) {
+        load_vz<VZ>(volz + (size_t)(r0 + 1) * a.RS + (size_t)(c0 + 1) * a.nZ, t);
+#pragma unroll
+        for (int e = 0; e < VZ; ++e) acc[e] = fmaf(w11, t[e], acc[e]);
+    }
+}
+
+template <int VZ, bool RAY>
+__global__ void __launch_bounds__(256) k_forward_fast(FastArgs a) {
+    const int lane = threadIdx.x & 31;
+    const int item = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+    const int zc = item % a.zchunks;
+    const int j = item / a.zchunks;
+    const int2 task = a.tasks[blockIdx.y];
+    const bool paired = task.y >= 0;
+    const int N = a.nY;
+    const bool ext = paired && a.even;   // lattice row / column N is needed by the partner angle
+    if (j > (ext ? N : N - 1)) return;   // uniform per warp
+    const int zv = zc * 32 + lane;
+    const bool zok = zv * VZ < a.nZ;
+    const int z0 = zok ? zv * VZ : 0;
+    const float* __restrict__ volz = a.vol + z0;
+
+    const double4 tr = a.trig[task.x];
+    const double c = tr.x, s = tr.y;
+    const double rowb = fma(-s, (double)j, tr.w);
+    const double colb = fma(c, (double)j, tr.z);
+    const int kmax = ext ? N : N - 1;
+    int klo, khi;
+    sample_range(rowb, colb, c, s, a.nY, a.nX, kmax, klo, khi);
+
+    float s_entry = 0.f;
+    if (RAY) {
+        const float t = (float)(j - a.C);
+        s_entry = fabsf(t) <= a.R ? -sqrtf(a.R * a.R - t * t) : 0.f;
+        if (fabsf(t) > a.R) klo = 1, khi = 0;
+    }
+    float acc[VZ], e0[VZ], eN[VZ];
+#pragma unroll
+    for (int e = 0; e < VZ; ++e) acc[e] = e0[e] = eN[e] = 0.f;
+
+    if (zok) {
+        const int nYm1 = a.nY - 1, nXm1 = a.nX - 1;
+        const int lo = max(klo, 1), hi = min(khi, N - 1);
+        for (int k = lo; k <= hi; ++k) {
+            const double row = fma(c, (double)k, rowb);
+            const double col = fma(s, (double)k, colb);
+            const float f = RAY ? ray_factor((float)(k - a.C), s_entry, a.alpha) : 1.f;
+            const double fr = floor(row), fc = floor(col);
+            const int r0 = (int)fr, c0 = (int)fc;
+            if ((unsigned)r0 < (unsigned)nYm1 && (unsigned)c0 < (unsigned)nXm1) {
+                // interior: all four taps in the image; a zero-weight ceil tap is
+                // redirected to the floor tap so no unrelated value is read
+                const float dr = (float)(row - fr), dc = (float)(col - fc);
+                const int o00 = r0 * a.RS + c0 * a.nZ;
+                const int dcol = (col > fc) ? a.nZ : 0;
+                const int o10 = o00 + ((row > fr) ? a.RS : 0);
+                float w00 = (1.f - dr) * (1.f - dc), w01 = (1.f - dr) * dc;
+                float w10 = dr * (1.f - dc), w11 = dr * dc;
+                if (RAY) { w00 *= f; w01 *= f; w10 *= f; w11 *= f; }
+                float t0[VZ], t1[VZ], t2[VZ], t3[VZ];
+                load_vz<VZ>(volz + o00, t0);
+                load_vz<VZ>(volz + o00 + dcol, t1);
+                load_vz<VZ>(volz + o10, t2);
+                load_vz<VZ>(volz + o10 + dcol, t3);
+#pragma unroll
+                for (int e = 0; e < VZ; ++e) {
+                    acc[e] = fmaf(w00, t0[e], acc[e]);
+                    acc[e] = fmaf(w01, t1[e], acc[e]);
+                    acc[e] = fmaf(w10, t2[e], acc[e]);
+                    acc[e] = fmaf(w11, t3[e], acc[e]);
+                }
+            } else {
+                sample_checked<VZ>(a, volz, row, col, f, acc);
+            }
+        }
+        if (klo <= 0 && khi >= 0) {
+            const float f = RAY ? ray_factor((float)(0 - a.C), s_entry, a.alpha) : 1.f;
+            sample_checked<VZ>(a, volz, rowb, colb, f, e0);
+        }
+        if (ext && klo <= N && khi >= N)
+            sample_checked<VZ>(a, volz, fma(c, (double)N, rowb), fma(s, (double)N, colb), 1.f, eN);
+    }
+    if (!zok) return;
+    if (j <= N - 1) {
+        float o[VZ];
+#pragma unroll
+        for (int e = 0; e < VZ; ++e) o[e] = acc[e] + e0[e];
+        float* dst = a.sino + ((size_t)j * a.nA + task.x) * a.nZ + z0;
+#pragma unroll
+        for (int q = 0; q < VZ / 4; ++q)
+            reinterpret_cast<float4*>(dst)[q] = make_float4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
+    }
+    if (paired) {
+        // partner detector j' = 2C - j over lattice k in [2C-N+1, 2C]
+        const int jp = 2 * a.C - j;
+        if (jp >= 0 && jp <= N - 1) {
+            float o[VZ];
+#pragma unroll
+            for (int e = 0; e < VZ; ++e) o[e] = acc[e] + (a.even ? eN[e] : e0[e]);
+            float* dst = a.sino + ((size_t)jp * a.nA + task.y) * a.nZ + z0;
+#pragma unroll
+            for (int q = 0; q < VZ / 4; ++q)
+                reinterpret_cast<float4*>(dst)[q] = make_float4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Matched transpose, fast path: 32 lanes along z, one pixel per warp.
+//
+// The forward's tap weight of pixel (i, j) from lattice sample (J, K) is
+// hat(i - row(J,K)) * hat(j - col(J,K)) with hat(d) = max(0, 1 - |d|) (the
+// floor / ceil weights (1-dr), dr are exactly that).  The pixel's offset to
+// its nearest lattice point (J0, K0) is formed once in float64 from the same
+// coordinate expression the forward uses; the offsets to the 3 x 3 candidate
+// lattice points follow in float32 by adding multiples of (s, -c) and
+// (-c, -s), small numbers, so every candidate weight agrees with the
+// forward's to ~1e-7 and the kernel gathers at most 3 detector rows per angle.
+// ---------------------------------------------------------------------------
+template <int VZ, bool RAY>
+__global__ void __launch_bounds__(256) k_adjoint_fast(Args a) {
+    const int lane = threadIdx.x & 31;
+    const long item = (long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+    const int zchunks = a.zchunks;
+    const int zc = (int)(item % zchunks);
+    const long p = item / zchunks;
+    if (p >= (long)a.nY * a.nX) return;
+    const int i = (int)(p / a.nX), j = (int)(p % a.nX);
+    const int zv = zc * 32 + lane;
+    const bool zok = zv * VZ < a.nZ;
+    const int z0 = zok ? zv * VZ : 0;
+    const size_t rs = (size_t)a.nA * a.nZ;
+    const int N = a.nY;
+    float acc[VZ];
+#pragma unroll
+    for (int e = 0; e < VZ; ++e) acc[e] = 0.f;
+    const float* __restrict__ bz = a.in + z0;
+    for (int th = 0; th < a.nA; ++th) {
+        const double4 tr = a.trig[th];
+        const double c = tr.x, s = tr.y;
+        const double ri = (double)i - tr.w, ci = (double)j - tr.z;
+        const double Jf = fma(-s, ri, c * ci), Kf = fma(c, ri, s * ci);
+        const int J0 = __double2int_rn(Jf), K0 = __double2int_rn(Kf);
+        const double row0 = fma(c, (double)K0, fma(-s, (double)J0, tr.w));
+        const double col0 = fma(s, (double)K0, fma(c, (double)J0, tr.z));
+        const float dr = (float)((double)i - row0), dc = (float)((double)j - col0);
+        const float sf = (float)s, cf = (float)c;
+#pragma unroll
+        for (int da = -1; da <= 1; ++da) {
+            const int J = J0 + da;
+            if ((unsigned)J >= (unsigned)a.nX) continue;
+            float s_entry = 0.f;
+            if (RAY) {
+                const float t = (float)(J - a.C);
+                if (fabsf(t) > a.R) continue;
+                s_entry = -sqrtf(a.R * a.R - t * t);
+            }
+            float W = 0.f;
+#pragma unroll
+            for (int db = -1; db <= 1; ++db) {
+                const int K = K0 + db;
+                if ((unsigned)K >= (unsigned)N) continue;
+                const float er = fmaf((float)da, sf, fmaf(-(float)db, cf, dr));
+                const float ec = fmaf(-(float)da, cf, fmaf(-(float)db, sf, dc));
+                float w = fmaxf(0.f, 1.f - fabsf(er)) * fmaxf(0.f, 1.f - fabsf(ec));
+                if (RAY) w *= ray_factor((float)(K - a.C), s_entry, a.alpha);
+                W += w;
+            }
+            if (W != 0.f && zok) {
+                float bv[VZ];
+                load_vz<VZ>(bz + (size_t)J * rs + (size_t)th * a.nZ, bv);
+#pragma unroll
+                for (int e = 0; e < VZ; ++e) acc[e] = fmaf(W, bv[e], acc[e]);
+            }
+        }
+    }
+    if (!zok) return;
+    if (a.mask) {
+        const float m = __ldg(a.mask + p);
+#pragma unroll
+        for (int e = 0; e < VZ; ++e) acc[e] *= m;
+    }
+    float* dst = a.out + (size_t)p * a.nZ + z0;
+#pragma unroll
+    for (int q = 0; q < VZ / 4; ++q)
+        reinterpret_cast<float4*>(dst)[q] = make_float4(acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]);
+}
+
+// ---------------------------------------------------------------------------
+// R2 backprojection, fast path: 32 lanes along z with VZ floats each (one
+// pixel per warp, angles in sequence); same arithmetic as k_backward_ref.
+// ---------------------------------------------------------------------------
+template <int VZ, bool RAY>
+__global__ void __launch_bounds__(256) k_backward_fast(Args a) {
+    const int lane = threadIdx.x & 31;
+    const long item = (long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+    const int zc = (int)(item % a.zchunks);
+    const long p = item / a.zchunks;
+    if (p >= (long)a.nY * a.nX) return;
+    const int i = (int)(p / a.nX), j = (int)(p % a.nX);
+    const int zv = zc * 32 + lane;
+    const bool zok = zv * VZ < a.nZ;
+    const int z0 = zok ? zv * VZ : 0;
+    float acc[VZ];
+#pragma unroll
+    for (int e = 0; e < VZ; ++e) acc[e] = 0.f;
+    if (a.circle[p] && zok) {
+        const double X = (double)(j - a.C), Y = (double)(i - a.C);
+        const double tlo = (double)(-a.C), thi = (double)(a.nY - 1 - a.C);
+        const size_t rs = (size_t)a.nA * a.nZ;
+        const float* __restrict__ bz = a.in + z0;
+#pragma unroll 2
+        for (int th = 0; th < a.nA; ++th) {
+            const double4 tr = a.trig[th];
+            const double t = __dsub_rn(__dmul_rn(X, tr.x), __dmul_rn(Y, tr.y));
+            if (!(t >= tlo && t <= thi)) continue;
+            const double ft = floor(t);
+            const int j0 = (int)ft + a.C;
+            const float* b0 = bz + (size_t)j0 * rs + (size_t)th * a.nZ;
+            float v0[VZ], v1[VZ];
+            load_vz<VZ>(b0, v0);
+            // t == floor(t): np.interp returns fp[j]; the second row is read with weight 0
+            const float w = (float)(t - ft);
+            load_vz<VZ>(b0 + (t != ft ? rs : 0), v1);
+            float f = 1.f;
+            if (RAY) {
+                const float tf = (float)t;
+                f = 0.f;
+                if (fabsf(tf) <= a.R) {
+                    const float sv = (float)__dadd_rn(__dmul_rn(X, tr.y), __dmul_rn(Y, tr.x));
+                    f = ray_factor(sv, -sqrtf(a.R * a.R - tf * tf), a.alpha);
+                }
+            }
+#pragma unroll
+            for (int e = 0; e < VZ; ++e) {
+                const float v = fmaf(w, v1[e] - v0[e], v0[e]);
+                acc[e] = RAY ? fmaf(v, f, acc[e]) : acc[e] + v;
+            }
+        }
+    }
+    if (!zok) return;
+    if (a.mask) {
+        const float m = __ldg(a.mask + p);
+#pragma unroll
+        for (int e = 0; e < VZ; ++e) acc[e] = m * acc[e];
+    }
+    float* dst = a.out + (size_t)p * a.nZ + z0;
+#pragma unroll
+    for (int q = 0; q < VZ / 4; ++q)
+        reinterpret_cast<float4*>(dst)[q] = make_float4(acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]);
+}
+
+__global__ void k_mask_mul(const float* __restrict__ x, const float* __restrict__ mask, float* __restrict__ out,
+                           long npix, int nZ) {
+    const long n = npix * nZ;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        out[i] = mask[i / nZ] * x[i];
 }
 
 // ---------------------------------------------------------------------------
@@ -503,10 +830,81 @@ void launch_abs(Op op, int abs_mode, const Args& a, long items, cudaStream_t st)
     }
 }
 
+// VZ of the fast forward for nZ slices (0 = use the generic kernel)
+int fast_vz(int nZ, bool aligned) {
+    if (!aligned) return 0;
+    auto eff = [&](int vz) {
+        if (nZ % vz) return 0.0;
+        const int vec = nZ / vz, ch = (vec + 31) / 32;
+        return (double)vec / (double)(ch * 32);
+    };
+    if (eff(8) >= 0.74) return 8;
+    if (eff(4) >= 0.74) return 4;
+    return 0;
+}
+
+int run_forward_fast(vam_parallel_plan* plan, const float* in, float* out, cudaStream_t st, int vz) {
+    const float* vol = in;
+    if (plan->abs_mode == VAM_ABS_MASK) {
+        const long npix = (long)plan->nY * plan->nX;
+        const long n = npix * plan->nZ;
+        k_mask_mul<<<(unsigned)std::min<long>((n + 255) / 256, 148L * 32), 256, 0, st>>>(in, plan->d_mask,
+                                                                                         plan->d_vol_scratch, npix, plan->nZ);
+        VAM_CHECK_LAUNCH("k_mask_mul");
+        vol = plan->d_vol_scratch;
+    }
+    FastArgs a;
+    a.vol = vol; a.sino = out; a.trig = plan->d_trig;
+    a.nY = plan->nY; a.nX = plan->nX; a.nZ = plan->nZ; a.nA = plan->nA; a.C = plan->C;
+    a.RS = plan->nX * plan->nZ;
+    a.zchunks = (plan->nZ / vz + 31) / 32;
+    a.even = (plan->nY % 2) == 0;
+    a.alpha = plan->abs_alpha; a.R = plan->abs_R;
+    const bool ray = plan->abs_mode == VAM_ABS_RAY;
+    a.tasks = ray ? plan->d_tasks_single : plan->d_tasks_paired;
+    const int ntask = ray ? plan->nA : plan->n_tasks_paired;
+    const long items = (long)(plan->nX + 1) * a.zchunks;
+    dim3 grid((unsigned)((items + kWarpsPerBlock - 1) / kWarpsPerBlock), (unsigned)ntask);
+    dim3 block(kWarpsPerBlock * kWarp);
+    if (vz == 8) {
+        if (ray) k_forward_fast<8, true><<<grid, block, 0, st>>>(a);
+        else k_forward_fast<8, false><<<grid, block, 0, st>>>(a);
+    } else {
+        if (ray) k_forward_fast<4, true><<<grid, block, 0, st>>>(a);
+        else k_forward_fast<4, false><<<grid, block, 0, st>>>(a);
+    }
+    VAM_CHECK_LAUNCH("k_forward_fast");
+    return VAM_OK;
+}
+
 int run(vam_parallel_plan* plan, Op op, const float* in, float* out, cudaStream_t st, const char* name) {
     VAM_REQUIRE(plan && in && out, VAM_ERR_ARG, std::string(name) + ": null argument");
     DeviceGuard g(plan->device);
     VAM_REQUIRE(g.ok, VAM_ERR_CUDA, std::string(name) + ": cannot select device");
+    const int vzf = fast_vz(plan->nZ, (((uintptr_t)in | (uintptr_t)out) & 31) == 0);
+    if (op == Op::Forward && !plan->has_occ && (long)plan->nY * plan->nX * plan->nZ < (1L << 31) && vzf)
+        return run_forward_fast(plan, in, out, st, vzf);
+    if (op != Op::Forward && !plan->has_occ && vzf) {
+        Args a;
+        std::memset(&a, 0, sizeof(a));
+        a.in = in; a.out = out; a.trig = plan->d_trig; a.circle = plan->d_circle;
+        a.mask = plan->abs_mode == VAM_ABS_MASK ? plan->d_mask : nullptr;
+        a.nY = plan->nY; a.nX = plan->nX; a.nZ = plan->nZ; a.nA = plan->nA; a.C = plan->C;
+        a.zchunks = (plan->nZ / vzf + 31) / 32;
+        a.alpha = plan->abs_alpha; a.R = plan->abs_R;
+        const long items = (long)plan->nY * plan->nX * a.zchunks;
+        dim3 grid((unsigned)((items + kWarpsPerBlock - 1) / kWarpsPerBlock)), block(kWarpsPerBlock * kWarp);
+        const bool ray = plan->abs_mode == VAM_ABS_RAY;
+        if (op == Op::BackwardRef) {
+            if (vzf == 8) { if (ray) k_backward_fast<8, true><<<grid, block, 0, st>>>(a); else k_backward_fast<8, false><<<grid, block, 0, st>>>(a); }
+            else { if (ray) k_backward_fast<4, true><<<grid, block, 0, st>>>(a); else k_backward_fast<4, false><<<grid, block, 0, st>>>(a); }
+        } else {
+            if (vzf == 8) { if (ray) k_adjoint_fast<8, true><<<grid, block, 0, st>>>(a); else k_adjoint_fast<8, false><<<grid, block, 0, st>>>(a); }
+            else { if (ray) k_adjoint_fast<4, true><<<grid, block, 0, st>>>(a); else k_adjoint_fast<4, false><<<grid, block, 0, st>>>(a); }
+        }
+        VAM_CHECK_LAUNCH(name);
+        return VAM_OK;
+    }
     const bool aligned = (((uintptr_t)in | (uintptr_t)out) & 15) == 0;
     Layout L = choose_layout(plan->nZ, aligned);
     Args a;
@@ -583,7 +981,31 @@ extern "C" int vam_parallel_plan_create(const vam_parallel_geom* geom, vam_paral
             circ[(size_t)i * p->nX + j] = !(r2 > 1.0);
         }
     }
+    // pair every angle with the one 180 degrees away (within 1e-9 degrees, mod 360)
+    std::vector<int2> paired, single;
+    {
+        std::vector<int> used(p->nA, 0);
+        for (int i = 0; i < p->nA; ++i) {
+            single.push_back(make_int2(i, -1));
+            if (used[i]) continue;
+            used[i] = 1;
+            int partner = -1;
+            for (int k = i + 1; k < p->nA && partner < 0; ++k) {
+                if (used[k]) continue;
+                double d = std::fmod(geom->angles_deg[k] - geom->angles_deg[i] - 180.0, 360.0);
+                if (d < 0) d += 360.0;
+                if (d < 1e-9 || 360.0 - d < 1e-9) partner = k;
+            }
+            if (partner >= 0) used[partner] = 1;
+            paired.push_back(make_int2(i, partner));
+        }
+    }
+    p->n_tasks_paired = (int)paired.size();
     cudaError_t e = cudaMalloc(&p->d_trig, sizeof(double4) * p->nA);
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_tasks_paired, sizeof(int2) * paired.size());
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_tasks_single, sizeof(int2) * single.size());
+    if (e == cudaSuccess) e = cudaMemcpy(p->d_tasks_paired, paired.data(), sizeof(int2) * paired.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(p->d_tasks_single, single.data(), sizeof(int2) * single.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMalloc(&p->d_circle, circ.size());
     if (e == cudaSuccess) e = cudaMemcpy(p->d_trig, trig.data(), sizeof(double4) * p->nA, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(p->d_circle, circ.data(), circ.size(), cudaMemcpyHostToDevice);
@@ -603,6 +1025,9 @@ extern "C" int vam_parallel_plan_destroy(vam_parallel_plan* p) {
     cudaFree(p->d_mask);
     cudaFree(p->d_occ);
     cudaFree(p->d_occ_flag);
+    cudaFree(p->d_tasks_paired);
+    cudaFree(p->d_tasks_single);
+    cudaFree(p->d_vol_scratch);
     delete p;
     return VAM_OK;
 }
@@ -617,6 +1042,8 @@ extern "C" int vam_parallel_set_absorption(vam_parallel_plan* p, int mode, const
     if (mode == VAM_ABS_MASK) {
         VAM_REQUIRE(mask_dev, VAM_ERR_ARG, "vam_parallel_set_absorption: MASK needs mask_dev");
         if (!p->d_mask) VAM_TRY_CUDA(cudaMalloc(&p->d_mask, sizeof(float) * (size_t)p->nY * p->nX));
+        if (!p->d_vol_scratch)
+            VAM_TRY_CUDA(cudaMalloc(&p->d_vol_scratch, sizeof(float) * (size_t)p->nY * p->nX * p->nZ));
         VAM_TRY_CUDA(cudaMemcpyAsync(p->d_mask, mask_dev, sizeof(float) * (size_t)p->nY * p->nX,
                                      cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
     }

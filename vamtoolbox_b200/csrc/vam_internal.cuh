@@ -69,4 +69,10 @@ struct vam_parallel_plan {
     float* d_occ;           // [nR][nA][nZ] occlusion sinogram, NaN = none
     uint8_t* d_occ_flag;    // [nA][nZ] forward shadow gate
     int has_occ;
+    // angle tasks of the fast forward: (a, b) with b the angle 180 degrees from a
+    // (both sampled from a's lattice), or b = -1 for an unpaired angle
+    int2* d_tasks_paired;
+    int n_tasks_paired;
+    int2* d_tasks_single;   // (a, -1) for every angle
+    float* d_vol_scratch;   // [nY][nX][nZ] masked copy of the input (VAM_ABS_MASK)
 };

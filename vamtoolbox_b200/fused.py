@@ -1,0 +1,115 @@
+"""Device-resident optimizer building blocks over the fused kernels (csrc/optim.cu).
+
+A :class:`Workspace` owns the reduction scratch and small device scalars so
+that an optimizer iteration issues only stream-ordered kernel launches (no
+allocation, no host synchronisation) and can be captured once in a CUDA
+graph with :func:`capture` and replayed.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from . import _lib
+
+
+class Workspace:
+    def __init__(self, device):
+        self.device = torch.device(device)
+        nbytes = int(_lib.load().vam_reduce_workspace_bytes(1 << 30))
+        self.work = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+
+    def stream(self):
+        return _lib.stream_ptr(torch.cuda.current_stream(self.device))
+
+    def scalar(self, n=1):
+        return torch.zeros(n, dtype=torch.float32, device=self.device)
+
+    # reductions -------------------------------------------------------------
+    def reduce(self, x, op, out):
+        _lib.call("vam_reduce", _lib.ptr(x), x.numel(), op, _lib.ptr(out), _lib.ptr(self.work), self.work.numel(),
+                  self.stream())
+        return out
+
+    def max(self, x, out):
+        return self.reduce(x, _lib.RED_MAX, out)
+
+    def ver(self, x, mask, out):
+        _lib.call("vam_metric_ver", _lib.ptr(x), _lib.ptr(mask), x.numel(), _lib.ptr(out), _lib.ptr(self.work),
+                  self.work.numel(), self.stream())
+        return out
+
+    # elementwise ------------------------------------------------------------
+    def scale(self, x, s, floor=None):
+        _lib.call("vam_scale_by_device", _lib.ptr(x), _lib.ptr(s), x.numel(), int(floor is not None),
+                  float(floor or 0.0), self.stream())
+        return x
+
+    def cal_threshold(self, x, xmax, target, d_h, g, out):
+        _lib.call("vam_cal_threshold", _lib.ptr(x), _lib.ptr(xmax), _lib.ptr(target), x.numel(), float(d_h), float(g),
+                  _lib.ptr(out), self.stream())
+        return out
+
+    def cal_update(self, b, db, db_prev, lr, momentum, it):
+        _lib.call("vam_cal_sino_update", _lib.ptr(b), _lib.ptr(db), _lib.ptr(db_prev), b.numel(), float(lr),
+                  float(momentum), int(it), self.stream())
+        return b
+
+    def osmo_model(self, xm, x, xmax, mask, gel, d):
+        _lib.call("vam_osmo_model_update", _lib.ptr(xm), _lib.ptr(x), _lib.ptr(xmax), _lib.ptr(mask), xm.numel(),
+                  int(gel), float(d), self.stream())
+        return xm
+
+    def bclp_dose_pass(self, dose, target, prm, mapped, operand, stats):
+        _lib.call("vam_bclp_dose_pass", _lib.ptr(dose), _lib.ptr(target), dose.numel(), ctypes.byref(prm),
+                  _lib.ptr(mapped), _lib.ptr(operand), _lib.ptr(stats), _lib.ptr(self.work), self.work.numel(),
+                  self.stream())
+
+    def bclp_update(self, g, grad, lr, p, q, lo, hi, stats):
+        has_hi = hi is not None
+        _lib.call("vam_bclp_sino_update", _lib.ptr(g), _lib.ptr(grad), g.numel(), float(lr), float(p), float(q),
+                  float(lo if lo is not None else -3.0e38), float(hi if has_hi else 0.0), int(has_hi), _lib.ptr(stats),
+                  self.stream())
+
+    def append(self, src, arr, counter):
+        n = src.numel()
+        _lib.call("vam_append", _lib.ptr(src), n, _lib.ptr(arr), _lib.ptr(counter), arr.numel() // n, self.stream())
+
+
+def bclp_params(response_model, eps, weight, p, device, keep):
+    """vam_bclp_params for an interpolation response model (tables on device)."""
+    f, m, dm, f0, inv_step = response_model.device_tables(device)
+    prm = _lib.BclpParams()
+    prm.table_f, prm.table_map, prm.table_dmap = f.data_ptr(), m.data_ptr(), dm.data_ptr()
+    prm.n_table = f.numel()
+    prm.table_f0, prm.table_inv_step = f0, inv_step
+    prm.p = float(p)
+    if isinstance(eps, torch.Tensor):
+        keep.append(eps)
+        prm.eps_dev, prm.eps = eps.data_ptr(), 0.0
+    else:
+        prm.eps = float(eps)
+    if isinstance(weight, torch.Tensor):
+        keep.append(weight)
+        prm.weight_dev, prm.weight = weight.data_ptr(), 0.0
+    else:
+        prm.weight = float(weight)
+    keep += [f, m, dm]
+    return prm
+
+
+def capture(fn, device):
+    """Capture fn() into a CUDA graph without executing it.
+
+    fn must only issue stream-ordered kernel launches on the current stream
+    (the C-ABI calls of this package) and no host synchronisation; its
+    buffers must stay alive as long as the graph.  Replay with graph.replay().
+    """
+    device = torch.device(device)
+    torch.cuda.synchronize(device)
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream(device=device)
+    with torch.cuda.graph(g, stream=s):
+        fn()
+    return g

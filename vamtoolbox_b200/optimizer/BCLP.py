@@ -1,0 +1,312 @@
+"""Band-constrained Lp-norm minimisation (BCLP): the reference's vamtoolbox/optimizer/BCLP.py.
+
+Iteration (BCLP.py:277-386, 477-534), with P the projector:
+    dose = P.backward(g); mapped = response(dose); e = mapped - f_T
+    eb = |e| - eps; v = eb > 0; loss = (sum v w |eb|^p)^(q/p)
+    grad = q loss^((q-p)/q) P.forward(v w |eb|^(p-1) sign(e) dresponse(dose))   (no prefactor if loss == 0)
+    g <- clip(g - lr grad, blb, bub)
+For the parallel beam, P.backward is the reference-parity backprojection
+(not the transpose of P.forward), exactly as the reference pairs them.
+
+engine="device": g, dose and every intermediate stay on the GPU; one
+iteration is five kernel launches (backprojection, fused dose pass with the
+loss / norm reductions, log append, forward projection, fused clamped
+update) captured once into a CUDA graph and replayed n_iter times; the loss
+scalar never leaves the device (the prefactor and the loss == 0 branch are a
+select inside the update kernel).  engine="host" is the reference's numpy
+loop calling the projector with host arrays (the plain per-call path).
+"""
+from __future__ import annotations
+
+import logging
+import time
+import warnings
+
+import numpy as np
+import torch
+
+from .. import geometry
+from ..fused import Workspace, bclp_params, capture
+from ..projectorconstructor import projectorconstructor
+from ..util import data as udata
+
+
+class LogPerf:
+    """Per-iteration loss and norm log (BCLP.py:14-135)."""
+
+    def __init__(self, options):
+        self.options = options
+        self.curr_iter = 0
+        n = options.n_iter + 1
+        for k in ("loss", "l0", "l1", "l2", "lf", "l0_eps0", "l1_eps0", "l2_eps0", "lf_eps0", "ver"):
+            setattr(self, k, np.full(n, np.nan))
+        self.iter_times = np.zeros(n)
+        self.t0 = np.nan
+        self.is_converged = False
+
+    def startTiming(self):
+        self.t0 = time.perf_counter()
+
+    def recordIterTime(self):
+        self.iter_times[self.curr_iter] = time.perf_counter() - self.t0
+
+    def save(self, filename):
+        np.savetxt(filename, np.column_stack([range(self.options.n_iter + 1), self.iter_times, self.loss, self.l0,
+                                              self.l1, self.l2, self.lf, self.l0_eps0, self.l1_eps0, self.l2_eps0,
+                                              self.lf_eps0]), delimiter=",",
+                   header="n,compute time,loss,L0 norm,L1 norm,L2 norm,Linf norm,L0 norm eps=0,L1 norm eps=0,"
+                          "L2 norm eps=0,Linf norm eps=0,",
+                   fmt=["%5.0i"] + ["%10.2f"] + ["%10.4f"] * 9)
+
+    def fill_from_stats(self, stats, q, p, upto):
+        """stats: [rows, 9] float array from vam_bclp_dose_pass."""
+        s = np.asarray(stats, dtype=np.float64)[:upto]
+        n = s.shape[0]
+        self.loss[:n] = s[:, 0] ** (q / p)
+        self.l0[:n], self.l0_eps0[:n] = s[:, 1], s[:, 2]
+        self.l1[:n], self.l1_eps0[:n] = s[:, 3], s[:, 4]
+        self.l2[:n], self.l2_eps0[:n] = np.sqrt(s[:, 5]), np.sqrt(s[:, 6])
+        self.lf[:n], self.lf_eps0[:n] = s[:, 7], s[:, 8]
+
+
+class BCLPNorm:
+    def __init__(self, target_geo, proj_geo, options):
+        self.logger = logging.getLogger(__name__)
+        self.target_geo = target_geo
+        self.target_geo.array = np.atleast_3d(self.target_geo.array)
+        self.proj_geo = proj_geo
+        self.options = options
+        self.logs = LogPerf(options)
+        self.logs.startTiming()
+        self.response_model = options.response_model
+        self.eps, self.weight = options.eps, options.weight
+        self.p, self.q = options.p, options.q
+        self.learning_rate = options.learning_rate
+        self.optim_alg = options.optim_alg
+        self.g0 = options.g0
+        self.glb, self.gub = options.blb, options.bub
+        self.bit_depth = options.bit_depth
+        self.dvol = 1
+        self.exit_param = options.exit_param
+        self.verbose = options.verbose
+        self.test_alternate_handling = getattr(options, "test_alternate_handling", False)
+        self.dose = self.mapped_dose = None
+        self.P = projectorconstructor(self.target_geo, self.proj_geo)
+        if self.response_model.checkResponseTarget(self.target_geo.array) is False:
+            warnings.warn("Target is either out of range of response function over non-negative real dose input, "
+                          "or contains inf/nan.")
+        if self.g0 is None:
+            f0 = self.response_model.map_inv(self.target_geo.array)
+            if callable(getattr(self.P, "inverseBackward", None)):
+                self.g0 = self.P.inverseBackward(f0, filter_option=options.filter)
+            else:
+                self.g0 = udata.filterSinogram(self.P.forward(f0), options.filter)
+                self.g0 *= np.pi / (2 * proj_geo.n_angles)
+        self.g0 = np.asarray(self.g0)
+        self.g0_shape = self.g0.shape
+        self.g0 = self.imposeSinogramConstraints(self.g0)
+
+    # -- shared helpers (BCLP.py:528-590) ------------------------------------
+    def imposeSinogramConstraints(self, g):
+        if self.bit_depth is not None:
+            g = udata.discretize(g, self.bit_depth, [0.0, np.amax(g)])
+        return np.clip(g, a_min=self.glb, a_max=self.gub)
+
+    def checkSinogramShape(self, g, desired_shape="flattened"):
+        if desired_shape == "flattened" and g.ndim > 1:
+            return np.reshape(g, -1)
+        if desired_shape == "cylindrical" and g.ndim == 1:
+            return np.reshape(g, self.g0_shape)
+        return g
+
+    def checkConvergence(self):
+        it = self.logs.curr_iter
+        zero = self.logs.loss[it] == 0.0
+        conv = False
+        if it >= 5 and self.exit_param is not None:
+            ch = np.abs(np.diff(self.logs.loss[it - 5:it + 1]))
+            conv = bool(np.mean(ch) <= self.exit_param * self.logs.loss[it])
+        return conv or zero
+
+    # -- host engine: the reference's numpy loop (BCLP.py:277-526) ---------------
+    def _host_state(self, g):
+        g = self.checkSinogramShape(g, "cylindrical")
+        dose = np.asarray(self.P.backward(g)).reshape(self.target_geo.array.shape)
+        mapped = self.response_model.map(dose)
+        e = mapped - self.target_geo.array
+        eb = np.abs(e) - self.eps
+        v = eb > 0
+        loss = (np.sum(v * self.weight * np.abs(eb) ** self.p) * self.dvol) ** (self.q / self.p)
+        return dose, mapped, e, eb, v, loss
+
+    def _host_norms(self, e, eb, v):
+        i = self.logs.curr_iter
+        L = self.logs
+        v0 = np.abs(e) > 0
+        L.l0[i], L.l0_eps0[i] = np.sum(v), np.sum(v0)
+        L.l1[i], L.l1_eps0[i] = np.sum(v * np.abs(eb)), np.sum(np.abs(e))
+        L.l2[i], L.l2_eps0[i] = np.sqrt(np.sum(v * eb ** 2)), np.sqrt(np.sum(e ** 2))
+        L.lf[i], L.lf_eps0[i] = np.amax(v * np.abs(eb)), np.amax(v0 * np.abs(e))
+
+    def gradientDescentHost(self):
+        g = self.checkSinogramShape(self.g0, "flattened")
+        for _ in range(self.logs.options.n_iter):
+            dose, mapped, e, eb, v, loss = self._host_state(g)
+            self.logs.loss[self.logs.curr_iter] = loss
+            operand = v * self.weight * (np.abs(eb) ** (self.p - 1)) * np.sign(e) * self.response_model.dmapdf(dose)
+            fwd = np.asarray(self.P.forward(operand))
+            grad = (self.q * loss ** ((self.q - self.p) / self.q)) * fwd if loss != 0.0 else fwd
+            g = self.imposeSinogramConstraints(g - self.learning_rate * self.checkSinogramShape(grad, "flattened"))
+            conv = self.checkConvergence() if self.exit_param is not None else False
+            self._host_norms(e, eb, v)
+            self.logs.recordIterTime()
+            self.logs.curr_iter += 1
+            if conv:
+                self.logs.is_converged = True
+                break
+        dose, mapped, e, eb, v, loss = self._host_state(g)
+        self.logs.loss[self.logs.curr_iter] = loss
+        self._host_norms(e, eb, v)
+        self.dose, self.mapped_dose = dose, mapped
+        return g
+
+    # -- device engine ---------------------------------------------------------
+    def _device_projector_ops(self):
+        P = self.P
+        plan = getattr(P, "plan", None)
+        if plan is not None and hasattr(plan, "backward_ref"):
+            return (lambda g, out: plan.backward_ref(g, out), lambda x, out: plan.forward(x, out),
+                    plan.shape_vol, plan.shape_sino, P.device)
+        if plan is not None and hasattr(plan, "deposit"):
+            return (lambda g, out: plan.deposit(g, out), lambda x, out: plan.integrate(x, out),
+                    plan.grid_shape, (plan.num_rays,), P.device)
+        raise TypeError("the device engine needs a vamtoolbox_b200 projector")
+
+    def _table_ok(self):
+        return getattr(self.response_model, "has_uniform_table", lambda: False)()
+
+    def device_iteration(self, reduce_stats=None):
+        """A :class:`DeviceIteration` holding this problem's device state (g = g0)."""
+        return DeviceIteration(self, reduce_stats=reduce_stats)
+
+    def gradientDescentDevice(self, graph=True):
+        it = self.device_iteration()
+        n_iter = self.logs.options.n_iter
+        q, p = self.q, self.p
+        dev = it.device
+        st = torch.cuda.current_stream(dev)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(n_iter + 1)]
+        ev[0].record(st)
+        eager = (not graph) or self.bit_depth is not None or self.exit_param is not None
+        done = n_iter
+        if eager:
+            for k in range(n_iter):
+                it.step()
+                if self.bit_depth is not None:
+                    it.g.copy_(udata.discretize_t(it.g, self.bit_depth, 0.0, torch.amax(it.g)))
+                    it.g.clamp_(min=self.glb, max=self.gub)
+                ev[k + 1].record(st)
+                if self.exit_param is not None:
+                    self.logs.fill_from_stats(it.log.cpu().numpy(), q, p, k + 1)
+                    self.logs.curr_iter = k
+                    if self.checkConvergence():
+                        self.logs.is_converged = True
+                        done = k + 1
+                        break
+        else:
+            gr = it.capture()
+            for k in range(n_iter):
+                gr.replay()
+                ev[k + 1].record(st)
+            del gr
+        it.state()  # dose / mapped dose / norms of the final sinogram
+        torch.cuda.synchronize(dev)
+        self.logs.curr_iter = done
+        rows = min(int(it.counter.item()), n_iter + 1)
+        self.logs.fill_from_stats(it.log[:rows].cpu().numpy(), q, p, rows)
+        for k in range(done):
+            self.logs.iter_times[k] = ev[0].elapsed_time(ev[k + 1]) / 1e3
+        tshape = self.target_geo.array.shape
+        self.dose_t, self.mapped_t, self.g_t = it.dose.reshape(tshape), it.mapped.reshape(tshape), it.g
+        self.dose = self.dose_t.double().cpu().numpy()
+        self.mapped_dose = self.mapped_t.double().cpu().numpy()
+        return it.g.double().cpu().numpy().reshape(-1)
+
+    def gradientDescent(self):
+        if getattr(self.options, "engine", "device") == "host":
+            return self.gradientDescentHost()
+        return self.gradientDescentDevice()
+
+
+class DeviceIteration:
+    """Device state and kernels of one BCLP iteration (the fused engine).
+
+    ``step()`` issues, on the current stream: the backprojection of g into
+    the dose, the fused dose pass (response, band error, operand and the 9
+    loss / norm sums), the log append, the forward projection of the operand
+    and the clamped sinogram update.  Nothing is allocated and nothing syncs,
+    so ``capture()`` records it once as a CUDA graph.  ``reduce_stats`` (a
+    callable on the 9-float stats tensor) is the hook where a z-sharded run
+    all-reduces the loss sums before the update.
+    """
+
+    def __init__(self, bclp, reduce_stats=None):
+        self.bclp = bclp
+        back, fwd, vol_shape, sino_shape, dev = bclp._device_projector_ops()
+        self.back, self.fwd, self.device = back, fwd, dev
+        self.vol_shape, self.sino_shape = vol_shape, sino_shape
+        n_iter = bclp.logs.options.n_iter
+        self.ws = Workspace(dev)
+        f32 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float32), device=dev)
+        self.fT = f32(bclp.target_geo.array).reshape(vol_shape).contiguous()
+        self.g = f32(bclp.g0).reshape(sino_shape).contiguous()
+        self.dose = torch.empty(vol_shape, dtype=torch.float32, device=dev)
+        self.mapped = torch.empty(vol_shape, dtype=torch.float32, device=dev)
+        self.operand = torch.empty(vol_shape, dtype=torch.float32, device=dev)
+        self.grad = torch.empty(sino_shape, dtype=torch.float32, device=dev)
+        self.stats = self.ws.scalar(9)
+        self.log = torch.full((n_iter + 1, 9), float("nan"), dtype=torch.float32, device=dev)
+        self.counter = torch.zeros(1, dtype=torch.int32, device=dev)
+        self._keep = []
+        if not bclp._table_ok():
+            raise NotImplementedError(
+                "the fused BCLP pass evaluates interpolation response models (the default); "
+                "use engine='host' for analytical or non-uniform response tables")
+        eps = f32(bclp.eps).reshape(vol_shape) if np.ndim(bclp.eps) else bclp.eps
+        weight = f32(bclp.weight).reshape(vol_shape) if np.ndim(bclp.weight) else bclp.weight
+        self.prm = bclp_params(bclp.response_model, eps, weight, bclp.p, dev, self._keep)
+        self.reduce_stats = reduce_stats
+        self.launches_per_step = 6
+
+    def state(self):
+        self.back(self.g, self.dose)
+        self.ws.bclp_dose_pass(self.dose, self.fT, self.prm, self.mapped, self.operand, self.stats)
+        if self.reduce_stats is not None:
+            self.reduce_stats(self.stats)
+        self.ws.append(self.stats, self.log, self.counter)
+
+    def update(self):
+        b = self.bclp
+        self.fwd(self.operand, self.grad)
+        self.ws.bclp_update(self.g, self.grad, b.learning_rate, b.p, b.q, b.glb, b.gub, self.stats)
+
+    def step(self):
+        self.state()
+        self.update()
+
+    def capture(self):
+        return capture(self.step, self.device)
+
+
+def minimizeBCLP(target_geo, proj_geo, options, output="packaged"):
+    bclp = BCLPNorm(target_geo, proj_geo, options)
+    g_opt = bclp.checkSinogramShape(bclp.gradientDescent(), "cylindrical")
+    if output == "packaged":
+        return (geometry.Sinogram(g_opt, proj_geo, options), geometry.Reconstruction(bclp.dose, proj_geo, options),
+                bclp.logs.loss)
+    if output == "full":
+        return (geometry.Sinogram(g_opt, proj_geo, options), geometry.Reconstruction(bclp.dose, proj_geo, options),
+                geometry.Reconstruction(bclp.mapped_dose, proj_geo, options), bclp.logs)
+    if output == "components":
+        return g_opt, bclp.dose, bclp.mapped_dose, bclp.logs
+    raise ValueError(f"unknown output {output!r}")

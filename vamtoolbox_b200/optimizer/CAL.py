@@ -1,0 +1,137 @@
+"""Computed axial lithography (CAL) gradient descent: the reference's vamtoolbox/optimizer/CAL.py.
+
+Loop (CAL.py:147-195): x_thresh = sigmoid(x - d_h, g); delta_b = A.forward(x_thresh - target);
+b = clip(b - lr (delta_b (1-m) + delta_b_prev m / (1 - m^(it+1))), 0); x = A.backward(b) / max;
+VER per iteration.  engine="device" keeps x unnormalised with max(x) as a
+device scalar read by the threshold kernel, records VER into a device log and,
+without momentum or an exit threshold, replays one CUDA graph per iteration
+(bit-depth quantisation runs the host loop).
+"""
+from __future__ import annotations
+
+import time
+
+import numpy as np
+import torch
+
+from .. import geometry, metrics
+from ..fused import Workspace, capture
+from ..projectorconstructor import projectorconstructor
+from ..util import data as udata
+
+
+def _threshold_reconstruction(x, target_geo, sigmoid):
+    """CAL.py:39-114 (used when d_h is None)."""
+    lo, hi = np.amin(x), np.amax(x)
+    tests = np.linspace(lo, hi, 100)
+    gel, void = target_geo.gel_inds, target_geo.void_inds
+    score = np.zeros(tests.size)
+    for i, t in enumerate(tests):
+        th = np.where(x > t, 1, 0)
+        score[i] = np.sum(th[gel]) / np.sum(gel) - np.sum(th[void]) / np.sum(void)
+    thr = tests[np.argmax(score)]
+    return 1 / (1 + np.exp(-(float(sigmoid) * (x - thr)))), thr
+
+
+def _cal_host(target_geo, proj_geo, options, A=None):
+    A = A if A is not None else projectorconstructor(target_geo, proj_geo)
+    err = np.full(options.n_iter, np.nan)
+    iter_times = np.zeros(options.n_iter)
+    t0 = time.perf_counter()
+    b = A.forward(target_geo.array)
+    b = np.clip(udata.filterSinogram(b, options.filter), a_min=0, a_max=None)
+    db_prev = np.zeros_like(b)
+    x = A.backward(b)
+    x = x / np.max(x)
+    err[0] = metrics.calcVER(target_geo, x)
+    iter_times[0] = time.perf_counter() - t0
+    x_opt, b_opt = x, b
+    for it in range(1, options.n_iter):
+        if options.d_h is not None:
+            xt = udata.sigmoid(x - options.d_h, options.sigmoid)
+        else:
+            xt, _ = _threshold_reconstruction(x, target_geo, options.sigmoid)
+        db = A.forward(xt - target_geo.array)
+        m = options.momentum
+        grad = db * (1 - m) + db_prev * m / (1 - m ** (it + 1))
+        b = np.clip(b - options.learning_rate * grad, a_min=0, a_max=None)
+        if options.bit_depth is not None:
+            b = udata.discretize(b, options.bit_depth, [0.0, np.max(b)])
+        x = A.backward(b)
+        x = x / np.amax(x)
+        db_prev = db
+        x_opt, b_opt = x, b
+        err[it] = metrics.calcVER(target_geo, x)
+        iter_times[it] = time.perf_counter() - t0
+        if options.exit_param is not None and err[it] <= options.exit_param:
+            break
+    b_opt = np.where(b_opt < 0, 0, b_opt)
+    b_opt = b_opt / np.amax(b_opt)
+    x_opt = A.backward(b_opt)
+    x_opt = x_opt / np.amax(x_opt)
+    return (geometry.Sinogram(b_opt, proj_geo, options), geometry.Reconstruction(x_opt, proj_geo, options), err)
+
+
+def minimizeCAL(target_geo, proj_geo, options):
+    from ..projector.Projector3DParallel import Projector3DParallel
+
+    A = projectorconstructor(target_geo, proj_geo)
+    if (getattr(options, "engine", "device") == "host" or options.d_h is None or options.bit_depth is not None
+            or not isinstance(A, Projector3DParallel)):
+        return _cal_host(target_geo, proj_geo, options, A)
+    dev = A.device
+    ws = Workspace(dev)
+    plan = A.plan
+    vs, ss = plan.shape_vol, plan.shape_sino
+    tgt = torch.as_tensor(np.ascontiguousarray(np.atleast_3d(target_geo.array), dtype=np.float32), device=dev)
+    mask = torch.as_tensor(metrics.region_mask(target_geo).reshape(vs), device=dev)
+    n_iter = options.n_iter
+    err_log = torch.full((max(n_iter, 1),), float("nan"), dtype=torch.float32, device=dev)
+    counter = torch.zeros(1, dtype=torch.int32, device=dev)
+    ver = ws.scalar()
+    xmax = ws.scalar()
+    # initial sinogram: forward, filter (cuFFT), clip
+    b = plan.forward(tgt)
+    b = udata.filterSinogram_t(b, options.filter).clamp_(min=0).contiguous()
+    x = plan.backward_ref(b)
+    ws.max(x, xmax)
+    ws.ver(x, mask, ver)
+    ws.append(ver, err_log, counter)
+    xt = torch.empty(vs, dtype=torch.float32, device=dev)
+    db = torch.empty(ss, dtype=torch.float32, device=dev)
+    db_prev = torch.zeros(ss, dtype=torch.float32, device=dev)
+    m, lr = float(options.momentum), float(options.learning_rate)
+
+    def step(it):
+        ws.cal_threshold(x, xmax, tgt, options.d_h, options.sigmoid, xt)
+        plan.forward(xt, db)
+        ws.cal_update(b, db, db_prev if m != 0 else None, lr, m, it)
+        plan.backward_ref(b, x)
+        ws.max(x, xmax)
+        ws.ver(x, mask, ver)
+        ws.append(ver, err_log, counter)
+
+    graphable = m == 0 and options.bit_depth is None and options.exit_param is None
+    if graphable and n_iter > 2:
+        gr = capture(lambda: step(1), dev)
+        for _ in range(1, n_iter):
+            gr.replay()
+    else:
+        for it in range(1, n_iter):
+            step(it)
+            if m != 0:
+                db_prev.copy_(db)
+            if options.exit_param is not None and float(ver.item()) <= options.exit_param:
+                break
+    # final positivity / normalisation / reconstruction (CAL.py:197-208)
+    bmax = ws.scalar()
+    b.clamp_(min=0)
+    ws.max(b, bmax)
+    ws.scale(b, bmax)
+    x_opt = plan.backward_ref(b)
+    ws.max(x_opt, xmax)
+    ws.scale(x_opt, xmax)
+    err = err_log.double().cpu().numpy()
+    err = np.where(np.arange(err.size) < int(counter.item()), err, np.nan)
+    return (geometry.Sinogram(b.double().cpu().numpy(), proj_geo, options),
+            geometry.Reconstruction(x_opt.double().cpu().numpy(), proj_geo, options), err)
