@@ -105,6 +105,14 @@ int vam_parallel_backward_ref(vam_parallel_plan* plan, const float* sino_dev, fl
 int vam_parallel_adjoint(vam_parallel_plan* plan, const float* sino_dev, float* vol_dev,
                          vam_stream_t stream);
 
+/* Builds the plan's matched-transpose weight table (16 bytes per pixel and
+ * angle: the detector rows that sample the pixel and their summed forward
+ * weights), after which vam_parallel_adjoint is a pure gather.  Allocates;
+ * call once before capturing adjoint calls in a graph, and again after
+ * vam_parallel_set_absorption.  Without it the adjoint enumerates the
+ * sampling lattice on the fly.  No counterpart in the reference. */
+int vam_parallel_prepare_adjoint(vam_parallel_plan* plan, vam_stream_t stream);
+
 /* ======================================================================= */
 /* Curved-ray tracer (graded-index medium)                                 */
 /* ======================================================================= */

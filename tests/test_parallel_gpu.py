@@ -198,3 +198,19 @@ def test_fast_paths_against_oracle(shape, ang, absn):
     lhs = float((Ax * dev(b).double()).sum())
     rhs = float((dev(x).double() * p.adjoint(dev(b)).double()).sum())
     assert abs(lhs - rhs) <= 1e-6 * abs(lhs)
+
+
+@pytest.mark.parametrize("absn", [None, "ray"])
+def test_adjoint_without_weight_table(absn):
+    """The on-the-fly matched transpose (used when the table is not built or is too large)."""
+    rng = np.random.default_rng(9)
+    shape, ang = (30, 30, 128), np.linspace(0, 360, 18, endpoint=False) + 0.7
+    p = plan_for(shape, ang)
+    p.adj_table_limit_bytes = 0
+    oabs = None
+    if absn == "ray":
+        p.set_absorption("ray", alpha_per_px=0.04, radius_px=13.0)
+        oabs = ("ray", 0.04, 13.0)
+    b = rng.uniform(0, 1, (30, 18, 128))
+    assert relL2(p.adjoint(dev(b)).cpu().numpy(), O.parallel_adjoint(b, ang, absorption=oabs)) < TOL
+    assert not p._adj_ready

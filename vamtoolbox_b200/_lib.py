@@ -77,6 +77,7 @@ _SIGS = {
     "vam_parallel_forward": ([_vp, _vp, _vp, _vp], _c_int),
     "vam_parallel_backward_ref": ([_vp, _vp, _vp, _vp], _c_int),
     "vam_parallel_adjoint": ([_vp, _vp, _vp, _vp], _c_int),
+    "vam_parallel_prepare_adjoint": ([_vp, _vp], _c_int),
     "vam_ray_plan_create": ([ctypes.POINTER(RayGeom), _vp, _vp, _c_f, ctypes.POINTER(_vp)], _c_int),
     "vam_ray_plan_destroy": ([_vp], _c_int),
     "vam_ray_set_medium": ([_vp, ctypes.POINTER(RayMedium), _vp], _c_int),

@@ -263,18 +263,40 @@ struct Acc {
 };
 
 // One bilinear sample (all taps checked), added with weight f into acc.
+// Lane-interleaved z vectors of the fast kernels: with Q = VZ / 4, lane l of
+// a warp owns slices zbase + 4l + 128q + (0..3), q < Q, so every float4 load
+// of the warp covers 512 contiguous bytes (four 128-byte lines).  p points at
+// the lane's first slice; qn is the number of its vectors inside the volume.
 template <int VZ>
-__device__ __forceinline__ void load_vz(const float* __restrict__ p, float* d) {
+__device__ __forceinline__ void load_vz(const float* __restrict__ p, float* d, int qn = VZ / 4) {
 #pragma unroll
     for (int q = 0; q < VZ / 4; ++q) {
-        const float4 t = __ldg(reinterpret_cast<const float4*>(p) + q);
+        float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (q < qn) t = __ldg(reinterpret_cast<const float4*>(p + 128 * q));
         d[4 * q] = t.x; d[4 * q + 1] = t.y; d[4 * q + 2] = t.z; d[4 * q + 3] = t.w;
     }
 }
 
 template <int VZ>
+__device__ __forceinline__ void store_vz(float* __restrict__ p, const float* d, int qn) {
+#pragma unroll
+    for (int q = 0; q < VZ / 4; ++q)
+        if (q < qn) *reinterpret_cast<float4*>(p + 128 * q) = make_float4(d[4 * q], d[4 * q + 1], d[4 * q + 2], d[4 * q + 3]);
+}
+
+// First slice and number of in-range vectors of a lane in z-chunk zc.
+template <int VZ>
+__device__ __forceinline__ void lane_z(int zc, int lane, int nZ, int& z0, int& qn) {
+    const int base = zc * 32 * VZ + 4 * lane;
+    qn = 0;
+#pragma unroll
+    for (int q = 0; q < VZ / 4; ++q) qn += (base + 128 * q < nZ) ? 1 : 0;
+    z0 = qn ? base : 0;
+}
+
+template <int VZ>
 __device__ __forceinline__ void sample_checked(const FastArgs& a, const float* __restrict__ volz, double row,
-                                               double col, float f, float (&acc)[VZ]) {
+                                               double col, float f, float (&acc)[VZ], int qn) {
     const double fr = floor(row), fc = floor(col);
     const int r0 = (int)fr, c0 = (int)fc;
     const bool rc = row > fr, cc = col > fc;
@@ -285,22 +307,22 @@ __device__ __forceinline__ void sample_checked(const FastArgs& a, const float* _
     const float w10 = dr * (1.f - dc) * f, w11 = dr * dc * f;
     float t[VZ];
     if (vr0 && vc0) {
-        load_vz<VZ>(volz + (size_t)r0 * a.RS + (size_t)c0 * a.nZ, t);
+        load_vz<VZ>(volz + (size_t)r0 * a.RS + (size_t)c0 * a.nZ, t, qn);
 #pragma unroll
         for (int e = 0; e < VZ; ++e) acc[e] = fmaf(w00, t[e], acc[e]);
     }
     if (vr0 && vc1) {
-        load_vz<VZ>(volz + (size_t)r0 * a.RS + (size_t)(c0 + 1) * a.nZ, t);
+        load_vz<VZ>(volz + (size_t)r0 * a.RS + (size_t)(c0 + 1) * a.nZ, t, qn);
 #pragma unroll
         for (int e = 0; e < VZ; ++e) acc[e] = fmaf(w01, t[e], acc[e]);
     }
     if (vr1 && vc0) {
-        load_vz<VZ>(volz + (size_t)(r0 + 1) * a.RS + (size_t)c0 * a.nZ, t);
+        load_vz<VZ>(volz + (size_t)(r0 + 1) * a.RS + (size_t)c0 * a.nZ, t, qn);
 #pragma unroll
         for (int e = 0; e < VZ; ++e) acc[e] = fmaf(w10, t[e], acc[e]);
     }
     if (vr1 && vc1) {
-        load_vz<VZ>(volz + (size_t)(r0 + 1) * a.RS + (size_t)(c0 + 1) * a.nZ, t);
+        load_vz<VZ>(volz + (size_t)(r0 + 1) * a.RS + (size_t)(c0 + 1) * a.nZ, t, qn);
 #pragma unroll
         for (int e = 0; e < VZ; ++e) acc[e] = fmaf(w11, t[e], acc[e]);
     }
@@ -317,9 +339,9 @@ __global__ void __launch_bounds__(256) k_forward_fast(FastArgs a) {
     const int N = a.nY;
     const bool ext = paired && a.even;   // lattice row / column N is needed by the partner angle
     if (j > (ext ? N : N - 1)) return;   // uniform per warp
-    const int zv = zc * 32 + lane;
-    const bool zok = zv * VZ < a.nZ;
-    const int z0 = zok ? zv * VZ : 0;
+    int z0, qn;
+    lane_z<VZ>(zc, lane, a.nZ, z0, qn);
+    const bool zok = qn > 0;
     const float* __restrict__ volz = a.vol + z0;
 
     const double4 tr = a.trig[task.x];
@@ -360,10 +382,10 @@ __global__ void __launch_bounds__(256) k_forward_fast(FastArgs a) {
                 float w10 = dr * (1.f - dc), w11 = dr * dc;
                 if (RAY) { w00 *= f; w01 *= f; w10 *= f; w11 *= f; }
                 float t0[VZ], t1[VZ], t2[VZ], t3[VZ];
-                load_vz<VZ>(volz + o00, t0);
-                load_vz<VZ>(volz + o00 + dcol, t1);
-                load_vz<VZ>(volz + o10, t2);
-                load_vz<VZ>(volz + o10 + dcol, t3);
+                load_vz<VZ>(volz + o00, t0, qn);
+                load_vz<VZ>(volz + o00 + dcol, t1, qn);
+                load_vz<VZ>(volz + o10, t2, qn);
+                load_vz<VZ>(volz + o10 + dcol, t3, qn);
 #pragma unroll
                 for (int e = 0; e < VZ; ++e) {
                     acc[e] = fmaf(w00, t0[e], acc[e]);
@@ -372,25 +394,22 @@ __global__ void __launch_bounds__(256) k_forward_fast(FastArgs a) {
                     acc[e] = fmaf(w11, t3[e], acc[e]);
                 }
             } else {
-                sample_checked<VZ>(a, volz, row, col, f, acc);
+                sample_checked<VZ>(a, volz, row, col, f, acc, qn);
             }
         }
         if (klo <= 0 && khi >= 0) {
             const float f = RAY ? ray_factor((float)(0 - a.C), s_entry, a.alpha) : 1.f;
-            sample_checked<VZ>(a, volz, rowb, colb, f, e0);
+            sample_checked<VZ>(a, volz, rowb, colb, f, e0, qn);
         }
         if (ext && klo <= N && khi >= N)
-            sample_checked<VZ>(a, volz, fma(c, (double)N, rowb), fma(s, (double)N, colb), 1.f, eN);
+            sample_checked<VZ>(a, volz, fma(c, (double)N, rowb), fma(s, (double)N, colb), 1.f, eN, qn);
     }
     if (!zok) return;
     if (j <= N - 1) {
         float o[VZ];
 #pragma unroll
         for (int e = 0; e < VZ; ++e) o[e] = acc[e] + e0[e];
-        float* dst = a.sino + ((size_t)j * a.nA + task.x) * a.nZ + z0;
-#pragma unroll
-        for (int q = 0; q < VZ / 4; ++q)
-            reinterpret_cast<float4*>(dst)[q] = make_float4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
+        store_vz<VZ>(a.sino + ((size_t)j * a.nA + task.x) * a.nZ + z0, o, qn);
     }
     if (paired) {
         // partner detector j' = 2C - j over lattice k in [2C-N+1, 2C]
@@ -399,10 +418,7 @@ __global__ void __launch_bounds__(256) k_forward_fast(FastArgs a) {
             float o[VZ];
 #pragma unroll
             for (int e = 0; e < VZ; ++e) o[e] = acc[e] + (a.even ? eN[e] : e0[e]);
-            float* dst = a.sino + ((size_t)jp * a.nA + task.y) * a.nZ + z0;
-#pragma unroll
-            for (int q = 0; q < VZ / 4; ++q)
-                reinterpret_cast<float4*>(dst)[q] = make_float4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
+            store_vz<VZ>(a.sino + ((size_t)jp * a.nA + task.y) * a.nZ + z0, o, qn);
         }
     }
 }
@@ -428,9 +444,9 @@ __global__ void __launch_bounds__(256) k_adjoint_fast(Args a) {
     const long p = item / zchunks;
     if (p >= (long)a.nY * a.nX) return;
     const int i = (int)(p / a.nX), j = (int)(p % a.nX);
-    const int zv = zc * 32 + lane;
-    const bool zok = zv * VZ < a.nZ;
-    const int z0 = zok ? zv * VZ : 0;
+    int z0, qn;
+    lane_z<VZ>(zc, lane, a.nZ, z0, qn);
+    const bool zok = qn > 0;
     const size_t rs = (size_t)a.nA * a.nZ;
     const int N = a.nY;
     float acc[VZ];
@@ -470,7 +486,7 @@ __global__ void __launch_bounds__(256) k_adjoint_fast(Args a) {
             }
             if (W != 0.f && zok) {
                 float bv[VZ];
-                load_vz<VZ>(bz + (size_t)J * rs + (size_t)th * a.nZ, bv);
+                load_vz<VZ>(bz + (size_t)J * rs + (size_t)th * a.nZ, bv, qn);
 #pragma unroll
                 for (int e = 0; e < VZ; ++e) acc[e] = fmaf(W, bv[e], acc[e]);
             }
@@ -482,10 +498,7 @@ __global__ void __launch_bounds__(256) k_adjoint_fast(Args a) {
 #pragma unroll
         for (int e = 0; e < VZ; ++e) acc[e] *= m;
     }
-    float* dst = a.out + (size_t)p * a.nZ + z0;
-#pragma unroll
-    for (int q = 0; q < VZ / 4; ++q)
-        reinterpret_cast<float4*>(dst)[q] = make_float4(acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]);
+    store_vz<VZ>(a.out + (size_t)p * a.nZ + z0, acc, qn);
 }
 
 // ---------------------------------------------------------------------------
@@ -500,9 +513,9 @@ __global__ void __launch_bounds__(256) k_backward_fast(Args a) {
     const long p = item / a.zchunks;
     if (p >= (long)a.nY * a.nX) return;
     const int i = (int)(p / a.nX), j = (int)(p % a.nX);
-    const int zv = zc * 32 + lane;
-    const bool zok = zv * VZ < a.nZ;
-    const int z0 = zok ? zv * VZ : 0;
+    int z0, qn;
+    lane_z<VZ>(zc, lane, a.nZ, z0, qn);
+    const bool zok = qn > 0;
     float acc[VZ];
 #pragma unroll
     for (int e = 0; e < VZ; ++e) acc[e] = 0.f;
@@ -520,17 +533,17 @@ __global__ void __launch_bounds__(256) k_backward_fast(Args a) {
             const int j0 = (int)ft + a.C;
             const float* b0 = bz + (size_t)j0 * rs + (size_t)th * a.nZ;
             float v0[VZ], v1[VZ];
-            load_vz<VZ>(b0, v0);
+            load_vz<VZ>(b0, v0, qn);
             // t == floor(t): np.interp returns fp[j]; the second row is read with weight 0
             const float w = (float)(t - ft);
-            load_vz<VZ>(b0 + (t != ft ? rs : 0), v1);
+            load_vz<VZ>(b0 + (t != ft ? rs : 0), v1, qn);
             float f = 1.f;
             if (RAY) {
-                const float tf = (float)t;
+                // |t| <= R is a discontinuity of the model: decide it on the float64 t
                 f = 0.f;
-                if (fabsf(tf) <= a.R) {
+                if (fabs(t) <= (double)a.R) {
                     const float sv = (float)__dadd_rn(__dmul_rn(X, tr.y), __dmul_rn(Y, tr.x));
-                    f = ray_factor(sv, -sqrtf(a.R * a.R - tf * tf), a.alpha);
+                    f = ray_factor(sv, (float)(-sqrt((double)a.R * a.R - t * t)), a.alpha);
                 }
             }
 #pragma unroll
@@ -546,10 +559,99 @@ __global__ void __launch_bounds__(256) k_backward_fast(Args a) {
 #pragma unroll
         for (int e = 0; e < VZ; ++e) acc[e] = m * acc[e];
     }
-    float* dst = a.out + (size_t)p * a.nZ + z0;
+    store_vz<VZ>(a.out + (size_t)p * a.nZ + z0, acc, qn);
+}
+
+// ---------------------------------------------------------------------------
+// Matched transpose from a weight table.
+//
+// k_adj_table evaluates, once per plan, for every pixel (i, j) and angle the
+// forward's own tap weights: the candidate lattice samples (J, K) around the
+// pixel's rotated position are evaluated with the forward's float64
+// coordinate expression and float32 weights, (1-dr)(1-dc) etc. times the RAY
+// factor, and summed per detector row J.  At most three rows J0-1..J0+1
+// touch a pixel (|J - J*| < |cos| + |sin| <= sqrt 2).  k_adjoint_table is then
+// a gather: per pixel and angle one 16-byte entry (broadcast over the warp)
+// and at most three sinogram rows.
+// ---------------------------------------------------------------------------
+template <bool RAY>
+__global__ void __launch_bounds__(256) k_adj_table(const double4* __restrict__ trig, float4* __restrict__ table, int nY,
+                                                   int nX, int nA, int C, float alpha, float R) {
+    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;   // over (pixel, angle), angle fastest
+    if (idx >= (long)nY * nX * nA) return;
+    const int th = (int)(idx % nA);
+    const long p = idx / nA;
+    const int i = (int)(p / nX), j = (int)(p % nX);
+    const double4 tr = trig[th];
+    const double c = tr.x, s = tr.y;
+    const double ri = (double)i - tr.w, ci = (double)j - tr.z;
+    const int J0 = __double2int_rn(fma(-s, ri, c * ci)), K0 = __double2int_rn(fma(c, ri, s * ci));
+    float W[3] = {0.f, 0.f, 0.f};
+    for (int da = -1; da <= 1; ++da) {
+        const int J = J0 + da;
+        if ((unsigned)J >= (unsigned)nX) continue;
+        float s_entry = 0.f;
+        if (RAY) {
+            const float t = (float)(J - C);
+            if (fabsf(t) > R) continue;
+            s_entry = -sqrtf(R * R - t * t);
+        }
+        const double rowb = fma(-s, (double)J, tr.w), colb = fma(c, (double)J, tr.z);
+        for (int db = -2; db <= 2; ++db) {
+            const int K = K0 + db;
+            if ((unsigned)K >= (unsigned)nY) continue;
+            const double row = fma(c, (double)K, rowb), col = fma(s, (double)K, colb);
+            const double fr = floor(row), fc = floor(col);
+            const int r0 = (int)fr, c0 = (int)fc;
+            const bool rc = row > fr, cc = col > fc;
+            if (!(i == r0 || (rc && i == r0 + 1))) continue;
+            if (!(j == c0 || (cc && j == c0 + 1))) continue;
+            const float dr = (float)(row - fr), dc = (float)(col - fc);
+            float w = ((i == r0) ? (1.f - dr) : dr) * ((j == c0) ? (1.f - dc) : dc);
+            if (RAY) w *= ray_factor((float)(K - C), s_entry, alpha);
+            W[da + 1] += w;
+        }
+    }
+    table[p * nA + th] = make_float4(__int_as_float(J0 - 1), W[0], W[1], W[2]);
+}
+
+template <int VZ>
+__global__ void __launch_bounds__(256) k_adjoint_table(Args a, const float4* __restrict__ table) {
+    const int lane = threadIdx.x & 31;
+    const long item = (long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+    const int zc = (int)(item % a.zchunks);
+    const long p = item / a.zchunks;
+    if (p >= (long)a.nY * a.nX) return;
+    int z0, qn;
+    lane_z<VZ>(zc, lane, a.nZ, z0, qn);
+    if (qn == 0) return;
+    const size_t rs = (size_t)a.nA * a.nZ;
+    const float* __restrict__ bz = a.in + z0;
+    const float4* __restrict__ tp = table + p * a.nA;
+    float acc[VZ];
 #pragma unroll
-    for (int q = 0; q < VZ / 4; ++q)
-        reinterpret_cast<float4*>(dst)[q] = make_float4(acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]);
+    for (int e = 0; e < VZ; ++e) acc[e] = 0.f;
+#pragma unroll 2
+    for (int th = 0; th < a.nA; ++th) {
+        const float4 ent = __ldg(tp + th);
+        const int J = __float_as_int(ent.x);
+        const float w[3] = {ent.y, ent.z, ent.w};
+#pragma unroll
+        for (int t = 0; t < 3; ++t) {
+            if (w[t] != 0.f) {
+                float bv[VZ];
+                load_vz<VZ>(bz + (size_t)(J + t) * rs + (size_t)th * a.nZ, bv, qn);
+#pragma unroll
+                for (int e = 0; e < VZ; ++e) acc[e] = fmaf(w[t], bv[e], acc[e]);
+            }
+        }
+    }
+    if (a.mask) {
+        const float m = __ldg(a.mask + p);
+#pragma unroll
+        for (int e = 0; e < VZ; ++e) acc[e] *= m;
+    }
+    store_vz<VZ>(a.out + (size_t)p * a.nZ + z0, acc, qn);
 }
 
 __global__ void k_mask_mul(const float* __restrict__ x, const float* __restrict__ mask, float* __restrict__ out,
@@ -632,11 +734,11 @@ __global__ void __launch_bounds__(256) k_backward_ref(Args a) {
                 }
             }
             if (ABS == VAM_ABS_RAY) {
-                const float tf = (float)t;
+                // |t| <= R is a discontinuity of the model: decide it on the float64 t
                 float f = 0.f;
-                if (fabsf(tf) <= a.R) {
+                if (fabs(t) <= (double)a.R) {
                     const float sv = (float)__dadd_rn(__dmul_rn(X, tr.y), __dmul_rn(Y, tr.x));
-                    f = ray_factor(sv, -sqrtf(a.R * a.R - tf * tf), a.alpha);
+                    f = ray_factor(sv, (float)(-sqrt((double)a.R * a.R - t * t)), a.alpha);
                 }
 #pragma unroll
                 for (int e = 0; e < VZ; ++e) v[e] *= f;
@@ -832,11 +934,10 @@ void launch_abs(Op op, int abs_mode, const Args& a, long items, cudaStream_t st)
 
 // VZ of the fast forward for nZ slices (0 = use the generic kernel)
 int fast_vz(int nZ, bool aligned) {
-    if (!aligned) return 0;
+    if (!aligned || nZ % 4) return 0;
     auto eff = [&](int vz) {
-        if (nZ % vz) return 0.0;
-        const int vec = nZ / vz, ch = (vec + 31) / 32;
-        return (double)vec / (double)(ch * 32);
+        const int per = 32 * vz, ch = (nZ + per - 1) / per;
+        return (double)nZ / (double)(ch * per);
     };
     if (eff(8) >= 0.74) return 8;
     if (eff(4) >= 0.74) return 4;
@@ -857,7 +958,7 @@ int run_forward_fast(vam_parallel_plan* plan, const float* in, float* out, cudaS
     a.vol = vol; a.sino = out; a.trig = plan->d_trig;
     a.nY = plan->nY; a.nX = plan->nX; a.nZ = plan->nZ; a.nA = plan->nA; a.C = plan->C;
     a.RS = plan->nX * plan->nZ;
-    a.zchunks = (plan->nZ / vz + 31) / 32;
+    a.zchunks = (plan->nZ + 32 * vz - 1) / (32 * vz);
     a.even = (plan->nY % 2) == 0;
     a.alpha = plan->abs_alpha; a.R = plan->abs_R;
     const bool ray = plan->abs_mode == VAM_ABS_RAY;
@@ -890,7 +991,7 @@ int run(vam_parallel_plan* plan, Op op, const float* in, float* out, cudaStream_
         a.in = in; a.out = out; a.trig = plan->d_trig; a.circle = plan->d_circle;
         a.mask = plan->abs_mode == VAM_ABS_MASK ? plan->d_mask : nullptr;
         a.nY = plan->nY; a.nX = plan->nX; a.nZ = plan->nZ; a.nA = plan->nA; a.C = plan->C;
-        a.zchunks = (plan->nZ / vzf + 31) / 32;
+        a.zchunks = (plan->nZ + 32 * vzf - 1) / (32 * vzf);
         a.alpha = plan->abs_alpha; a.R = plan->abs_R;
         const long items = (long)plan->nY * plan->nX * a.zchunks;
         dim3 grid((unsigned)((items + kWarpsPerBlock - 1) / kWarpsPerBlock)), block(kWarpsPerBlock * kWarp);
@@ -898,6 +999,9 @@ int run(vam_parallel_plan* plan, Op op, const float* in, float* out, cudaStream_
         if (op == Op::BackwardRef) {
             if (vzf == 8) { if (ray) k_backward_fast<8, true><<<grid, block, 0, st>>>(a); else k_backward_fast<8, false><<<grid, block, 0, st>>>(a); }
             else { if (ray) k_backward_fast<4, true><<<grid, block, 0, st>>>(a); else k_backward_fast<4, false><<<grid, block, 0, st>>>(a); }
+        } else if (plan->d_adj_table && plan->adj_table_abs == plan->abs_mode) {
+            if (vzf == 8) k_adjoint_table<8><<<grid, block, 0, st>>>(a, plan->d_adj_table);
+            else k_adjoint_table<4><<<grid, block, 0, st>>>(a, plan->d_adj_table);
         } else {
             if (vzf == 8) { if (ray) k_adjoint_fast<8, true><<<grid, block, 0, st>>>(a); else k_adjoint_fast<8, false><<<grid, block, 0, st>>>(a); }
             else { if (ray) k_adjoint_fast<4, true><<<grid, block, 0, st>>>(a); else k_adjoint_fast<4, false><<<grid, block, 0, st>>>(a); }
@@ -960,6 +1064,7 @@ extern "C" int vam_parallel_plan_create(const vam_parallel_geom* geom, vam_paral
     p->nY = geom->n_y; p->nX = geom->n_x; p->nZ = geom->n_z; p->nA = geom->n_angles;
     p->C = geom->n_y / 2;
     p->device = geom->device;
+    p->adj_table_abs = -1;
     // per-angle tables exactly as numpy evaluates them (Projector3DParallel.py:135-143)
     std::vector<double4> trig(p->nA);
     for (int i = 0; i < p->nA; ++i) {
@@ -1028,6 +1133,7 @@ extern "C" int vam_parallel_plan_destroy(vam_parallel_plan* p) {
     cudaFree(p->d_tasks_paired);
     cudaFree(p->d_tasks_single);
     cudaFree(p->d_vol_scratch);
+    cudaFree(p->d_adj_table);
     delete p;
     return VAM_OK;
 }
@@ -1089,6 +1195,23 @@ extern "C" int vam_parallel_get_occlusion_sinogram(vam_parallel_plan* p, float* 
     DeviceGuard g(p->device);
     VAM_TRY_CUDA(cudaMemcpyAsync(out_dev, p->d_occ, sizeof(float) * (size_t)p->nY * p->nA * p->nZ,
                                  cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+    return VAM_OK;
+}
+
+extern "C" int vam_parallel_prepare_adjoint(vam_parallel_plan* p, vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(p, VAM_ERR_ARG, "vam_parallel_prepare_adjoint: null plan");
+    DeviceGuard g(p->device);
+    const size_t n = (size_t)p->nY * p->nX * p->nA;
+    if (!p->d_adj_table) VAM_TRY_CUDA(cudaMalloc(&p->d_adj_table, sizeof(float4) * n));
+    cudaStream_t st = (cudaStream_t)stream;
+    const unsigned nb = (unsigned)((n + 255) / 256);
+    if (p->abs_mode == VAM_ABS_RAY)
+        k_adj_table<true><<<nb, 256, 0, st>>>(p->d_trig, p->d_adj_table, p->nY, p->nX, p->nA, p->C, p->abs_alpha, p->abs_R);
+    else
+        k_adj_table<false><<<nb, 256, 0, st>>>(p->d_trig, p->d_adj_table, p->nY, p->nX, p->nA, p->C, 0.f, 0.f);
+    VAM_CHECK_LAUNCH("k_adj_table");
+    p->adj_table_abs = p->abs_mode;
     return VAM_OK;
 }
 

@@ -51,6 +51,7 @@ struct RayArgs {
     float norm[3];        // 2/span (0 for a 2D z axis)
     double half_span[3];  // span/2
     double inv_voxel[3];  // 1/voxel (0 for a 2D z axis)
+    float half_span_f[3], inv_voxel_f[3];
     double bmax[3], bmin[3];  // exit bounds: max + voxel, min - voxel
     float h;              // parameter step, float32 as the reference multiplies it
     float h_idx;          // step / voxel_x
@@ -74,39 +75,33 @@ __device__ __forceinline__ float unnorm(float x, float nrm, int size, bool borde
     return ix;
 }
 
-// Trilinear sample of the packed index texels with border padding.
+// Trilinear sample of the packed index texels with border padding.  The
+// coordinate is clamped into [0, size-1], so the upper corner is out of range
+// only when its weight is exactly 0; clamping its index keeps every load in
+// bounds without a branch.
 __device__ __forceinline__ float4 sample_n(const RayArgs& a, const float* x) {
     const float ix = unnorm(x[0], a.norm[0], a.nx, true);
     const float iy = unnorm(x[1], a.norm[1], a.ny, true);
     const float iz = unnorm(x[2], a.norm[2], a.nz, true);
-    const int x0 = (int)floorf(ix), y0 = (int)floorf(iy), z0 = (int)floorf(iz);
-    const float wx1 = ix - (float)x0, wy1 = iy - (float)y0, wz1 = iz - (float)z0;
+    const float fx = floorf(ix), fy = floorf(iy), fz = floorf(iz);
+    const int x0 = (int)fx, y0 = (int)fy, z0 = (int)fz;
+    const int x1 = min(x0 + 1, a.nx - 1), y1 = min(y0 + 1, a.ny - 1), z1 = min(z0 + 1, a.nz - 1);
+    const float wx1 = ix - fx, wy1 = iy - fy, wz1 = iz - fz;
     const float wx0 = 1.f - wx1, wy0 = 1.f - wy1, wz0 = 1.f - wz1;
-    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-    for (int cz = 0; cz < 2; ++cz) {
-        const int Z = z0 + cz;
-        if (Z >= a.nz) continue;
-        const float wz = cz ? wz1 : wz0;
-#pragma unroll
-        for (int cy = 0; cy < 2; ++cy) {
-            const int Y = y0 + cy;
-            if (Y >= a.ny) continue;
-            const float wyz = (cy ? wy1 : wy0) * wz;
-#pragma unroll
-            for (int cx = 0; cx < 2; ++cx) {
-                const int X = x0 + cx;
-                if (X >= a.nx) continue;
-                const float w = (cx ? wx1 : wx0) * wyz;
-                const float4 t = __ldg(a.nfield + ((size_t)X * a.ny + Y) * a.nz + Z);
-                acc.x = fmaf(w, t.x, acc.x);
-                acc.y = fmaf(w, t.y, acc.y);
-                acc.z = fmaf(w, t.z, acc.z);
-                acc.w = fmaf(w, t.w, acc.w);
-            }
-        }
-    }
-    return acc;
+    const int sy = a.nz, sx = a.ny * a.nz;
+    const float4* f = a.nfield;
+    const float4 t000 = __ldg(f + x0 * sx + y0 * sy + z0), t100 = __ldg(f + x1 * sx + y0 * sy + z0);
+    const float4 t010 = __ldg(f + x0 * sx + y1 * sy + z0), t110 = __ldg(f + x1 * sx + y1 * sy + z0);
+    const float4 t001 = __ldg(f + x0 * sx + y0 * sy + z1), t101 = __ldg(f + x1 * sx + y0 * sy + z1);
+    const float4 t011 = __ldg(f + x0 * sx + y1 * sy + z1), t111 = __ldg(f + x1 * sx + y1 * sy + z1);
+    const float w000 = wx0 * wy0 * wz0, w100 = wx1 * wy0 * wz0, w010 = wx0 * wy1 * wz0, w110 = wx1 * wy1 * wz0;
+    const float w001 = wx0 * wy0 * wz1, w101 = wx1 * wy0 * wz1, w011 = wx0 * wy1 * wz1, w111 = wx1 * wy1 * wz1;
+    float4 r;
+    r.x = w000 * t000.x + w100 * t100.x + w010 * t010.x + w110 * t110.x + w001 * t001.x + w101 * t101.x + w011 * t011.x + w111 * t111.x;
+    r.y = w000 * t000.y + w100 * t100.y + w010 * t010.y + w110 * t110.y + w001 * t001.y + w101 * t101.y + w011 * t011.y + w111 * t111.y;
+    r.z = w000 * t000.z + w100 * t100.z + w010 * t010.z + w110 * t110.z + w001 * t001.z + w101 * t101.z + w011 * t011.z + w111 * t111.z;
+    r.w = w000 * t000.w + w100 * t100.w + w010 * t010.w + w110 * t110.w + w001 * t001.w + w101 * t101.w + w011 * t011.w + w111 * t111.w;
+    return r;
 }
 
 // (n, grad n) at x for the configured index kind (medium.py:276-473)
@@ -141,29 +136,24 @@ __device__ __forceinline__ float alpha_at(const RayArgs& a, const float* x) {
     const float ix = unnorm(x[0], a.norm[0], a.nx, false);
     const float iy = unnorm(x[1], a.norm[1], a.ny, false);
     const float iz = unnorm(x[2], a.norm[2], a.nz, false);
+    // far outside the grid every corner is zero padding
+    if (!(ix > -1.f && ix < (float)a.nx && iy > -1.f && iy < (float)a.ny && iz > -1.f && iz < (float)a.nz)) return 0.f;
     const float fx = floorf(ix), fy = floorf(iy), fz = floorf(iz);
     const int x0 = (int)fx, y0 = (int)fy, z0 = (int)fz;
     const float wx1 = ix - fx, wy1 = iy - fy, wz1 = iz - fz;
-    float acc = 0.f;
-#pragma unroll
-    for (int cz = 0; cz < 2; ++cz) {
-        const int Z = z0 + cz;
-        if ((unsigned)Z >= (unsigned)a.nz) continue;
-        const float wz = cz ? wz1 : 1.f - wz1;
-#pragma unroll
-        for (int cy = 0; cy < 2; ++cy) {
-            const int Y = y0 + cy;
-            if ((unsigned)Y >= (unsigned)a.ny) continue;
-            const float wyz = (cy ? wy1 : 1.f - wy1) * wz;
-#pragma unroll
-            for (int cx = 0; cx < 2; ++cx) {
-                const int X = x0 + cx;
-                if ((unsigned)X >= (unsigned)a.nx) continue;
-                acc = fmaf((cx ? wx1 : 1.f - wx1) * wyz, __ldg(a.afield + ((size_t)X * a.ny + Y) * a.nz + Z), acc);
-            }
-        }
-    }
-    return acc;
+    // per-axis weights of the two corners, zeroed for a corner outside the grid
+    const float ax0 = x0 >= 0 ? 1.f - wx1 : 0.f, ax1 = x0 + 1 < a.nx ? wx1 : 0.f;
+    const float ay0 = y0 >= 0 ? 1.f - wy1 : 0.f, ay1 = y0 + 1 < a.ny ? wy1 : 0.f;
+    const float az0 = z0 >= 0 ? 1.f - wz1 : 0.f, az1 = z0 + 1 < a.nz ? wz1 : 0.f;
+    const int X0 = max(x0, 0), X1 = min(x0 + 1, a.nx - 1);
+    const int Y0 = max(y0, 0), Y1 = min(y0 + 1, a.ny - 1);
+    const int Z0 = max(z0, 0), Z1 = min(z0 + 1, a.nz - 1);
+    const int sy = a.nz, sx = a.ny * a.nz;
+    const float* f = a.afield;
+    return ax0 * (ay0 * (az0 * __ldg(f + X0 * sx + Y0 * sy + Z0) + az1 * __ldg(f + X0 * sx + Y0 * sy + Z1)) +
+                  ay1 * (az0 * __ldg(f + X0 * sx + Y1 * sy + Z0) + az1 * __ldg(f + X0 * sx + Y1 * sy + Z1))) +
+           ax1 * (ay0 * (az0 * __ldg(f + X1 * sx + Y0 * sy + Z0) + az1 * __ldg(f + X1 * sx + Y0 * sy + Z1)) +
+                  ay1 * (az0 * __ldg(f + X1 * sx + Y1 * sy + Z0) + az1 * __ldg(f + X1 * sx + Y1 * sy + Z1)));
 }
 
 // dv/dstep and dx/dstep of the three parametrisations (pyTorchRayTrace.py:694-735)
@@ -178,7 +168,7 @@ __device__ __forceinline__ void dx_dstep(const RayArgs& a, float n, const float*
     else if (a.param == VAM_PARAM_OPTICAL) {
         const float in2 = 1.f / (n * n);
         dx[0] = v[0] * in2; dx[1] = v[1] * in2; dx[2] = v[2] * in2;
-    } else { dx[0] = v[0] / n; dx[1] = v[1] / n; dx[2] = v[2] / n; }
+    } else { const float rn = 1.f / n; dx[0] = v[0] * rn; dx[1] = v[1] * rn; dx[2] = v[2] * rn; }
 }
 
 struct RayState {
@@ -223,7 +213,7 @@ __device__ __forceinline__ void ray_step(const RayArgs& a, RayState& st, float& 
     ds = sqrtf(dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2]);
     alpha = alpha_at(a, st.xi);
     st.att = st.att + alpha * ds;
-    st.E = st.E0 * expf(-st.att);
+    st.E = st.E0 * __expf(-st.att);
 }
 
 // Exit test of pyTorchRayTrace.py:1343-1424 (position past max+voxel moving
@@ -249,12 +239,30 @@ struct Corners {
 __device__ __forceinline__ void corners_at(const RayArgs& a, const float* x, Corners& c) {
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        const double idx = ((double)x[d] + a.half_span[d]) * a.inv_voxel[d];
-        const double fl = floor(idx), ce = ceil(idx);
-        c.lo[d] = (int)fmax(fmin(fl, 2.0e9), -2.0e9);
-        c.hi[d] = (int)fmax(fmin(ce, 2.0e9), -2.0e9);
-        c.wlo[d] = (float)(1.0 - (idx - fl));
-        c.whi[d] = (float)(1.0 - (ce - idx));
+        if (d == 2 && a.twod) {  // 2-D: the z index is exactly 0 (1/inf voxel), one neighbour
+            c.lo[2] = c.hi[2] = 0;
+            c.wlo[2] = c.whi[2] = 1.f;
+            continue;
+        }
+        // float32 index; its error (< 3e-5 for grids up to 1024) only matters
+        // for the floor / ceil decision near an integer, which is then redone
+        // in float64 exactly as the reference forms it
+        const float idxf = (x[d] + a.half_span_f[d]) * a.inv_voxel_f[d];
+        const float flf = floorf(idxf);
+        const float frf = idxf - flf;
+        if (frf > 2e-4f && frf < 1.f - 2e-4f && fabsf(idxf) < 1.0e6f) {
+            c.lo[d] = (int)flf;
+            c.hi[d] = c.lo[d] + 1;
+            c.wlo[d] = 1.f - frf;
+            c.whi[d] = frf;
+        } else {
+            const double idx = ((double)x[d] + a.half_span[d]) * a.inv_voxel[d];
+            const double fl = floor(idx), ce = ceil(idx);
+            c.lo[d] = (int)fmax(fmin(fl, 2.0e9), -2.0e9);
+            c.hi[d] = (int)fmax(fmin(ce, 2.0e9), -2.0e9);
+            c.wlo[d] = (float)(1.0 - (idx - fl));
+            c.whi[d] = (float)(1.0 - (ce - idx));
+        }
     }
 }
 
@@ -429,6 +437,8 @@ RayArgs make_args(const vam_ray_plan* p) {
         a.half_span[d] = span / 2.0;
         const double iv = 1.0 / g.voxel[d];
         a.inv_voxel[d] = std::isfinite(iv) ? iv : 0.0;
+        a.half_span_f[d] = (float)a.half_span[d];
+        a.inv_voxel_f[d] = (float)a.inv_voxel[d];
         a.bmax[d] = g.coord_max[d] + g.voxel[d];
         a.bmin[d] = g.coord_min[d] - g.voxel[d];
     }

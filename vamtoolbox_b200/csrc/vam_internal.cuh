@@ -75,4 +75,8 @@ struct vam_parallel_plan {
     int n_tasks_paired;
     int2* d_tasks_single;   // (a, -1) for every angle
     float* d_vol_scratch;   // [nY][nX][nZ] masked copy of the input (VAM_ABS_MASK)
+    // matched-transpose weights: per pixel and angle, the first of <= 3
+    // detector rows (as int bits) and their summed forward tap weights
+    float4* d_adj_table;    // [nY*nX][nA]
+    int adj_table_abs;      // absorption mode the table was built for (-1: none built)
 };

@@ -53,6 +53,9 @@ class ParallelPlan:
         self._h = h
         self.absorption = None
         self.has_occlusion = False
+        self._adj_ready = False
+        # matched-transpose weight table: 16 B per pixel and angle (skipped above this size)
+        self.adj_table_limit_bytes = 8 << 30
 
     @property
     def handle(self):
@@ -84,6 +87,17 @@ class ParallelPlan:
                       float(radius_px), self._stream())
             torch.cuda.current_stream(self.device).synchronize()
         self.absorption = mode
+        self._adj_ready = False
+
+    def prepare_adjoint(self):
+        """Build the matched-transpose weight table (allocates; not during graph capture)."""
+        nbytes = 16 * self.shape_vol[0] * self.shape_vol[1] * self.angles.size
+        if nbytes > self.adj_table_limit_bytes:
+            return False
+        with torch.cuda.device(self.device):
+            _lib.call("vam_parallel_prepare_adjoint", self._h, self._stream())
+        self._adj_ready = True
+        return True
 
     def set_occlusion(self, insert):
         ins = torch.as_tensor(np.ascontiguousarray(np.atleast_3d(insert), dtype=np.float32), device=self.device)
@@ -128,6 +142,8 @@ class ParallelPlan:
 
     def adjoint(self, sino, out=None):
         self._check(sino, self.shape_sino, "adjoint input")
+        if not self._adj_ready and not torch.cuda.is_current_stream_capturing():
+            self.prepare_adjoint()
         if out is None:
             out = torch.empty(self.shape_vol, dtype=torch.float32, device=self.device)
         self._check(out, self.shape_vol, "adjoint output")
