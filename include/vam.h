@@ -208,6 +208,22 @@ enum vam_reduce_op { VAM_RED_MAX = 0, VAM_RED_MIN = 1, VAM_RED_SUM = 2 };
 int vam_reduce(const float* x_dev, int64_t n, int op, float* out_dev, void* work_dev,
                size_t work_bytes, vam_stream_t stream);
 
+/* Same reduction as vam_reduce for callers that cannot allocate device memory
+ * (code running between cudaStreamBeginCapture and EndCapture in global
+ * capture mode, where cudaMalloc is not permitted, or a host that reserves
+ * all device memory up front and must not trigger cudaMalloc's implicit
+ * synchronisation while a print is exposing).  No counterpart in the
+ * reference.  Its scratch is one static device array of 4096 doubles (32 KiB)
+ * inside the library, held on every GPU that loads it until process exit; one
+ * partial per 2048 inputs, so n is limited to 8388608 elements (larger n:
+ * VAM_ERR_SHAPE, nothing launched).  Allocates nothing and calls no
+ * allocating routine.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  All calls share the one array: calls that overlap on the GPU
+ * (different streams, no ordering) race; each call writes every partial it
+ * reads, so nothing carries over between calls. */
+int vam_reduce_noalloc(const float* x_dev, int64_t n, int op, float* out_dev, vam_stream_t stream);
+
 /* Volumetric error rate (vamtoolbox/metrics.py:47-87): out_dev[0] =
  * #(void >= min(gel)) / (#gel + #void).  mask_dev: 1 = gel, 2 = void, 0 = outside. */
 int vam_metric_ver(const float* x_dev, const uint8_t* mask_dev, int64_t n, float* out_dev,

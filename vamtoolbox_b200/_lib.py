@@ -87,6 +87,7 @@ _SIGS = {
     "vam_ray_active_at_cap": ([_vp, ctypes.POINTER(_c_i64)], _c_int),
     "vam_reduce_workspace_bytes": ([_c_i64], ctypes.c_size_t),
     "vam_reduce": ([_vp, _c_i64, _c_int, _vp, _vp, ctypes.c_size_t, _vp], _c_int),
+    "vam_reduce_noalloc": ([_vp, _c_i64, _c_int, _vp, _vp], _c_int),
     "vam_metric_ver": ([_vp, _vp, _c_i64, _vp, _vp, ctypes.c_size_t, _vp], _c_int),
     "vam_bclp_dose_pass": ([_vp, _vp, _c_i64, ctypes.POINTER(BclpParams), _vp, _vp, _vp, _vp, ctypes.c_size_t, _vp],
                            _c_int),

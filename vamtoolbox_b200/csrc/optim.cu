@@ -9,6 +9,8 @@
 #include <math.h>
 
 #include <cmath>
+#include <mutex>
+#include <string>
 
 #include "vam_internal.cuh"
 
@@ -333,6 +335,74 @@ extern "C" int vam_reduce(const float* x, int64_t n, int op, float* out, void* w
             return set_error(VAM_ERR_ARG, "vam_reduce: unknown op");
     }
     VAM_CHECK_LAUNCH("vam_reduce");
+    return VAM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// No-allocation reduction: scratch in a static device array
+// ---------------------------------------------------------------------------
+namespace vam {
+namespace {
+constexpr int kNoAllocMaxBlocks = 4096;                       // 32 KiB of partials
+constexpr int64_t kNoAllocPerBlock = (int64_t)kThreads * 8;  // inputs per partial
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) double g_noalloc_partials[kNoAllocMaxBlocks];
+
+std::mutex g_noalloc_mu;
+double* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_partials on the current device.  In host code
+// the symbol is only a host-side stand-in, never a device pointer, so the
+// address is looked up once per device and cached.
+int noalloc_scratch(double** out) {
+    int dev = -1;
+    VAM_TRY_CUDA(cudaGetDevice(&dev));
+    VAM_REQUIRE(dev >= 0 && dev < kNoAllocMaxDevices, VAM_ERR_ARG, "vam_reduce_noalloc: device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+        if (e != cudaSuccess || !p)
+            return set_error(VAM_ERR_CUDA, std::string("vam_reduce_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        g_noalloc_addr[dev] = static_cast<double*>(p);
+    }
+    *out = g_noalloc_addr[dev];
+    return VAM_OK;
+}
+}  // namespace
+}  // namespace vam
+
+extern "C" int vam_reduce_noalloc(const float* x, int64_t n, int op, float* out, vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(x && out, VAM_ERR_ARG, "vam_reduce_noalloc: null argument");
+    VAM_REQUIRE(n > 0, VAM_ERR_SHAPE, "vam_reduce_noalloc: empty input");
+    VAM_REQUIRE(op == VAM_RED_MAX || op == VAM_RED_MIN || op == VAM_RED_SUM, VAM_ERR_ARG, "vam_reduce_noalloc: unknown op");
+    const int64_t nb64 = (n + kNoAllocPerBlock - 1) / kNoAllocPerBlock;
+    VAM_REQUIRE(nb64 <= kNoAllocMaxBlocks, VAM_ERR_SHAPE,
+                "vam_reduce_noalloc: n = " + std::to_string((long long)n) + " exceeds the maximum of " +
+                    std::to_string((long long)kNoAllocMaxBlocks * kNoAllocPerBlock) + " elements (static scratch of " +
+                    std::to_string(kNoAllocMaxBlocks) + " partials)");
+    double* part = nullptr;
+    int rc = noalloc_scratch(&part);
+    if (rc != VAM_OK) return rc;
+    const int nb = (int)nb64;
+    cudaStream_t st = (cudaStream_t)stream;
+    switch (op) {
+        case VAM_RED_MAX:
+            k_reduce_partial<VAM_RED_MAX><<<nb, kThreads, 0, st>>>(x, n, part);
+            k_reduce_final<VAM_RED_MAX><<<1, kThreads, 0, st>>>(part, nb, out);
+            break;
+        case VAM_RED_MIN:
+            k_reduce_partial<VAM_RED_MIN><<<nb, kThreads, 0, st>>>(x, n, part);
+            k_reduce_final<VAM_RED_MIN><<<1, kThreads, 0, st>>>(part, nb, out);
+            break;
+        default:
+            k_reduce_partial<VAM_RED_SUM><<<nb, kThreads, 0, st>>>(x, n, part);
+            k_reduce_final<VAM_RED_SUM><<<1, kThreads, 0, st>>>(part, nb, out);
+            break;
+    }
+    VAM_CHECK_LAUNCH("vam_reduce_noalloc");
     return VAM_OK;
 }
 
