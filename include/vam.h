@@ -105,6 +105,21 @@ int vam_parallel_backward_ref(vam_parallel_plan* plan, const float* sino_dev, fl
 int vam_parallel_adjoint(vam_parallel_plan* plan, const float* sino_dev, float* vol_dev,
                          vam_stream_t stream);
 
+/* Launch shapes of the parallel-beam kernels, chosen per problem by an
+ * autotuner (vamtoolbox_b200/autotune.py times the candidates on the device
+ * and caches the winner per device and problem shape).  Vector widths are the
+ * slices each lane carries (4 or 8; 0 = automatic); backward_batch is the
+ * number of angles whose detector rows one warp loads together (1, 2 or 4);
+ * adjoint_table selects the table-driven transpose once it is prepared.
+ * No counterpart in the reference. */
+typedef struct {
+    int32_t forward_vz, backward_vz, adjoint_vz;
+    int32_t backward_batch;
+    int32_t adjoint_table;
+} vam_parallel_tuning;
+int vam_parallel_set_tuning(vam_parallel_plan* plan, const vam_parallel_tuning* tuning);
+int vam_parallel_get_tuning(vam_parallel_plan* plan, vam_parallel_tuning* tuning);
+
 /* Builds the plan's matched-transpose weight table (16 bytes per pixel and
  * angle: the detector rows that sample the pixel and their summed forward
  * weights), after which vam_parallel_adjoint is a pure gather.  Allocates;

@@ -214,3 +214,45 @@ def test_adjoint_without_weight_table(absn):
     b = rng.uniform(0, 1, (30, 18, 128))
     assert relL2(p.adjoint(dev(b)).cpu().numpy(), O.parallel_adjoint(b, ang, absorption=oabs)) < TOL
     assert not p._adj_ready
+
+
+TUNINGS = [dict(forward_vz=fv, backward_vz=bv, backward_batch=bb, adjoint_vz=av, adjoint_table=at)
+           for fv, (bv, bb), (av, at) in [(4, (4, 1), (4, 1)), (8, (8, 1), (8, 1)), (4, (4, 2), (4, 0)),
+                                          (8, (8, 2), (8, 0)), (4, (4, 4), (8, 1))]]
+
+
+@pytest.mark.parametrize("tuning", TUNINGS, ids=lambda t: "-".join(str(v) for v in t.values()))
+@pytest.mark.parametrize("absn", [None, "ray"])
+def test_every_launch_shape_matches_oracle(tuning, absn):
+    """Each launch shape the autotuner can pick (vector width, angle batch, table) gives the oracle's result,
+    including an angle count that is not a multiple of the batch and paired + unpaired angles."""
+    rng = np.random.default_rng(77)
+    shape = (29, 29, 256)
+    ang = np.concatenate([np.linspace(0, 360, 14, endpoint=False), [7.3, 101.9, 250.1]])
+    x = rng.uniform(0, 1, shape)
+    b = rng.uniform(0, 1, (shape[0], ang.size, shape[2]))
+    p = plan_for(shape, ang)
+    oabs = None
+    if absn == "ray":
+        p.set_absorption("ray", alpha_per_px=0.05, radius_px=12.5)
+        oabs = ("ray", 0.05, 12.5)
+    p.set_tuning(tuning)
+    assert p.get_tuning() == tuning
+    assert relL2(p.forward(dev(x)).cpu().numpy(), O.parallel_forward(x, ang, absorption=oabs)) < TOL
+    assert relL2(p.backward_ref(dev(b)).cpu().numpy(), O.parallel_backward_ref(b, ang, absorption=oabs)) < TOL
+    assert relL2(p.adjoint(dev(b)).cpu().numpy(), O.parallel_adjoint(b, ang, absorption=oabs)) < TOL
+
+
+def test_autotune_caches_winner(tmp_path, monkeypatch):
+    monkeypatch.setenv("VAMTOOLBOX_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
+    from vamtoolbox_b200 import autotune as AT
+
+    p = plan_for((40, 40, 128), np.linspace(0, 180, 30, endpoint=False))
+    first = p.autotune()
+    d = AT._load(str(tmp_path / "tune.json"))
+    key = AT.problem_key(p)
+    assert d[key]["tuning"] == first and set(d[key]["ms"]) == {"forward", "backward", "adjoint"}
+    q = plan_for((40, 40, 128), np.linspace(0, 180, 30, endpoint=False))
+    assert q.autotune() == first
+    with pytest.raises(Exception):
+        q.set_tuning({"backward_batch": 3})

@@ -58,6 +58,11 @@ class RayMedium(ctypes.Structure):
                 ("absorb_at_grid_dev", _vp)]
 
 
+class ParallelTuning(ctypes.Structure):
+    _fields_ = [("forward_vz", _c_i32), ("backward_vz", _c_i32), ("adjoint_vz", _c_i32),
+                ("backward_batch", _c_i32), ("adjoint_table", _c_i32)]
+
+
 class BclpParams(ctypes.Structure):
     _fields_ = [("table_f", _vp), ("table_map", _vp), ("table_dmap", _vp), ("n_table", _c_i32),
                 ("table_f0", _c_f), ("table_inv_step", _c_f),
@@ -78,6 +83,8 @@ _SIGS = {
     "vam_parallel_backward_ref": ([_vp, _vp, _vp, _vp], _c_int),
     "vam_parallel_adjoint": ([_vp, _vp, _vp, _vp], _c_int),
     "vam_parallel_prepare_adjoint": ([_vp, _vp], _c_int),
+    "vam_parallel_set_tuning": ([_vp, ctypes.POINTER(ParallelTuning)], _c_int),
+    "vam_parallel_get_tuning": ([_vp, ctypes.POINTER(ParallelTuning)], _c_int),
     "vam_ray_plan_create": ([ctypes.POINTER(RayGeom), _vp, _vp, _c_f, ctypes.POINTER(_vp)], _c_int),
     "vam_ray_plan_destroy": ([_vp], _c_int),
     "vam_ray_set_medium": ([_vp, ctypes.POINTER(RayMedium), _vp], _c_int),

@@ -654,6 +654,87 @@ __global__ void __launch_bounds__(256) k_adjoint_table(Args a, const float4* __r
     store_vz<VZ>(a.out + (size_t)p * a.nZ + z0, acc, qn);
 }
 
+// ---------------------------------------------------------------------------
+// R2 backprojection, batched: cos / sin of every angle staged in shared
+// memory, and B angles per step whose detector-row loads are all issued
+// before any is consumed, so each warp keeps 2B row loads in flight instead
+// of waiting on one angle's float64 chain and loads at a time.
+// ---------------------------------------------------------------------------
+template <int VZ, int B, bool RAY>
+__global__ void __launch_bounds__(256) k_backward_batched(Args a) {
+    extern __shared__ double2 s_cs[];
+    for (int t = threadIdx.x; t < a.nA; t += blockDim.x) s_cs[t] = make_double2(a.trig[t].x, a.trig[t].y);
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const long item = (long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+    const int zc = (int)(item % a.zchunks);
+    const long p = item / a.zchunks;
+    if (p >= (long)a.nY * a.nX) return;
+    const int i = (int)(p / a.nX), j = (int)(p % a.nX);
+    int z0, qn;
+    lane_z<VZ>(zc, lane, a.nZ, z0, qn);
+    if (qn == 0) return;
+    float acc[VZ];
+#pragma unroll
+    for (int e = 0; e < VZ; ++e) acc[e] = 0.f;
+    if (a.circle[p]) {
+        const double X = (double)(j - a.C), Y = (double)(i - a.C);
+        const double tlo = (double)(-a.C), thi = (double)(a.nY - 1 - a.C);
+        const size_t rs = (size_t)a.nA * a.nZ;
+        const float* __restrict__ bz = a.in + z0;
+        for (int th0 = 0; th0 < a.nA; th0 += B) {
+            size_t o0[B], o1[B];
+            float w[B], f[B];
+            bool ok[B];
+#pragma unroll
+            for (int u = 0; u < B; ++u) {
+                const int th = th0 + u;
+                ok[u] = th < a.nA;
+                const double2 cs = s_cs[ok[u] ? th : 0];
+                const double t = __dsub_rn(__dmul_rn(X, cs.x), __dmul_rn(Y, cs.y));
+                ok[u] = ok[u] && (t >= tlo && t <= thi);
+                const double ft = floor(t);
+                const int j0 = ok[u] ? (int)ft + a.C : 0;
+                w[u] = (float)(t - ft);
+                o0[u] = (size_t)j0 * rs + (size_t)th * a.nZ;
+                o1[u] = o0[u] + ((t != ft) ? rs : 0);
+                f[u] = 1.f;
+                if (RAY) {
+                    f[u] = 0.f;
+                    if (fabs(t) <= (double)a.R) {
+                        const float sv = (float)__dadd_rn(__dmul_rn(X, cs.y), __dmul_rn(Y, cs.x));
+                        f[u] = ray_factor(sv, (float)(-sqrt((double)a.R * a.R - t * t)), a.alpha);
+                    }
+                }
+            }
+            float v0[B][VZ], v1[B][VZ];
+#pragma unroll
+            for (int u = 0; u < B; ++u) {
+                if (ok[u]) {
+                    load_vz<VZ>(bz + o0[u], v0[u], qn);
+                    load_vz<VZ>(bz + o1[u], v1[u], qn);
+                } else {
+#pragma unroll
+                    for (int e = 0; e < VZ; ++e) v0[u][e] = v1[u][e] = 0.f;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < B; ++u)
+#pragma unroll
+                for (int e = 0; e < VZ; ++e) {
+                    const float v = fmaf(w[u], v1[u][e] - v0[u][e], v0[u][e]);
+                    acc[e] = RAY ? fmaf(v, f[u], acc[e]) : acc[e] + v;
+                }
+        }
+    }
+    if (a.mask) {
+        const float m = __ldg(a.mask + p);
+#pragma unroll
+        for (int e = 0; e < VZ; ++e) acc[e] = m * acc[e];
+    }
+    store_vz<VZ>(a.out + (size_t)p * a.nZ + z0, acc, qn);
+}
+
 __global__ void k_mask_mul(const float* __restrict__ x, const float* __restrict__ mask, float* __restrict__ out,
                            long npix, int nZ) {
     const long n = npix * nZ;
@@ -982,7 +1063,11 @@ int run(vam_parallel_plan* plan, Op op, const float* in, float* out, cudaStream_
     VAM_REQUIRE(plan && in && out, VAM_ERR_ARG, std::string(name) + ": null argument");
     DeviceGuard g(plan->device);
     VAM_REQUIRE(g.ok, VAM_ERR_CUDA, std::string(name) + ": cannot select device");
-    const int vzf = fast_vz(plan->nZ, (((uintptr_t)in | (uintptr_t)out) & 31) == 0);
+    int vzf = fast_vz(plan->nZ, (((uintptr_t)in | (uintptr_t)out) & 31) == 0);
+    if (vzf) {  // tuned vector width (4 or 8 slices per lane), when it fits the slice count
+        const int want = op == Op::Forward ? plan->tune_fwd_vz : (op == Op::BackwardRef ? plan->tune_bwd_vz : plan->tune_adj_vz);
+        if (want == 4 || (want == 8 && fast_vz(plan->nZ, true) == 8)) vzf = want;
+    }
     if (op == Op::Forward && !plan->has_occ && (long)plan->nY * plan->nX * plan->nZ < (1L << 31) && vzf)
         return run_forward_fast(plan, in, out, st, vzf);
     if (op != Op::Forward && !plan->has_occ && vzf) {
@@ -997,9 +1082,23 @@ int run(vam_parallel_plan* plan, Op op, const float* in, float* out, cudaStream_
         dim3 grid((unsigned)((items + kWarpsPerBlock - 1) / kWarpsPerBlock)), block(kWarpsPerBlock * kWarp);
         const bool ray = plan->abs_mode == VAM_ABS_RAY;
         if (op == Op::BackwardRef) {
-            if (vzf == 8) { if (ray) k_backward_fast<8, true><<<grid, block, 0, st>>>(a); else k_backward_fast<8, false><<<grid, block, 0, st>>>(a); }
+            // the batched kernel stages cos / sin of every angle in shared memory (16 B per angle)
+            const int batch = (size_t)plan->nA * sizeof(double2) <= 48 * 1024 ? plan->tune_bwd_batch : 1;
+            if (batch >= 2) {
+                const size_t smem = sizeof(double2) * plan->nA;
+                if (vzf == 8) {
+                    if (ray) k_backward_batched<8, 2, true><<<grid, block, smem, st>>>(a);
+                    else k_backward_batched<8, 2, false><<<grid, block, smem, st>>>(a);
+                } else if (batch >= 4) {
+                    if (ray) k_backward_batched<4, 4, true><<<grid, block, smem, st>>>(a);
+                    else k_backward_batched<4, 4, false><<<grid, block, smem, st>>>(a);
+                } else {
+                    if (ray) k_backward_batched<4, 2, true><<<grid, block, smem, st>>>(a);
+                    else k_backward_batched<4, 2, false><<<grid, block, smem, st>>>(a);
+                }
+            } else if (vzf == 8) { if (ray) k_backward_fast<8, true><<<grid, block, 0, st>>>(a); else k_backward_fast<8, false><<<grid, block, 0, st>>>(a); }
             else { if (ray) k_backward_fast<4, true><<<grid, block, 0, st>>>(a); else k_backward_fast<4, false><<<grid, block, 0, st>>>(a); }
-        } else if (plan->d_adj_table && plan->adj_table_abs == plan->abs_mode) {
+        } else if (plan->d_adj_table && plan->adj_table_abs == plan->abs_mode && plan->tune_adj_table) {
             if (vzf == 8) k_adjoint_table<8><<<grid, block, 0, st>>>(a, plan->d_adj_table);
             else k_adjoint_table<4><<<grid, block, 0, st>>>(a, plan->d_adj_table);
         } else {
@@ -1065,6 +1164,8 @@ extern "C" int vam_parallel_plan_create(const vam_parallel_geom* geom, vam_paral
     p->C = geom->n_y / 2;
     p->device = geom->device;
     p->adj_table_abs = -1;
+    p->tune_bwd_batch = 2;
+    p->tune_adj_table = 1;
     // per-angle tables exactly as numpy evaluates them (Projector3DParallel.py:135-143)
     std::vector<double4> trig(p->nA);
     for (int i = 0; i < p->nA; ++i) {
@@ -1195,6 +1296,33 @@ extern "C" int vam_parallel_get_occlusion_sinogram(vam_parallel_plan* p, float* 
     DeviceGuard g(p->device);
     VAM_TRY_CUDA(cudaMemcpyAsync(out_dev, p->d_occ, sizeof(float) * (size_t)p->nY * p->nA * p->nZ,
                                  cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+    return VAM_OK;
+}
+
+extern "C" int vam_parallel_set_tuning(vam_parallel_plan* p, const vam_parallel_tuning* t) {
+    clear_error();
+    VAM_REQUIRE(p && t, VAM_ERR_ARG, "vam_parallel_set_tuning: null argument");
+    auto vz_ok = [](int v) { return v == 0 || v == 4 || v == 8; };
+    VAM_REQUIRE(vz_ok(t->forward_vz) && vz_ok(t->backward_vz) && vz_ok(t->adjoint_vz), VAM_ERR_ARG,
+                "vam_parallel_set_tuning: vector widths must be 0 (auto), 4 or 8");
+    VAM_REQUIRE(t->backward_batch == 0 || t->backward_batch == 1 || t->backward_batch == 2 || t->backward_batch == 4,
+                VAM_ERR_ARG, "vam_parallel_set_tuning: backward_batch must be 0 (auto), 1, 2 or 4");
+    p->tune_fwd_vz = t->forward_vz;
+    p->tune_bwd_vz = t->backward_vz;
+    p->tune_adj_vz = t->adjoint_vz;
+    p->tune_bwd_batch = t->backward_batch == 0 ? 2 : t->backward_batch;
+    p->tune_adj_table = t->adjoint_table;
+    return VAM_OK;
+}
+
+extern "C" int vam_parallel_get_tuning(vam_parallel_plan* p, vam_parallel_tuning* t) {
+    clear_error();
+    VAM_REQUIRE(p && t, VAM_ERR_ARG, "vam_parallel_get_tuning: null argument");
+    t->forward_vz = p->tune_fwd_vz;
+    t->backward_vz = p->tune_bwd_vz;
+    t->adjoint_vz = p->tune_adj_vz;
+    t->backward_batch = p->tune_bwd_batch;
+    t->adjoint_table = p->tune_adj_table;
     return VAM_OK;
 }
 

@@ -53,6 +53,10 @@ struct RayArgs {
     double inv_voxel[3];  // 1/voxel (0 for a 2D z axis)
     float half_span_f[3], inv_voxel_f[3];
     double bmax[3], bmin[3];  // exit bounds: max + voxel, min - voxel
+    // the same bounds as float32 thresholds that decide every float32 x exactly
+    // as the float64 compare does: x > bmax <=> x > bmax_f (bmax rounded down),
+    // x < bmin <=> x < bmin_f (bmin rounded up)
+    float bmax_f[3], bmin_f[3];
     float h;              // parameter step, float32 as the reference multiplies it
     float h_idx;          // step / voxel_x
     int max_steps, check, twod;
@@ -79,10 +83,11 @@ __device__ __forceinline__ float unnorm(float x, float nrm, int size, bool borde
 // coordinate is clamped into [0, size-1], so the upper corner is out of range
 // only when its weight is exactly 0; clamping its index keeps every load in
 // bounds without a branch.
-__device__ __forceinline__ float4 sample_n(const RayArgs& a, const float* x) {
-    const float ix = unnorm(x[0], a.norm[0], a.nx, true);
-    const float iy = unnorm(x[1], a.norm[1], a.ny, true);
-    const float iz = unnorm(x[2], a.norm[2], a.nz, true);
+// u: the unclamped unnormalised coordinates (unnorm with border = false)
+__device__ __forceinline__ float4 sample_n(const RayArgs& a, const float* u) {
+    const float ix = fminf((float)(a.nx - 1), fmaxf(u[0], 0.f));
+    const float iy = fminf((float)(a.ny - 1), fmaxf(u[1], 0.f));
+    const float iz = fminf((float)(a.nz - 1), fmaxf(u[2], 0.f));
     const float fx = floorf(ix), fy = floorf(iy), fz = floorf(iz);
     const int x0 = (int)fx, y0 = (int)fy, z0 = (int)fz;
     const int x1 = min(x0 + 1, a.nx - 1), y1 = min(y0 + 1, a.ny - 1), z1 = min(z0 + 1, a.nz - 1);
@@ -105,9 +110,16 @@ __device__ __forceinline__ float4 sample_n(const RayArgs& a, const float* x) {
 }
 
 // (n, grad n) at x for the configured index kind (medium.py:276-473)
-__device__ __forceinline__ void index_at(const RayArgs& a, const float* x, float& n, float* gn) {
+__device__ __forceinline__ void grid_coords(const RayArgs& a, const float* x, float* u) {
+    u[0] = unnorm(x[0], a.norm[0], a.nx, false);
+    u[1] = unnorm(x[1], a.norm[1], a.ny, false);
+    u[2] = unnorm(x[2], a.norm[2], a.nz, false);
+}
+
+// u: grid_coords(x), read only by the GRID kind
+__device__ __forceinline__ void index_at(const RayArgs& a, const float* x, const float* u, float& n, float* gn) {
     if (a.n_kind == VAM_INDEX_GRID) {
-        const float4 t = sample_n(a, x);
+        const float4 t = sample_n(a, u);
         n = t.x; gn[0] = t.y; gn[1] = t.z; gn[2] = t.w;
     } else if (a.n_kind == VAM_INDEX_LUNEBURG) {
         const float r = sqrtf(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
@@ -126,16 +138,15 @@ __device__ __forceinline__ void index_at(const RayArgs& a, const float* x, float
 }
 
 // attenuation coefficient at x (medium.py:753-915; GRID uses zero padding)
-__device__ __forceinline__ float alpha_at(const RayArgs& a, const float* x) {
+// u: grid_coords(x), read only by the GRID kind
+__device__ __forceinline__ float alpha_at(const RayArgs& a, const float* x, const float* u) {
     if (a.a_kind == VAM_ALPHA_CYLINDER || a.a_kind == VAM_ALPHA_BALL) {
         float r2 = x[0] * x[0] + x[1] * x[1];
         if (a.a_kind == VAM_ALPHA_BALL) r2 += x[2] * x[2];
         return sqrtf(r2) < a.a_R ? a.a_val : 0.f;
     }
     if (a.a_kind != VAM_ALPHA_GRID) return 0.f;
-    const float ix = unnorm(x[0], a.norm[0], a.nx, false);
-    const float iy = unnorm(x[1], a.norm[1], a.ny, false);
-    const float iz = unnorm(x[2], a.norm[2], a.nz, false);
+    const float ix = u[0], iy = u[1], iz = u[2];
     // far outside the grid every corner is zero padding
     if (!(ix > -1.f && ix < (float)a.nx && iy > -1.f && iy < (float)a.ny && iz > -1.f && iz < (float)a.nz)) return 0.f;
     const float fx = floorf(ix), fy = floorf(iy), fz = floorf(iz);
@@ -188,8 +199,9 @@ __device__ __forceinline__ void ray_init(const RayArgs& a, int64_t r, float E0, 
     st.E = E0;
     st.active = true;
     if (a.solver == VAM_ODE_LEAPFROG) {  // half step back in v (pyTorchRayTrace.py:816-828)
-        float n, gn[3], dv[3];
-        index_at(a, st.xp, n, gn);
+        float n, gn[3], dv[3], u[3];
+        grid_coords(a, st.xp, u);
+        index_at(a, st.xp, u, n, gn);
         dv_dstep(a, n, gn, dv);
 #pragma unroll
         for (int d = 0; d < 3; ++d) st.vp[d] = st.vp[d] - dv[d] * a.h / 2.f;
@@ -201,8 +213,9 @@ __device__ __forceinline__ void ray_init(const RayArgs& a, int64_t r, float E0, 
 __device__ __forceinline__ void ray_step(const RayArgs& a, RayState& st, float& ds, float& alpha) {
 #pragma unroll
     for (int d = 0; d < 3; ++d) { st.xi[d] = st.xp[d]; st.vi[d] = st.vp[d]; }
-    float n, gn[3], dv[3], dx[3];
-    index_at(a, st.xi, n, gn);
+    float n, gn[3], dv[3], dx[3], u[3];
+    grid_coords(a, st.xi, u);
+    index_at(a, st.xi, u, n, gn);
     dv_dstep(a, n, gn, dv);
 #pragma unroll
     for (int d = 0; d < 3; ++d) st.vp[d] = st.vi[d] + dv[d] * a.h;
@@ -211,19 +224,21 @@ __device__ __forceinline__ void ray_step(const RayArgs& a, RayState& st, float& 
 #pragma unroll
     for (int d = 0; d < 3; ++d) { dx[d] = dx[d] * a.h; st.xp[d] = st.xi[d] + dx[d]; }
     ds = sqrtf(dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2]);
-    alpha = alpha_at(a, st.xi);
+    alpha = alpha_at(a, st.xi, u);
     st.att = st.att + alpha * ds;
     st.E = st.E0 * __expf(-st.att);
 }
 
 // Exit test of pyTorchRayTrace.py:1343-1424 (position past max+voxel moving
-// outward, or below min-voxel moving inward's opposite), float64 bounds.
+// outward, or below min-voxel moving inward's opposite).  The reference
+// compares against float64 bounds; the float32 thresholds give the same answer
+// for every float32 position.
 __device__ __forceinline__ bool exited(const RayArgs& a, const RayState& st) {
     bool ex = false;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        const double x = (double)st.xp[d];
-        ex |= (x > a.bmax[d] && st.vp[d] > 0.f) || (x < a.bmin[d] && st.vp[d] < 0.f);
+        const float x = st.xp[d];
+        ex |= (x > a.bmax_f[d] && st.vp[d] > 0.f) || (x < a.bmin_f[d] && st.vp[d] < 0.f);
     }
     return ex;
 }
@@ -266,9 +281,40 @@ __device__ __forceinline__ void corners_at(const RayArgs& a, const float* x, Cor
     }
 }
 
+// The 4 (2-D) or 8 corners of a Corners set as element offsets into an
+// [nx][ny][nz] field, their trilinear weights (x weight * y weight * z weight,
+// the reference's product order) and whether each lies inside the grid.
+// Offsets of outside corners are clamped into the grid and never dereferenced.
+template <bool TWOD>
+struct CornerList {
+    static constexpr int kN = TWOD ? 4 : 8;
+    int off[kN];
+    float w[kN];
+    bool in[kN];
+};
+
+template <bool TWOD>
+__device__ __forceinline__ void corner_list(const RayArgs& a, const Corners& c, CornerList<TWOD>& L) {
+    const int sx = a.ny * a.nz, sy = a.nz;
+    const bool vx0 = (unsigned)c.lo[0] < (unsigned)a.nx, vx1 = (unsigned)c.hi[0] < (unsigned)a.nx;
+    const bool vy0 = (unsigned)c.lo[1] < (unsigned)a.ny, vy1 = (unsigned)c.hi[1] < (unsigned)a.ny;
+    const bool vz0 = TWOD || (unsigned)c.lo[2] < (unsigned)a.nz, vz1 = TWOD || (unsigned)c.hi[2] < (unsigned)a.nz;
+    const int ox0 = min(max(c.lo[0], 0), a.nx - 1) * sx, ox1 = min(max(c.hi[0], 0), a.nx - 1) * sx;
+    const int oy0 = min(max(c.lo[1], 0), a.ny - 1) * sy, oy1 = min(max(c.hi[1], 0), a.ny - 1) * sy;
+    const int oz0 = TWOD ? 0 : min(max(c.lo[2], 0), a.nz - 1), oz1 = TWOD ? 0 : min(max(c.hi[2], 0), a.nz - 1);
+#pragma unroll
+    for (int cn = 0; cn < CornerList<TWOD>::kN; ++cn) {
+        L.in[cn] = ((cn & 1) ? vx1 : vx0) && ((cn & 2) ? vy1 : vy0) && ((cn & 4) ? vz1 : vz0);
+        L.off[cn] = ((cn & 1) ? ox1 : ox0) + ((cn & 2) ? oy1 : oy0) + ((cn & 4) ? oz1 : oz0);
+        L.w[cn] = ((cn & 1) ? c.whi[0] : c.wlo[0]) * ((cn & 2) ? c.whi[1] : c.wlo[1]) *
+                  ((cn & 4) ? c.whi[2] : c.wlo[2]);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // integrate (forward)
 // ---------------------------------------------------------------------------
+template <bool TWOD>
 __global__ void __launch_bounds__(kRayThreads) k_ray_integrate(RayArgs a, const float* __restrict__ fa,
                                                                float* __restrict__ g) {
     const int64_t r = (int64_t)blockIdx.x * kRayThreads + threadIdx.x;
@@ -276,26 +322,23 @@ __global__ void __launch_bounds__(kRayThreads) k_ray_integrate(RayArgs a, const 
     RayState st;
     ray_init(a, r, a.energy0, st);
     float integral = 0.f;
-    const int ncorner = a.twod ? 4 : 8;
+    int until_check = 0;  // the exit test runs at steps 0, check, 2 check, ...
     for (int step = 0; step < a.max_steps; ++step) {
-        if (st.active) {
-            float ds, alpha;
-            ray_step(a, st, ds, alpha);
-            Corners c;
-            corners_at(a, st.xp, c);
-            const float eh = a.h_idx * st.E;
-            for (int cn = 0; cn < ncorner; ++cn) {
-                const int X = (cn & 1) ? c.hi[0] : c.lo[0];
-                const int Y = (cn & 2) ? c.hi[1] : c.lo[1];
-                const int Z = (cn & 4) ? c.hi[2] : c.lo[2];
-                if ((unsigned)X >= (unsigned)a.nx || (unsigned)Y >= (unsigned)a.ny || (unsigned)Z >= (unsigned)a.nz)
-                    continue;
-                const float w = ((cn & 1) ? c.whi[0] : c.wlo[0]) * ((cn & 2) ? c.whi[1] : c.wlo[1]) *
-                                ((cn & 4) ? c.whi[2] : c.wlo[2]);
-                integral = fmaf(__ldg(fa + ((size_t)X * a.ny + Y) * a.nz + Z), w * eh, integral);
-            }
-            if (step % a.check == 0 && exited(a, st)) st.active = false;
+        float ds, alpha;
+        ray_step(a, st, ds, alpha);
+        Corners c;
+        corners_at(a, st.xp, c);
+        CornerList<TWOD> L;
+        corner_list<TWOD>(a, c, L);
+        const float eh = a.h_idx * st.E;
+#pragma unroll
+        for (int cn = 0; cn < CornerList<TWOD>::kN; ++cn)
+            if (L.in[cn]) integral = fmaf(__ldg(fa + L.off[cn]), L.w[cn] * eh, integral);
+        if (until_check == 0) {
+            until_check = a.check;
+            if (exited(a, st)) { st.active = false; break; }
         }
+        --until_check;
     }
     g[r] = integral;
     if (st.active) atomicAdd(a.active, 1ULL);
@@ -304,36 +347,33 @@ __global__ void __launch_bounds__(kRayThreads) k_ray_integrate(RayArgs a, const 
 // ---------------------------------------------------------------------------
 // deposit (adjoint)
 // ---------------------------------------------------------------------------
+template <bool TWOD>
 __global__ void __launch_bounds__(kRayThreads) k_ray_deposit(RayArgs a, const float* __restrict__ gin,
                                                              float* __restrict__ dose) {
     const int64_t r = (int64_t)blockIdx.x * kRayThreads + threadIdx.x;
     if (r >= a.nr) return;
     RayState st;
     ray_init(a, r, gin[r], st);
-    const int ncorner = a.twod ? 4 : 8;
     const bool zero = st.E0 == 0.f;  // a zero-energy ray deposits nothing; still traced for the cap count
+    int until_check = 0;
     for (int step = 0; step < a.max_steps; ++step) {
-        if (st.active) {
-            float ds, alpha;
-            ray_step(a, st, ds, alpha);
-            if (!zero) {
-                Corners c;
-                corners_at(a, st.xp, c);
-                const float eh = a.h_idx * st.E;
-                for (int cn = 0; cn < ncorner; ++cn) {
-                    const int X = (cn & 1) ? c.hi[0] : c.lo[0];
-                    const int Y = (cn & 2) ? c.hi[1] : c.lo[1];
-                    const int Z = (cn & 4) ? c.hi[2] : c.lo[2];
-                    if ((unsigned)X >= (unsigned)a.nx || (unsigned)Y >= (unsigned)a.ny ||
-                        (unsigned)Z >= (unsigned)a.nz)
-                        continue;
-                    const float w = ((cn & 1) ? c.whi[0] : c.wlo[0]) * ((cn & 2) ? c.whi[1] : c.wlo[1]) *
-                                    ((cn & 4) ? c.whi[2] : c.wlo[2]);
-                    atomicAdd(dose + ((size_t)X * a.ny + Y) * a.nz + Z, w * eh);
-                }
-            }
-            if (step % a.check == 0 && exited(a, st)) st.active = false;
+        float ds, alpha;
+        ray_step(a, st, ds, alpha);
+        if (!zero) {
+            Corners c;
+            corners_at(a, st.xp, c);
+            CornerList<TWOD> L;
+            corner_list<TWOD>(a, c, L);
+            const float eh = a.h_idx * st.E;
+#pragma unroll
+            for (int cn = 0; cn < CornerList<TWOD>::kN; ++cn)
+                if (L.in[cn]) atomicAdd(dose + L.off[cn], L.w[cn] * eh);
         }
+        if (until_check == 0) {
+            until_check = a.check;
+            if (exited(a, st)) { st.active = false; break; }
+        }
+        --until_check;
     }
     if (st.active) atomicAdd(a.active, 1ULL);
 }
@@ -341,36 +381,32 @@ __global__ void __launch_bounds__(kRayThreads) k_ray_deposit(RayArgs a, const fl
 // ---------------------------------------------------------------------------
 // d<w, integrate(f)>/d alpha_att: pass 1 totals, pass 2 suffix sums
 // ---------------------------------------------------------------------------
+template <bool TWOD>
 __global__ void __launch_bounds__(kRayThreads) k_ray_grad_att(RayArgs a, const float* __restrict__ fa,
                                                               const float* __restrict__ w, float* __restrict__ grad) {
     const int64_t r = (int64_t)blockIdx.x * kRayThreads + threadIdx.x;
     if (r >= a.nr) return;
     const float wr = w[r];
     if (wr == 0.f) return;
-    const int ncorner = a.twod ? 4 : 8;
     float total = 0.f;
     for (int pass = 0; pass < 2; ++pass) {
         RayState st;
         ray_init(a, r, a.energy0, st);
         float prefix = 0.f;
+        int until_check = 0;
         for (int step = 0; step < a.max_steps; ++step) {
             if (!st.active) break;
             float ds, alpha;
             ray_step(a, st, ds, alpha);
             Corners c;
             corners_at(a, st.xp, c);
+            CornerList<TWOD> L;
+            corner_list<TWOD>(a, c, L);
             const float eh = a.h_idx * st.E;
             float contrib = 0.f;
-            for (int cn = 0; cn < ncorner; ++cn) {
-                const int X = (cn & 1) ? c.hi[0] : c.lo[0];
-                const int Y = (cn & 2) ? c.hi[1] : c.lo[1];
-                const int Z = (cn & 4) ? c.hi[2] : c.lo[2];
-                if ((unsigned)X >= (unsigned)a.nx || (unsigned)Y >= (unsigned)a.ny || (unsigned)Z >= (unsigned)a.nz)
-                    continue;
-                const float wt = ((cn & 1) ? c.whi[0] : c.wlo[0]) * ((cn & 2) ? c.whi[1] : c.wlo[1]) *
-                                 ((cn & 4) ? c.whi[2] : c.wlo[2]);
-                contrib = fmaf(__ldg(fa + ((size_t)X * a.ny + Y) * a.nz + Z), wt * eh, contrib);
-            }
+#pragma unroll
+            for (int cn = 0; cn < CornerList<TWOD>::kN; ++cn)
+                if (L.in[cn]) contrib = fmaf(__ldg(fa + L.off[cn]), L.w[cn] * eh, contrib);
             if (pass == 1 && ds > 0.f) {
                 // att(step) = sum alpha(x_i) ds  ->  d integral / d alpha(x_i at this step)
                 //   = -ds * (contributions of this and all later steps)
@@ -400,7 +436,11 @@ __global__ void __launch_bounds__(kRayThreads) k_ray_grad_att(RayArgs a, const f
                 }
             }
             prefix += contrib;
-            if (step % a.check == 0 && exited(a, st)) st.active = false;
+            if (until_check == 0) {
+                until_check = a.check;
+                if (exited(a, st)) st.active = false;
+            }
+            --until_check;
         }
         total = prefix;
     }
@@ -441,6 +481,10 @@ RayArgs make_args(const vam_ray_plan* p) {
         a.inv_voxel_f[d] = (float)a.inv_voxel[d];
         a.bmax[d] = g.coord_max[d] + g.voxel[d];
         a.bmin[d] = g.coord_min[d] - g.voxel[d];
+        a.bmax_f[d] = (float)a.bmax[d];
+        if (std::isfinite(a.bmax[d]) && (double)a.bmax_f[d] > a.bmax[d]) a.bmax_f[d] = std::nextafter(a.bmax_f[d], -INFINITY);
+        a.bmin_f[d] = (float)a.bmin[d];
+        if (std::isfinite(a.bmin[d]) && (double)a.bmin_f[d] < a.bmin[d]) a.bmin_f[d] = std::nextafter(a.bmin_f[d], INFINITY);
     }
     a.h = (float)g.step_size;
     a.h_idx = (float)(g.step_size / g.voxel[0]);
@@ -483,6 +527,8 @@ extern "C" int vam_ray_plan_create(const vam_ray_geom* geom, const float* x0, co
                 VAM_ERR_ARG, "vam_ray_plan_create: step size and voxel must be positive");
     VAM_REQUIRE(g.n_z > 1 ? (std::isfinite(g.voxel[2]) && g.voxel[2] > 0.0) : true, VAM_ERR_ARG,
                 "vam_ray_plan_create: 3D grid needs a finite voxel[2]");
+    VAM_REQUIRE((int64_t)g.n_x * g.n_y * g.n_z < ((int64_t)1 << 31), VAM_ERR_SHAPE,
+                "vam_ray_plan_create: the grid must have fewer than 2^31 voxels");
     DeviceGuard dg(g.device);
     VAM_REQUIRE(dg.ok, VAM_ERR_CUDA, "vam_ray_plan_create: cannot select device");
     auto* p = new vam_ray_plan();
@@ -560,7 +606,8 @@ extern "C" int vam_ray_integrate(vam_ray_plan* p, const float* f, float* g, vam_
     VAM_TRY_CUDA(cudaMemsetAsync(p->d_active, 0, sizeof(unsigned long long), st));
     RayArgs a = make_args(p);
     const unsigned nb = (unsigned)((p->g.num_rays + kRayThreads - 1) / kRayThreads);
-    k_ray_integrate<<<nb, kRayThreads, 0, st>>>(a, p->d_scratch, g);
+    if (a.twod) k_ray_integrate<true><<<nb, kRayThreads, 0, st>>>(a, p->d_scratch, g);
+    else k_ray_integrate<false><<<nb, kRayThreads, 0, st>>>(a, p->d_scratch, g);
     VAM_CHECK_LAUNCH("k_ray_integrate");
     return VAM_OK;
 }
@@ -576,7 +623,8 @@ extern "C" int vam_ray_deposit(vam_ray_plan* p, const float* gin, float* dose, v
     VAM_TRY_CUDA(cudaMemsetAsync(p->d_active, 0, sizeof(unsigned long long), st));
     RayArgs a = make_args(p);
     const unsigned nb = (unsigned)((p->g.num_rays + kRayThreads - 1) / kRayThreads);
-    k_ray_deposit<<<nb, kRayThreads, 0, st>>>(a, gin, p->d_scratch);
+    if (a.twod) k_ray_deposit<true><<<nb, kRayThreads, 0, st>>>(a, gin, p->d_scratch);
+    else k_ray_deposit<false><<<nb, kRayThreads, 0, st>>>(a, gin, p->d_scratch);
     VAM_CHECK_LAUNCH("k_ray_deposit");
     k_mul<<<ew_blocks(nv), 256, 0, st>>>(p->d_scratch, p->d_absorb, dose, nv);
     VAM_CHECK_LAUNCH("k_mul");
@@ -597,7 +645,8 @@ extern "C" int vam_ray_grad_alpha(vam_ray_plan* p, const float* f, const float* 
     const unsigned nb = (unsigned)((p->g.num_rays + kRayThreads - 1) / kRayThreads);
     if (grad_att) {
         k_mul<<<ew_blocks(nv), 256, 0, st>>>(f, p->d_absorb, p->d_scratch, nv);
-        k_ray_grad_att<<<nb, kRayThreads, 0, st>>>(a, p->d_scratch, w, grad_att);
+        if (a.twod) k_ray_grad_att<true><<<nb, kRayThreads, 0, st>>>(a, p->d_scratch, w, grad_att);
+        else k_ray_grad_att<false><<<nb, kRayThreads, 0, st>>>(a, p->d_scratch, w, grad_att);
         VAM_CHECK_LAUNCH("k_ray_grad_att");
     }
     if (grad_abs) {
@@ -605,7 +654,8 @@ extern "C" int vam_ray_grad_alpha(vam_ray_plan* p, const float* f, const float* 
         VAM_TRY_CUDA(cudaMemsetAsync(p->d_active, 0, sizeof(unsigned long long), st));
         // deposit of w with unit start energy, times the forward's energy0:
         // sum_r w_r * energy0 * exp(-att) * (h/voxel) * w_corner at every voxel
-        k_ray_deposit<<<nb, kRayThreads, 0, st>>>(a, w, p->d_scratch);
+        if (a.twod) k_ray_deposit<true><<<nb, kRayThreads, 0, st>>>(a, w, p->d_scratch);
+        else k_ray_deposit<false><<<nb, kRayThreads, 0, st>>>(a, w, p->d_scratch);
         VAM_CHECK_LAUNCH("k_ray_deposit");
         k_mul_acc<<<ew_blocks(nv), 256, 0, st>>>(p->d_scratch, f, p->energy0, grad_abs, nv);
         VAM_CHECK_LAUNCH("k_mul_acc");

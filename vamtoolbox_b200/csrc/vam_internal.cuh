@@ -79,4 +79,6 @@ struct vam_parallel_plan {
     // detector rows (as int bits) and their summed forward tap weights
     float4* d_adj_table;    // [nY*nX][nA]
     int adj_table_abs;      // absorption mode the table was built for (-1: none built)
+    // tuning (vam_parallel_set_tuning): vector widths 0 = automatic
+    int tune_fwd_vz, tune_bwd_vz, tune_adj_vz, tune_bwd_batch, tune_adj_table;
 };

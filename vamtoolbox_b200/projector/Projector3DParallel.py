@@ -99,6 +99,30 @@ class ParallelPlan:
         self._adj_ready = True
         return True
 
+    _TUNING_FIELDS = ("forward_vz", "backward_vz", "adjoint_vz", "backward_batch", "adjoint_table")
+
+    def set_tuning(self, tuning):
+        """Set launch shapes: dict with any of forward_vz / backward_vz / adjoint_vz (0, 4, 8),
+        backward_batch (1, 2, 4) and adjoint_table (0, 1); missing keys keep their value."""
+        cur = self.get_tuning()
+        unknown = set(tuning) - set(self._TUNING_FIELDS)
+        if unknown:
+            raise KeyError(f"unknown tuning fields {sorted(unknown)}")
+        cur.update({k: int(v) for k, v in tuning.items()})
+        t = _lib.ParallelTuning(*(cur[k] for k in self._TUNING_FIELDS))
+        _lib.call("vam_parallel_set_tuning", self._h, ctypes.byref(t))
+
+    def get_tuning(self):
+        t = _lib.ParallelTuning()
+        _lib.call("vam_parallel_get_tuning", self._h, ctypes.byref(t))
+        return {k: int(getattr(t, k)) for k in self._TUNING_FIELDS}
+
+    def autotune(self, use_cache=True):
+        """Time the launch-shape candidates on this plan's device (or reuse the cached winner)."""
+        from ..autotune import autotune
+
+        return autotune(self, use_cache=use_cache)
+
     def set_occlusion(self, insert):
         ins = torch.as_tensor(np.ascontiguousarray(np.atleast_3d(insert), dtype=np.float32), device=self.device)
         if tuple(ins.shape) != self.shape_vol:
