@@ -108,7 +108,8 @@ int vam_parallel_adjoint(vam_parallel_plan* plan, const float* sino_dev, float* 
 /* Launch shapes of the parallel-beam kernels, chosen per problem by an
  * autotuner (vamtoolbox_b200/autotune.py times the candidates on the device
  * and caches the winner per device and problem shape).  Vector widths are the
- * slices each lane carries (4 or 8; 0 = automatic); backward_batch is the
+ * slices each lane of a fast kernel carries (4 or 8; 1 = the generic kernel;
+ * 0 = automatic; the fast kernels need nZ % 4 == 0); backward_batch is the
  * number of angles whose detector rows one warp loads together (1, 2 or 4);
  * adjoint_table selects the table-driven transpose once it is prepared.
  * No counterpart in the reference. */
@@ -119,6 +120,40 @@ typedef struct {
 } vam_parallel_tuning;
 int vam_parallel_set_tuning(vam_parallel_plan* plan, const vam_parallel_tuning* tuning);
 int vam_parallel_get_tuning(vam_parallel_plan* plan, vam_parallel_tuning* tuning);
+
+/* Batched calls over many plans (targets of uneven size, different angle
+ * counts, 2-D slices next to 3-D volumes) in ONE persistent launch fed by a
+ * device work queue.  Each work item is one forward / backward_ref / adjoint
+ * call exactly as the single-plan entry points describe it, and produces
+ * bit-identical results; items run concurrently, so no item may read another
+ * item's output or write another item's input or output.  A fast forward in
+ * mask mode uses its plan's scratch volume, so one plan appears at most once
+ * per batch with VAM_OP_FORWARD.
+ *
+ * The calls' descriptions travel by value in the launch's parameters (48
+ * calls per launch; longer lists become consecutive launches), so a submit
+ * makes no CUDA call but a counter reset and the launches: it is stream
+ * ordered, allocates nothing and may be captured in a CUDA graph with any
+ * list.  A batch object (its queue counters) is driven from one stream at a
+ * time.
+ *
+ * Replaces running the reference's per-target projector calls one target at a
+ * time (vamtoolbox/projector/Projector3DParallel.py:113-207 per target). */
+typedef struct vam_batch vam_batch;
+enum { VAM_OP_FORWARD = 0, VAM_OP_BACKWARD_REF = 1, VAM_OP_ADJOINT = 2 };
+typedef struct {
+    vam_parallel_plan* plan;
+    int32_t op;        /* VAM_OP_* */
+    const float* in;   /* volume (forward) or sinogram, device */
+    float* out;        /* sinogram (forward) or volume, device */
+} vam_work;
+int vam_batch_create(int32_t device, vam_batch** out);
+int vam_batch_destroy(vam_batch* batch);
+int vam_batch_submit(vam_batch* batch, const vam_work* work, int32_t n, vam_stream_t stream);
+/* validate and describe a work list without launching (reports a bad list before a capture) */
+int vam_batch_prepare(vam_batch* batch, const vam_work* work, int32_t n, vam_stream_t stream);
+/* blocks (over all calls' grids) of the last submitted list and persistent CTAs of its launch */
+int vam_batch_info(vam_batch* batch, int64_t* virtual_blocks, int32_t* ctas);
 
 /* Builds the plan's matched-transpose weight table (16 bytes per pixel and
  * angle: the detector rows that sample the pixel and their summed forward

@@ -218,7 +218,7 @@ def test_adjoint_without_weight_table(absn):
 
 TUNINGS = [dict(forward_vz=fv, backward_vz=bv, backward_batch=bb, adjoint_vz=av, adjoint_table=at)
            for fv, (bv, bb), (av, at) in [(4, (4, 1), (4, 1)), (8, (8, 1), (8, 1)), (4, (4, 2), (4, 0)),
-                                          (8, (8, 2), (8, 0)), (4, (4, 4), (8, 1))]]
+                                          (8, (8, 2), (8, 0)), (4, (4, 4), (8, 1)), (1, (1, 1), (1, 0))]]
 
 
 @pytest.mark.parametrize("tuning", TUNINGS, ids=lambda t: "-".join(str(v) for v in t.values()))

@@ -63,6 +63,13 @@ class ParallelTuning(ctypes.Structure):
                 ("backward_batch", _c_i32), ("adjoint_table", _c_i32)]
 
 
+OP_FORWARD, OP_BACKWARD_REF, OP_ADJOINT = 0, 1, 2
+
+
+class Work(ctypes.Structure):
+    _fields_ = [("plan", _vp), ("op", _c_i32), ("in_", _vp), ("out", _vp)]
+
+
 class BclpParams(ctypes.Structure):
     _fields_ = [("table_f", _vp), ("table_map", _vp), ("table_dmap", _vp), ("n_table", _c_i32),
                 ("table_f0", _c_f), ("table_inv_step", _c_f),
@@ -85,6 +92,11 @@ _SIGS = {
     "vam_parallel_prepare_adjoint": ([_vp, _vp], _c_int),
     "vam_parallel_set_tuning": ([_vp, ctypes.POINTER(ParallelTuning)], _c_int),
     "vam_parallel_get_tuning": ([_vp, ctypes.POINTER(ParallelTuning)], _c_int),
+    "vam_batch_create": ([_c_i32, ctypes.POINTER(_vp)], _c_int),
+    "vam_batch_destroy": ([_vp], _c_int),
+    "vam_batch_submit": ([_vp, ctypes.POINTER(Work), _c_i32, _vp], _c_int),
+    "vam_batch_prepare": ([_vp, ctypes.POINTER(Work), _c_i32, _vp], _c_int),
+    "vam_batch_info": ([_vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(_c_i32)], _c_int),
     "vam_ray_plan_create": ([ctypes.POINTER(RayGeom), _vp, _vp, _c_f, ctypes.POINTER(_vp)], _c_int),
     "vam_ray_plan_destroy": ([_vp], _c_int),
     "vam_ray_set_medium": ([_vp, ctypes.POINTER(RayMedium), _vp], _c_int),

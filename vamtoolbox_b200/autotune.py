@@ -21,9 +21,10 @@ import torch
 
 from . import _lib
 
-FORWARD_VZ = (4, 8)
-BACKWARD = ((4, 1), (8, 1), (4, 2), (8, 2), (4, 4))  # (slices per lane, angles per batch)
-ADJOINT = ((4, 1), (8, 1), (4, 0), (8, 0))           # (slices per lane, weight table on)
+# slices per lane: 1 = the generic kernel, 4 / 8 = the fast kernels (nZ % 4 == 0)
+FORWARD_VZ = (1, 4, 8)
+BACKWARD = ((1, 1), (4, 1), (8, 1), (4, 2), (8, 2), (4, 4))  # (slices per lane, angles per batch)
+ADJOINT = ((1, 0), (4, 1), (8, 1), (4, 0), (8, 0))           # (slices per lane, weight table on)
 
 _lock = threading.Lock()
 
@@ -75,40 +76,44 @@ def _time(fn, reps, warm):
     return best
 
 
-def measure(plan, reps=3, warm=1):
-    """Time every candidate on the plan's device; returns (tuning dict, timings in ms)."""
+def measure(plan, reps=3, warm=1, ops=("forward", "backward", "adjoint")):
+    """Time every candidate of ``ops`` on the plan's device; returns (tuning dict, timings in ms).
+    Ops left out keep the plan's current shape (the adjoint's weight table is then not built)."""
     dev = plan.device
     with torch.cuda.device(dev):
         g = torch.Generator(device=dev).manual_seed(0)
         x = torch.rand(plan.shape_vol, device=dev, generator=g)
         b = torch.rand(plan.shape_sino, device=dev, generator=g)
         ob, ox = torch.empty_like(b), torch.empty_like(x)
-        table = plan.prepare_adjoint()
+        table = plan.prepare_adjoint() if "adjoint" in ops else False
         times = {"forward": {}, "backward": {}, "adjoint": {}}
         base = plan.get_tuning()
-        for vz in FORWARD_VZ:
+        for vz in FORWARD_VZ if "forward" in ops else ():
             plan.set_tuning(dict(base, forward_vz=vz))
             times["forward"][str(vz)] = _time(lambda: plan.forward(x, ob), reps, warm)
-        for vz, bt in BACKWARD:
+        for vz, bt in BACKWARD if "backward" in ops else ():
             plan.set_tuning(dict(base, backward_vz=vz, backward_batch=bt))
             times["backward"][f"{vz},{bt}"] = _time(lambda: plan.backward_ref(b, ox), reps, warm)
-        for vz, tb in ADJOINT:
+        for vz, tb in ADJOINT if "adjoint" in ops else ():
             if tb and not table:
                 continue
             plan.set_tuning(dict(base, adjoint_vz=vz, adjoint_table=tb))
             times["adjoint"][f"{vz},{tb}"] = _time(lambda: plan.adjoint(b, ox), reps, warm)
         plan.set_tuning(base)
-    fv = int(min(times["forward"], key=times["forward"].get))
-    bv, bb = map(int, min(times["backward"], key=times["backward"].get).split(","))
-    av, at = map(int, min(times["adjoint"], key=times["adjoint"].get).split(","))
-    best = dict(forward_vz=fv, backward_vz=bv, backward_batch=bb, adjoint_vz=av, adjoint_table=at)
+    best = dict(base)
+    if times["forward"]:
+        best["forward_vz"] = int(min(times["forward"], key=times["forward"].get))
+    if times["backward"]:
+        best["backward_vz"], best["backward_batch"] = map(int, min(times["backward"], key=times["backward"].get).split(","))
+    if times["adjoint"]:
+        best["adjoint_vz"], best["adjoint_table"] = map(int, min(times["adjoint"], key=times["adjoint"].get).split(","))
     return best, times
 
 
-def autotune(plan, use_cache=True, reps=3, warm=1):
+def autotune(plan, use_cache=True, reps=3, warm=1, ops=("forward", "backward", "adjoint")):
     """Apply the cached or freshly measured best launch shapes to ``plan``; returns them."""
     path = cache_path()
-    key = problem_key(plan)
+    key = problem_key(plan) + ("" if len(ops) == 3 else "|" + ",".join(ops))
     if use_cache:
         hit = _load(path).get(key)
         if isinstance(hit, dict) and "tuning" in hit:
@@ -117,7 +122,7 @@ def autotune(plan, use_cache=True, reps=3, warm=1):
                 return plan.get_tuning()
             except (_lib.VamError, TypeError, KeyError):
                 pass
-    best, times = measure(plan, reps, warm)
+    best, times = measure(plan, reps, warm, ops)
     plan.set_tuning(best)
     if use_cache:
         try:

@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "vam_internal.cuh"
@@ -126,14 +127,14 @@ __device__ __forceinline__ void sample_range(double rowb, double colb, double c,
 // R1 forward
 // ---------------------------------------------------------------------------
 template <int VZ, bool OCC, int ABS>
-__global__ void __launch_bounds__(256) k_forward(Args a) {
+__device__ __forceinline__ void k_forward_body(const Args& a, unsigned bx, unsigned by) {
     const int lane = threadIdx.x & 31;
     const int LZ = 1 << a.lz_shift;
     const int LK = 32 >> a.lz_shift;
     const int zl = lane & (LZ - 1);
     const int kl = lane >> a.lz_shift;
-    const long item = (long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
-    const int theta = blockIdx.y;
+    const long item = (long)bx * kWarpsPerBlock + (threadIdx.x >> 5);
+    const int theta = by;
     const int zc = (int)(item % a.zchunks);
     const int j = (int)(item / a.zchunks);
     if (j >= a.nX) return;  // uniform per warp
@@ -233,6 +234,11 @@ __global__ void __launch_bounds__(256) k_forward(Args a) {
     if (kl == 0 && zok) store_vec<VZ>(a.out + ((size_t)j * a.nA + theta) * a.nZ + z0, acc);
 }
 
+template <int VZ, bool OCC, int ABS>
+__global__ void __launch_bounds__(256) k_forward(Args a) {
+    k_forward_body<VZ, OCC, ABS>(a, blockIdx.x, blockIdx.y);
+}
+
 // ---------------------------------------------------------------------------
 // R1 forward, fast path: 32 lanes along z (VZ floats each), one lattice row
 // (angle, detector) per warp, angle pairs (a, a+180) sampled from one lattice.
@@ -329,12 +335,12 @@ __device__ __forceinline__ void sample_checked(const FastArgs& a, const float* _
 }
 
 template <int VZ, bool RAY>
-__global__ void __launch_bounds__(256) k_forward_fast(FastArgs a) {
+__device__ __forceinline__ void k_forward_fast_body(const FastArgs& a, unsigned bx, unsigned by) {
     const int lane = threadIdx.x & 31;
-    const int item = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+    const int item = bx * kWarpsPerBlock + (threadIdx.x >> 5);
     const int zc = item % a.zchunks;
     const int j = item / a.zchunks;
-    const int2 task = a.tasks[blockIdx.y];
+    const int2 task = a.tasks[by];
     const bool paired = task.y >= 0;
     const int N = a.nY;
     const bool ext = paired && a.even;   // lattice row / column N is needed by the partner angle
@@ -423,6 +429,11 @@ __global__ void __launch_bounds__(256) k_forward_fast(FastArgs a) {
     }
 }
 
+template <int VZ, bool RAY>
+__global__ void __launch_bounds__(256) k_forward_fast(FastArgs a) {
+    k_forward_fast_body<VZ, RAY>(a, blockIdx.x, blockIdx.y);
+}
+
 // ---------------------------------------------------------------------------
 // Matched transpose, fast path: 32 lanes along z, one pixel per warp.
 //
@@ -436,9 +447,9 @@ __global__ void __launch_bounds__(256) k_forward_fast(FastArgs a) {
 // forward's to ~1e-7 and the kernel gathers at most 3 detector rows per angle.
 // ---------------------------------------------------------------------------
 template <int VZ, bool RAY>
-__global__ void __launch_bounds__(256) k_adjoint_fast(Args a) {
+__device__ __forceinline__ void k_adjoint_fast_body(const Args& a, unsigned bx, unsigned by) {
     const int lane = threadIdx.x & 31;
-    const long item = (long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+    const long item = (long)bx * kWarpsPerBlock + (threadIdx.x >> 5);
     const int zchunks = a.zchunks;
     const int zc = (int)(item % zchunks);
     const long p = item / zchunks;
@@ -501,14 +512,19 @@ __global__ void __launch_bounds__(256) k_adjoint_fast(Args a) {
     store_vz<VZ>(a.out + (size_t)p * a.nZ + z0, acc, qn);
 }
 
+template <int VZ, bool RAY>
+__global__ void __launch_bounds__(256) k_adjoint_fast(Args a) {
+    k_adjoint_fast_body<VZ, RAY>(a, blockIdx.x, blockIdx.y);
+}
+
 // ---------------------------------------------------------------------------
 // R2 backprojection, fast path: 32 lanes along z with VZ floats each (one
 // pixel per warp, angles in sequence); same arithmetic as k_backward_ref.
 // ---------------------------------------------------------------------------
 template <int VZ, bool RAY>
-__global__ void __launch_bounds__(256) k_backward_fast(Args a) {
+__device__ __forceinline__ void k_backward_fast_body(const Args& a, unsigned bx, unsigned by) {
     const int lane = threadIdx.x & 31;
-    const long item = (long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+    const long item = (long)bx * kWarpsPerBlock + (threadIdx.x >> 5);
     const int zc = (int)(item % a.zchunks);
     const long p = item / a.zchunks;
     if (p >= (long)a.nY * a.nX) return;
@@ -560,6 +576,11 @@ __global__ void __launch_bounds__(256) k_backward_fast(Args a) {
         for (int e = 0; e < VZ; ++e) acc[e] = m * acc[e];
     }
     store_vz<VZ>(a.out + (size_t)p * a.nZ + z0, acc, qn);
+}
+
+template <int VZ, bool RAY>
+__global__ void __launch_bounds__(256) k_backward_fast(Args a) {
+    k_backward_fast_body<VZ, RAY>(a, blockIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------------------
@@ -616,9 +637,9 @@ __global__ void __launch_bounds__(256) k_adj_table(const double4* __restrict__ t
 }
 
 template <int VZ>
-__global__ void __launch_bounds__(256) k_adjoint_table(Args a, const float4* __restrict__ table) {
+__device__ __forceinline__ void k_adjoint_table_body(const Args& a, const float4* __restrict__ table, unsigned bx, unsigned by) {
     const int lane = threadIdx.x & 31;
-    const long item = (long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+    const long item = (long)bx * kWarpsPerBlock + (threadIdx.x >> 5);
     const int zc = (int)(item % a.zchunks);
     const long p = item / a.zchunks;
     if (p >= (long)a.nY * a.nX) return;
@@ -654,6 +675,11 @@ __global__ void __launch_bounds__(256) k_adjoint_table(Args a, const float4* __r
     store_vz<VZ>(a.out + (size_t)p * a.nZ + z0, acc, qn);
 }
 
+template <int VZ>
+__global__ void __launch_bounds__(256) k_adjoint_table(Args a, const float4* __restrict__ table) {
+    k_adjoint_table_body<VZ>(a, table, blockIdx.x, blockIdx.y);
+}
+
 // ---------------------------------------------------------------------------
 // R2 backprojection, batched: cos / sin of every angle staged in shared
 // memory, and B angles per step whose detector-row loads are all issued
@@ -661,12 +687,12 @@ __global__ void __launch_bounds__(256) k_adjoint_table(Args a, const float4* __r
 // of waiting on one angle's float64 chain and loads at a time.
 // ---------------------------------------------------------------------------
 template <int VZ, int B, bool RAY>
-__global__ void __launch_bounds__(256) k_backward_batched(Args a) {
+__device__ __forceinline__ void k_backward_batched_body(const Args& a, unsigned bx, unsigned by) {
     extern __shared__ double2 s_cs[];
     for (int t = threadIdx.x; t < a.nA; t += blockDim.x) s_cs[t] = make_double2(a.trig[t].x, a.trig[t].y);
     __syncthreads();
     const int lane = threadIdx.x & 31;
-    const long item = (long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+    const long item = (long)bx * kWarpsPerBlock + (threadIdx.x >> 5);
     const int zc = (int)(item % a.zchunks);
     const long p = item / a.zchunks;
     if (p >= (long)a.nY * a.nX) return;
@@ -735,6 +761,11 @@ __global__ void __launch_bounds__(256) k_backward_batched(Args a) {
     store_vz<VZ>(a.out + (size_t)p * a.nZ + z0, acc, qn);
 }
 
+template <int VZ, int B, bool RAY>
+__global__ void __launch_bounds__(256) k_backward_batched(Args a) {
+    k_backward_batched_body<VZ, B, RAY>(a, blockIdx.x, blockIdx.y);
+}
+
 __global__ void k_mask_mul(const float* __restrict__ x, const float* __restrict__ mask, float* __restrict__ out,
                            long npix, int nZ) {
     const long n = npix * nZ;
@@ -763,13 +794,13 @@ __device__ __forceinline__ double interp_nan(double t, double ft, int j0, int nY
 }
 
 template <int VZ, bool OCC, int ABS>
-__global__ void __launch_bounds__(256) k_backward_ref(Args a) {
+__device__ __forceinline__ void k_backward_ref_body(const Args& a, unsigned bx, unsigned by) {
     const int lane = threadIdx.x & 31;
     const int LZ = 1 << a.lz_shift;
     const int LK = 32 >> a.lz_shift;
     const int zl = lane & (LZ - 1);
     const int kl = lane >> a.lz_shift;
-    const long item = (long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+    const long item = (long)bx * kWarpsPerBlock + (threadIdx.x >> 5);
     const int zc = (int)(item % a.zchunks);
     const long p = item / a.zchunks;
     if (p >= (long)a.nY * a.nX) return;
@@ -839,17 +870,22 @@ __global__ void __launch_bounds__(256) k_backward_ref(Args a) {
     if (kl == 0 && zok) store_vec<VZ>(a.out + (size_t)p * a.nZ + z0, acc);
 }
 
+template <int VZ, bool OCC, int ABS>
+__global__ void __launch_bounds__(256) k_backward_ref(Args a) {
+    k_backward_ref_body<VZ, OCC, ABS>(a, blockIdx.x, blockIdx.y);
+}
+
 // ---------------------------------------------------------------------------
 // Matched transpose of k_forward
 // ---------------------------------------------------------------------------
 template <int VZ, bool OCC, int ABS>
-__global__ void __launch_bounds__(256) k_adjoint(Args a) {
+__device__ __forceinline__ void k_adjoint_body(const Args& a, unsigned bx, unsigned by) {
     const int lane = threadIdx.x & 31;
     const int LZ = 1 << a.lz_shift;
     const int LK = 32 >> a.lz_shift;
     const int zl = lane & (LZ - 1);
     const int kl = lane >> a.lz_shift;
-    const long item = (long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+    const long item = (long)bx * kWarpsPerBlock + (threadIdx.x >> 5);
     const int zc = (int)(item % a.zchunks);
     const long p = item / a.zchunks;
     if (p >= (long)a.nY * a.nX) return;
@@ -936,6 +972,11 @@ __global__ void __launch_bounds__(256) k_adjoint(Args a) {
     if (kl == 0 && zok) store_vec<VZ>(a.out + (size_t)p * a.nZ + z0, acc);
 }
 
+template <int VZ, bool OCC, int ABS>
+__global__ void __launch_bounds__(256) k_adjoint(Args a) {
+    k_adjoint_body<VZ, OCC, ABS>(a, blockIdx.x, blockIdx.y);
+}
+
 // ---------------------------------------------------------------------------
 // Occlusion sinogram: first row k where warp(insert) > 0, as (k - C); NaN if none.
 // ---------------------------------------------------------------------------
@@ -991,142 +1032,355 @@ __global__ void k_occ_flag(const float* __restrict__ occ, uint8_t* __restrict__ 
 
 enum class Op { Forward, BackwardRef, Adjoint };
 
-template <int VZ, bool OCC, int ABS>
-void launch_one(Op op, const Args& a, long items, cudaStream_t st) {
-    dim3 block(kWarpsPerBlock * kWarp);
-    if (op == Op::Forward) {
-        dim3 grid((unsigned)((items + kWarpsPerBlock - 1) / kWarpsPerBlock), (unsigned)a.nA);
-        k_forward<VZ, OCC, ABS><<<grid, block, 0, st>>>(a);
-    } else {
-        dim3 grid((unsigned)((items + kWarpsPerBlock - 1) / kWarpsPerBlock));
-        if (op == Op::BackwardRef) k_backward_ref<VZ, OCC, ABS><<<grid, block, 0, st>>>(a);
-        else k_adjoint<VZ, OCC, ABS><<<grid, block, 0, st>>>(a);
-    }
-}
-
-template <int VZ, bool OCC>
-void launch_abs(Op op, int abs_mode, const Args& a, long items, cudaStream_t st) {
-    switch (abs_mode) {
-        case VAM_ABS_MASK: launch_one<VZ, OCC, VAM_ABS_MASK>(op, a, items, st); break;
-        case VAM_ABS_RAY: launch_one<VZ, OCC, VAM_ABS_RAY>(op, a, items, st); break;
-        default: launch_one<VZ, OCC, VAM_ABS_NONE>(op, a, items, st); break;
-    }
-}
-
-// VZ of the fast forward for nZ slices (0 = use the generic kernel)
-int fast_vz(int nZ, bool aligned) {
+// Slices per lane of the fast kernels for nZ slices (0 = use the generic
+// kernel): the widest vector whose lanes are at least min_eff busy.  The fast
+// forward gathers about four times as many samples per second as the generic
+// one, so it pays even with half of its lanes idle; the backprojectors' fast
+// and generic kernels are closer, so they ask for busier lanes.
+int fast_vz(int nZ, bool aligned, double min_eff) {
     if (!aligned || nZ % 4) return 0;
     auto eff = [&](int vz) {
         const int per = 32 * vz, ch = (nZ + per - 1) / per;
         return (double)nZ / (double)(ch * per);
     };
     if (eff(8) >= 0.74) return 8;
-    if (eff(4) >= 0.74) return 4;
+    if (eff(4) >= min_eff) return 4;
     return 0;
 }
 
-int run_forward_fast(vam_parallel_plan* plan, const float* in, float* out, cudaStream_t st, int vz) {
-    const float* vol = in;
-    if (plan->abs_mode == VAM_ABS_MASK) {
-        const long npix = (long)plan->nY * plan->nX;
-        const long n = npix * plan->nZ;
-        k_mask_mul<<<(unsigned)std::min<long>((n + 255) / 256, 148L * 32), 256, 0, st>>>(in, plan->d_mask,
-                                                                                         plan->d_vol_scratch, npix, plan->nZ);
-        VAM_CHECK_LAUNCH("k_mask_mul");
-        vol = plan->d_vol_scratch;
-    }
-    FastArgs a;
-    a.vol = vol; a.sino = out; a.trig = plan->d_trig;
-    a.nY = plan->nY; a.nX = plan->nX; a.nZ = plan->nZ; a.nA = plan->nA; a.C = plan->C;
-    a.RS = plan->nX * plan->nZ;
-    a.zchunks = (plan->nZ + 32 * vz - 1) / (32 * vz);
-    a.even = (plan->nY % 2) == 0;
-    a.alpha = plan->abs_alpha; a.R = plan->abs_R;
-    const bool ray = plan->abs_mode == VAM_ABS_RAY;
-    a.tasks = ray ? plan->d_tasks_single : plan->d_tasks_paired;
-    const int ntask = ray ? plan->nA : plan->n_tasks_paired;
-    const long items = (long)(plan->nX + 1) * a.zchunks;
-    dim3 grid((unsigned)((items + kWarpsPerBlock - 1) / kWarpsPerBlock), (unsigned)ntask);
-    dim3 block(kWarpsPerBlock * kWarp);
-    if (vz == 8) {
-        if (ray) k_forward_fast<8, true><<<grid, block, 0, st>>>(a);
-        else k_forward_fast<8, false><<<grid, block, 0, st>>>(a);
-    } else {
-        if (ray) k_forward_fast<4, true><<<grid, block, 0, st>>>(a);
-        else k_forward_fast<4, false><<<grid, block, 0, st>>>(a);
-    }
-    VAM_CHECK_LAUNCH("k_forward_fast");
-    return VAM_OK;
-}
+// ---------------------------------------------------------------------------
+// Dispatch.  describe() decides which kernel body serves a call (fast or
+// generic path, vector width, angle batch, weight table) and fills its
+// arguments and grid; a direct call launches that one kernel, a batch runs the
+// same body for many calls inside one persistent launch.  Both paths therefore
+// compute bit-identical results.
+// ---------------------------------------------------------------------------
+enum Kind : int { KF_FAST = 0, KF_GEN, KB_BATCHED, KB_FAST, KB_GEN, KA_TABLE, KA_FAST, KA_GEN };
 
-int run(vam_parallel_plan* plan, Op op, const float* in, float* out, cudaStream_t st, const char* name) {
+struct Item {
+    int kind;
+    int vz;          // slices per lane of the template instance (1, 4 or 8)
+    int ray, occ, absm, batch;
+    unsigned gx, gy;  // the call's own grid (blocks of kWarpsPerBlock warps)
+    unsigned smem;    // dynamic shared memory of the body
+    int pre_nz;
+    long long tstart;  // first ticket of the call inside a batch
+    long long cost;    // samples the call evaluates (batch ordering and ticket sizes)
+    unsigned chunk;    // blocks of the call's grid per ticket
+    int family;        // 1 forward, 2 backward_ref, 4 adjoint
+    // pre-pass of the fast forward in mask mode: pre_out = mask * pre_in
+    const float* pre_in;
+    const float* pre_mask;
+    float* pre_out;
+    long long pre_npix;
+    Args a;
+    FastArgs f;
+    const float4* table;
+};
+static_assert(sizeof(Item) % 8 == 0, "Item is copied to shared memory in 8-byte words");
+
+int describe(vam_parallel_plan* plan, Op op, const float* in, float* out, Item& it, const char* name) {
     VAM_REQUIRE(plan && in && out, VAM_ERR_ARG, std::string(name) + ": null argument");
-    DeviceGuard g(plan->device);
-    VAM_REQUIRE(g.ok, VAM_ERR_CUDA, std::string(name) + ": cannot select device");
-    int vzf = fast_vz(plan->nZ, (((uintptr_t)in | (uintptr_t)out) & 31) == 0);
-    if (vzf) {  // tuned vector width (4 or 8 slices per lane), when it fits the slice count
-        const int want = op == Op::Forward ? plan->tune_fwd_vz : (op == Op::BackwardRef ? plan->tune_bwd_vz : plan->tune_adj_vz);
-        if (want == 4 || (want == 8 && fast_vz(plan->nZ, true) == 8)) vzf = want;
+    std::memset(&it, 0, sizeof(it));
+    it.cost = (long long)plan->nY * plan->nX * plan->nZ * plan->nA;
+    it.family = op == Op::Forward ? 1 : (op == Op::BackwardRef ? 2 : 4);
+    it.gy = 1;
+    // slices per lane: tuned (1 = generic kernel, 4 or 8 = fast kernel) or automatic (0)
+    const bool fast_ok = (((uintptr_t)in | (uintptr_t)out) & 31) == 0 && plan->nZ % 4 == 0;
+    const int want = op == Op::Forward ? plan->tune_fwd_vz : (op == Op::BackwardRef ? plan->tune_bwd_vz : plan->tune_adj_vz);
+    int vzf = 0;
+    if (fast_ok) {
+        if (want == 4 || want == 8) vzf = want;
+        else if (want == 0) vzf = fast_vz(plan->nZ, true, op == Op::Forward ? 0.45 : 0.74);
     }
-    if (op == Op::Forward && !plan->has_occ && (long)plan->nY * plan->nX * plan->nZ < (1L << 31) && vzf)
-        return run_forward_fast(plan, in, out, st, vzf);
+    const bool ray = plan->abs_mode == VAM_ABS_RAY;
+    if (op == Op::Forward && !plan->has_occ && (long)plan->nY * plan->nX * plan->nZ < (1L << 31) && vzf) {
+        FastArgs& a = it.f;
+        a.vol = in;
+        if (plan->abs_mode == VAM_ABS_MASK) {
+            it.pre_in = in; it.pre_mask = plan->d_mask; it.pre_out = plan->d_vol_scratch;
+            it.pre_npix = (long long)plan->nY * plan->nX; it.pre_nz = plan->nZ;
+            a.vol = plan->d_vol_scratch;
+        }
+        a.sino = out; a.trig = plan->d_trig;
+        a.nY = plan->nY; a.nX = plan->nX; a.nZ = plan->nZ; a.nA = plan->nA; a.C = plan->C;
+        a.RS = plan->nX * plan->nZ;
+        a.zchunks = (plan->nZ + 32 * vzf - 1) / (32 * vzf);
+        a.even = (plan->nY % 2) == 0;
+        a.alpha = plan->abs_alpha; a.R = plan->abs_R;
+        a.tasks = ray ? plan->d_tasks_single : plan->d_tasks_paired;
+        const long items = (long)(plan->nX + 1) * a.zchunks;
+        it.kind = KF_FAST; it.vz = vzf; it.ray = ray;
+        it.gx = (unsigned)((items + kWarpsPerBlock - 1) / kWarpsPerBlock);
+        it.gy = (unsigned)(ray ? plan->nA : plan->n_tasks_paired);
+        return VAM_OK;
+    }
     if (op != Op::Forward && !plan->has_occ && vzf) {
-        Args a;
-        std::memset(&a, 0, sizeof(a));
+        Args& a = it.a;
         a.in = in; a.out = out; a.trig = plan->d_trig; a.circle = plan->d_circle;
         a.mask = plan->abs_mode == VAM_ABS_MASK ? plan->d_mask : nullptr;
         a.nY = plan->nY; a.nX = plan->nX; a.nZ = plan->nZ; a.nA = plan->nA; a.C = plan->C;
         a.zchunks = (plan->nZ + 32 * vzf - 1) / (32 * vzf);
         a.alpha = plan->abs_alpha; a.R = plan->abs_R;
         const long items = (long)plan->nY * plan->nX * a.zchunks;
-        dim3 grid((unsigned)((items + kWarpsPerBlock - 1) / kWarpsPerBlock)), block(kWarpsPerBlock * kWarp);
-        const bool ray = plan->abs_mode == VAM_ABS_RAY;
+        it.gx = (unsigned)((items + kWarpsPerBlock - 1) / kWarpsPerBlock);
+        it.vz = vzf; it.ray = ray;
         if (op == Op::BackwardRef) {
             // the batched kernel stages cos / sin of every angle in shared memory (16 B per angle)
             const int batch = (size_t)plan->nA * sizeof(double2) <= 48 * 1024 ? plan->tune_bwd_batch : 1;
             if (batch >= 2) {
-                const size_t smem = sizeof(double2) * plan->nA;
-                if (vzf == 8) {
-                    if (ray) k_backward_batched<8, 2, true><<<grid, block, smem, st>>>(a);
-                    else k_backward_batched<8, 2, false><<<grid, block, smem, st>>>(a);
-                } else if (batch >= 4) {
-                    if (ray) k_backward_batched<4, 4, true><<<grid, block, smem, st>>>(a);
-                    else k_backward_batched<4, 4, false><<<grid, block, smem, st>>>(a);
-                } else {
-                    if (ray) k_backward_batched<4, 2, true><<<grid, block, smem, st>>>(a);
-                    else k_backward_batched<4, 2, false><<<grid, block, smem, st>>>(a);
-                }
-            } else if (vzf == 8) { if (ray) k_backward_fast<8, true><<<grid, block, 0, st>>>(a); else k_backward_fast<8, false><<<grid, block, 0, st>>>(a); }
-            else { if (ray) k_backward_fast<4, true><<<grid, block, 0, st>>>(a); else k_backward_fast<4, false><<<grid, block, 0, st>>>(a); }
+                it.kind = KB_BATCHED;
+                it.batch = vzf == 8 ? 2 : (batch >= 4 ? 4 : 2);
+                it.smem = (unsigned)(sizeof(double2) * plan->nA);
+            } else {
+                it.kind = KB_FAST;
+            }
         } else if (plan->d_adj_table && plan->adj_table_abs == plan->abs_mode && plan->tune_adj_table) {
-            if (vzf == 8) k_adjoint_table<8><<<grid, block, 0, st>>>(a, plan->d_adj_table);
-            else k_adjoint_table<4><<<grid, block, 0, st>>>(a, plan->d_adj_table);
+            it.kind = KA_TABLE;
+            it.table = plan->d_adj_table;
         } else {
-            if (vzf == 8) { if (ray) k_adjoint_fast<8, true><<<grid, block, 0, st>>>(a); else k_adjoint_fast<8, false><<<grid, block, 0, st>>>(a); }
-            else { if (ray) k_adjoint_fast<4, true><<<grid, block, 0, st>>>(a); else k_adjoint_fast<4, false><<<grid, block, 0, st>>>(a); }
+            it.kind = KA_FAST;
         }
-        VAM_CHECK_LAUNCH(name);
         return VAM_OK;
     }
     const bool aligned = (((uintptr_t)in | (uintptr_t)out) & 15) == 0;
     Layout L = choose_layout(plan->nZ, aligned);
-    Args a;
+    Args& a = it.a;
     a.in = in; a.out = out; a.trig = plan->d_trig; a.circle = plan->d_circle;
     a.mask = plan->d_mask; a.occ = plan->d_occ; a.occ_flag = plan->d_occ_flag;
     a.nY = plan->nY; a.nX = plan->nX; a.nZ = plan->nZ; a.nA = plan->nA; a.C = plan->C;
     a.lz_shift = L.lz_shift; a.zvec = L.zvec; a.zchunks = L.zchunks;
     a.alpha = plan->abs_alpha; a.R = plan->abs_R;
-    long items = (op == Op::Forward) ? (long)plan->nX * L.zchunks : (long)plan->nY * plan->nX * L.zchunks;
-    const bool occ = plan->has_occ != 0;
-    if (L.VZ == 4) {
-        if (occ) launch_abs<4, true>(op, plan->abs_mode, a, items, st);
-        else launch_abs<4, false>(op, plan->abs_mode, a, items, st);
+    const long items = (op == Op::Forward) ? (long)plan->nX * L.zchunks : (long)plan->nY * plan->nX * L.zchunks;
+    it.kind = op == Op::Forward ? KF_GEN : (op == Op::BackwardRef ? KB_GEN : KA_GEN);
+    it.vz = L.VZ; it.occ = plan->has_occ != 0; it.absm = plan->abs_mode;
+    it.gx = (unsigned)((items + kWarpsPerBlock - 1) / kWarpsPerBlock);
+    it.gy = op == Op::Forward ? (unsigned)plan->nA : 1u;
+    return VAM_OK;
+}
+
+// ---- the body of a described call, for one block (bx, by) of its grid
+// The bodies receive a local copy of their arguments: read once from the
+// launch's parameter space into registers, instead of an indexed
+// constant-cache load at every use inside the sample loops.
+template <int FAM, int VZ, bool OCC, int ABS>
+__device__ __forceinline__ void gen_body(const Item& it, unsigned bx, unsigned by) {
+    const Args a = it.a;
+    if constexpr ((FAM & 1) != 0) if (it.kind == KF_GEN) k_forward_body<VZ, OCC, ABS>(a, bx, by);
+    if constexpr ((FAM & 2) != 0) if (it.kind == KB_GEN) k_backward_ref_body<VZ, OCC, ABS>(a, bx, by);
+    if constexpr ((FAM & 4) != 0) if (it.kind == KA_GEN) k_adjoint_body<VZ, OCC, ABS>(a, bx, by);
+}
+
+template <int FAM, int VZ, bool OCC>
+__device__ __forceinline__ void gen_body_fam(const Item& it, unsigned bx, unsigned by) {
+    if (it.absm == VAM_ABS_MASK) gen_body<FAM, VZ, OCC, VAM_ABS_MASK>(it, bx, by);
+    else if (it.absm == VAM_ABS_RAY) gen_body<FAM, VZ, OCC, VAM_ABS_RAY>(it, bx, by);
+    else gen_body<FAM, VZ, OCC, VAM_ABS_NONE>(it, bx, by);
+}
+
+template <int FAM, bool RAY>
+__device__ __forceinline__ void fast_body(const Item& it, unsigned bx, unsigned by) {
+    if constexpr ((FAM & 1) != 0) {
+        if (it.kind == KF_FAST) {
+            const FastArgs f = it.f;
+            if (it.vz == 8) k_forward_fast_body<8, RAY>(f, bx, by);
+            else k_forward_fast_body<4, RAY>(f, bx, by);
+        }
+    }
+    if constexpr ((FAM & 2) != 0) {
+        if (it.kind == KB_BATCHED) {
+            const Args a = it.a;
+            if (it.vz == 8) k_backward_batched_body<8, 2, RAY>(a, bx, by);
+            else if (it.batch == 4) k_backward_batched_body<4, 4, RAY>(a, bx, by);
+            else k_backward_batched_body<4, 2, RAY>(a, bx, by);
+        } else if (it.kind == KB_FAST) {
+            const Args a = it.a;
+            if (it.vz == 8) k_backward_fast_body<8, RAY>(a, bx, by);
+            else k_backward_fast_body<4, RAY>(a, bx, by);
+        }
+    }
+    if constexpr ((FAM & 4) != 0) {
+        if (it.kind == KA_FAST) {
+            const Args a = it.a;
+            if (it.vz == 8) k_adjoint_fast_body<8, RAY>(a, bx, by);
+            else k_adjoint_fast_body<4, RAY>(a, bx, by);
+        }
+    }
+}
+
+// FAM: the op families (1 forward, 2 backward_ref, 4 adjoint) this instance
+// carries; a batch launches the narrowest instance covering its calls, so a
+// forward-only batch is not compiled around the backprojectors' registers.
+template <int FAM>
+__device__ __forceinline__ void item_body(const Item& it, unsigned bx, unsigned by) {
+    if (it.kind == KF_GEN || it.kind == KB_GEN || it.kind == KA_GEN) {
+        if (it.vz == 4) { if (it.occ) gen_body_fam<FAM, 4, true>(it, bx, by); else gen_body_fam<FAM, 4, false>(it, bx, by); }
+        else { if (it.occ) gen_body_fam<FAM, 1, true>(it, bx, by); else gen_body_fam<FAM, 1, false>(it, bx, by); }
+    } else if (it.kind == KA_TABLE) {
+        if constexpr ((FAM & 4) != 0) {
+            const Args a = it.a;
+            if (it.vz == 8) k_adjoint_table_body<8>(a, it.table, bx, by);
+            else k_adjoint_table_body<4>(a, it.table, bx, by);
+        }
+    } else if (it.ray) {
+        fast_body<FAM, true>(it, bx, by);
     } else {
-        if (occ) launch_abs<1, true>(op, plan->abs_mode, a, items, st);
-        else launch_abs<1, false>(op, plan->abs_mode, a, items, st);
+        fast_body<FAM, false>(it, bx, by);
+    }
+}
+
+// ---- direct call: one launch of the described body's own kernel
+template <int VZ, bool OCC, int ABS>
+void launch_gen3(const Item& it, dim3 grid, cudaStream_t st) {
+    const dim3 block(kWarpsPerBlock * kWarp);
+    if (it.kind == KF_GEN) k_forward<VZ, OCC, ABS><<<grid, block, 0, st>>>(it.a);
+    else if (it.kind == KB_GEN) k_backward_ref<VZ, OCC, ABS><<<grid, block, 0, st>>>(it.a);
+    else k_adjoint<VZ, OCC, ABS><<<grid, block, 0, st>>>(it.a);
+}
+
+template <int VZ, bool OCC>
+void launch_gen2(const Item& it, dim3 grid, cudaStream_t st) {
+    if (it.absm == VAM_ABS_MASK) launch_gen3<VZ, OCC, VAM_ABS_MASK>(it, grid, st);
+    else if (it.absm == VAM_ABS_RAY) launch_gen3<VZ, OCC, VAM_ABS_RAY>(it, grid, st);
+    else launch_gen3<VZ, OCC, VAM_ABS_NONE>(it, grid, st);
+}
+
+template <bool RAY>
+void launch_fast(const Item& it, dim3 grid, cudaStream_t st) {
+    const dim3 block(kWarpsPerBlock * kWarp);
+    switch (it.kind) {
+        case KF_FAST:
+            if (it.vz == 8) k_forward_fast<8, RAY><<<grid, block, 0, st>>>(it.f);
+            else k_forward_fast<4, RAY><<<grid, block, 0, st>>>(it.f);
+            break;
+        case KB_BATCHED:
+            if (it.vz == 8) k_backward_batched<8, 2, RAY><<<grid, block, it.smem, st>>>(it.a);
+            else if (it.batch == 4) k_backward_batched<4, 4, RAY><<<grid, block, it.smem, st>>>(it.a);
+            else k_backward_batched<4, 2, RAY><<<grid, block, it.smem, st>>>(it.a);
+            break;
+        case KB_FAST:
+            if (it.vz == 8) k_backward_fast<8, RAY><<<grid, block, 0, st>>>(it.a);
+            else k_backward_fast<4, RAY><<<grid, block, 0, st>>>(it.a);
+            break;
+        case KA_FAST:
+            if (it.vz == 8) k_adjoint_fast<8, RAY><<<grid, block, 0, st>>>(it.a);
+            else k_adjoint_fast<4, RAY><<<grid, block, 0, st>>>(it.a);
+            break;
+        default: break;
+    }
+}
+
+int launch_item(const Item& it, cudaStream_t st, const char* name) {
+    if (it.pre_in) {
+        const long long n = it.pre_npix * it.pre_nz;
+        k_mask_mul<<<(unsigned)std::min<long long>((n + 255) / 256, 148LL * 32), 256, 0, st>>>(
+            it.pre_in, it.pre_mask, it.pre_out, (long)it.pre_npix, it.pre_nz);
+        VAM_CHECK_LAUNCH("k_mask_mul");
+    }
+    const dim3 grid(it.gx, it.gy);
+    if (it.kind == KF_GEN || it.kind == KB_GEN || it.kind == KA_GEN) {
+        if (it.vz == 4) { if (it.occ) launch_gen2<4, true>(it, grid, st); else launch_gen2<4, false>(it, grid, st); }
+        else { if (it.occ) launch_gen2<1, true>(it, grid, st); else launch_gen2<1, false>(it, grid, st); }
+    } else if (it.kind == KA_TABLE) {
+        const dim3 block(kWarpsPerBlock * kWarp);
+        if (it.vz == 8) k_adjoint_table<8><<<grid, block, 0, st>>>(it.a, it.table);
+        else k_adjoint_table<4><<<grid, block, 0, st>>>(it.a, it.table);
+    } else if (it.ray) {
+        launch_fast<true>(it, grid, st);
+    } else {
+        launch_fast<false>(it, grid, st);
     }
     VAM_CHECK_LAUNCH(name);
     return VAM_OK;
+}
+
+int run(vam_parallel_plan* plan, Op op, const float* in, float* out, cudaStream_t st, const char* name) {
+    VAM_REQUIRE(plan, VAM_ERR_ARG, std::string(name) + ": null argument");
+    DeviceGuard g(plan->device);
+    VAM_REQUIRE(g.ok, VAM_ERR_CUDA, std::string(name) + ": cannot select device");
+    Item it;
+    const int rc = describe(plan, op, in, out, it, name);
+    if (rc != VAM_OK) return rc;
+    return launch_item(it, st, name);
+}
+
+// ---------------------------------------------------------------------------
+// Batched calls: one persistent launch over the virtual blocks of many calls.
+//
+// Every call of a batch keeps its own grid; the calls' blocks are numbered
+// consecutively (largest call first) into virtual blocks, and each resident
+// CTA takes the next virtual block from a device counter (the work queue),
+// finds its call by binary search, copies the call's description into shared
+// memory and runs the call's body for that block.  Calls of uneven size (2-D
+// slices next to 3-D volumes, different angle counts) therefore fill the
+// device together instead of one after another.
+// ---------------------------------------------------------------------------
+// The calls of one launch travel by value in the kernel's parameter space
+// (__grid_constant__, up to 32 KB): a CTA reads its call's description through
+// the constant cache, which keeps those reads off the L1 data path that the
+// gather kernels saturate, and a graph capture records the list with the launch.
+constexpr int kBatchMaxItems = 48;
+struct BatchParams {
+    int n;
+    long long total;  // tickets
+    unsigned long long* counter;
+    Item items[kBatchMaxItems];
+};
+static_assert(sizeof(BatchParams) < 32000, "batch parameters must fit the 32 KB kernel parameter space");
+
+// The forward bodies fit 64 registers, so the forward-only instance asks for
+// four resident CTAs per SM; the others keep the backprojectors' 80.
+template <int FAM>
+__global__ void __launch_bounds__(256, FAM == 1 ? 4 : 3) k_batch(const __grid_constant__ BatchParams P) {
+    __shared__ long long s_t;
+    __shared__ int s_idx;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const long long t = (long long)atomicAdd(P.counter, 1ULL);
+            int lo = 0, hi = P.n - 1;  // the last call whose first ticket is <= t
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (P.items[mid].tstart <= t) lo = mid;
+                else hi = mid - 1;
+            }
+            s_t = t;
+            s_idx = lo;
+        }
+        __syncthreads();
+        const long long t = s_t;
+        const int idx = s_idx;
+        __syncthreads();  // s_t / s_idx are rewritten next round
+        if (t >= P.total) return;  // uniform: every thread read the same s_t
+        const Item& it = P.items[idx];
+        const unsigned gx = it.gx, nb = it.gx * it.gy;  // a call's grid has < 2^32 blocks
+        const unsigned b0 = (unsigned)(t - it.tstart) * it.chunk;
+        const unsigned n = min(it.chunk, nb - b0);
+        unsigned bx = b0 % gx, by = b0 / gx;
+        for (unsigned k = 0; k < n; ++k) {
+            item_body<FAM>(it, bx, by);
+            if (it.smem) __syncthreads();  // the next block restages the body's shared memory
+            if (++bx == gx) { bx = 0; ++by; }
+        }
+    }
+}
+
+using BatchKernel = void (*)(BatchParams);
+BatchKernel batch_kernel(int fam) {
+    switch (fam) {
+        case 1: return k_batch<1>;
+        case 2: return k_batch<2>;
+        case 4: return k_batch<4>;
+        default: return k_batch<7>;
+    }
+}
+
+// mask pre-pass of every fast forward of a batch (blockIdx.y = call)
+__global__ void k_batch_premask(const __grid_constant__ BatchParams P) {
+    const Item& it = P.items[blockIdx.y];
+    if (!it.pre_in) return;
+    const long long n = it.pre_npix * it.pre_nz;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        it.pre_out[i] = it.pre_mask[i / it.pre_nz] * it.pre_in[i];
 }
 
 // numpy linspace(-1, 1, n)[i]
@@ -1302,9 +1556,9 @@ extern "C" int vam_parallel_get_occlusion_sinogram(vam_parallel_plan* p, float* 
 extern "C" int vam_parallel_set_tuning(vam_parallel_plan* p, const vam_parallel_tuning* t) {
     clear_error();
     VAM_REQUIRE(p && t, VAM_ERR_ARG, "vam_parallel_set_tuning: null argument");
-    auto vz_ok = [](int v) { return v == 0 || v == 4 || v == 8; };
+    auto vz_ok = [](int v) { return v == 0 || v == 1 || v == 4 || v == 8; };
     VAM_REQUIRE(vz_ok(t->forward_vz) && vz_ok(t->backward_vz) && vz_ok(t->adjoint_vz), VAM_ERR_ARG,
-                "vam_parallel_set_tuning: vector widths must be 0 (auto), 4 or 8");
+                "vam_parallel_set_tuning: vector widths must be 0 (auto), 1 (generic kernel), 4 or 8");
     VAM_REQUIRE(t->backward_batch == 0 || t->backward_batch == 1 || t->backward_batch == 2 || t->backward_batch == 4,
                 VAM_ERR_ARG, "vam_parallel_set_tuning: backward_batch must be 0 (auto), 1, 2 or 4");
     p->tune_fwd_vz = t->forward_vz;
@@ -1356,4 +1610,195 @@ extern "C" int vam_parallel_backward_ref(vam_parallel_plan* p, const float* sino
 extern "C" int vam_parallel_adjoint(vam_parallel_plan* p, const float* sino, float* vol, vam_stream_t stream) {
     clear_error();
     return run(p, Op::Adjoint, sino, vol, (cudaStream_t)stream, "vam_parallel_adjoint");
+}
+
+// ---------------------------------------------------------------------------
+// batches
+// ---------------------------------------------------------------------------
+struct vam_batch {
+    int device;
+    unsigned long long* d_counter;
+    int sms;
+    int per_sm[8];             // resident CTAs per SM of k_batch<fam> (fam 1, 2, 4, 7)
+    std::vector<Item> host;    // the described calls of the last list, in queue order
+    std::vector<int> group;    // first call of each launch (kBatchMaxItems calls per launch)
+    std::vector<long long> tickets;  // tickets of each launch
+    std::vector<int> fam;      // op families of each launch
+    long long blocks;          // blocks of all calls' grids
+    unsigned smem;
+    int any_pre;
+    int ctas;                  // persistent CTAs of the last launch
+};
+
+extern "C" int vam_batch_create(int32_t device, vam_batch** out) {
+    clear_error();
+    VAM_REQUIRE(out, VAM_ERR_ARG, "vam_batch_create: null argument");
+    *out = nullptr;
+    DeviceGuard g(device);
+    VAM_REQUIRE(g.ok, VAM_ERR_CUDA, "vam_batch_create: cannot select device");
+    int sms = 0;
+    VAM_TRY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    int per_sm[8] = {0};
+    // residency with the largest dynamic shared memory a call may ask for (48 KB, the batched
+    // backprojection's trig table), so a list never needs a runtime query (which would not be
+    // allowed during graph capture); the opt-in limit is raised first, as 48 KB plus the
+    // kernel's static shared memory exceeds the default
+    for (int fam : {1, 2, 4, 7}) {
+        VAM_TRY_CUDA(cudaFuncSetAttribute(batch_kernel(fam), cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+        VAM_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[fam], batch_kernel(fam),
+                                                                   kWarpsPerBlock * kWarp, 48 * 1024));
+        VAM_REQUIRE(per_sm[fam] > 0, VAM_ERR_NOTSUP, "vam_batch_create: the batch kernel cannot be resident");
+    }
+    auto* b = new vam_batch();
+    b->device = device;
+    b->sms = sms;
+    for (int i = 0; i < 8; ++i) b->per_sm[i] = per_sm[i];
+    b->blocks = 0;
+    b->smem = 0;
+    b->any_pre = 0;
+    b->ctas = 0;
+    const cudaError_t e = cudaMalloc(&b->d_counter, sizeof(unsigned long long) * 64);
+    if (e != cudaSuccess) {
+        delete b;
+        return set_error(VAM_ERR_NOMEM, std::string("vam_batch_create: ") + cudaGetErrorString(e));
+    }
+    *out = b;
+    return VAM_OK;
+}
+
+extern "C" int vam_batch_destroy(vam_batch* b) {
+    if (!b) return VAM_OK;
+    DeviceGuard g(b->device);
+    cudaFree(b->d_counter);
+    delete b;
+    return VAM_OK;
+}
+
+namespace vam {
+namespace {
+// Relative time per sample of each body (fast forward = 1), measured on
+// B200: the generic kernels gather fewer samples per second than the fast
+// ones, and a single slice (nZ = 1) far fewer, so tickets are sized in
+// estimated time, not in samples.
+double time_weight(const Item& it) {
+    const bool slice = it.a.nZ == 1 || it.f.nZ == 1;
+    switch (it.kind) {
+        case KF_FAST: return 1.0;
+        case KF_GEN: return slice ? 27.0 : 4.0;
+        case KB_BATCHED: case KB_FAST: return 1.2;
+        case KB_GEN: return slice ? 10.0 : 2.0;
+        case KA_TABLE: return 1.5;
+        case KA_FAST: return 3.5;
+        default: return slice ? 27.0 : 4.0;
+    }
+}
+
+// describe every call, order the queue, size the tickets; no CUDA call
+int batch_prepare(vam_batch* b, const vam_work* work, int32_t n) {
+    VAM_REQUIRE(n <= kBatchMaxItems * 64, VAM_ERR_SHAPE, "vam_batch: at most 3072 calls per list");
+    std::vector<Item> items((size_t)n);
+    for (int i = 0; i < n; ++i) {
+        const vam_work& w = work[i];
+        VAM_REQUIRE(w.plan, VAM_ERR_ARG, "vam_batch: work item without a plan");
+        VAM_REQUIRE(w.plan->device == b->device, VAM_ERR_ARG, "vam_batch: plan on another device than the batch");
+        VAM_REQUIRE(w.op >= VAM_OP_FORWARD && w.op <= VAM_OP_ADJOINT, VAM_ERR_ARG, "vam_batch: unknown op");
+        const Op op = w.op == VAM_OP_FORWARD ? Op::Forward : (w.op == VAM_OP_BACKWARD_REF ? Op::BackwardRef : Op::Adjoint);
+        const int rc = describe(w.plan, op, w.in, w.out, items[i], "vam_batch");
+        if (rc != VAM_OK) return rc;
+        VAM_REQUIRE((long long)items[i].gx * items[i].gy < (1LL << 32), VAM_ERR_SHAPE, "vam_batch: call grid too large");
+        items[i].cost = (long long)std::llround((double)items[i].cost * time_weight(items[i]));
+    }
+    // largest call first, so the small ones fill the tail of the queue
+    std::stable_sort(items.begin(), items.end(), [](const Item& x, const Item& y) { return x.cost > y.cost; });
+    b->group.clear();
+    b->tickets.clear();
+    b->fam.clear();
+    b->smem = 0;
+    b->any_pre = 0;
+    b->blocks = 0;
+    for (int g0 = 0; g0 < n; g0 += kBatchMaxItems) {
+        const int g1 = std::min(n, g0 + kBatchMaxItems);
+        int fam = 0;
+        long long cost = 0;
+        for (int i = g0; i < g1; ++i) {
+            fam |= items[i].family;
+            cost += std::max(items[i].cost, 1LL);
+            b->smem = std::max(b->smem, items[i].smem);
+            b->any_pre |= items[i].pre_in != nullptr;
+        }
+        if (fam != 1 && fam != 2 && fam != 4) fam = 7;
+        // tickets: about 8 per resident CTA over the launch, each call's share proportional to
+        // its samples; a ticket is a run of consecutive blocks of one call
+        const double want = 8.0 * b->sms * b->per_sm[fam];
+        long long total = 0;
+        for (int i = g0; i < g1; ++i) {
+            Item& it = items[i];
+            const long long nb = (long long)it.gx * it.gy;
+            long long tk = (long long)std::llround(want * (double)std::max(it.cost, 1LL) / (double)cost);
+            tk = std::max(1LL, std::min(tk, nb));
+            it.chunk = (unsigned)((nb + tk - 1) / tk);
+            tk = (nb + it.chunk - 1) / it.chunk;
+            it.tstart = total;
+            total += tk;
+            b->blocks += nb;
+        }
+        b->group.push_back(g0);
+        b->tickets.push_back(total);
+        b->fam.push_back(fam);
+    }
+    b->host.swap(items);
+    return VAM_OK;
+}
+}  // namespace
+}  // namespace vam
+
+extern "C" int vam_batch_prepare(vam_batch* b, const vam_work* work, int32_t n, vam_stream_t stream) {
+    clear_error();
+    (void)stream;
+    VAM_REQUIRE(b && work && n > 0, VAM_ERR_ARG, "vam_batch_prepare: null argument or empty work list");
+    return batch_prepare(b, work, n);
+}
+
+extern "C" int vam_batch_submit(vam_batch* b, const vam_work* work, int32_t n, vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(b && work && n > 0, VAM_ERR_ARG, "vam_batch_submit: null argument or empty work list");
+    DeviceGuard g(b->device);
+    VAM_REQUIRE(g.ok, VAM_ERR_CUDA, "vam_batch_submit: cannot select device");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int rc = batch_prepare(b, work, n);
+    if (rc != VAM_OK) return rc;
+    const int groups = (int)b->group.size();
+    VAM_TRY_CUDA(cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long) * groups, st));
+    static BatchParams P;  // 15 KB: too large for the stack of every caller thread
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    for (int k = 0; k < groups; ++k) {
+        const int g0 = b->group[k];
+        const int g1 = k + 1 < groups ? b->group[k + 1] : n;
+        std::memset(&P, 0, sizeof(P));
+        P.n = g1 - g0;
+        P.total = b->tickets[k];
+        P.counter = b->d_counter + k;
+        std::memcpy(P.items, b->host.data() + g0, sizeof(Item) * (size_t)(g1 - g0));
+        bool pre = false;
+        for (int i = 0; i < P.n; ++i) pre |= P.items[i].pre_in != nullptr;
+        if (pre) {
+            k_batch_premask<<<dim3(64, (unsigned)P.n), 256, 0, st>>>(P);
+            VAM_CHECK_LAUNCH("k_batch_premask");
+        }
+        const int fam = b->fam[k];
+        const long long ctas = std::min<long long>((long long)b->sms * b->per_sm[fam], P.total);
+        b->ctas = (int)ctas;
+        batch_kernel(fam)<<<(unsigned)ctas, kWarpsPerBlock * kWarp, b->smem, st>>>(P);
+        VAM_CHECK_LAUNCH("k_batch");
+    }
+    return VAM_OK;
+}
+
+extern "C" int vam_batch_info(vam_batch* b, int64_t* virtual_blocks, int32_t* ctas) {
+    clear_error();
+    VAM_REQUIRE(b, VAM_ERR_ARG, "vam_batch_info: null argument");
+    if (virtual_blocks) *virtual_blocks = b->blocks;
+    if (ctas) *ctas = b->ctas;
+    return VAM_OK;
 }

@@ -108,8 +108,33 @@ def capture(fn, device):
     """
     device = torch.device(device)
     torch.cuda.synchronize(device)
-    g = torch.cuda.CUDAGraph()
+    g = torch.cuda.CUDAGraph(keep_graph=True)  # keeps the cudaGraph_t readable (graph_kernel_nodes)
     s = torch.cuda.Stream(device=device)
     with torch.cuda.graph(g, stream=s):
         fn()
+    g.instantiate()
     return g
+
+
+def graph_kernel_nodes(graph):
+    """Number of kernel nodes in a captured torch CUDA graph (the launches one replay issues),
+    read back through the CUDA runtime; None when the graph cannot be inspected."""
+    try:
+        from cuda.bindings import runtime as rt
+
+        h = rt.cudaGraph_t(init_value=int(graph.raw_cuda_graph()))
+        err, _, num = rt.cudaGraphGetNodes(h, numNodes=0)
+        if int(err) != 0:
+            return None
+        err, nodes, num = rt.cudaGraphGetNodes(h, numNodes=num)
+        if int(err) != 0:
+            return None
+        kernel = rt.cudaGraphNodeType.cudaGraphNodeTypeKernel
+        count = 0
+        for nd in nodes[:num]:
+            e2, t = rt.cudaGraphNodeGetType(nd)
+            if int(e2) == 0 and t == kernel:
+                count += 1
+        return count
+    except Exception:
+        return None

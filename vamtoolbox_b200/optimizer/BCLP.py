@@ -221,11 +221,16 @@ class BCLPNorm:
             del gr
         it.state()  # dose / mapped dose / norms of the final sinogram
         torch.cuda.synchronize(dev)
+        return self.finish_device(it, done, [ev[0].elapsed_time(ev[k + 1]) / 1e3 for k in range(done)])
+
+    def finish_device(self, it, done, iter_times):
+        """Logs, dose and sinogram of a device run from its iteration state (after a final ``it.state()``)."""
+        n_iter = self.logs.options.n_iter
         self.logs.curr_iter = done
         rows = min(int(it.counter.item()), n_iter + 1)
-        self.logs.fill_from_stats(it.log[:rows].cpu().numpy(), q, p, rows)
+        self.logs.fill_from_stats(it.log[:rows].cpu().numpy(), self.q, self.p, rows)
         for k in range(done):
-            self.logs.iter_times[k] = ev[0].elapsed_time(ev[k + 1]) / 1e3
+            self.logs.iter_times[k] = iter_times[k]
         tshape = self.target_geo.array.shape
         self.dose_t, self.mapped_t, self.g_t = it.dose.reshape(tshape), it.mapped.reshape(tshape), it.g
         self.dose = self.dose_t.double().cpu().numpy()
@@ -276,7 +281,6 @@ class DeviceIteration:
         weight = f32(bclp.weight).reshape(vol_shape) if np.ndim(bclp.weight) else bclp.weight
         self.prm = bclp_params(bclp.response_model, eps, weight, bclp.p, dev, self._keep)
         self.reduce_stats = reduce_stats
-        self.launches_per_step = 6
 
     def state(self):
         self.back(self.g, self.dose)

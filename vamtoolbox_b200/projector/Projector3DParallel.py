@@ -117,11 +117,11 @@ class ParallelPlan:
         _lib.call("vam_parallel_get_tuning", self._h, ctypes.byref(t))
         return {k: int(getattr(t, k)) for k in self._TUNING_FIELDS}
 
-    def autotune(self, use_cache=True):
-        """Time the launch-shape candidates on this plan's device (or reuse the cached winner)."""
+    def autotune(self, use_cache=True, ops=("forward", "backward", "adjoint")):
+        """Time the launch-shape candidates of ``ops`` on this plan's device (or reuse the cached winner)."""
         from ..autotune import autotune
 
-        return autotune(self, use_cache=use_cache)
+        return autotune(self, use_cache=use_cache, ops=tuple(ops))
 
     def set_occlusion(self, insert):
         ins = torch.as_tensor(np.ascontiguousarray(np.atleast_3d(insert), dtype=np.float32), device=self.device)

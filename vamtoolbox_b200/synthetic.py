@@ -11,13 +11,15 @@ import numpy as np
 
 
 def ellipses_2d(n=256, seed=0, radius=120.0):
-    """Union of 3-8 ellipses (semi-axes 10-80 px) minus 2-4 circular holes inside a disk."""
+    """Union of 3-8 ellipses minus 2-4 circular holes inside a disk; semi-axes 10-80 px and holes
+    4-20 px at the default radius of 120 px, scaled with the radius otherwise."""
     rng = np.random.default_rng(seed)
     y, x = np.mgrid[:n, :n] - (n - 1) / 2
     img = np.zeros((n, n), dtype=bool)
+    k = radius / 120.0
     for _ in range(rng.integers(3, 9)):
-        a, b = rng.uniform(10, 80, 2)
-        r = rng.uniform(0, radius - max(a, b) * 0.5)
+        a, b = rng.uniform(10, 80, 2) * k
+        r = rng.uniform(0, max(radius - max(a, b) * 0.5, 0.0))
         phi = rng.uniform(0, 2 * np.pi)
         cx, cy = r * np.cos(phi), r * np.sin(phi)
         th = rng.uniform(0, np.pi)
@@ -25,7 +27,7 @@ def ellipses_2d(n=256, seed=0, radius=120.0):
         yr = -(x - cx) * np.sin(th) + (y - cy) * np.cos(th)
         img |= (xr / a) ** 2 + (yr / b) ** 2 <= 1
     for _ in range(rng.integers(2, 5)):
-        rr = rng.uniform(4, 20)
+        rr = rng.uniform(4, 20) * k
         cx, cy = rng.uniform(-radius / 2, radius / 2, 2)
         img &= ~((x - cx) ** 2 + (y - cy) ** 2 <= rr ** 2)
     img &= x ** 2 + y ** 2 <= radius ** 2
