@@ -109,7 +109,9 @@ int vam_parallel_adjoint(vam_parallel_plan* plan, const float* sino_dev, float* 
  * autotuner (vamtoolbox_b200/autotune.py times the candidates on the device
  * and caches the winner per device and problem shape).  Vector widths are the
  * slices each lane of a fast kernel carries (4 or 8; 1 = the generic kernel;
- * 0 = automatic; the fast kernels need nZ % 4 == 0); backward_batch is the
+ * 0 = automatic; the fast kernels need nZ % 4 == 0; for a single slice any
+ * value but 0 and 1 selects the shared-memory tile kernels, which 0 picks from
+ * 192 (forward) and 320 (backprojection) pixels up); backward_batch is the
  * number of angles whose detector rows one warp loads together (1, 2 or 4);
  * adjoint_table selects the table-driven transpose once it is prepared.
  * No counterpart in the reference. */

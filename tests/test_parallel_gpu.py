@@ -256,3 +256,30 @@ def test_autotune_caches_winner(tmp_path, monkeypatch):
     assert q.autotune() == first
     with pytest.raises(Exception):
         q.set_tuning({"backward_batch": 3})
+
+
+@pytest.mark.parametrize("n,na", [(40, 30), (33, 17), (128, 180), (257, 90)])
+@pytest.mark.parametrize("absn", [None, "mask", "ray"])
+@pytest.mark.parametrize("path", ["tiles", "generic"])
+def test_single_slice_paths_against_oracle(n, na, absn, path):
+    """2-D slices: the shared-memory tile kernels (default) and the generic kernels both match the oracle."""
+    rng = np.random.default_rng(n + na)
+    ang = np.sort(rng.uniform(0, 360, na))
+    ang[0] = 0.0
+    x = rng.uniform(0, 1, (n, n, 1))
+    b = rng.uniform(0, 1, (n, na, 1))
+    p = plan_for(x.shape, ang)
+    oabs = None
+    if absn == "mask":
+        m = rng.uniform(0.3, 1.0, (n, n))
+        p.set_absorption("mask", mask=m)
+        oabs = ("mask", m)
+    elif absn == "ray":
+        p.set_absorption("ray", alpha_per_px=0.02, radius_px=n / 2 - 1.5)
+        oabs = ("ray", 0.02, n / 2 - 1.5)
+    if path == "generic":
+        p.set_tuning({"forward_vz": 1, "backward_vz": 1, "adjoint_vz": 1})
+    else:
+        p.set_tuning({"forward_vz": 4, "backward_vz": 4})  # tiles at every size
+    assert relL2(p.forward(dev(x)).cpu().numpy(), O.parallel_forward(x, ang, absorption=oabs)) < TOL
+    assert relL2(p.backward_ref(dev(b)).cpu().numpy(), O.parallel_backward_ref(b, ang, absorption=oabs)) < TOL

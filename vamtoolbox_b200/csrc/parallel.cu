@@ -766,6 +766,207 @@ __global__ void __launch_bounds__(256) k_backward_batched(Args a) {
     k_backward_batched_body<VZ, B, RAY>(a, blockIdx.x, blockIdx.y);
 }
 
+// ---------------------------------------------------------------------------
+// 2-D slices (nZ = 1): shared-memory tiles.
+//
+// With one slice there is no contiguous axis to put lanes on: a warp's taps
+// land in up to 32 different cache lines.  These kernels stage, per tile, the
+// region of the image (forward) or of the sinogram (backprojection) the tile's
+// samples touch, with coalesced row loads, and gather from shared memory.
+// The per-sample arithmetic is the generic kernels' (float64 coordinates and
+// np.interp bin, float32 weights); taps that fall outside the staged region
+// (not expected: the region is the tile's exact footprint plus a margin) are
+// read from global memory with the same bounds checks.
+// ---------------------------------------------------------------------------
+constexpr int k2J = 64;     // forward: detector bins per tile
+constexpr int k2K = 64;     // forward: samples per bin per tile
+constexpr int k2Box = 96;   // forward: staged box side >= sqrt(2) (k2J + k2K - 2) + 5
+constexpr int k2Stride = k2Box + 1;
+constexpr int k2Smem = (k2Box * k2Stride + 4 * k2J) * 4;  // box + the k-group partial sums
+constexpr int kB2 = 16;     // backprojection: pixel tile side
+constexpr int kB2A = 32;    // backprojection: angles per staged block (one per lane when staging)
+constexpr int kB2W = 30;    // backprojection: window bins per angle >= sqrt(2) (kB2 - 1) + 6
+constexpr int kB2Smem = kB2A * kB2W * 4 + kB2A * 4 + kB2A * 16;
+
+// grid (ceil(nX / k2J), nA); 256 threads = 64 bins x 4 groups of samples.
+//
+// Per tile the box [rlo, rlo + H) x [clo, clo + W) covers the footprint of all
+// its samples with a margin of one pixel below and two above (rows and cols are
+// affine in j and k, so the corners bound them); it is staged unclipped, with
+// zeros outside the image, which is exactly the zero padding of the reference's
+// warp, so every tap is an unconditional shared-memory read.  Each bin's
+// coordinates are the reference's float64 values at the tile's first sample;
+// the offsets along the ray are float32 (coordinate error below 2e-5 pixel on
+// a continuous bilinear interpolant).
+template <bool RAY>
+__device__ __forceinline__ void k_forward_2d_body(const Args& a, unsigned bx, unsigned by) {
+    extern __shared__ float s_f2[];
+    float* box = s_f2;
+    float* part = s_f2 + k2Box * k2Stride;
+    const int theta = by;
+    const int tj = threadIdx.x % k2J, tk = threadIdx.x / k2J;
+    const int j0 = bx * k2J, j = j0 + tj;
+    const int j1 = min(j0 + k2J, a.nX) - 1;
+    const double4 tr = a.trig[theta];
+    const double c = tr.x, s = tr.y;
+    const float cf = (float)c, sf = (float)s;
+    const double rowb = fma(-s, (double)j, tr.w), colb = fma(c, (double)j, tr.z);
+    float s_entry = 0.f;
+    bool live = j < a.nX;
+    if (RAY) {
+        const float t = (float)(j - a.C);
+        if (fabsf(t) > a.R) live = false;
+        else s_entry = -sqrtf(a.R * a.R - t * t);
+    }
+    const double rb0 = fma(-s, (double)j0, tr.w), rb1 = fma(-s, (double)j1, tr.w);
+    const double cb0 = fma(c, (double)j0, tr.z), cb1 = fma(c, (double)j1, tr.z);
+    auto to_int = [](double v) { return (int)fmax(fmin(floor(v), 1e9), -1e9); };
+    float acc = 0.f;
+    for (int k0 = 0; k0 < a.nY; k0 += k2K) {
+        const int k1 = min(k0 + k2K, a.nY) - 1;
+        double rmin = 1e300, rmax = -1e300, cmin = 1e300, cmax = -1e300;
+        for (int q = 0; q < 4; ++q) {
+            const double rb = (q & 1) ? rb1 : rb0, cb = (q & 1) ? cb1 : cb0;
+            const double kk = (q & 2) ? (double)k1 : (double)k0;
+            const double r = fma(c, kk, rb), cl = fma(s, kk, cb);
+            rmin = fmin(rmin, r); rmax = fmax(rmax, r); cmin = fmin(cmin, cl); cmax = fmax(cmax, cl);
+        }
+        const int rlo = to_int(rmin) - 1, rhi = to_int(rmax) + 2;
+        const int clo = to_int(cmin) - 1, chi = to_int(cmax) + 2;
+        // the whole tile samples outside the image: every tap is zero padding (uniform)
+        if (rhi < 0 || rlo > a.nY - 1 || chi < 0 || clo > a.nX - 1) continue;
+        const int H = min(rhi - rlo + 1, k2Box), W = min(chi - clo + 1, k2Box);
+        // warp w stages rows w, w + 8, ...; lanes run along the row (coalesced, no division)
+        for (int r = (int)(threadIdx.x >> 5); r < H; r += kWarpsPerBlock) {
+            const int gr = rlo + r;
+            const bool rin = (unsigned)gr < (unsigned)a.nY;
+            for (int cc = (int)(threadIdx.x & 31); cc < W; cc += 32) {
+                const int gc = clo + cc;
+                float v = 0.f;
+                if (rin && (unsigned)gc < (unsigned)a.nX) {
+                    const size_t g = (size_t)gr * a.nX + gc;
+                    v = a.mask ? __ldg(a.mask + g) * __ldg(a.in + g) : __ldg(a.in + g);
+                }
+                box[r * k2Stride + cc] = v;
+            }
+        }
+        __syncthreads();
+        if (live) {
+            const float rl0 = (float)(fma(c, (double)k0, rowb) - (double)rlo);
+            const float cl0 = (float)(fma(s, (double)k0, colb) - (double)clo);
+            for (int kk = tk; kk <= k1 - k0; kk += 4) {
+                const float row = fmaf(cf, (float)kk, rl0), col = fmaf(sf, (float)kk, cl0);
+                const float fr = floorf(row), fc = floorf(col);
+                const float dr = row - fr, dc = col - fc;
+                // clamped for memory safety only: the margins keep every weighted tap inside the box
+                const int r0 = min(max((int)fr, 0), H - 2), c0 = min(max((int)fc, 0), W - 2);
+                const float* t0 = box + r0 * k2Stride + c0;
+                const float w00 = (1.f - dr) * (1.f - dc), w01 = (1.f - dr) * dc;
+                const float w10 = dr * (1.f - dc), w11 = dr * dc;
+                float v = w00 * t0[0];
+                v = fmaf(w01, t0[1], v);
+                v = fmaf(w10, t0[k2Stride], v);
+                v = fmaf(w11, t0[k2Stride + 1], v);
+                if (RAY) v *= ray_factor((float)(k0 + kk - a.C), s_entry, a.alpha);
+                acc += v;
+            }
+        }
+        __syncthreads();
+    }
+    part[tk * k2J + tj] = acc;
+    __syncthreads();
+    if (tk == 0 && j < a.nX) {
+        const float sum = ((part[tj] + part[k2J + tj]) + part[2 * k2J + tj]) + part[3 * k2J + tj];
+        a.out[(size_t)j * a.nA + theta] = sum;
+    }
+}
+
+template <bool RAY>
+__global__ void __launch_bounds__(256) k_forward_2d(Args a) {
+    k_forward_2d_body<RAY>(a, blockIdx.x, blockIdx.y);
+}
+
+// grid (ceil(nX / 16) * ceil(nY / 16)); 256 threads = one 16 x 16 pixel tile
+template <bool RAY>
+__device__ __forceinline__ void k_backward_2d_body(const Args& a, unsigned bx, unsigned by) {
+    (void)by;
+    extern __shared__ float s_b2[];
+    float* win = s_b2;                                            // [kB2A][kB2W]
+    int* wlo = reinterpret_cast<int*>(s_b2 + kB2A * kB2W);        // [kB2A] first staged detector row
+    double2* cs = reinterpret_cast<double2*>(s_b2 + kB2A * kB2W + kB2A);  // [kB2A]
+    const int tiles_x = (a.nX + kB2 - 1) / kB2;
+    const int ti = bx / tiles_x, tjx = bx - ti * tiles_x;
+    const int i0 = ti * kB2, jx0 = tjx * kB2;
+    const int i = i0 + (int)threadIdx.x / kB2, j = jx0 + (int)threadIdx.x % kB2;
+    const bool inside = i < a.nY && j < a.nX;
+    const long p = (long)i * a.nX + j;
+    const bool on = inside && a.circle[p];
+    const double X = (double)(j - a.C), Y = (double)(i - a.C);
+    const double tlo = (double)(-a.C), thi = (double)(a.nY - 1 - a.C);
+    // tile corners for the windows
+    const double Xa = (double)(jx0 - a.C), Xb = (double)(min(jx0 + kB2, a.nX) - 1 - a.C);
+    const double Ya = (double)(i0 - a.C), Yb = (double)(min(i0 + kB2, a.nY) - 1 - a.C);
+    float acc = 0.f;
+    for (int th0 = 0; th0 < a.nA; th0 += kB2A) {
+        const int na = min(kB2A, a.nA - th0);
+        if (threadIdx.x < (unsigned)na) {
+            const double4 tr = a.trig[th0 + threadIdx.x];
+            cs[threadIdx.x] = make_double2(tr.x, tr.y);
+            double tmin = 1e300, tmax = -1e300;
+            for (int q = 0; q < 4; ++q) {
+                const double x = (q & 1) ? Xb : Xa, y = (q & 2) ? Yb : Ya;
+                const double t = __dsub_rn(__dmul_rn(x, tr.x), __dmul_rn(y, tr.y));
+                tmin = fmin(tmin, t); tmax = fmax(tmax, t);
+            }
+            wlo[threadIdx.x] = max((int)fmax(fmin(floor(tmin), 1e9), -1e9) + a.C - 2, 0);
+        }
+        __syncthreads();
+        // warp w stages window bins w, w + 8, ...; lane = angle (consecutive angles are contiguous)
+        const int sa = (int)(threadIdx.x & 31);
+        if (sa < na)
+            for (int w = (int)(threadIdx.x >> 5); w < kB2W; w += kWarpsPerBlock) {
+                const int row = wlo[sa] + w;
+                win[sa * kB2W + w] = row < a.nY ? __ldg(a.in + (size_t)row * a.nA + th0 + sa) : 0.f;
+            }
+        __syncthreads();
+        if (on) {
+            for (int al = 0; al < na; ++al) {
+                const double2 cc = cs[al];
+                const double t = __dsub_rn(__dmul_rn(X, cc.x), __dmul_rn(Y, cc.y));
+                if (!(t >= tlo && t <= thi)) continue;  // np.interp left = right = 0
+                const double ft = floor(t);
+                const int j0 = (int)ft + a.C;
+                const int wi = j0 - wlo[al];
+                const int th = th0 + al;
+                auto row = [&](int r, int wr) -> float {
+                    return (unsigned)wr < (unsigned)kB2W ? win[al * kB2W + wr] : __ldg(a.in + (size_t)r * a.nA + th);
+                };
+                float v = row(j0, wi);
+                if (t != ft) v = fmaf((float)(t - ft), row(j0 + 1, wi + 1) - v, v);
+                if (RAY) {
+                    float f = 0.f;
+                    if (fabs(t) <= (double)a.R) {
+                        const float sv = (float)__dadd_rn(__dmul_rn(X, cc.y), __dmul_rn(Y, cc.x));
+                        f = ray_factor(sv, (float)(-sqrt((double)a.R * a.R - t * t)), a.alpha);
+                    }
+                    v *= f;
+                }
+                acc += v;
+            }
+        }
+        __syncthreads();
+    }
+    if (inside) {
+        if (a.mask) acc = __ldg(a.mask + p) * acc;
+        a.out[p] = acc;
+    }
+}
+
+template <bool RAY>
+__global__ void __launch_bounds__(256) k_backward_2d(Args a) {
+    k_backward_2d_body<RAY>(a, blockIdx.x, blockIdx.y);
+}
+
 __global__ void k_mask_mul(const float* __restrict__ x, const float* __restrict__ mask, float* __restrict__ out,
                            long npix, int nZ) {
     const long n = npix * nZ;
@@ -1055,7 +1256,7 @@ int fast_vz(int nZ, bool aligned, double min_eff) {
 // same body for many calls inside one persistent launch.  Both paths therefore
 // compute bit-identical results.
 // ---------------------------------------------------------------------------
-enum Kind : int { KF_FAST = 0, KF_GEN, KB_BATCHED, KB_FAST, KB_GEN, KA_TABLE, KA_FAST, KA_GEN };
+enum Kind : int { KF_FAST = 0, KF_GEN, KB_BATCHED, KB_FAST, KB_GEN, KA_TABLE, KA_FAST, KA_GEN, KF_2D, KB_2D };
 
 struct Item {
     int kind;
@@ -1094,6 +1295,35 @@ int describe(vam_parallel_plan* plan, Op op, const float* in, float* out, Item& 
         else if (want == 0) vzf = fast_vz(plan->nZ, true, op == Op::Forward ? 0.45 : 0.74);
     }
     const bool ray = plan->abs_mode == VAM_ABS_RAY;
+    // 2-D slice: shared-memory tiles when tuned to them (any width but 1), or automatically for
+    // slices wide enough to fill the device with tiles (forward from 192, backprojection from 320 px)
+    const bool tiles_2d = want == 0 ? plan->nX >= (op == Op::Forward ? 192 : 320) : want != 1;
+    if (plan->nZ == 1 && !plan->has_occ && op != Op::Adjoint && tiles_2d) {
+        Args& a = it.a;
+        a.in = in; a.out = out; a.trig = plan->d_trig; a.circle = plan->d_circle;
+        a.mask = plan->abs_mode == VAM_ABS_MASK ? plan->d_mask : nullptr;
+        a.nY = plan->nY; a.nX = plan->nX; a.nZ = 1; a.nA = plan->nA; a.C = plan->C;
+        a.alpha = plan->abs_alpha; a.R = plan->abs_R;
+        it.ray = ray;
+        it.vz = 1;
+        if (op == Op::Forward) {
+            if (a.mask) {  // stage the masked image once per call instead of per tile
+                it.pre_in = in; it.pre_mask = plan->d_mask; it.pre_out = plan->d_vol_scratch;
+                it.pre_npix = (long long)plan->nY * plan->nX; it.pre_nz = 1;
+                a.in = plan->d_vol_scratch;
+                a.mask = nullptr;
+            }
+            it.kind = KF_2D;
+            it.gx = (unsigned)((plan->nX + k2J - 1) / k2J);
+            it.gy = (unsigned)plan->nA;
+            it.smem = k2Smem;
+        } else {
+            it.kind = KB_2D;
+            it.gx = (unsigned)(((plan->nX + kB2 - 1) / kB2) * ((plan->nY + kB2 - 1) / kB2));
+            it.smem = kB2Smem;
+        }
+        return VAM_OK;
+    }
     if (op == Op::Forward && !plan->has_occ && (long)plan->nY * plan->nX * plan->nZ < (1L << 31) && vzf) {
         FastArgs& a = it.f;
         a.vol = in;
@@ -1185,10 +1415,16 @@ __device__ __forceinline__ void fast_body(const Item& it, unsigned bx, unsigned 
             const FastArgs f = it.f;
             if (it.vz == 8) k_forward_fast_body<8, RAY>(f, bx, by);
             else k_forward_fast_body<4, RAY>(f, bx, by);
+        } else if (it.kind == KF_2D) {
+            const Args a = it.a;
+            k_forward_2d_body<RAY>(a, bx, by);
         }
     }
     if constexpr ((FAM & 2) != 0) {
-        if (it.kind == KB_BATCHED) {
+        if (it.kind == KB_2D) {
+            const Args a = it.a;
+            k_backward_2d_body<RAY>(a, bx, by);
+        } else if (it.kind == KB_BATCHED) {
             const Args a = it.a;
             if (it.vz == 8) k_backward_batched_body<8, 2, RAY>(a, bx, by);
             else if (it.batch == 4) k_backward_batched_body<4, 4, RAY>(a, bx, by);
@@ -1249,6 +1485,8 @@ template <bool RAY>
 void launch_fast(const Item& it, dim3 grid, cudaStream_t st) {
     const dim3 block(kWarpsPerBlock * kWarp);
     switch (it.kind) {
+        case KF_2D: k_forward_2d<RAY><<<grid, block, it.smem, st>>>(it.a); break;
+        case KB_2D: k_backward_2d<RAY><<<grid, block, it.smem, st>>>(it.a); break;
         case KF_FAST:
             if (it.vz == 8) k_forward_fast<8, RAY><<<grid, block, 0, st>>>(it.f);
             else k_forward_fast<4, RAY><<<grid, block, 0, st>>>(it.f);
@@ -1689,6 +1927,8 @@ double time_weight(const Item& it) {
         case KB_GEN: return slice ? 10.0 : 2.0;
         case KA_TABLE: return 1.5;
         case KA_FAST: return 3.5;
+        case KF_2D: return 4.0;
+        case KB_2D: return 2.0;
         default: return slice ? 27.0 : 4.0;
     }
 }

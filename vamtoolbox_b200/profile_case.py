@@ -1,6 +1,7 @@
 """Small, self-contained runs of one hot-path kernel, for profilers.
 
     python -m vamtoolbox_b200.profile_case parallel --size 256 --angles 360 --calls 2
+    python -m vamtoolbox_b200.profile_case parallel --size 512 --angles 720 --slices 1
     python -m vamtoolbox_b200.profile_case ray --size 96 --angles 120 --calls 1
 
 ``parallel`` runs forward, reference-parity backprojection and the matched
@@ -21,15 +22,16 @@ import numpy as np
 import torch
 
 
-def run_parallel(n, na, calls, tuning):
+def run_parallel(n, na, calls, tuning, nz=None):
     from .projector.Projector3DParallel import ParallelPlan
 
-    p = ParallelPlan(n, n, n, np.linspace(0, 360, na, endpoint=False))
+    nz = n if nz is None else nz
+    p = ParallelPlan(n, n, nz, np.linspace(0, 360, na, endpoint=False))
     if tuning:
         p.set_tuning(tuning)
     g = torch.Generator(device="cuda").manual_seed(0)
-    x = torch.rand((n, n, n), device="cuda", generator=g)
-    b = torch.rand((n, na, n), device="cuda", generator=g)
+    x = torch.rand((n, n, nz), device="cuda", generator=g)
+    b = torch.rand((n, na, nz), device="cuda", generator=g)
     ob, ox = torch.empty_like(b), torch.empty_like(x)
     p.prepare_adjoint()
     for _ in range(calls):
@@ -37,7 +39,7 @@ def run_parallel(n, na, calls, tuning):
         p.backward_ref(b, ox)
         p.adjoint(b, ox)
     torch.cuda.synchronize()
-    return f"parallel {n}^3 x {na}: tuning {p.get_tuning()}"
+    return f"parallel {n}^2 x {nz} x {na}: tuning {p.get_tuning()}"
 
 
 def run_ray(n, na, calls):
@@ -101,6 +103,7 @@ def main(argv=None):
     ap.add_argument("--size", type=int, default=None)
     ap.add_argument("--angles", type=int, default=None)
     ap.add_argument("--calls", type=int, default=1)
+    ap.add_argument("--slices", type=int, default=None, help="parallel case: nZ (default: size; 1 = a 2-D slice)")
     ap.add_argument("--tuning", default="", help="comma list key=value of launch shapes (parallel case)")
     a = ap.parse_args(argv)
     if a.case == "summarize":
@@ -109,7 +112,7 @@ def main(argv=None):
     torch.cuda.set_device(0)
     if a.case == "parallel":
         tuning = dict((k, int(v)) for k, v in (kv.split("=") for kv in a.tuning.split(",") if kv))
-        print(run_parallel(a.size or 256, a.angles or 360, a.calls, tuning))
+        print(run_parallel(a.size or 256, a.angles or 360, a.calls, tuning, a.slices))
     else:
         print(run_ray(a.size or 96, a.angles or 120, a.calls))
 
