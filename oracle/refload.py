@@ -130,6 +130,48 @@ def load():
     return pkg
 
 
+class _NoInferenceMode:
+    """Stands in for torch.inference_mode while a module is imported: as a decorator it returns the
+    function unchanged, as a context manager it does nothing, so the reference's tracer records
+    autograd graphs."""
+
+    def __init__(self, *a, **k):
+        pass
+
+    def __call__(self, fn):
+        return fn
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+
+def load_autograd_tracer():
+    """Second copies of the reference's pyTorchRayTrace.py and medium.py, imported with
+    torch.inference_mode neutralised (their decorators are applied at import), so gradients can be
+    taken through the reference's own ray tracer.  Returns (tracer module, medium module)."""
+    import importlib.util
+
+    import torch
+
+    load()
+    orig = torch.inference_mode
+    torch.inference_mode = _NoInferenceMode
+    try:
+        mods = []
+        for name, rel in (("vamtoolbox.projector._rt_autograd", "projector/pyTorchRayTrace.py"),
+                          ("vamtoolbox._medium_autograd", "medium.py")):
+            spec = importlib.util.spec_from_file_location(name, os.path.join(REF, "vamtoolbox", rel))
+            m = importlib.util.module_from_spec(spec)
+            spec.loader.exec_module(m)
+            mods.append(m)
+    finally:
+        torch.inference_mode = orig
+    return mods[0], mods[1]
+
+
 def fresh_options(pkg, **kw):
     """Options(...) with the class-level default dicts restored first.
 

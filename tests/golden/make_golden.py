@@ -176,6 +176,46 @@ def ray_cases(vam):
     np.savez_compressed(OUT / "raytrace.npz", **out)
 
 
+def ray_autograd_cases(vam):
+    """Gradients of L = <w, forward(f)> with respect to f and to the attenuation grid, taken by
+    autograd through the reference's own ray tracer (inference_mode neutralised)."""
+    import torch
+
+    RT, MED = refload.load_autograd_tracer()
+    geo = vam.geometry
+    rng = np.random.default_rng(7)
+    n, nz = 12, 6
+    tg = geo.TargetGeometry(target=rng.uniform(0, 1, (n, n, nz)))
+    cv = tg.constructCoordVec()
+    xg, yg, _ = np.meshgrid(*cv, indexing="ij")
+    R = np.amax(cv[0])
+    n_x = 1.30 + 0.05 * (xg ** 2 + yg ** 2) / R ** 2
+    alpha_np = 20.0 * (1 + 0.3 * rng.uniform(-1, 1, xg.shape))
+    alpha_x = torch.as_tensor(alpha_np).requires_grad_(True)
+    im = MED.IndexModel(cv, type="interpolation", form="freeform", n_x=torch.as_tensor(n_x))
+    am = MED.AttenuationModel(cv, type="interpolation", form="freeform", alpha_x=alpha_x)
+    ab = MED.AttenuationModel(cv, type="analytical", form="homogeneous_cylinder", R=1, alpha_internal=10.0)
+    ang = np.linspace(0, 360, 5, endpoint=False)
+    pg = geo.ProjectionGeometry(ang, "ray_trace", CUDA=False, index_model=im, attenuation_model=am,
+                                absorption_model=ab, ray_trace_method="eikonal",
+                                eikonal_parametrization="physical_path_length",
+                                ray_trace_ode_solver="forward_symplectic_euler", ray_trace_ray_config="parallel",
+                                inclination_angle=0.0, ray_density=1)
+    P = RT.PyTorchRayTracingPropagator(tg, pg)
+    P.output_torch_tensor = True
+    f = rng.uniform(0, 1, (n, n, nz))
+    f_leaf = torch.as_tensor(f).requires_grad_(True)
+    g = P.forward(f_leaf * 1.0)  # the reference scales its input in place: hand it a non-leaf copy
+    w = rng.uniform(0, 1, tuple(g.shape))
+    L = (g * torch.as_tensor(w, dtype=g.dtype)).sum()
+    L.backward()
+    out = {"ag_xv": cv[0], "ag_yv": cv[1], "ag_zv": cv[2], "ag_n": n_x, "ag_alpha": alpha_np, "ag_angles": ang,
+           "ag_f": f, "ag_w": w, "ag_fwd": g.detach().numpy(), "ag_L": np.array(float(L.detach())),
+           "ag_grad_f": f_leaf.grad.numpy(), "ag_grad_alpha": alpha_x.grad.numpy(),
+           "ag_absorption": np.array([1.0, 10.0])}
+    np.savez_compressed(OUT / "ray_autograd.npz", **out)
+
+
 def optimizer_cases(vam):
     geo = vam.geometry
     out = {}
@@ -235,6 +275,7 @@ def main():
     vam = refload.load()
     parallel_cases(vam)
     ray_cases(vam)
+    ray_autograd_cases(vam)
     optimizer_cases(vam)
     for p in sorted(OUT.glob("*.npz")):
         print(p.name, p.stat().st_size)

@@ -91,3 +91,35 @@ def test_ray_integrate_gradients():
                          - ray_integrate(f, plan, alpha - h * d, im, am, ab)).double() * w.double()).sum() / (2 * h))
             an = float((alpha.grad.double() * d.double()).sum())
             assert abs(fd - an) <= 2e-2 * abs(fd) + 1e-5, (fd, an)
+
+
+def test_ray_gradients_match_reference_autograd(golden):
+    """Gradients of L = <w, integrate(f)> w.r.t. f and the attenuation grid, against autograd through the
+    reference's own PyTorch ray tracer (float64 fields there, float32 here).  Tolerances: relative L2
+    1e-4 for d/df (a linear map: the deposit), 2e-3 for d/dalpha (float32 exp / suffix sums of the
+    attenuance against the reference's float64 autograd graph)."""
+    from tests.conftest import relL2
+    from vamtoolbox_b200 import geometry, medium
+    from vamtoolbox_b200.autograd import ray_integrate
+    from vamtoolbox_b200.projector.pyTorchRayTrace import RayPlan
+
+    G = golden["ray_autograd"]
+    cv = [G["ag_xv"], G["ag_yv"], G["ag_zv"]]
+    tg = geometry.TargetGeometry(target=np.zeros((cv[0].size, cv[1].size, cv[2].size)))
+    assert all(np.array_equal(a, b) for a, b in zip(tg.constructCoordVec(), cv))
+    im = medium.IndexModel(cv, type="interpolation", form="freeform", n_x=torch.as_tensor(G["ag_n"]))
+    am = medium.AttenuationModel(cv, type="interpolation", form="freeform", alpha_x=torch.as_tensor(G["ag_alpha"]))
+    R_abs, a_abs = G["ag_absorption"]
+    ab = medium.AttenuationModel(cv, type="analytical", form="homogeneous_cylinder", R=float(R_abs),
+                                 alpha_internal=float(a_abs))
+    plan = RayPlan(cv, G["ag_angles"], im, am, ab)
+    f = torch.as_tensor(G["ag_f"], device="cuda", dtype=torch.float32).requires_grad_(True)
+    alpha = torch.as_tensor(G["ag_alpha"], device="cuda", dtype=torch.float32).requires_grad_(True)
+    w = torch.as_tensor(G["ag_w"], device="cuda", dtype=torch.float32)
+    g = ray_integrate(f, plan, alpha, im, am, ab)
+    assert relL2(g.detach().cpu().numpy(), G["ag_fwd"]) < 1e-4
+    L = (g * w).sum()
+    L.backward()
+    assert abs(float(L) - float(G["ag_L"])) <= 1e-4 * abs(float(G["ag_L"]))
+    assert relL2(f.grad.cpu().numpy(), G["ag_grad_f"]) < 1e-4
+    assert relL2(alpha.grad.cpu().numpy(), G["ag_grad_alpha"]) < 2e-3

@@ -103,3 +103,24 @@ def test_ray_oracle_analytic_medium(golden):
     assert relL2(g, R["ha_fwd"]) < 1e-6
     d, _ = O.ray_trace("deposit", dict(xv=xv, yv=yv, zv=zv), x0, v0, 1.0, g=R["ha_g"], **kw)
     assert relL2(d, R["ha_bwd"]) < 1e-6
+
+
+def test_ray_oracle_gradient_matches_reference_autograd(golden):
+    """d<w, forward(f)>/df through the reference's autograd equals the oracle's deposit of w (the exact
+    transpose), with the absorbing cylinder applied at the grid points."""
+    import torch
+
+    G = golden["ray_autograd"]
+    xv, yv, zv = G["ag_xv"], G["ag_yv"], G["ag_zv"]
+    x0, v0, _ = O.setup_rays_parallel(xv, yv, zv, G["ag_angles"])
+    _, aval = G["ag_absorption"]
+    Rc = min((xv.max() - xv.min()) / 2, (yv.max() - yv.min()) / 2, (zv.max() - zv.min()) / 2)
+    xg, yg, zg = np.meshgrid(xv, yv, zv, indexing="ij")
+    r = torch.linalg.norm(torch.as_tensor(np.stack([xg.ravel(), yg.ravel()], 1)), dim=1).numpy()
+    absorb = np.where(r < Rc, aval, 0.0).reshape(xg.shape)
+    kw = dict(step_size=(xv[1] - xv[0]) / 2, max_num_step=3 * xv.size, n_kind=1, n_grid=G["ag_n"], a_kind=3,
+              a_grid=G["ag_alpha"], absorb=absorb)
+    g, _ = O.ray_trace("integrate", dict(xv=xv, yv=yv, zv=zv), x0, v0, 1.0, f=G["ag_f"], **kw)
+    assert relL2(g, G["ag_fwd"]) < 1e-6
+    d, _ = O.ray_trace("deposit", dict(xv=xv, yv=yv, zv=zv), x0, v0, 1.0, g=G["ag_w"], **kw)
+    assert relL2(d, G["ag_grad_f"]) < 1e-6

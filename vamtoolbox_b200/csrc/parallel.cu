@@ -562,11 +562,9 @@ __device__ __forceinline__ void k_backward_fast_body(const Args& a, unsigned bx,
                     f = ray_factor(sv, (float)(-sqrt((double)a.R * a.R - t * t)), a.alpha);
                 }
             }
+            const float w1 = RAY ? w * f : w, w0 = RAY ? (1.f - w) * f : 1.f - w;
 #pragma unroll
-            for (int e = 0; e < VZ; ++e) {
-                const float v = fmaf(w, v1[e] - v0[e], v0[e]);
-                acc[e] = RAY ? fmaf(v, f, acc[e]) : acc[e] + v;
-            }
+            for (int e = 0; e < VZ; ++e) acc[e] = fmaf(w1, v1[e], fmaf(w0, v0[e], acc[e]));
         }
     }
     if (!zok) return;
@@ -744,13 +742,14 @@ __device__ __forceinline__ void k_backward_batched_body(const Args& a, unsigned 
                     for (int e = 0; e < VZ; ++e) v0[u][e] = v1[u][e] = 0.f;
                 }
             }
+            // acc += (1 - w) v0 + w v1 (times the ray factor): two FMAs per slice
 #pragma unroll
-            for (int u = 0; u < B; ++u)
+            for (int u = 0; u < B; ++u) {
+                const float w1 = RAY ? w[u] * f[u] : w[u];
+                const float w0 = RAY ? (1.f - w[u]) * f[u] : 1.f - w[u];
 #pragma unroll
-                for (int e = 0; e < VZ; ++e) {
-                    const float v = fmaf(w[u], v1[u][e] - v0[u][e], v0[u][e]);
-                    acc[e] = RAY ? fmaf(v, f[u], acc[e]) : acc[e] + v;
-                }
+                for (int e = 0; e < VZ; ++e) acc[e] = fmaf(w1, v1[u][e], fmaf(w0, v0[u][e], acc[e]));
+            }
         }
     }
     if (a.mask) {
