@@ -538,31 +538,32 @@ __device__ __forceinline__ void k_backward_fast_body(const Args& a, unsigned bx,
     if (a.circle[p] && zok) {
         const double X = (double)(j - a.C), Y = (double)(i - a.C);
         const double tlo = (double)(-a.C), thi = (double)(a.nY - 1 - a.C);
-        const size_t rs = (size_t)a.nA * a.nZ;
+        const int rs = a.nA * a.nZ, nYm1 = a.nY - 1;  // sinogram below 2^31 elements on this path
         const float* __restrict__ bz = a.in + z0;
 #pragma unroll 2
         for (int th = 0; th < a.nA; ++th) {
             const double4 tr = a.trig[th];
             const double t = __dsub_rn(__dmul_rn(X, tr.x), __dmul_rn(Y, tr.y));
-            if (!(t >= tlo && t <= thi)) continue;
+            // np.interp(left = right = 0): out-of-range angles read clamped rows with zero weight
+            const bool ok = t >= tlo && t <= thi;
             const double ft = floor(t);
-            const int j0 = (int)ft + a.C;
-            const float* b0 = bz + (size_t)j0 * rs + (size_t)th * a.nZ;
+            const int j0 = min(max((int)fmax(fmin(ft, 1e9), -1e9) + a.C, 0), nYm1);
             float v0[VZ], v1[VZ];
-            load_vz<VZ>(b0, v0, qn);
+            load_vz<VZ>(bz + j0 * rs + th * a.nZ, v0, qn);
             // t == floor(t): np.interp returns fp[j]; the second row is read with weight 0
             const float w = (float)(t - ft);
-            load_vz<VZ>(b0 + (t != ft ? rs : 0), v1, qn);
-            float f = 1.f;
+            load_vz<VZ>(bz + min(j0 + 1, nYm1) * rs + th * a.nZ, v1, qn);
+            float f = ok ? 1.f : 0.f;
             if (RAY) {
                 // |t| <= R is a discontinuity of the model: decide it on the float64 t
-                f = 0.f;
-                if (fabs(t) <= (double)a.R) {
+                if (ok && fabs(t) <= (double)a.R) {
                     const float sv = (float)__dadd_rn(__dmul_rn(X, tr.y), __dmul_rn(Y, tr.x));
                     f = ray_factor(sv, (float)(-sqrt((double)a.R * a.R - t * t)), a.alpha);
+                } else {
+                    f = 0.f;
                 }
             }
-            const float w1 = RAY ? w * f : w, w0 = RAY ? (1.f - w) * f : 1.f - w;
+            const float w1 = w * f, w0 = (1.f - w) * f;
 #pragma unroll
             for (int e = 0; e < VZ; ++e) acc[e] = fmaf(w1, v1[e], fmaf(w0, v0[e], acc[e]));
         }
@@ -704,52 +705,48 @@ __device__ __forceinline__ void k_backward_batched_body(const Args& a, unsigned 
     if (a.circle[p]) {
         const double X = (double)(j - a.C), Y = (double)(i - a.C);
         const double tlo = (double)(-a.C), thi = (double)(a.nY - 1 - a.C);
-        const size_t rs = (size_t)a.nA * a.nZ;
+        // 32-bit offsets: the fast path is taken only for sinograms below 2^31 elements
+        const int rs = a.nA * a.nZ, nYm1 = a.nY - 1;
         const float* __restrict__ bz = a.in + z0;
         for (int th0 = 0; th0 < a.nA; th0 += B) {
-            size_t o0[B], o1[B];
-            float w[B], f[B];
-            bool ok[B];
+            int o0[B], o1[B];
+            float w0[B], w1[B];
 #pragma unroll
             for (int u = 0; u < B; ++u) {
-                const int th = th0 + u;
-                ok[u] = th < a.nA;
-                const double2 cs = s_cs[ok[u] ? th : 0];
+                // a batch past the last angle rereads the last angle with zero weights
+                const int th = min(th0 + u, a.nA - 1);
+                const double2 cs = s_cs[th];
                 const double t = __dsub_rn(__dmul_rn(X, cs.x), __dmul_rn(Y, cs.y));
-                ok[u] = ok[u] && (t >= tlo && t <= thi);
+                // np.interp(left = right = 0): an angle outside [xp[0], xp[-1]] adds nothing; its taps
+                // are clamped reads with zero weight instead of a branch
+                const bool ok = th0 + u < a.nA && t >= tlo && t <= thi;
                 const double ft = floor(t);
-                const int j0 = ok[u] ? (int)ft + a.C : 0;
-                w[u] = (float)(t - ft);
-                o0[u] = (size_t)j0 * rs + (size_t)th * a.nZ;
-                o1[u] = o0[u] + ((t != ft) ? rs : 0);
-                f[u] = 1.f;
+                const int j0 = min(max((int)fmax(fmin(ft, 1e9), -1e9) + a.C, 0), nYm1);
+                const float w = (float)(t - ft);
+                float f = 1.f;
                 if (RAY) {
-                    f[u] = 0.f;
+                    f = 0.f;
                     if (fabs(t) <= (double)a.R) {
                         const float sv = (float)__dadd_rn(__dmul_rn(X, cs.y), __dmul_rn(Y, cs.x));
-                        f[u] = ray_factor(sv, (float)(-sqrt((double)a.R * a.R - t * t)), a.alpha);
+                        f = ray_factor(sv, (float)(-sqrt((double)a.R * a.R - t * t)), a.alpha);
                     }
                 }
+                w1[u] = ok ? w * f : 0.f;        // t == floor(t): w = 0, the second row is not used
+                w0[u] = ok ? (1.f - w) * f : 0.f;
+                o0[u] = j0 * rs + th * a.nZ;
+                o1[u] = min(j0 + 1, nYm1) * rs + th * a.nZ;
             }
             float v0[B][VZ], v1[B][VZ];
 #pragma unroll
             for (int u = 0; u < B; ++u) {
-                if (ok[u]) {
-                    load_vz<VZ>(bz + o0[u], v0[u], qn);
-                    load_vz<VZ>(bz + o1[u], v1[u], qn);
-                } else {
-#pragma unroll
-                    for (int e = 0; e < VZ; ++e) v0[u][e] = v1[u][e] = 0.f;
-                }
+                load_vz<VZ>(bz + o0[u], v0[u], qn);
+                load_vz<VZ>(bz + o1[u], v1[u], qn);
             }
             // acc += (1 - w) v0 + w v1 (times the ray factor): two FMAs per slice
 #pragma unroll
-            for (int u = 0; u < B; ++u) {
-                const float w1 = RAY ? w[u] * f[u] : w[u];
-                const float w0 = RAY ? (1.f - w[u]) * f[u] : 1.f - w[u];
+            for (int u = 0; u < B; ++u)
 #pragma unroll
-                for (int e = 0; e < VZ; ++e) acc[e] = fmaf(w1, v1[u][e], fmaf(w0, v0[u][e], acc[e]));
-            }
+                for (int e = 0; e < VZ; ++e) acc[e] = fmaf(w1[u], v1[u][e], fmaf(w0[u], v0[u][e], acc[e]));
         }
     }
     if (a.mask) {
@@ -1344,7 +1341,7 @@ int describe(vam_parallel_plan* plan, Op op, const float* in, float* out, Item& 
         it.gy = (unsigned)(ray ? plan->nA : plan->n_tasks_paired);
         return VAM_OK;
     }
-    if (op != Op::Forward && !plan->has_occ && vzf) {
+    if (op != Op::Forward && !plan->has_occ && vzf && (long long)plan->nY * plan->nA * plan->nZ < (1LL << 31)) {
         Args& a = it.a;
         a.in = in; a.out = out; a.trig = plan->d_trig; a.circle = plan->d_circle;
         a.mask = plan->abs_mode == VAM_ABS_MASK ? plan->d_mask : nullptr;
