@@ -102,8 +102,8 @@ class ParallelPlan:
     _TUNING_FIELDS = ("forward_vz", "backward_vz", "adjoint_vz", "backward_batch", "adjoint_table")
 
     def set_tuning(self, tuning):
-        """Set launch shapes: dict with any of forward_vz / backward_vz / adjoint_vz (0, 4, 8),
-        backward_batch (1, 2, 4) and adjoint_table (0, 1); missing keys keep their value."""
+        """Set launch shapes: dict with any of forward_vz / backward_vz / adjoint_vz (0 auto, 1 generic,
+        4, 8), backward_batch (1, 2, 4) and adjoint_table (0, 1); missing keys keep their value."""
         cur = self.get_tuning()
         unknown = set(tuning) - set(self._TUNING_FIELDS)
         if unknown:
