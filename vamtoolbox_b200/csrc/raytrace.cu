@@ -71,6 +71,16 @@ struct RayArgs {
 
 constexpr int kRayThreads = 128;
 
+// CFG selects how the medium and the integrator are known: 0 reads them from
+// the arguments at run time, 1 is the common configuration fixed at compile
+// time (grid index, grid attenuation, physical path length, forward symplectic
+// Euler), so the step has no configuration branches.
+constexpr int kCfgRuntime = 0, kCfgGridSymplectic = 1;
+template <int CFG> __device__ __forceinline__ int n_kind(const RayArgs& a) { return CFG == kCfgGridSymplectic ? (int)VAM_INDEX_GRID : a.n_kind; }
+template <int CFG> __device__ __forceinline__ int a_kind(const RayArgs& a) { return CFG == kCfgGridSymplectic ? (int)VAM_ALPHA_GRID : a.a_kind; }
+template <int CFG> __device__ __forceinline__ int param(const RayArgs& a) { return CFG == kCfgGridSymplectic ? (int)VAM_PARAM_PHYSICAL : a.param; }
+template <int CFG> __device__ __forceinline__ int solver(const RayArgs& a) { return CFG == kCfgGridSymplectic ? (int)VAM_ODE_SYMPLECTIC_EULER : a.solver; }
+
 // grid_sample(align_corners=True) unnormalised coordinate of axis d
 __device__ __forceinline__ float unnorm(float x, float nrm, int size, bool border) {
     float u = x * nrm;
@@ -117,11 +127,12 @@ __device__ __forceinline__ void grid_coords(const RayArgs& a, const float* x, fl
 }
 
 // u: grid_coords(x), read only by the GRID kind
+template <int CFG>
 __device__ __forceinline__ void index_at(const RayArgs& a, const float* x, const float* u, float& n, float* gn) {
-    if (a.n_kind == VAM_INDEX_GRID) {
+    if (n_kind<CFG>(a) == VAM_INDEX_GRID) {
         const float4 t = sample_n(a, u);
         n = t.x; gn[0] = t.y; gn[1] = t.z; gn[2] = t.w;
-    } else if (a.n_kind == VAM_INDEX_LUNEBURG) {
+    } else if (n_kind<CFG>(a) == VAM_INDEX_LUNEBURG) {
         const float r = sqrtf(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
         if (r < a.lune_R) {
             n = a.n_sur * powf(2.f - powf(r / a.lune_R, a.lune_p), 1.f / a.lune_p);
@@ -139,13 +150,15 @@ __device__ __forceinline__ void index_at(const RayArgs& a, const float* x, const
 
 // attenuation coefficient at x (medium.py:753-915; GRID uses zero padding)
 // u: grid_coords(x), read only by the GRID kind
+template <int CFG>
 __device__ __forceinline__ float alpha_at(const RayArgs& a, const float* x, const float* u) {
-    if (a.a_kind == VAM_ALPHA_CYLINDER || a.a_kind == VAM_ALPHA_BALL) {
+    const int ak = a_kind<CFG>(a);
+    if (ak == VAM_ALPHA_CYLINDER || ak == VAM_ALPHA_BALL) {
         float r2 = x[0] * x[0] + x[1] * x[1];
-        if (a.a_kind == VAM_ALPHA_BALL) r2 += x[2] * x[2];
+        if (ak == VAM_ALPHA_BALL) r2 += x[2] * x[2];
         return sqrtf(r2) < a.a_R ? a.a_val : 0.f;
     }
-    if (a.a_kind != VAM_ALPHA_GRID) return 0.f;
+    if (ak != VAM_ALPHA_GRID) return 0.f;
     const float ix = u[0], iy = u[1], iz = u[2];
     // far outside the grid every corner is zero padding
     if (!(ix > -1.f && ix < (float)a.nx && iy > -1.f && iy < (float)a.ny && iz > -1.f && iz < (float)a.nz)) return 0.f;
@@ -168,15 +181,17 @@ __device__ __forceinline__ float alpha_at(const RayArgs& a, const float* x, cons
 }
 
 // dv/dstep and dx/dstep of the three parametrisations (pyTorchRayTrace.py:694-735)
+template <int CFG>
 __device__ __forceinline__ void dv_dstep(const RayArgs& a, float n, const float* gn, float* dv) {
-    if (a.param == VAM_PARAM_CANONICAL) { dv[0] = n * gn[0]; dv[1] = n * gn[1]; dv[2] = n * gn[2]; }
-    else if (a.param == VAM_PARAM_OPTICAL) { dv[0] = gn[0] / n; dv[1] = gn[1] / n; dv[2] = gn[2] / n; }
+    if (param<CFG>(a) == VAM_PARAM_CANONICAL) { dv[0] = n * gn[0]; dv[1] = n * gn[1]; dv[2] = n * gn[2]; }
+    else if (param<CFG>(a) == VAM_PARAM_OPTICAL) { dv[0] = gn[0] / n; dv[1] = gn[1] / n; dv[2] = gn[2] / n; }
     else { dv[0] = gn[0]; dv[1] = gn[1]; dv[2] = gn[2]; }
 }
 
+template <int CFG>
 __device__ __forceinline__ void dx_dstep(const RayArgs& a, float n, const float* v, float* dx) {
-    if (a.param == VAM_PARAM_CANONICAL) { dx[0] = v[0]; dx[1] = v[1]; dx[2] = v[2]; }
-    else if (a.param == VAM_PARAM_OPTICAL) {
+    if (param<CFG>(a) == VAM_PARAM_CANONICAL) { dx[0] = v[0]; dx[1] = v[1]; dx[2] = v[2]; }
+    else if (param<CFG>(a) == VAM_PARAM_OPTICAL) {
         const float in2 = 1.f / (n * n);
         dx[0] = v[0] * in2; dx[1] = v[1] * in2; dx[2] = v[2] * in2;
     } else { const float rn = 1.f / n; dx[0] = v[0] * rn; dx[1] = v[1] * rn; dx[2] = v[2] * rn; }
@@ -188,6 +203,7 @@ struct RayState {
     bool active;
 };
 
+template <int CFG>
 __device__ __forceinline__ void ray_init(const RayArgs& a, int64_t r, float E0, RayState& st) {
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
@@ -198,11 +214,11 @@ __device__ __forceinline__ void ray_init(const RayArgs& a, int64_t r, float E0, 
     st.E0 = E0;
     st.E = E0;
     st.active = true;
-    if (a.solver == VAM_ODE_LEAPFROG) {  // half step back in v (pyTorchRayTrace.py:816-828)
+    if (solver<CFG>(a) == VAM_ODE_LEAPFROG) {  // half step back in v (pyTorchRayTrace.py:816-828)
         float n, gn[3], dv[3], u[3];
         grid_coords(a, st.xp, u);
-        index_at(a, st.xp, u, n, gn);
-        dv_dstep(a, n, gn, dv);
+        index_at<CFG>(a, st.xp, u, n, gn);
+        dv_dstep<CFG>(a, n, gn, dv);
 #pragma unroll
         for (int d = 0; d < 3; ++d) st.vp[d] = st.vp[d] - dv[d] * a.h / 2.f;
     }
@@ -210,21 +226,22 @@ __device__ __forceinline__ void ray_init(const RayArgs& a, int64_t r, float E0, 
 
 // One step of the configured ODE solver; returns the physical length ds and
 // the attenuation alpha(x_i) used for the energy update.
+template <int CFG>
 __device__ __forceinline__ void ray_step(const RayArgs& a, RayState& st, float& ds, float& alpha) {
 #pragma unroll
     for (int d = 0; d < 3; ++d) { st.xi[d] = st.xp[d]; st.vi[d] = st.vp[d]; }
     float n, gn[3], dv[3], dx[3], u[3];
     grid_coords(a, st.xi, u);
-    index_at(a, st.xi, u, n, gn);
-    dv_dstep(a, n, gn, dv);
+    index_at<CFG>(a, st.xi, u, n, gn);
+    dv_dstep<CFG>(a, n, gn, dv);
 #pragma unroll
     for (int d = 0; d < 3; ++d) st.vp[d] = st.vi[d] + dv[d] * a.h;
-    if (a.solver == VAM_ODE_EULER) dx_dstep(a, n, st.vi, dx);
-    else dx_dstep(a, n, st.vp, dx);
+    if (solver<CFG>(a) == VAM_ODE_EULER) dx_dstep<CFG>(a, n, st.vi, dx);
+    else dx_dstep<CFG>(a, n, st.vp, dx);
 #pragma unroll
     for (int d = 0; d < 3; ++d) { dx[d] = dx[d] * a.h; st.xp[d] = st.xi[d] + dx[d]; }
     ds = sqrtf(dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2]);
-    alpha = alpha_at(a, st.xi, u);
+    alpha = alpha_at<CFG>(a, st.xi, u);
     st.att = st.att + alpha * ds;
     st.E = st.E0 * __expf(-st.att);
 }
@@ -314,18 +331,18 @@ __device__ __forceinline__ void corner_list(const RayArgs& a, const Corners& c, 
 // ---------------------------------------------------------------------------
 // integrate (forward)
 // ---------------------------------------------------------------------------
-template <bool TWOD>
+template <bool TWOD, int CFG>
 __global__ void __launch_bounds__(kRayThreads) k_ray_integrate(RayArgs a, const float* __restrict__ fa,
                                                                float* __restrict__ g) {
     const int64_t r = (int64_t)blockIdx.x * kRayThreads + threadIdx.x;
     if (r >= a.nr) return;
     RayState st;
-    ray_init(a, r, a.energy0, st);
+    ray_init<CFG>(a, r, a.energy0, st);
     float integral = 0.f;
     int until_check = 0;  // the exit test runs at steps 0, check, 2 check, ...
     for (int step = 0; step < a.max_steps; ++step) {
         float ds, alpha;
-        ray_step(a, st, ds, alpha);
+        ray_step<CFG>(a, st, ds, alpha);
         Corners c;
         corners_at(a, st.xp, c);
         CornerList<TWOD> L;
@@ -347,18 +364,18 @@ __global__ void __launch_bounds__(kRayThreads) k_ray_integrate(RayArgs a, const 
 // ---------------------------------------------------------------------------
 // deposit (adjoint)
 // ---------------------------------------------------------------------------
-template <bool TWOD>
+template <bool TWOD, int CFG>
 __global__ void __launch_bounds__(kRayThreads) k_ray_deposit(RayArgs a, const float* __restrict__ gin,
                                                              float* __restrict__ dose) {
     const int64_t r = (int64_t)blockIdx.x * kRayThreads + threadIdx.x;
     if (r >= a.nr) return;
     RayState st;
-    ray_init(a, r, gin[r], st);
+    ray_init<CFG>(a, r, gin[r], st);
     const bool zero = st.E0 == 0.f;  // a zero-energy ray deposits nothing; still traced for the cap count
     int until_check = 0;
     for (int step = 0; step < a.max_steps; ++step) {
         float ds, alpha;
-        ray_step(a, st, ds, alpha);
+        ray_step<CFG>(a, st, ds, alpha);
         if (!zero) {
             Corners c;
             corners_at(a, st.xp, c);
@@ -381,7 +398,7 @@ __global__ void __launch_bounds__(kRayThreads) k_ray_deposit(RayArgs a, const fl
 // ---------------------------------------------------------------------------
 // d<w, integrate(f)>/d alpha_att: pass 1 totals, pass 2 suffix sums
 // ---------------------------------------------------------------------------
-template <bool TWOD>
+template <bool TWOD, int CFG>
 __global__ void __launch_bounds__(kRayThreads) k_ray_grad_att(RayArgs a, const float* __restrict__ fa,
                                                               const float* __restrict__ w, float* __restrict__ grad) {
     const int64_t r = (int64_t)blockIdx.x * kRayThreads + threadIdx.x;
@@ -391,13 +408,13 @@ __global__ void __launch_bounds__(kRayThreads) k_ray_grad_att(RayArgs a, const f
     float total = 0.f;
     for (int pass = 0; pass < 2; ++pass) {
         RayState st;
-        ray_init(a, r, a.energy0, st);
+        ray_init<CFG>(a, r, a.energy0, st);
         float prefix = 0.f;
         int until_check = 0;
         for (int step = 0; step < a.max_steps; ++step) {
             if (!st.active) break;
             float ds, alpha;
-            ray_step(a, st, ds, alpha);
+            ray_step<CFG>(a, st, ds, alpha);
             Corners c;
             corners_at(a, st.xp, c);
             CornerList<TWOD> L;
@@ -500,6 +517,23 @@ RayArgs make_args(const vam_ray_plan* p) {
     a.active = p->d_active;
     return a;
 }
+
+bool grid_symplectic(const RayArgs& a) {
+    return a.n_kind == VAM_INDEX_GRID && a.a_kind == VAM_ALPHA_GRID && a.param == VAM_PARAM_PHYSICAL &&
+           a.solver == VAM_ODE_SYMPLECTIC_EULER;
+}
+
+// one of the four instances (2-D / 3-D x run-time / fixed configuration) of a ray kernel
+#define VAM_RAY_LAUNCH(K, nb, st, ...)                                                                  \
+    do {                                                                                                \
+        if (grid_symplectic(a)) {                                                                       \
+            if (a.twod) K<true, kCfgGridSymplectic><<<nb, kRayThreads, 0, st>>>(__VA_ARGS__);           \
+            else K<false, kCfgGridSymplectic><<<nb, kRayThreads, 0, st>>>(__VA_ARGS__);                 \
+        } else {                                                                                        \
+            if (a.twod) K<true, kCfgRuntime><<<nb, kRayThreads, 0, st>>>(__VA_ARGS__);                  \
+            else K<false, kCfgRuntime><<<nb, kRayThreads, 0, st>>>(__VA_ARGS__);                        \
+        }                                                                                               \
+    } while (0)
 
 int ew_blocks(int64_t n) {
     int64_t b = (n + 255) / 256;
@@ -606,8 +640,7 @@ extern "C" int vam_ray_integrate(vam_ray_plan* p, const float* f, float* g, vam_
     VAM_TRY_CUDA(cudaMemsetAsync(p->d_active, 0, sizeof(unsigned long long), st));
     RayArgs a = make_args(p);
     const unsigned nb = (unsigned)((p->g.num_rays + kRayThreads - 1) / kRayThreads);
-    if (a.twod) k_ray_integrate<true><<<nb, kRayThreads, 0, st>>>(a, p->d_scratch, g);
-    else k_ray_integrate<false><<<nb, kRayThreads, 0, st>>>(a, p->d_scratch, g);
+    VAM_RAY_LAUNCH(k_ray_integrate, nb, st, a, p->d_scratch, g);
     VAM_CHECK_LAUNCH("k_ray_integrate");
     return VAM_OK;
 }
@@ -623,8 +656,7 @@ extern "C" int vam_ray_deposit(vam_ray_plan* p, const float* gin, float* dose, v
     VAM_TRY_CUDA(cudaMemsetAsync(p->d_active, 0, sizeof(unsigned long long), st));
     RayArgs a = make_args(p);
     const unsigned nb = (unsigned)((p->g.num_rays + kRayThreads - 1) / kRayThreads);
-    if (a.twod) k_ray_deposit<true><<<nb, kRayThreads, 0, st>>>(a, gin, p->d_scratch);
-    else k_ray_deposit<false><<<nb, kRayThreads, 0, st>>>(a, gin, p->d_scratch);
+    VAM_RAY_LAUNCH(k_ray_deposit, nb, st, a, gin, p->d_scratch);
     VAM_CHECK_LAUNCH("k_ray_deposit");
     k_mul<<<ew_blocks(nv), 256, 0, st>>>(p->d_scratch, p->d_absorb, dose, nv);
     VAM_CHECK_LAUNCH("k_mul");
@@ -645,8 +677,7 @@ extern "C" int vam_ray_grad_alpha(vam_ray_plan* p, const float* f, const float* 
     const unsigned nb = (unsigned)((p->g.num_rays + kRayThreads - 1) / kRayThreads);
     if (grad_att) {
         k_mul<<<ew_blocks(nv), 256, 0, st>>>(f, p->d_absorb, p->d_scratch, nv);
-        if (a.twod) k_ray_grad_att<true><<<nb, kRayThreads, 0, st>>>(a, p->d_scratch, w, grad_att);
-        else k_ray_grad_att<false><<<nb, kRayThreads, 0, st>>>(a, p->d_scratch, w, grad_att);
+        VAM_RAY_LAUNCH(k_ray_grad_att, nb, st, a, p->d_scratch, w, grad_att);
         VAM_CHECK_LAUNCH("k_ray_grad_att");
     }
     if (grad_abs) {
@@ -654,8 +685,7 @@ extern "C" int vam_ray_grad_alpha(vam_ray_plan* p, const float* f, const float* 
         VAM_TRY_CUDA(cudaMemsetAsync(p->d_active, 0, sizeof(unsigned long long), st));
         // deposit of w with unit start energy, times the forward's energy0:
         // sum_r w_r * energy0 * exp(-att) * (h/voxel) * w_corner at every voxel
-        if (a.twod) k_ray_deposit<true><<<nb, kRayThreads, 0, st>>>(a, w, p->d_scratch);
-        else k_ray_deposit<false><<<nb, kRayThreads, 0, st>>>(a, w, p->d_scratch);
+        VAM_RAY_LAUNCH(k_ray_deposit, nb, st, a, w, p->d_scratch);
         VAM_CHECK_LAUNCH("k_ray_deposit");
         k_mul_acc<<<ew_blocks(nv), 256, 0, st>>>(p->d_scratch, f, p->energy0, grad_abs, nv);
         VAM_CHECK_LAUNCH("k_mul_acc");
