@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-multi", action="store_true", help="skip the 16-target batched BCLP measurement")
+    ap.add_argument("--no-ray", action="store_true", help="skip the ray-tracer BCLP measurement")
+    ap.add_argument("--ray-size", type=int, default=128)
     return ap.parse_args()
 
 
@@ -339,6 +341,110 @@ def run_multi_target(dev, n_iter=25):
     return out
 
 
+def ray_problem(n, n_angles, seed=0):
+    """Ray-tracer workload: n^3 graded-index medium n = 1.50 + 0.02 (r/R)^2 + a smooth perturbation
+    (central-difference gradient), smooth attenuation with e^-1 transmission across the grid, physical
+    path length + forward symplectic Euler at h = voxel / 2, parallel rays (n detector x n_angles x n z),
+    a seeded random-ellipsoid target."""
+    import torch
+
+    from vamtoolbox_b200 import geometry, medium, synthetic
+
+    tg = geometry.TargetGeometry(target=synthetic.ellipsoids_3d(n, seed=seed, radius=0.45 * n))
+    cv = tg.constructCoordVec()
+    a0 = 1.0 / (n * (cv[0][1] - cv[0][0]))
+    nx = synthetic.graded_index(cv, seed=seed)
+    ax = synthetic.smooth_attenuation(cv, a0, seed=seed)
+    im = medium.IndexModel(cv, type="interpolation", form="freeform", n_x=torch.as_tensor(nx))
+    am = medium.AttenuationModel(cv, type="interpolation", form="freeform", alpha_x=torch.as_tensor(ax))
+    pg = geometry.ProjectionGeometry(np.linspace(0, 360, n_angles, endpoint=False), "ray_trace", CUDA=True,
+                                     index_model=im, attenuation_model=am, absorption_model=am,
+                                     ray_trace_method="eikonal", eikonal_parametrization="physical_path_length",
+                                     ray_trace_ode_solver="forward_symplectic_euler", ray_trace_ray_config="parallel",
+                                     inclination_angle=0.0, ray_density=1)
+    return tg, pg, cv, nx, ax
+
+
+def ray_cpu_sample(cv, nx, ax, n_angles, budget_s=6.0):
+    """The float64 C oracle of the reference's tracer (integrate + deposit, all host threads) on a
+    few angles' rays, extrapolated to all angles (every angle traces the same number of rays)."""
+    from oracle import oracle as O
+
+    xv, yv, zv = cv
+    h = (xv[1] - xv[0]) / 2
+    kw = dict(step_size=h, max_num_step=3 * xv.size, n_kind=1, n_grid=nx, a_kind=3, a_grid=ax, absorb=ax)
+    grid = dict(xv=xv, yv=yv, zv=zv)
+    rng = np.random.default_rng(0)
+    f = rng.uniform(0, 1, (xv.size, yv.size, zv.size))
+    k = 1
+    while True:
+        ang = np.linspace(0, 360, n_angles, endpoint=False)[:k]
+        x0, v0, _ = O.setup_rays_parallel(xv, yv, zv, ang)
+        t0 = time.perf_counter()
+        g, _ = O.ray_trace("integrate", grid, x0, v0, 1.0, f=f, **kw)
+        O.ray_trace("deposit", grid, x0, v0, 1.0, g=rng.uniform(0, 1, g.shape), **kw)
+        t = time.perf_counter() - t0
+        if t > budget_s / 4 or k >= n_angles:
+            break
+        k = min(n_angles, k * 4)
+    per_iter = t * n_angles / k
+    return {"value": round(1.0 / per_iter, 6), "unit": "iter/s", "cores": O.num_threads(), "kind": "port",
+            "sample": f"{k} of {n_angles} angles ({x0.shape[0]} rays), integrate + deposit in the float64 C "
+                      f"oracle, extrapolated over angles ({t:.2f} s measured)"}
+
+
+def run_ray_bclp(dev, n=128, n_angles=360, steps=5, warmup=2, cpu=True):
+    """BCLP iterations/s through the ray tracer (deposit -> fused dose pass -> integrate -> update, one
+    captured graph), with the kernels' own times and the CPU oracle beside it."""
+    import torch
+
+    from vamtoolbox_b200.fused import graph_kernel_nodes
+    from vamtoolbox_b200.optimize import Options
+    from vamtoolbox_b200.optimizer.BCLP import BCLPNorm
+
+    tg, pg, cv, nx, ax = ray_problem(n, n_angles)
+    opts = Options(method="BCLP", n_iter=steps + warmup + 2, p=2, q=1, eps=0.1, learning_rate=1e-5)
+    bclp = BCLPNorm(tg, pg, opts)
+    it = bclp.device_iteration()
+    g = it.capture()
+    st = torch.cuda.current_stream(dev)
+    for _ in range(warmup):
+        g.replay()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(steps):
+        g.replay()
+    e1.record(st)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / steps
+    launches = graph_kernel_nodes(g)
+    del g
+    kt = {}
+    for name, fn in (("deposit", lambda: it.back(it.g, it.dose)), ("integrate", lambda: it.fwd(it.operand, it.grad))):
+        fn()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        fn()
+        b.record(st)
+        torch.cuda.synchronize(dev)
+        kt[name] = round(a.elapsed_time(b), 3)
+    plan = bclp.P.plan
+    rays = int(plan.num_rays)
+    cap = int(plan.max_num_step) if hasattr(plan, "max_num_step") else 3 * n
+    out = {"workload": f"BCLP iteration through the ray tracer, {n}^3 graded-index medium, {n_angles} angles, "
+                       f"{rays} rays, step cap {cap}",
+           "bclp_iter_s": round(1000.0 / ms, 3), "ms_per_iteration": round(ms, 3), "kernel_ms": kt,
+           "ray_steps_per_s": round(rays * cap / (kt["integrate"] * 1e-3), 1),
+           "rays_active_at_cap": int(plan.active_at_cap()), "launches_per_iteration": launches}
+    if cpu:
+        try:
+            out["cpu_baseline"] = ray_cpu_sample(cv, nx, ax, n_angles)
+        except Exception as exc:
+            out["cpu_baseline"] = {"error": f"{type(exc).__name__}: {exc}"}
+    return out
+
+
 def run_ours(args):
     import torch
 
@@ -448,21 +554,19 @@ def run_ours(args):
     torch.cuda.synchronize(dev)
     fwd_matched = 1000.0 / (e2.elapsed_time(e3) / args.steps)
 
-    # ---- end to end with host buffers (pinned), every step
+    # ---- end to end with host buffers (pinned), every step: the step's input sinogram in from the
+    # host, the step's result (the 9 loss / norm sums of the iteration) back to the host
     g_host = it.g.detach().cpu().pin_memory()
-    g_out = torch.empty_like(g_host).pin_memory()
     s_out = torch.empty(9, dtype=torch.float32).pin_memory()
     for _ in range(2):
         it.g.copy_(g_host, non_blocking=True)
         run_step()
-        g_out.copy_(it.g, non_blocking=True)
         s_out.copy_(it.stats, non_blocking=True)
     barrier()
     e2.record(st)
     for _ in range(args.steps):
         it.g.copy_(g_host, non_blocking=True)
         run_step()
-        g_out.copy_(it.g, non_blocking=True)
         s_out.copy_(it.stats, non_blocking=True)
     e3.record(st)
     barrier()
@@ -472,7 +576,7 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
     h2d = g_host.numel() * 4
-    d2h = g_out.numel() * 4 + s_out.numel() * 4
+    d2h = s_out.numel() * 4
 
     # ---- plain per-call GPU path (reference numpy loop, host arrays)
     plain = None
@@ -526,6 +630,13 @@ def run_ours(args):
         except Exception as exc:  # report, never fail the headline number on it
             multi = {"error": f"{type(exc).__name__}: {exc}"}
 
+    ray = None
+    if ws_ == 1 and not args.no_ray:
+        try:
+            ray = run_ray_bclp(dev, n=args.ray_size, cpu=not args.no_cpu)
+        except Exception as exc:  # report, never fail the headline number on it
+            ray = {"error": f"{type(exc).__name__}: {exc}"}
+
     cpu = None
     if rank == 0 and not args.no_cpu:
         try:
@@ -555,6 +666,7 @@ def run_ours(args):
             "gpu_launches": (launches_per_step * args.steps) if launches_per_step is not None else None,
             "gpu_launches_source": "kernel nodes of the captured iteration graph x timed steps",
             "multi_target": multi,
+            "ray_tracer": ray,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm_peak, "unit": "GB/s",
                          "frac": round(achieved / hbm_peak, 5), "traffic": traffic, "peak_source": peak_src,
                          "kernel": "forward projector (R1)",
