@@ -963,11 +963,29 @@ __global__ void __launch_bounds__(256) k_backward_2d(Args a) {
     k_backward_2d_body<RAY>(a, blockIdx.x, blockIdx.y);
 }
 
+// out = mask (per pixel, broadcast over z) * x; with nZ % 4 == 0 and aligned buffers four
+// slices of one pixel per thread and 16-byte load
 __global__ void k_mask_mul(const float* __restrict__ x, const float* __restrict__ mask, float* __restrict__ out,
                            long npix, int nZ) {
     const long n = npix * nZ;
-    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-        out[i] = mask[i / nZ] * x[i];
+    const long stride = (long)gridDim.x * blockDim.x, t0 = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (nZ % 128 == 0 && (((uintptr_t)x | (uintptr_t)out) & 15) == 0) {
+        // one warp per pixel row along z: no index division
+        const int q = nZ / 4, lane = threadIdx.x & 31;
+        const long nwarps = stride >> 5;
+        for (long pix = t0 >> 5; pix < npix; pix += nwarps) {
+            const float m = __ldg(mask + pix);
+            const float4* xs = reinterpret_cast<const float4*>(x) + pix * q;
+            float4* os = reinterpret_cast<float4*>(out) + pix * q;
+            for (int i = lane; i < q; i += 32) {
+                float4 v = __ldg(xs + i);
+                v.x *= m; v.y *= m; v.z *= m; v.w *= m;
+                os[i] = v;
+            }
+        }
+        return;
+    }
+    for (long i = t0; i < n; i += stride) out[i] = mask[i / nZ] * x[i];
 }
 
 // ---------------------------------------------------------------------------
