@@ -221,6 +221,8 @@ class BCLPNorm:
             del gr
         it.state()  # dose / mapped dose / norms of the final sinogram
         torch.cuda.synchronize(dev)
+        # device time per iteration of the loop (CUDA events on the engine's stream)
+        self.options.device_iteration_ms = ev[0].elapsed_time(ev[done]) / done if done else None
         return self.finish_device(it, done, [ev[0].elapsed_time(ev[k + 1]) / 1e3 for k in range(done)])
 
     def finish_device(self, it, done, iter_times):

@@ -111,18 +111,27 @@ def minimizeCAL(target_geo, proj_geo, options):
         ws.ver(x, mask, ver)
         ws.append(ver, err_log, counter)
 
+    st = torch.cuda.current_stream(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    done = 0
     graphable = m == 0 and options.bit_depth is None and options.exit_param is None
     if graphable and n_iter > 2:
         gr = capture(lambda: step(1), dev)
+        ev0.record(st)
         for _ in range(1, n_iter):
             gr.replay()
+        ev1.record(st)
+        done = n_iter - 1
     else:
+        ev0.record(st)
         for it in range(1, n_iter):
             step(it)
+            done += 1
             if m != 0:
                 db_prev.copy_(db)
             if options.exit_param is not None and float(ver.item()) <= options.exit_param:
                 break
+        ev1.record(st)
     # final positivity / normalisation / reconstruction (CAL.py:197-208)
     bmax = ws.scalar()
     b.clamp_(min=0)
@@ -133,5 +142,7 @@ def minimizeCAL(target_geo, proj_geo, options):
     ws.scale(x_opt, xmax)
     err = err_log.double().cpu().numpy()
     err = np.where(np.arange(err.size) < int(counter.item()), err, np.nan)
+    # device time per iteration of the loop (CUDA events on the engine's stream)
+    options.device_iteration_ms = ev0.elapsed_time(ev1) / done if done else None
     return (geometry.Sinogram(b.double().cpu().numpy(), proj_geo, options),
             geometry.Reconstruction(x_opt.double().cpu().numpy(), proj_geo, options), err)

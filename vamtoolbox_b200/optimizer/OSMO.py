@@ -99,16 +99,27 @@ def minimizeOSMO(target_geo, proj_geo, options):
         ws.ver(x, mask, ver)
         ws.append(ver, err_log, counter)
 
+    st = torch.cuda.current_stream(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    done = 0
     if options.exit_param is None and n_iter > 2:
         gr = capture(step, dev)
+        ev0.record(st)
         for _ in range(1, n_iter):
             gr.replay()
+        ev1.record(st)
+        done = n_iter - 1
     else:
+        ev0.record(st)
         for _ in range(1, n_iter):
             step()
+            done += 1
             if options.exit_param is not None and float(ver.item()) <= options.exit_param:
                 break
+        ev1.record(st)
     err = err_log.double().cpu().numpy()
+    # device time per iteration of the loop (CUDA events on the engine's stream)
+    options.device_iteration_ms = ev0.elapsed_time(ev1) / done if done else None
     err = np.where(np.arange(err.size) < int(counter.item()), err, np.nan)
     return (geometry.Sinogram(b.double().cpu().numpy(), proj_geo, options),
             geometry.Reconstruction(x.double().cpu().numpy(), proj_geo, options), err)
