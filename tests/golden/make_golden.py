@@ -251,6 +251,23 @@ def optimizer_cases(vam):
     out["bclp_loss"] = logs.loss
     out["bclp_norms"] = np.stack([logs.l0, logs.l1, logs.l2, logs.lf, logs.l0_eps0, logs.l1_eps0,
                                   logs.l2_eps0, logs.lf_eps0])
+    # BCLP with the fourth-power band norm and per-voxel weights (1 inside the target, 0.5 outside)
+    w = np.where(tgray > 0.15, 1.0, 0.5)
+    out["bclp4_weight"] = w
+    tg = geo.TargetGeometry(target=tgray.copy())
+    pg = geo.ProjectionGeometry(ang, "parallel", CUDA=False, attenuation_field=np.zeros((n, n, nz)))
+    opts = refload.fresh_options(vam, method="BCLP", n_iter=4, p=4, q=1, eps=0.05, weight=w, learning_rate=0.02,
+                                 response_model=rm, filter="ram-lak")
+    sino, dose, mapped, logs = vam.optimize.optimize(tg, pg, opts, output="full")
+    out["bclp4_sino"], out["bclp4_dose"], out["bclp4_loss"] = sino.array, dose.array, logs.loss
+    # 2-D CAL: a single slice (the reference stores 2-D targets as n x n x 1 arrays)
+    t2 = t[:, :, 0].copy()
+    out["cal2d_target"] = t2
+    tg = geo.TargetGeometry(target=t2.copy())
+    pg = geo.ProjectionGeometry(ang, "parallel", CUDA=False, attenuation_field=np.zeros((n, n, 1)))
+    opts = refload.fresh_options(vam, method="CAL", n_iter=5, learning_rate=0.4, d_h=0.5, sigmoid=0.01)
+    s2, r2, e2 = vam.optimize.optimize(tg, pg, opts)
+    out["cal2d_sino"], out["cal2d_recon"], out["cal2d_err"] = s2.array, r2.array, e2
     # response model tables
     out["resp_f"], out["resp_map"], out["resp_dmap"] = rm.interp_f_0, rm.interp_map_0, rm.interp_dmapdf_0
     out["resp_inv_probe"] = rm.map_inv(np.linspace(-0.1, 1.1, 37))

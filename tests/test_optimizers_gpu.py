@@ -112,3 +112,33 @@ def test_options_do_not_leak_between_instances():
     a = opts(method="CAL", learning_rate=0.4)
     b = opts(method="CAL")
     assert a.learning_rate == 0.4 and b.learning_rate == 0.01
+
+
+@pytest.mark.parametrize("engine", ["device", "host"])
+def test_bclp_p4_weighted_matches_reference(golden, engine):
+    """BCLP with the fourth-power band norm and per-voxel weights (1 inside the target, 0.5 outside)."""
+    from vamtoolbox_b200.optimize import optimize
+    from vamtoolbox_b200.response import ResponseModel
+
+    O = golden["optim"]
+    tg, pg = geo(O["bclp_target"], O["angles"])
+    sino, dose, mapped, logs = optimize(tg, pg, opts(method="BCLP", n_iter=4, p=4, q=1, eps=0.05,
+                                                     weight=O["bclp4_weight"], learning_rate=0.02,
+                                                     response_model=ResponseModel(B=12, M=0.6), filter="ram-lak",
+                                                     engine=engine), output="full")
+    assert relL2(sino.array, O["bclp4_sino"]) < 1e-4
+    assert relL2(dose.array, O["bclp4_dose"]) < 1e-4
+    assert np.allclose(logs.loss, O["bclp4_loss"], rtol=1e-4)
+
+
+@pytest.mark.parametrize("engine", ["device", "host"])
+def test_cal_single_slice_matches_reference(golden, engine):
+    """CAL on a 2-D target (stored as n x n x 1, as the reference does)."""
+    from vamtoolbox_b200.optimize import optimize
+
+    O = golden["optim"]
+    tg, pg = geo(O["cal2d_target"], O["angles"])
+    s, r, e = optimize(tg, pg, opts(method="CAL", n_iter=5, learning_rate=0.4, d_h=0.5, sigmoid=0.01, engine=engine))
+    assert relL2(np.reshape(s.array, O["cal2d_sino"].shape), O["cal2d_sino"]) < 1e-4
+    assert relL2(np.reshape(r.array, O["cal2d_recon"].shape), O["cal2d_recon"]) < 1e-4
+    assert counts_close(e, O["cal2d_err"], tg)
