@@ -142,3 +142,20 @@ def test_cal_single_slice_matches_reference(golden, engine):
     assert relL2(np.reshape(s.array, O["cal2d_sino"].shape), O["cal2d_sino"]) < 1e-4
     assert relL2(np.reshape(r.array, O["cal2d_recon"].shape), O["cal2d_recon"]) < 1e-4
     assert counts_close(e, O["cal2d_err"], tg)
+
+
+def test_device_filters_match_reference(golden):
+    """cuFFT versions of the sinogram and OSMO target filters against the reference's numpy outputs."""
+    import torch
+
+    from vamtoolbox_b200.util import data as udata
+
+    G = golden["optim"]
+    s = udata.filterSinogram_t(torch.as_tensor(G["filt_sino_in"], device="cuda"), "ram-lak").cpu().numpy()
+    assert np.allclose(s, G["filt_sino_ramlak"], atol=1e-10)
+    t = udata.filterTargetOSMO_t(torch.as_tensor(G["target"], device="cuda"), "ram-lak").cpu().numpy()
+    assert np.allclose(t, G["filt_osmo"], atol=1e-10)
+    for name in ("shepp-logan", "cosine", "hamming", "hanning"):
+        x = np.random.default_rng(1).uniform(size=(20, 20, 3))
+        assert np.allclose(udata.filterTargetOSMO_t(torch.as_tensor(x, device="cuda"), name).cpu().numpy(),
+                           udata.filterTargetOSMO(x, name), atol=1e-10), name

@@ -124,3 +124,14 @@ def test_ray_oracle_gradient_matches_reference_autograd(golden):
     assert relL2(g, G["ag_fwd"]) < 1e-6
     d, _ = O.ray_trace("deposit", dict(xv=xv, yv=yv, zv=zv), x0, v0, 1.0, g=G["ag_w"], **kw)
     assert relL2(d, G["ag_grad_f"]) < 1e-6
+
+
+def test_host_filters_match_reference(golden):
+    """The sinogram and OSMO target filters (numpy) against the reference's own outputs."""
+    from vamtoolbox_b200.util import data as udata
+
+    G = golden["optim"]
+    for name in ("ram-lak", "shepp-logan", "cosine", "hamming", "hanning"):
+        assert np.allclose(udata._get_fourier_filter(64, name)[:, 0], G["filt_" + name], rtol=0, atol=1e-12), name
+    assert np.allclose(udata.filterSinogram(G["filt_sino_in"].copy(), "ram-lak"), G["filt_sino_ramlak"], atol=1e-12)
+    assert np.allclose(udata.filterTargetOSMO(G["target"].copy(), "ram-lak"), G["filt_osmo"], atol=1e-12)

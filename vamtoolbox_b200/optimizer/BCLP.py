@@ -99,6 +99,9 @@ class BCLPNorm:
             f0 = self.response_model.map_inv(self.target_geo.array)
             if callable(getattr(self.P, "inverseBackward", None)):
                 self.g0 = self.P.inverseBackward(f0, filter_option=options.filter)
+            elif hasattr(getattr(self.P, "plan", None), "backward_ref"):  # parallel beam: cuFFT filter on the device
+                g0 = udata.filterSinogram_t(self.P.forward_t(f0).to(torch.float64), options.filter)
+                self.g0 = (g0 * (np.pi / (2 * proj_geo.n_angles))).cpu().numpy()
             else:
                 self.g0 = udata.filterSinogram(self.P.forward(f0), options.filter)
                 self.g0 *= np.pi / (2 * proj_geo.n_angles)

@@ -2,6 +2,7 @@
 from __future__ import annotations
 
 import numpy as np
+import torch
 
 from .. import geometry, metrics
 from ..projectorconstructor import projectorconstructor
@@ -11,7 +12,10 @@ from ..util import data as udata
 def minimizeFBP(target_geo, proj_geo, options):
     A = projectorconstructor(target_geo, proj_geo)
     err = np.full(options.n_iter, np.nan)
-    b = udata.filterSinogram(A.forward(target_geo.array), options.filter)
+    if hasattr(getattr(A, "plan", None), "backward_ref"):  # parallel beam: cuFFT filter on the device
+        b = udata.filterSinogram_t(A.forward_t(target_geo.array).to(torch.float64), options.filter).cpu().numpy()
+    else:
+        b = udata.filterSinogram(A.forward(target_geo.array), options.filter)
     if getattr(options, "offset", False):
         b = b + np.broadcast_to(np.abs(np.min(b, axis=0)), b.shape)
     else:

@@ -74,8 +74,8 @@ def minimizeOSMO(target_geo, proj_geo, options):
     err_log = torch.full((max(n_iter, 1),), float("nan"), dtype=torch.float32, device=dev)
     counter = torch.zeros(1, dtype=torch.int32, device=dev)
     ver, xmax, bmax = ws.scalar(), ws.scalar(), ws.scalar()
-    xm = torch.as_tensor(np.ascontiguousarray(np.real(udata.filterTargetOSMO(target_geo.array, options.filter)),
-                                              dtype=np.float32), device=dev).reshape(vs).contiguous()
+    tgt = torch.as_tensor(np.ascontiguousarray(target_geo.array, dtype=np.float64), device=dev)
+    xm = udata.filterTargetOSMO_t(tgt, options.filter).to(torch.float32).reshape(vs).contiguous()
     b = plan.forward(xm).clamp_(min=0)
     x = plan.backward_ref(b)
     ws.max(x, xmax)

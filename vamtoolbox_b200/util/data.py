@@ -38,14 +38,11 @@ def circle_inside_mask(ny, nx):
     return ~_circle_outside(ny, nx)
 
 
-def filterTargetOSMO(x, filter_name):
-    """Radial 2-D Fourier filter of each z slice (util/data.py:43-113)."""
+def _osmo_filter(n_y, n_x, filter_name):
+    """The radial 2-D frequency filter of filterTargetOSMO (util/data.py:43-113), n_y x n_x, float64."""
     filter_types = ("ram-lak", "shepp-logan", "cosine", "hamming", "hanning", None)
     if filter_name not in filter_types:
         raise ValueError("Unknown filter: %s" % filter_name)
-    if filter_name is None or filter_name.lower() == "none":
-        return x
-    n_y, n_x = x.shape[0], x.shape[1]
     f_y, f_x = np.meshgrid(np.linspace(-1, 1, n_y), np.linspace(-1, 1, n_x), indexing="ij")
     f = np.sqrt(f_x ** 2 + f_y ** 2)
     filt = np.real(f)
@@ -61,12 +58,35 @@ def filterTargetOSMO(x, filter_name):
     elif filter_name == "hanning":
         w = np.abs(np.hanning(n_x))
         filt *= np.abs(np.sqrt(np.outer(w, w)))
+    return filt
+
+
+def filterTargetOSMO(x, filter_name):
+    """Radial 2-D Fourier filter of each z slice (util/data.py:43-113)."""
+    if filter_name is None or filter_name.lower() == "none":
+        return x
+    filt = _osmo_filter(x.shape[0], x.shape[1], filter_name)
     X = scipy.fft.fftshift(fft2(x, axes=(0, 1)), axes=(0, 1))
     if x.ndim == 2:
         out = ifft2(scipy.fft.ifftshift(X * filt, axes=(0, 1)), axes=(0, 1))
     else:
         out = ifft2(scipy.fft.ifftshift(X * filt[:, :, np.newaxis], axes=(0, 1)), axes=(0, 1))
     return out.astype(float)
+
+
+def filterTargetOSMO_t(x, filter_name):
+    """Device version of filterTargetOSMO for a [nY, nX] or [nY, nX, nZ] torch tensor: float64 cuFFT
+    (through torch.fft) of every slice, the same filter, the real part; returned in x's dtype."""
+    import torch
+
+    if filter_name is None or filter_name.lower() == "none":
+        return x
+    filt = torch.as_tensor(_osmo_filter(x.shape[0], x.shape[1], filter_name), device=x.device, dtype=torch.float64)
+    if x.ndim == 3:
+        filt = filt[:, :, None]
+    X = torch.fft.fftshift(torch.fft.fft2(x.to(torch.float64), dim=(0, 1)), dim=(0, 1))
+    out = torch.fft.ifft2(torch.fft.ifftshift(X * filt, dim=(0, 1)), dim=(0, 1)).real
+    return out.to(x.dtype).contiguous()
 
 
 def _get_fourier_filter(size, filter_name):
