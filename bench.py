@@ -59,6 +59,7 @@ def parse():
     ap.add_argument("--no-multi", action="store_true", help="skip the 16-target batched BCLP measurement")
     ap.add_argument("--no-ray", action="store_true", help="skip the ray-tracer BCLP measurement")
     ap.add_argument("--no-configs", action="store_true", help="skip the 2-D CAL / OSMO / grayscale BCLP legs")
+    ap.add_argument("--no-algebraic", action="store_true", help="skip the propagation-matrix / SpMV leg")
     ap.add_argument("--ray-size", type=int, default=128)
     return ap.parse_args()
 
@@ -510,6 +511,80 @@ def run_configs():
     return out
 
 
+def run_algebraic(dev, n=128, n_angles=360, reps=5):
+    """Algebraic propagation: the ray tracer's propagation matrix of one n^2 slice (n_angles angles) built
+    on the device, then applied z-tiled to an n^2 x n volume forward and backward (CSR kernel); beside it
+    the reference's CPU path for the same product (a SciPy CSR matrix times the tiled block)."""
+    import scipy.sparse
+    import torch
+
+    from vamtoolbox_b200 import geometry, medium, synthetic
+    from vamtoolbox_b200.projector.pyTorchAlgebraicPropagation import PyTorchAlgebraicPropagator
+    from vamtoolbox_b200.projector.pyTorchRayTrace import PyTorchRayTracingPropagator
+
+    tg2 = geometry.TargetGeometry(target=np.zeros((n, n)))
+    cv = tg2.constructCoordVec()
+    a0 = 1.0 / (n * (cv[0][1] - cv[0][0]))
+    im = medium.IndexModel(cv, type="interpolation", form="freeform",
+                           n_x=torch.as_tensor(synthetic.graded_index(cv, seed=0)))
+    am = medium.AttenuationModel(cv, type="interpolation", form="freeform",
+                                 alpha_x=torch.as_tensor(synthetic.smooth_attenuation(cv, a0)))
+    pg = geometry.ProjectionGeometry(np.linspace(0, 360, n_angles, endpoint=False), "ray_trace", CUDA=True,
+                                     index_model=im, attenuation_model=am, absorption_model=am,
+                                     eikonal_parametrization="physical_path_length",
+                                     ray_trace_ode_solver="forward_symplectic_euler", ray_trace_ray_config="parallel")
+    P = PyTorchRayTracingPropagator(tg2, pg)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    P.output_torch_tensor = True
+    M = P.buildPropagationMatrix()
+    torch.cuda.synchronize(dev)
+    t_build = time.perf_counter() - t0
+    tg3 = geometry.TargetGeometry(target=np.zeros((n, n, n)))
+    A = PyTorchAlgebraicPropagator(tg3, None, output_torch_tensor=True, matrix=M)
+    x = torch.rand(n * n * n, device=dev)
+    b = torch.rand(A.n_row_eff, device=dev)
+    st = torch.cuda.current_stream(dev)
+
+    def tim(fn):
+        fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / reps
+
+    t_f, t_b = tim(lambda: A.forward(x)), tim(lambda: A.backward(b))
+    nnz = int(M._nnz())
+    # compulsory bytes of one product: the matrix once (4 B value + 4 B column + row pointers), x and y
+    fwd_bytes = nnz * 8 + (A.n_row_internal + 1) * 8 + 4 * (A.n_col_eff + A.n_row_eff)
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        pass
+    hbm = peaks.get("hbm_gbs") or 6650.0
+    idx = M.indices().cpu().numpy()
+    S = scipy.sparse.csr_matrix((M.values().cpu().numpy(), (idx[0], idx[1])), shape=tuple(M.shape))
+    X = np.random.default_rng(0).uniform(size=(S.shape[1], n)).astype(np.float32)
+    t0 = time.perf_counter()
+    S @ X
+    t_cpu = time.perf_counter() - t0
+    return {"workload": f"propagation matrix of one {n}^2 slice x {n_angles} angles, z-tiled over {n} layers",
+            "nnz": nnz, "matrix_build_s": round(t_build, 4), "forward_ms": round(t_f, 4), "backward_ms": round(t_b, 4),
+            "fwd_adj_per_s": round(1000.0 / (t_f + t_b), 3),
+            "roofline_forward": {"bound": "hbm", "achieved": round(fwd_bytes / (t_f * 1e-3) / 1e9, 1), "peak": hbm,
+                                 "unit": "GB/s", "frac": round(fwd_bytes / (t_f * 1e-3) / 1e9 / hbm, 4),
+                                 "algorithmic_bytes": fwd_bytes},
+            "cpu_baseline": {"value": round(1000.0 / (t_cpu * 1e3), 4), "unit": "forward products/s",
+                             "cores": 1, "kind": "reference",
+                             "sample": "the same CSR matrix times the tiled block in SciPy (the reference's CPU "
+                                       "algebraic propagation), one product"}}
+
+
 def run_ours(args):
     import torch
 
@@ -699,6 +774,13 @@ def run_ours(args):
     if ws_ == 1 and not args.no_configs:
         configs = run_configs()
 
+    algebraic = None
+    if ws_ == 1 and not args.no_algebraic:
+        try:
+            algebraic = run_algebraic(dev)
+        except Exception as exc:  # report, never fail the headline number on it
+            algebraic = {"error": f"{type(exc).__name__}: {exc}"}
+
     ray = None
     if ws_ == 1 and not args.no_ray:
         try:
@@ -736,6 +818,7 @@ def run_ours(args):
             "gpu_launches_source": "kernel nodes of the captured iteration graph x timed steps",
             "multi_target": multi,
             "ray_tracer": ray,
+            "algebraic": algebraic,
             "configs": configs,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm_peak, "unit": "GB/s",
                          "frac": round(achieved / hbm_peak, 5), "traffic": traffic, "peak_source": peak_src,

@@ -247,6 +247,29 @@ int vam_ray_grad_alpha(vam_ray_plan* plan, const float* f_dev, const float* w_de
  * pyTorchRayTrace.py:464-467).  Synchronises the device. */
 int vam_ray_active_at_cap(vam_ray_plan* plan, int64_t* out_count);
 
+/* The propagation matrix of vam_ray_integrate, one CSR row per ray, replacing
+ * PyTorchRayTracingPropagator.buildPropagationMatrix / recordEnergyUntilExit
+ * (vamtoolbox/projector/pyTorchRayTrace.py:169-197, 573-690, 901-937,
+ * 1146-1252): row r lists, in step order, the voxels (C-order index over the
+ * [n_x][n_y][n_z] grid) ray r deposits into, starting with the plan's
+ * energy0, and the weights (h / voxel) * E * trilinear weight * absorption at
+ * the voxel; a
+ * voxel met twice appears twice (the reference sums them when it coalesces).
+ * vam_ray_record_count writes row_nnz[num_rays] (device); the caller forms
+ * row_ptr[num_rays + 1] (exclusive scan) and vam_ray_record_fill writes
+ * cols / vals.  Column indices are 32-bit (grids below 2^31 voxels). */
+int vam_ray_record_count(vam_ray_plan* plan, int64_t* row_nnz_dev, vam_stream_t stream);
+int vam_ray_record_fill(vam_ray_plan* plan, const int64_t* row_ptr_dev, int32_t* cols_dev, float* vals_dev,
+                        vam_stream_t stream);
+
+/* y[row][z] = sum_k vals[k] * x[cols[k]][z] over the CSR row, for a dense x of
+ * ztile columns per matrix column (the algebraic propagator's z tiling:
+ * PyTorchAlgebraicPropagator.forward / backward,
+ * vamtoolbox/projector/pyTorchAlgebraicPropagation.py:146-181; the backward
+ * passes the transposed matrix in CSR form).  Deterministic. */
+int vam_csr_spmm(int64_t nrows, const int64_t* row_ptr_dev, const int32_t* cols_dev, const float* vals_dev,
+                 const float* x_dev, int32_t ztile, float* y_dev, vam_stream_t stream);
+
 /* ======================================================================= */
 /* Optimizer iteration bodies (vamtoolbox/optimizer/*.py)                   */
 /* ======================================================================= */

@@ -124,6 +124,7 @@ def load():
     pkg.projector.Projector3DParallel = importlib.import_module("vamtoolbox.projector.Projector3DParallel")
     pkg.projector.Projector2DParallel = importlib.import_module("vamtoolbox.projector.Projector2DParallel")
     pkg.projector.pyTorchRayTrace = importlib.import_module("vamtoolbox.projector.pyTorchRayTrace")
+    pkg.projector.pyTorchAlgebraicPropagation = importlib.import_module("vamtoolbox.projector.pyTorchAlgebraicPropagation")
     for opt in ("CAL", "OSMO", "BCLP", "PM", "FBP"):
         setattr(pkg.optimizer, opt, importlib.import_module("vamtoolbox.optimizer." + opt))
     _loaded = pkg

@@ -151,6 +151,10 @@ def ray_cases(vam):
         out[f"{tag}_g"] = gin
         out[f"{tag}_bwd"] = dose
         out[f"{tag}_step"] = np.array([P.tracing_step_size, P.max_num_step])
+        # the propagation matrix (coalesced COO) of the same tracer
+        M = P.buildPropagationMatrix()
+        out[f"{tag}_mat_rows"], out[f"{tag}_mat_cols"] = M.row.astype(np.int64), M.col.astype(np.int64)
+        out[f"{tag}_mat_vals"], out[f"{tag}_mat_shape"] = M.data.astype(np.float64), np.array(M.shape)
     # analytic media: homogeneous index (n_sur = 1) and absorbing cylinder
     n, nz = 12, 4
     tg = geo.TargetGeometry(target=np.ones((n, n, nz)))
@@ -174,6 +178,33 @@ def ray_cases(vam):
     out["ha_bwd"] = P.backward(gin.copy())
     out["ha_params"] = np.array([1.0, 30.0, np.amax(cv[0]) - np.amin(cv[0])])
     np.savez_compressed(OUT / "raytrace.npz", **out)
+
+
+def algebraic_cases(vam):
+    """The reference's PyTorchAlgebraicPropagator on the 2-D (one z layer) propagation matrix of the r2
+    tracer case, z-tiled over a three-layer volume, loaded from a SciPy .npz file."""
+    import os
+    import tempfile
+
+    import scipy.sparse
+
+    R = np.load(OUT / "raytrace.npz")
+    shape = tuple(R["r2_mat_shape"])
+    M = scipy.sparse.coo_matrix((R["r2_mat_vals"], (R["r2_mat_rows"], R["r2_mat_cols"])), shape=shape)
+    rng = np.random.default_rng(11)
+    n = int(round(np.sqrt(shape[1])))
+    x = rng.uniform(0, 1, (n, n, 3))
+    b = rng.uniform(0, 1, shape[0] * 3)
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "propagation_matrix.npz")
+        scipy.sparse.save_npz(path, M.tocsr())
+        tg = vam.geometry.TargetGeometry(target=x.copy())
+        pg = vam.geometry.ProjectionGeometry(np.linspace(0, 360, 5, endpoint=False), "algebraic", CUDA=False,
+                                             loading_path_for_matrix=path)
+        A = vam.projector.pyTorchAlgebraicPropagation.PyTorchAlgebraicPropagator(tg, pg)
+        fwd, bwd = A.forward(x), A.backward(b)
+    np.savez_compressed(OUT / "algebraic.npz", x=x, b=b, fwd=np.asarray(fwd), bwd=np.asarray(bwd),
+                        z_tiling=np.array(A.z_tiling))
 
 
 def ray_autograd_cases(vam):
@@ -292,6 +323,7 @@ def main():
     vam = refload.load()
     parallel_cases(vam)
     ray_cases(vam)
+    algebraic_cases(vam)
     ray_autograd_cases(vam)
     optimizer_cases(vam)
     for p in sorted(OUT.glob("*.npz")):

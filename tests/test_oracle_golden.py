@@ -135,3 +135,15 @@ def test_host_filters_match_reference(golden):
         assert np.allclose(udata._get_fourier_filter(64, name)[:, 0], G["filt_" + name], rtol=0, atol=1e-12), name
     assert np.allclose(udata.filterSinogram(G["filt_sino_in"].copy(), "ram-lak"), G["filt_sino_ramlak"], atol=1e-12)
     assert np.allclose(udata.filterTargetOSMO(G["target"].copy(), "ram-lak"), G["filt_osmo"], atol=1e-12)
+
+
+@pytest.mark.parametrize("tag", ["r3", "r2"])
+def test_reference_propagation_matrix_is_its_forward(golden, tag):
+    """The reference's recorded propagation matrix applied to f reproduces its ray-traced forward of f
+    (absorption included): the fixture pins what the matrix means."""
+    import scipy.sparse
+
+    R = golden["raytrace"]
+    A = scipy.sparse.coo_matrix((R[f"{tag}_mat_vals"], (R[f"{tag}_mat_rows"], R[f"{tag}_mat_cols"])),
+                                shape=tuple(R[f"{tag}_mat_shape"])).tocsr()
+    assert relL2(A @ R[f"{tag}_f"].reshape(-1), R[f"{tag}_fwd"]) < 1e-6

@@ -92,6 +92,9 @@ _SIGS = {
     "vam_parallel_prepare_adjoint": ([_vp, _vp], _c_int),
     "vam_parallel_set_tuning": ([_vp, ctypes.POINTER(ParallelTuning)], _c_int),
     "vam_parallel_get_tuning": ([_vp, ctypes.POINTER(ParallelTuning)], _c_int),
+    "vam_ray_record_count": ([_vp, _vp, _vp], _c_int),
+    "vam_ray_record_fill": ([_vp, _vp, _vp, _vp, _vp], _c_int),
+    "vam_csr_spmm": ([ctypes.c_int64, _vp, _vp, _vp, _vp, _c_i32, _vp, _vp], _c_int),
     "vam_batch_create": ([_c_i32, ctypes.POINTER(_vp)], _c_int),
     "vam_batch_destroy": ([_vp], _c_int),
     "vam_batch_submit": ([_vp, ctypes.POINTER(Work), _c_i32, _vp], _c_int),

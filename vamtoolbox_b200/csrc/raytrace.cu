@@ -463,6 +463,96 @@ __global__ void __launch_bounds__(kRayThreads) k_ray_grad_att(RayArgs a, const f
     }
 }
 
+// ---------------------------------------------------------------------------
+// record: the propagation matrix of the integrate operator, one CSR row per ray
+// (pyTorchRayTrace.py:573-690, 901-937, 1146-1252).  Row r holds, in step
+// order, the (voxel, weight) pairs ray r deposits with unit start energy:
+// (h / voxel) * E(step) * trilinear corner weight, times the absorption at the
+// voxel (the reference's right multiplication by a diagonal matrix); a voxel
+// met twice (the floor / ceil double count, or two steps in one voxel) appears
+// twice, as in the reference before it coalesces.  With count, pass 1 writes
+// the row lengths; without, pass 2 fills cols / vals from row_ptr[r].
+// ---------------------------------------------------------------------------
+template <bool TWOD, int CFG>
+__global__ void __launch_bounds__(kRayThreads) k_ray_record(RayArgs a, const float* __restrict__ absorb,
+                                                            int64_t* __restrict__ count,
+                                                            const int64_t* __restrict__ row_ptr,
+                                                            int32_t* __restrict__ cols, float* __restrict__ vals) {
+    const int64_t r = (int64_t)blockIdx.x * kRayThreads + threadIdx.x;
+    if (r >= a.nr) return;
+    RayState st;
+    ray_init<CFG>(a, r, a.energy0, st);  // the reference's start energy: ray_density^-1 (2-D) or ^-2 (3-D)
+    int64_t k = count ? 0 : row_ptr[r];
+    int until_check = 0;
+    for (int step = 0; step < a.max_steps; ++step) {
+        float ds, alpha;
+        ray_step<CFG>(a, st, ds, alpha);
+        Corners c;
+        corners_at(a, st.xp, c);
+        CornerList<TWOD> L;
+        corner_list<TWOD>(a, c, L);
+        const float eh = a.h_idx * st.E;
+#pragma unroll
+        for (int cn = 0; cn < CornerList<TWOD>::kN; ++cn) {
+            if (!L.in[cn]) continue;
+            if (!count) {
+                cols[k] = L.off[cn];
+                vals[k] = L.w[cn] * eh * __ldg(absorb + L.off[cn]);
+            }
+            ++k;
+        }
+        if (until_check == 0) {
+            until_check = a.check;
+            if (exited(a, st)) { st.active = false; break; }
+        }
+        --until_check;
+    }
+    if (count) count[r] = k;
+}
+
+// Y[row][z] = sum over the row's entries of val * X[col][z]  (CSR times a z-tiled dense block).
+// A warp per row; with one z per row the lanes split the row's entries and a shuffle tree sums them,
+// otherwise the lanes run along z.  Fixed orders throughout: deterministic.
+__global__ void __launch_bounds__(256) k_csr_spmm(int64_t nrows, const int64_t* __restrict__ row_ptr,
+                                                  const int32_t* __restrict__ cols, const float* __restrict__ vals,
+                                                  const float* __restrict__ X, int ztile, float* __restrict__ Y,
+                                                  int vec4) {
+    const int lane = threadIdx.x & 31;
+    const int64_t row = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (row >= nrows) return;
+    const int64_t b = row_ptr[row], e = row_ptr[row + 1];
+    if (ztile == 1) {
+        float acc = 0.f;
+        for (int64_t k = b + lane; k < e; k += 32) acc = fmaf(__ldg(vals + k), __ldg(X + __ldg(cols + k)), acc);
+        for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+        if (lane == 0) Y[row] = acc;
+        return;
+    }
+    if (vec4) {  // ztile % 4 == 0, 16-byte aligned: a warp covers 128 columns of a row with one 512-byte load
+        for (int z0 = 0; z0 < ztile; z0 += 128) {
+            const int z = z0 + 4 * lane;
+            float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (z < ztile)
+                for (int64_t k = b; k < e; ++k) {
+                    const float v = __ldg(vals + k);
+                    const float4 xv = __ldg(reinterpret_cast<const float4*>(X + (int64_t)__ldg(cols + k) * ztile + z));
+                    acc.x = fmaf(v, xv.x, acc.x); acc.y = fmaf(v, xv.y, acc.y);
+                    acc.z = fmaf(v, xv.z, acc.z); acc.w = fmaf(v, xv.w, acc.w);
+                }
+            if (z < ztile) *reinterpret_cast<float4*>(Y + row * ztile + z) = acc;
+        }
+        return;
+    }
+    for (int z0 = 0; z0 < ztile; z0 += 32) {
+        const int z = z0 + lane;
+        float acc = 0.f;
+        if (z < ztile)
+            for (int64_t k = b; k < e; ++k)
+                acc = fmaf(__ldg(vals + k), __ldg(X + (int64_t)__ldg(cols + k) * ztile + z), acc);
+        if (z < ztile) Y[row * ztile + z] = acc;
+    }
+}
+
 __global__ void k_mul(const float* __restrict__ a, const float* __restrict__ b, float* __restrict__ out, int64_t n) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         out[i] = a[i] * b[i];
@@ -700,5 +790,49 @@ extern "C" int vam_ray_active_at_cap(vam_ray_plan* p, int64_t* out) {
     unsigned long long v = 0;
     VAM_TRY_CUDA(cudaMemcpy(&v, p->d_active, sizeof(v), cudaMemcpyDeviceToHost));
     *out = (int64_t)v;
+    return VAM_OK;
+}
+
+extern "C" int vam_ray_record_count(vam_ray_plan* p, int64_t* row_nnz, vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(p && row_nnz, VAM_ERR_ARG, "vam_ray_record_count: null argument");
+    VAM_REQUIRE(p->has_medium, VAM_ERR_ARG, "vam_ray_record_count: no medium bound (vam_ray_set_medium)");
+    DeviceGuard dg(p->g.device);
+    cudaStream_t st = (cudaStream_t)stream;
+    RayArgs a = make_args(p);
+    const unsigned nb = (unsigned)((p->g.num_rays + kRayThreads - 1) / kRayThreads);
+    VAM_RAY_LAUNCH(k_ray_record, nb, st, a, p->d_absorb, row_nnz, nullptr, nullptr, nullptr);
+    VAM_CHECK_LAUNCH("k_ray_record");
+    return VAM_OK;
+}
+
+extern "C" int vam_ray_record_fill(vam_ray_plan* p, const int64_t* row_ptr, int32_t* cols, float* vals,
+                                   vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(p && row_ptr && cols && vals, VAM_ERR_ARG, "vam_ray_record_fill: null argument");
+    VAM_REQUIRE(p->has_medium, VAM_ERR_ARG, "vam_ray_record_fill: no medium bound (vam_ray_set_medium)");
+    VAM_REQUIRE((int64_t)p->g.n_x * p->g.n_y * p->g.n_z < ((int64_t)1 << 31), VAM_ERR_SHAPE,
+                "vam_ray_record_fill: column indices are 32-bit");
+    DeviceGuard dg(p->g.device);
+    cudaStream_t st = (cudaStream_t)stream;
+    RayArgs a = make_args(p);
+    const unsigned nb = (unsigned)((p->g.num_rays + kRayThreads - 1) / kRayThreads);
+    VAM_RAY_LAUNCH(k_ray_record, nb, st, a, p->d_absorb, nullptr, row_ptr, cols, vals);
+    VAM_CHECK_LAUNCH("k_ray_record");
+    return VAM_OK;
+}
+
+extern "C" int vam_csr_spmm(int64_t nrows, const int64_t* row_ptr, const int32_t* cols, const float* vals,
+                            const float* x, int32_t ztile, float* y, vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(row_ptr && x && y && (cols || nrows == 0) && (vals || nrows == 0), VAM_ERR_ARG,
+                "vam_csr_spmm: null argument");
+    VAM_REQUIRE(nrows >= 0 && ztile >= 1, VAM_ERR_SHAPE, "vam_csr_spmm: nrows >= 0 and ztile >= 1 required");
+    if (nrows == 0) return VAM_OK;
+    const int64_t nb = (nrows + 7) / 8;
+    VAM_REQUIRE(nb < ((int64_t)1 << 31), VAM_ERR_SHAPE, "vam_csr_spmm: too many rows");
+    const int vec4 = ztile % 4 == 0 && (((uintptr_t)x | (uintptr_t)y) & 15) == 0;
+    k_csr_spmm<<<(unsigned)nb, 256, 0, (cudaStream_t)stream>>>(nrows, row_ptr, cols, vals, x, ztile, y, vec4);
+    VAM_CHECK_LAUNCH("k_csr_spmm");
     return VAM_OK;
 }

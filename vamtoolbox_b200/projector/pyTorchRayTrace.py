@@ -185,6 +185,22 @@ class RayPlan:
             _lib.call("vam_ray_grad_alpha", self._h, _lib.ptr(f), _lib.ptr(w), _lib.ptr(grad_att), _lib.ptr(grad_abs),
                       self._s())
 
+    def record(self):
+        """The integrate operator as a CSR matrix (one row per ray, C-order voxel columns): returns
+        (row_ptr int64 [num_rays + 1], cols int32, vals float32) on the device, uncoalesced (a voxel met
+        twice appears twice, as in the reference before it coalesces)."""
+        nr = self.num_rays
+        cnt = torch.empty(nr, dtype=torch.int64, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.call("vam_ray_record_count", self._h, _lib.ptr(cnt), self._s())
+            row_ptr = torch.zeros(nr + 1, dtype=torch.int64, device=self.device)
+            torch.cumsum(cnt, 0, out=row_ptr[1:])
+            nnz = int(row_ptr[-1].item())
+            cols = torch.empty(max(nnz, 1), dtype=torch.int32, device=self.device)
+            vals = torch.empty(max(nnz, 1), dtype=torch.float32, device=self.device)
+            _lib.call("vam_ray_record_fill", self._h, _lib.ptr(row_ptr), _lib.ptr(cols), _lib.ptr(vals), self._s())
+        return row_ptr, cols[:nnz], vals[:nnz]
+
     def active_at_cap(self):
         v = ctypes.c_int64()
         with torch.cuda.device(self.device):
@@ -245,6 +261,24 @@ class PyTorchRayTracingPropagator:
         if self.output_torch_tensor:
             return d
         return np.squeeze(d.cpu().numpy())
+
+    def buildPropagationMatrix(self):
+        """The forward propagation matrix (pyTorchRayTrace.py:169-197): rows = rays, columns = voxels
+        (C order over the [nX][nY][nZ] grid), coalesced; a torch sparse COO tensor when
+        ``output_torch_tensor``, else a scipy.sparse.coo_array."""
+        row_ptr, cols, vals = self.plan.record()
+        nvox = int(np.prod(self.plan.grid_shape))
+        rows = torch.repeat_interleave(torch.arange(self.plan.num_rays, device=self.device),
+                                       row_ptr[1:] - row_ptr[:-1])
+        A = torch.sparse_coo_tensor(torch.vstack((rows, cols.to(torch.int64))), vals,
+                                    size=(self.plan.num_rays, nvox), device=self.device,
+                                    check_invariants=False).coalesce()  # indices in range by construction
+        if self.output_torch_tensor:
+            return A
+        import scipy.sparse
+
+        idx = A.indices().cpu().numpy()
+        return scipy.sparse.coo_array((A.values().cpu().numpy(), (idx[0], idx[1])), shape=tuple(A.shape))
 
     def inverseBackward(self, f, filter_option="ram-lak", **kwargs):
         """Filtered initial sinogram (pyTorchRayTrace.py:135-166)."""

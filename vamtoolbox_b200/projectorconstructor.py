@@ -42,9 +42,10 @@ def projectorconstructor(target_geo, proj_geo, optical_params=None, **projector_
             proj_geo.attenuation_field = np.where(ins, np.inf, 0)
 
     if proj_geo.ray_type == "algebraic":
-        raise NotImplementedError(
-            "the algebraic (sparse-matrix) propagator is not part of this package's projection path")
-    if proj_geo.ray_type == "ray_trace":
+        from .projector.pyTorchAlgebraicPropagation import PyTorchAlgebraicPropagator
+
+        A = PyTorchAlgebraicPropagator(target_geo, proj_geo, **projector_kwargs)
+    elif proj_geo.ray_type == "ray_trace":
         from .projector.pyTorchRayTrace import PyTorchRayTracingPropagator
 
         A = PyTorchRayTracingPropagator(target_geo, proj_geo, **projector_kwargs)
