@@ -355,6 +355,82 @@ int vam_osmo_model_update(float* xm_dev, const float* x_dev, const float* xmax_d
 int vam_append(const float* src_dev, int32_t n, float* arr_dev, int32_t* counter_dev, int32_t cap_rows,
                vam_stream_t stream);
 
+/* ======================================================================= */
+/* Output formats: projector frames (vamtoolbox/imagesequence.py) and      */
+/* fan-beam rebinning (vamtoolbox/geometry.py:736-944)                     */
+/* ======================================================================= */
+
+/* Element type of the sinograms handled below (the reference keeps the
+ * caller's numpy dtype through these steps). */
+enum vam_dtype { VAM_DTYPE_F32 = 0, VAM_DTYPE_F64 = 1 };
+
+/* Order-1 rotation of every (r, z) plane of a sinogram [nR][nA][nZ] into
+ * [oR][nA][oZ], zero outside the input: ndimage.rotate(sino, angle,
+ * axes=(0, 2), reshape=True, order=1) as called by ImageSeq's _rotate
+ * (vamtoolbox/imagesequence.py:396-401).  affine (host, 6 doubles) =
+ * {m00, m01, m10, m11, off0, off1}: output (o0, o1) samples the input at
+ * ((m00*o0 + off0) + m01*o1, (m10*o0 + off1) + m11*o1), scipy's rot_matrix
+ * and offset.  flip_r / flip_z mirror the input first (_invertU / _invertV,
+ * imagesequence.py:358-365).  Double arithmetic, stored in dtype. */
+int vam_sino_rotate(const void* in_dev, int dtype, int32_t nR, int32_t nA, int32_t nZ, int32_t flip_r,
+                    int32_t flip_z, const double* affine, void* out_dev, int32_t oR, int32_t oZ,
+                    vam_stream_t stream);
+
+/* Bilinear resize of every (r, z) plane to [oR][nA][oZ]: cv2.resize(plane,
+ * (oZ, oR), interpolation=INTER_LINEAR) as called by _scaleSize
+ * (imagesequence.py:368-378): half-pixel centres, edge clamp, z interpolated
+ * before r, in the input's dtype.  out_dev is always double [oR][nA][oZ]:
+ * _scaleSize collects the planes in a float64 array.  flip_r / flip_z as above. */
+int vam_sino_resize(const void* in_dev, int dtype, int32_t nR, int32_t nA, int32_t nZ, int32_t flip_r,
+                    int32_t flip_z, void* out_dev, int32_t oR, int32_t oZ, vam_stream_t stream);
+
+/* Workspace of vam_select_pair, in bytes (independent of n). */
+size_t vam_select_workspace_bytes(void);
+
+/* out_dev[0], out_dev[1] (dtype) = the k0-th and k1-th smallest of x[0..n)
+ * (0-based, k1 == k0 or k0 + 1): the two sorted elements np.percentile
+ * (method 'linear') blends, imagesequence.py:129-133.  NaN sorts last and
+ * any NaN makes both outputs NaN (np.percentile returns NaN then).  Radix
+ * select on the device; stream-ordered, no host synchronisation.
+ * work_dev: vam_select_workspace_bytes(), 8-byte aligned. */
+int vam_select_pair(const void* x_dev, int dtype, int64_t n, int64_t k0, int64_t k1, void* out_dev,
+                    void* work_dev, size_t work_bytes, vam_stream_t stream);
+
+typedef struct {
+    int32_t n_u, n_v;             /* frame width (multiple of 4) and height, ImageConfig (imagesequence.py:55-58) */
+    const int32_t* src_col_dev;   /* [n_u] sinogram row r shown in frame column u, -1 = blank */
+    const int32_t* src_row_dev;   /* [n_v] sinogram z shown in frame row v, -1 = blank */
+    int32_t bit_depth;            /* 0..32; max value 2^bit_depth - 1 (imagesequence.py:127) */
+    int32_t has_norm;             /* divide by norm_value, multiply by the max value (:129-133) */
+    double norm_value;            /* the percentile value */
+    int32_t norm_dtype;           /* vam_dtype of the percentile value (numpy promotes the array to it) */
+    int32_t has_scale;            /* multiply by intensity_scale (:135-138) */
+    double intensity_scale;
+    int32_t scale_is_f64;         /* the scale is a float64 numpy scalar (promotes a float32 array) */
+} vam_frame_params;
+
+/* frames_dev[a][v][u] (uint8, 16-byte aligned, nA frames of n_v x n_u) from
+ * the sinogram [nR][nA][nZ]: 0 where src_row[v] or src_col[u] is -1, else
+ * the quantised sino[src_col[u]][a][src_row[v]]: ImageSeq.__init__
+ * (imagesequence.py:127-174), whose chain x / norm * max, * scale,
+ * np.minimum(., max), astype(uint8/16/32) and the store into a uint8 frame
+ * (low byte) is replayed in the reference's dtypes; the insertion offsets,
+ * array copies and flips of _insertImage / _arrayInsertImage (:303-355) are
+ * carried by the two tables.  nA <= 65535. */
+int vam_imageseq_frames(const void* sino_dev, int dtype, int32_t nR, int32_t nA, int32_t nZ,
+                        const vam_frame_params* prm, uint8_t* frames_dev, vam_stream_t stream);
+
+/* Fan-beam rebinning, rebinFanBeam (vamtoolbox/geometry.py:736-944):
+ * out[p][a][z] = tinv[p] * (dxv[p] * interp) for p < nP (the vial width in
+ * projector pixels), interp being interpn's bilinear sample of the sinogram
+ * padded to nP rows (input row p - pad_lo, zero outside [0, nR)).  Tables
+ * from the host grid search: xi_dev[nP] lower x index (-1: out of bounds),
+ * xw_dev[nP][4] = {y0, 1 - y0, dxv_dxp, 1/T}, ti_dev[nP][nA] lower angle index
+ * (-1: out of bounds), tw_dev[nP][nA][2] = {y1, 1 - y1}.  out_dev [nP][nA][nZ]. */
+int vam_rebin_fan(const void* in_dev, int dtype, int32_t nR, int32_t nA, int32_t nZ, int32_t nP,
+                  int32_t pad_lo, const int32_t* xi_dev, const double* xw_dev, const int32_t* ti_dev,
+                  const double* tw_dev, void* out_dev, vam_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -127,6 +127,8 @@ def load():
     pkg.projector.pyTorchAlgebraicPropagation = importlib.import_module("vamtoolbox.projector.pyTorchAlgebraicPropagation")
     for opt in ("CAL", "OSMO", "BCLP", "PM", "FBP"):
         setattr(pkg.optimizer, opt, importlib.import_module("vamtoolbox.optimizer." + opt))
+    # frame output (cv2 / dill / PIL are present here; its preview player is not imported)
+    pkg.imagesequence = importlib.import_module("vamtoolbox.imagesequence")
     _loaded = pkg
     return pkg
 

@@ -7,7 +7,8 @@ VAM_REFERENCE_ROOT):
 
 Every array stored here is produced by the reference's own Python code
 (Projector3DParallelPython, Projector2DParallelPython, the PyTorch ray tracer
-on the CPU, the CAL / OSMO / BCLP optimizers), loaded through
+on the CPU, the CAL / OSMO / BCLP optimizers, ImageSeq and rebinFanBeam),
+loaded through
 oracle/refload.py.  The only restated routine on that path is
 skimage.transform.warp (absent here), see oracle/refload.py.  Inputs are
 seeded synthetic targets; sizes are small so the fixtures stay a few hundred KB.
@@ -318,14 +319,76 @@ def optimizer_cases(vam):
     np.savez_compressed(OUT / "optim.npz", **out)
 
 
+# Frame-sequence configurations: (sinogram dtype, ImageConfig keywords).  Frames are 64 x 48.
+FORMAT_CASES = [
+    ("float64", {}),
+    ("float64", {"normalization_percentile": 99.5}),
+    ("float32", {"normalization_percentile": 99.0, "intensity_scale": 0.8}),
+    ("float64", {"invert_u": True, "invert_v": True, "u_offset": 3, "v_offset": -2}),
+    ("float64", {"rotate_angle": 30.0, "normalization_percentile": 100}),
+    ("float32", {"rotate_angle": -12.5, "invert_u": True}),
+    ("float64", {"size_scale": 1.5, "normalization_percentile": 98}),
+    ("float32", {"size_scale": 0.7}),
+    ("float64", {"array_num": 3, "array_offset": 10, "v_offset": 1, "normalization_percentile": 99}),
+    ("float64", {"array_num": 2, "array_offset": 12}),
+    ("float64", {"bit_depth": 10, "normalization_percentile": 99}),
+    ("float64", {"bit_depth": 16, "intensity_scale": 300.0}),
+    ("float32", {"bit_depth": 32, "intensity_scale": 3e7}),
+    ("float64", {"rotate_angle": 90.0, "size_scale": 1.25, "invert_v": True, "normalization_percentile": 97.5,
+                 "bit_depth": 12}),
+    ("float32", {"normalization_percentile": 50, "invert_v": True, "array_num": 0}),
+]
+# Fan-beam rebinning cases: (nR, nA, nZ, vial_width, dtype, n_write, throw_ratio).
+REBIN_CASES = [
+    (20, 36, 5, 25, "float64", 1.5, 1.7),
+    (30, 72, 3, 30, "float64", 1.48, 2.0),
+    (16, 90, 4, 21, "float32", 1.52, 1.2),
+    (40, 60, 2, 47, "float64", 1.33, 3.5),
+]
+
+
+def format_cases(vam):
+    """ImageSeq frames (vamtoolbox/imagesequence.py:85-174) and rebinFanBeam
+    (vamtoolbox/geometry.py:736-944), both run by the reference itself."""
+    import json
+
+    ims = vam.imagesequence
+    rng = np.random.default_rng(7)
+    out = {}
+    for i, (dt, kw) in enumerate(FORMAT_CASES):
+        # values on a 1/1024 lattice: exact in float32 and float64, and the fixture compresses
+        sino = (rng.integers(0, 3 * 1024, size=(24, 7, 20)) / 1024.0).astype(dt)
+        cfg = ims.ImageConfig((64, 48), **kw)
+        out[f"seq{i}_sino"] = sino
+        out[f"seq{i}_cfg"] = np.array(json.dumps(kw))
+        out[f"seq{i}_frames"] = np.stack(ims.ImageSeq(cfg, sino.copy()).images)
+    for i, (nr, na, nz, vw, dt, n_write, throw) in enumerate(REBIN_CASES):
+        angles = np.linspace(0, 360, na, endpoint=False)
+        arr = (rng.integers(0, 1024, size=(nr, na, nz)) / 1024.0).astype(dt)
+        pg = vam.geometry.ProjectionGeometry(angles, ray_type="parallel", CUDA=False)
+        res = vam.geometry.rebinFanBeam(vam.geometry.Sinogram(arr.copy(), pg), vw, (1920, 1080), n_write, throw)
+        out[f"rebin{i}_sino"] = arr
+        out[f"rebin{i}_angles"] = angles
+        out[f"rebin{i}_args"] = np.array([vw, 1920, 1080, n_write, throw])
+        out[f"rebin{i}_out"] = res.array
+    np.savez_compressed(OUT / "formats.npz", **out)
+
+
+GROUPS = {"parallel": parallel_cases, "ray": ray_cases, "algebraic": algebraic_cases,
+          "ray_autograd": ray_autograd_cases, "optim": optimizer_cases, "formats": format_cases}
+
+
 def main():
+    import argparse
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--only", nargs="*", choices=sorted(GROUPS), help="regenerate only these fixture groups")
+    args = ap.parse_args()
     warnings.simplefilter("ignore")
     vam = refload.load()
-    parallel_cases(vam)
-    ray_cases(vam)
-    algebraic_cases(vam)
-    ray_autograd_cases(vam)
-    optimizer_cases(vam)
+    for name, fn in GROUPS.items():
+        if not args.only or name in args.only:
+            fn(vam)
     for p in sorted(OUT.glob("*.npz")):
         print(p.name, p.stat().st_size)
 

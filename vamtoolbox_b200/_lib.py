@@ -77,6 +77,15 @@ class BclpParams(ctypes.Structure):
 
 
 # name -> (argtypes, restype)
+class FrameParams(ctypes.Structure):
+    _fields_ = [("n_u", _c_i32), ("n_v", _c_i32), ("src_col_dev", _vp), ("src_row_dev", _vp),
+                ("bit_depth", _c_i32), ("has_norm", _c_i32), ("norm_value", _c_d), ("norm_dtype", _c_i32),
+                ("has_scale", _c_i32), ("intensity_scale", _c_d), ("scale_is_f64", _c_i32)]
+
+
+DTYPE_F32, DTYPE_F64 = 0, 1
+
+
 _SIGS = {
     "vam_last_error_string": ([], ctypes.c_char_p),
     "vam_version": ([], ctypes.c_char_p),
@@ -119,6 +128,13 @@ _SIGS = {
     "vam_scale_by_device": ([_vp, _vp, _c_i64, _c_int, _c_f, _vp], _c_int),
     "vam_osmo_model_update": ([_vp, _vp, _vp, _vp, _c_i64, _c_int, _c_f, _vp], _c_int),
     "vam_append": ([_vp, _c_i32, _vp, _vp, _c_i32, _vp], _c_int),
+    "vam_sino_rotate": ([_vp, _c_int, _c_i32, _c_i32, _c_i32, _c_i32, _c_i32, ctypes.POINTER(_c_d), _vp, _c_i32,
+                         _c_i32, _vp], _c_int),
+    "vam_sino_resize": ([_vp, _c_int, _c_i32, _c_i32, _c_i32, _c_i32, _c_i32, _vp, _c_i32, _c_i32, _vp], _c_int),
+    "vam_select_workspace_bytes": ([], ctypes.c_size_t),
+    "vam_select_pair": ([_vp, _c_int, _c_i64, _c_i64, _c_i64, _vp, _vp, ctypes.c_size_t, _vp], _c_int),
+    "vam_imageseq_frames": ([_vp, _c_int, _c_i32, _c_i32, _c_i32, ctypes.POINTER(FrameParams), _vp, _vp], _c_int),
+    "vam_rebin_fan": ([_vp, _c_int, _c_i32, _c_i32, _c_i32, _c_i32, _c_i32, _vp, _vp, _vp, _vp, _vp, _vp], _c_int),
 }
 
 _lib = None

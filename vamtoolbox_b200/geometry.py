@@ -4,8 +4,8 @@ Mirrors vamtoolbox/geometry.py (ProjectionGeometry :30-193, Volume / TargetGeome
 / Sinogram / Reconstruction :196-659, loadVolume :662-679, getCircleMask /
 getInds :682-733) so that user code written for the reference constructs the
 same objects.  Arrays stay numpy on this side; the projectors move them to
-the device.  ``rebinFanBeam`` (geometry.py:736-944) is not part of the
-projection hot path and is not provided.
+the device.  ``rebinFanBeam`` (geometry.py:736-944) resamples on the GPU
+(libvamcore vam_rebin_fan) from grid-search tables built here.
 """
 from __future__ import annotations
 
@@ -229,3 +229,138 @@ def getInds(target):
     """Boolean gel / void masks inside the circle (geometry.py:714-733)."""
     circle = getCircleMask(target)
     return np.logical_and(target > 0, circle), np.logical_and(target == 0, circle)
+
+
+def fan_beam_tables(angles, n_r, vial_width, N_screen, n_write, throw_ratio):
+    """Sampling tables of rebinFanBeam (vamtoolbox/geometry.py:736-944), in float64.
+
+    Follows the reference's formulas step by step: projector coordinate xp,
+    refraction of the ray from projector pixel xp at the air/vial wall
+    (xps, theta10, thetai, thetat, thetav), Fresnel transmission T (s and p
+    averaged), the vial coordinate xv it samples and the differential-area
+    factor np.gradient(xv) (negative values zeroed), and the sampled angle
+    angle + thetav in degrees wrapped by the reference's rules (:900-909).
+    Returns (xp, xv, theta_samp [nP][nA], dxv_dxp [nP], T [nP]).
+    """
+    angles = np.asarray(angles)
+    n_angles = angles.size
+    N_U = N_screen[0]
+    n1, n2 = 1, n_write
+    vial_width = int(vial_width)
+    trp = throw_ratio * N_U
+    Rv = (vial_width / 2) * np.sqrt(1 + ((vial_width) / (2 * trp)) ** 2)
+    xp = np.linspace(-vial_width / 2, vial_width / 2, vial_width)
+    phi = np.arctan(xp / trp)
+    xps = (xp - xp * np.sqrt(1 - (1 + (xp / trp) ** 2) * (1 - (Rv / trp) ** 2))) / (1 + (xp / trp) ** 2)
+    theta10 = np.arcsin(xps / Rv)
+    thetai = np.arcsin(xps / Rv) + phi
+    thetat = np.arcsin((n1 / n2) * np.sin(thetai))
+    thetav = theta10 - thetat
+    thetavD = (180 / np.pi) * thetav
+    Ts = 1 - ((n1 * np.cos(thetai) - n2 * np.cos(thetat)) / ((n1 * np.cos(thetai) + n2 * np.cos(thetat)))) ** 2
+    Tp = 1 - ((n1 * np.cos(thetat) - n2 * np.cos(thetai)) / ((n1 * np.cos(thetat) + n2 * np.cos(thetai)))) ** 2
+    T = (Ts + Tp) / 2
+    T[T < 0] = 0
+    xv = (xps * np.cos(thetav)) - (np.sin(thetav) * np.sqrt((Rv ** 2) - (xps ** 2)))
+    dxv_dxp = np.gradient(xv)
+    dxv_dxp[T < 0] = 0
+    dxv_dxp[dxv_dxp < 0] = 0
+    theta_samp, _ = np.meshgrid(angles, xv)
+    theta_samp = theta_samp + np.transpose(np.tile(thetavD, (n_angles, 1)))
+    min_theta, max_theta = angles[0], angles[-1]
+    diff_theta = abs(angles[1] - angles[0])
+    theta_samp[theta_samp > max_theta] = theta_samp[theta_samp > max_theta] - 360
+    theta_samp[theta_samp < min_theta] = 360 + theta_samp[theta_samp < min_theta]
+    theta_samp[theta_samp > max_theta - diff_theta] = min_theta
+    theta_samp[(theta_samp <= max_theta - diff_theta) & (theta_samp > max_theta)] = max_theta
+    return xp, xv, theta_samp, dxv_dxp, T
+
+
+def grid_search(grid, x):
+    """Lower cell index and fractional position of x on an ascending grid, as
+    scipy's RegularGridInterpolator (method 'linear') finds them: i =
+    searchsorted(grid, x) - 1 clipped to [0, n-2], y = (x - grid[i]) /
+    (grid[i+1] - grid[i]); out-of-bounds points (x < grid[0] or x > grid[-1])
+    get i = -1 (interpn's fill_value=0)."""
+    grid = np.asarray(grid, dtype=np.float64)
+    x = np.asarray(x, dtype=np.float64)
+    i = np.clip(np.searchsorted(grid, x, side="left") - 1, 0, grid.size - 2)
+    y = (x - grid[i]) / (grid[i + 1] - grid[i])
+    oob = (x < grid[0]) | (x > grid[-1])
+    return np.where(oob, -1, i).astype(np.int32), y
+
+
+def rebinFanBeam(sinogram, vial_width, N_screen, n_write, throw_ratio):
+    """Rebin a parallel-beam sinogram for a non-telecentric projector and a
+    vial that is not index matched (vamtoolbox/geometry.py:736-944; Orth et
+    al., Opt. Express 29, 11037 (2021)).
+
+    Each output sample (xp, angle, z) is scipy interpn's bilinear sample of
+    the sinogram at (xv(xp), angle + thetav(xp)), times dxv_dxp, divided by
+    the Fresnel transmission T.  Like the reference, the input sinogram's
+    array is replaced by its copy padded to vial_width rows, and the result
+    has that shape and the input's dtype.  The per-sample work runs on the
+    GPU; a numpy array comes back as numpy, a torch tensor stays on its device.
+    """
+    import torch
+
+    angles = np.asarray(sinogram.proj_geo.angles)
+    arr = sinogram.array
+    is_torch = isinstance(arr, torch.Tensor)
+    n_r, n_a, n_z = (int(d) for d in arr.shape)
+    vial_width = int(vial_width)
+    if n_a < 2:
+        raise ValueError(f"There are {n_a} point(s) in dimension 1, but method linear requires at least 2 points.")
+    if not np.all(np.diff(angles) > 0):
+        raise ValueError("The points in dimension 1 must be strictly ascending")
+    xp, xv, theta_samp, dxv_dxp, T = fan_beam_tables(angles, n_r, vial_width, N_screen, n_write, throw_ratio)
+
+    pd = int((vial_width - n_r) / 2)
+    if is_torch:
+        import torch.nn.functional as F
+
+        padded = arr
+        if pd > 0:
+            padded = F.pad(padded.movedim(0, -1), (pd, pd)).movedim(-1, 0)
+        if padded.shape[0] < vial_width:
+            padded = F.pad(padded.movedim(0, -1), (0, 1)).movedim(-1, 0)
+        sinogram.array = padded.contiguous()
+    else:
+        padded = arr
+        if pd > 0:
+            padded = np.pad(padded, ((pd, pd), (0, 0), (0, 0)), mode="constant")
+        if np.shape(padded)[0] < vial_width:
+            padded = np.pad(padded, ((0, 1), (0, 0), (0, 0)), mode="constant")
+        sinogram.array = padded
+    n_p = int(padded.shape[0])
+    if n_p != vial_width:
+        raise ValueError(f"There are {vial_width} points and {n_p} values in dimension 0")
+
+    xi, y0 = grid_search(xp, xv)
+    ti, y1 = grid_search(angles, theta_samp)
+    xw = np.stack([y0, 1 - y0, dxv_dxp, 1 / T], axis=1)
+    tw = np.stack([y1, 1 - y1], axis=2)
+    dt = arr.dtype
+    if is_torch:
+        dev = arr.device if arr.is_cuda else torch.device("cuda", torch.cuda.current_device())
+        np_dt = np.float64 if dt == torch.float64 else (np.float32 if dt == torch.float32 else None)
+        src = arr.to(dev).contiguous()
+    else:
+        np_dt = dt.type if dt in (np.float32, np.float64) else None
+        dev = torch.device("cuda", torch.cuda.current_device())
+        src = torch.from_numpy(np.ascontiguousarray(arr)).to(dev) if np_dt is not None else None
+    if np_dt is None:
+        raise TypeError(f"sinogram dtype {dt} is not supported (float32 or float64)")
+    from . import _lib
+
+    code = _lib.DTYPE_F64 if np_dt == np.float64 else _lib.DTYPE_F32
+    with torch.cuda.device(dev):
+        t_xi = torch.from_numpy(xi).to(dev)
+        t_xw = torch.from_numpy(np.ascontiguousarray(xw)).to(dev)
+        t_ti = torch.from_numpy(np.ascontiguousarray(ti)).to(dev)
+        t_tw = torch.from_numpy(np.ascontiguousarray(tw)).to(dev)
+        out = torch.empty((n_p, n_a, n_z), dtype=src.dtype, device=dev)
+        _lib.call("vam_rebin_fan", _lib.ptr(src), code, n_r, n_a, n_z, n_p, max(pd, 0), _lib.ptr(t_xi),
+                  _lib.ptr(t_xw), _lib.ptr(t_ti), _lib.ptr(t_tw), _lib.ptr(out), _lib.stream_ptr())
+    result = out if is_torch else out.cpu().numpy()
+    return Sinogram(result, sinogram.proj_geo)
