@@ -25,6 +25,7 @@ Reported beside the headline:
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -60,6 +61,7 @@ def parse():
     ap.add_argument("--no-ray", action="store_true", help="skip the ray-tracer BCLP measurement")
     ap.add_argument("--no-configs", action="store_true", help="skip the 2-D CAL / OSMO / grayscale BCLP legs")
     ap.add_argument("--no-algebraic", action="store_true", help="skip the propagation-matrix / SpMV leg")
+    ap.add_argument("--no-formats", action="store_true", help="skip the projector-frame / fan-beam rebin leg")
     ap.add_argument("--ray-size", type=int, default=128)
     return ap.parse_args()
 
@@ -585,6 +587,110 @@ def run_algebraic(dev, n=128, n_angles=360, reps=5):
                                        "algebraic propagation), one product"}}
 
 
+def run_formats(dev, n=256, n_angles=360, screen=(1920, 1080), reps=5, cpu=True):
+    """Output formats: the n x n_angles x n float64 sinogram of the headline configuration converted to
+    n_angles projector frames of screen[0] x screen[1] (99.5th-percentile normalisation, the DLP
+    workflow's settings), and rebinned for a fan-beam projector (vial 300 px wide).  Device time with
+    the sinogram resident, the frame kernel alone against the HBM roofline, end to end from a host
+    array to host images, and the oracle's numpy port of the reference's CPU code beside it."""
+    import torch
+
+    from vamtoolbox_b200 import _lib, geometry
+    from vamtoolbox_b200 import imagesequence as ims
+
+    rng = np.random.default_rng(3)
+    sino = (rng.random((n, n_angles, n)) ** 3 * 40.0)
+    sino[: n // 10] = 0.0
+    cfg = ims.ImageConfig(screen, normalization_percentile=99.5, invert_u=True)
+    st = torch.cuda.current_stream(dev)
+    t_dev = torch.from_numpy(sino).to(dev)
+
+    def tim(fn, k=reps):
+        fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(k):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / k
+
+    t_pipeline = tim(lambda: ims.device_frames(t_dev, cfg))
+    frames = ims.device_frames(t_dev, cfg)
+    # the percentile select and the frame call alone (blank fill + window gather), through the C ABI
+    P = ims._prepare(t_dev, cfg)
+    k0, k1, gamma = ims.percentile_ranks(t_dev.numel(), cfg.normalization_percentile, np.dtype(np.float64))
+    pair = torch.empty(2, dtype=torch.float64, device=dev)
+    wb = _lib.load().vam_select_workspace_bytes()
+    work = torch.empty(wb, dtype=torch.uint8, device=dev)
+    sel = lambda: _lib.call("vam_select_pair", _lib.ptr(t_dev), _lib.DTYPE_F64, t_dev.numel(), k0, k1,
+                            _lib.ptr(pair), _lib.ptr(work), wb, _lib.stream_ptr())
+    t_select = tim(sel)
+    col, row = ims.placement_tables(cfg, n, n, n, n, True, False)
+    prm = P.prm
+    prm.n_u, prm.n_v = screen
+    prm.box_v0, prm.box_v1, prm.box_u0, prm.box_u1 = ims.table_box(col, row)
+    col_d, row_d = torch.from_numpy(col).to(dev), torch.from_numpy(row).to(dev)
+    prm.src_col_dev, prm.src_row_dev = col_d.data_ptr(), row_d.data_ptr()
+    kern = lambda: _lib.call("vam_imageseq_frames", _lib.ptr(t_dev), _lib.DTYPE_F64, n, n_angles, n,
+                             ctypes.byref(prm), _lib.ptr(frames), _lib.stream_ptr())
+    t_frames = tim(kern)
+    frame_bytes = frames.numel() + t_dev.numel() * 8 + 4 * (screen[0] + screen[1])
+    # end to end through ImageSeq: host float64 array in, host images out (page-locked, reused by
+    # torch's host caching allocator once a sequence is released)
+    ims.ImageSeq(cfg, sino)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for _ in range(3):
+        seq = ims.ImageSeq(cfg, sino)
+        del seq
+    torch.cuda.synchronize(dev)
+    t_e2e = (time.perf_counter() - t0) / 3
+    # fan-beam rebinning of the same sinogram
+    pg = geometry.ProjectionGeometry(np.linspace(0, 360, n_angles, endpoint=False))
+
+    def rebin():
+        return geometry.rebinFanBeam(geometry.Sinogram(t_dev, pg), 300, screen, 1.5, 1.7)
+
+    t_rebin = tim(rebin, 3)
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        pass
+    hbm = peaks.get("hbm_gbs") or 6650.0
+    out = {"workload": f"{n}x{n_angles}x{n} float64 sinogram -> {n_angles} frames {screen[0]}x{screen[1]} uint8, "
+                       "99.5th-percentile normalisation; fan-beam rebin to a 300 px vial",
+           "frames_per_s_device": round(n_angles / (t_pipeline * 1e-3), 1),
+           "pipeline_ms": round(t_pipeline, 4), "select_ms": round(t_select, 4), "frame_kernel_ms": round(t_frames, 4),
+           "e2e": {"value": round(n_angles / t_e2e, 1), "unit": "frames/s", "h2d_bytes_per_step": int(sino.nbytes),
+                   "d2h_bytes_per_step": int(frames.numel()),
+                   "path": "ImageSeq(cfg, numpy sinogram).images"},
+           "roofline_frames": {"bound": "hbm", "achieved": round(frame_bytes / (t_frames * 1e-3) / 1e9, 1),
+                               "peak": hbm, "unit": "GB/s",
+                               "frac": round(frame_bytes / (t_frames * 1e-3) / 1e9 / hbm, 4),
+                               "algorithmic_bytes": int(frame_bytes)},
+           "rebin_ms": round(t_rebin, 4)}
+    if cpu:
+        from oracle import formats as ofmt
+
+        t0 = time.perf_counter()
+        ofmt.image_frames(sino, ofmt.config(screen[0], screen[1], normalization_percentile=99.5, invert_u=True))
+        t_cpu = time.perf_counter() - t0
+        nz_s = 16
+        t0 = time.perf_counter()
+        ofmt.rebin_fan(sino[:, :, :nz_s], pg.angles, 300, screen, 1.5, 1.7)
+        t_cpu_rebin = (time.perf_counter() - t0) * n / nz_s
+        out["cpu_baseline"] = {"value": round(n_angles / t_cpu, 2), "unit": "frames/s", "cores": 1, "kind": "port",
+                               "sample": "the whole sequence through the oracle's numpy port of ImageSeq "
+                                         "(percentile, quantise, insert)",
+                               "rebin_ms": round(t_cpu_rebin * 1e3, 1),
+                               "rebin_sample": f"{nz_s} of {n} z slices through the numpy port of rebinFanBeam, "
+                                               "scaled to all slices"}
+    return out
+
+
 def run_ours(args):
     import torch
 
@@ -781,6 +887,13 @@ def run_ours(args):
         except Exception as exc:  # report, never fail the headline number on it
             algebraic = {"error": f"{type(exc).__name__}: {exc}"}
 
+    fmt = None
+    if ws_ == 1 and not args.no_formats:
+        try:
+            fmt = run_formats(dev, cpu=not args.no_cpu)
+        except Exception as exc:  # report, never fail the headline number on it
+            fmt = {"error": f"{type(exc).__name__}: {exc}"}
+
     ray = None
     if ws_ == 1 and not args.no_ray:
         try:
@@ -819,6 +932,7 @@ def run_ours(args):
             "multi_target": multi,
             "ray_tracer": ray,
             "algebraic": algebraic,
+            "output_formats": fmt,
             "configs": configs,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm_peak, "unit": "GB/s",
                          "frac": round(achieved / hbm_peak, 5), "traffic": traffic, "peak_source": peak_src,

@@ -407,6 +407,8 @@ typedef struct {
     int32_t has_scale;            /* multiply by intensity_scale (:135-138) */
     double intensity_scale;
     int32_t scale_is_f64;         /* the scale is a float64 numpy scalar (promotes a float32 array) */
+    int32_t box_v0, box_v1;       /* frame rows [v0, v1) and columns [u0, u1) that may show the image; */
+    int32_t box_u0, box_u1;       /* outside this box every pixel is 0 whatever the tables say */
 } vam_frame_params;
 
 /* frames_dev[a][v][u] (uint8, 16-byte aligned, nA frames of n_v x n_u) from
@@ -416,7 +418,10 @@ typedef struct {
  * np.minimum(., max), astype(uint8/16/32) and the store into a uint8 frame
  * (low byte) is replayed in the reference's dtypes; the insertion offsets,
  * array copies and flips of _insertImage / _arrayInsertImage (:303-355) are
- * carried by the two tables.  nA <= 65535. */
+ * carried by the two tables.  nA <= 65535.  The blank area outside the box
+ * is written with contiguous zero stores, the box by the gather kernel; a
+ * box equal to the frame makes it one gather pass (used to fetch just the
+ * image window, frame = window). */
 int vam_imageseq_frames(const void* sino_dev, int dtype, int32_t nR, int32_t nA, int32_t nZ,
                         const vam_frame_params* prm, uint8_t* frames_dev, vam_stream_t stream);
 

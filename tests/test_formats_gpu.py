@@ -204,3 +204,22 @@ def test_rebin_rejects_too_narrow_vial():
     pg = geometry.ProjectionGeometry(np.linspace(0, 360, 10, endpoint=False))
     with pytest.raises(ValueError):
         geometry.rebinFanBeam(geometry.Sinogram(np.zeros((30, 10, 2)), pg), 20, (1920, 1080), 1.5, 1.7)
+
+
+@pytest.mark.parametrize("shape,screen,kw", [
+    ((37, 5, 23), (68, 52), dict(normalization_percentile=95.0)),                 # odd window, n_u % 16 != 0
+    ((24, 4, 20), (64, 100), dict(array_num=4, array_offset=12, invert_v=True)),  # overlapping copies
+    ((24, 4, 20), (64, 100), dict(array_num=3, array_offset=30, v_offset=4)),     # gaps between copies
+    ((30, 3, 18), (96, 64), dict(rotate_angle=20.0, size_scale=1.3, invert_u=True)),
+    ((16, 2, 16), (64, 48), dict(array_num=0)),                                   # nothing inserted
+])
+def test_device_frames_and_images_match_oracle(shape, screen, kw):
+    rng = np.random.default_rng(17)
+    sino = rng.random(shape) * 300.0
+    cfg = ims.ImageConfig(screen, **kw)
+    seq = ims.ImageSeq(cfg, sino, keep_device_frames=True)
+    full = seq.frames_device.cpu().numpy()
+    assert np.array_equal(full, np.stack(seq.images))
+    ref = formats.image_frames(sino, formats.config(*screen, **kw))
+    transformed = "rotate_angle" in kw or "size_scale" in kw
+    assert_frames_close(full, ref, transformed, kw)

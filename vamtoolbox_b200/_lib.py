@@ -80,7 +80,8 @@ class BclpParams(ctypes.Structure):
 class FrameParams(ctypes.Structure):
     _fields_ = [("n_u", _c_i32), ("n_v", _c_i32), ("src_col_dev", _vp), ("src_row_dev", _vp),
                 ("bit_depth", _c_i32), ("has_norm", _c_i32), ("norm_value", _c_d), ("norm_dtype", _c_i32),
-                ("has_scale", _c_i32), ("intensity_scale", _c_d), ("scale_is_f64", _c_i32)]
+                ("has_scale", _c_i32), ("intensity_scale", _c_d), ("scale_is_f64", _c_i32),
+                ("box_v0", _c_i32), ("box_v1", _c_i32), ("box_u0", _c_i32), ("box_u1", _c_i32)]
 
 
 DTYPE_F32, DTYPE_F64 = 0, 1

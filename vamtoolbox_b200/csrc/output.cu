@@ -213,22 +213,31 @@ __global__ void __launch_bounds__(kThreads) k_sel_hist(const T* __restrict__ x, 
     const K dmask = (K)((1u << width) - 1u);
     const int lane = threadIdx.x & 31;
     unsigned long long nans = 0;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    // every lane of a warp runs the same number of iterations (the loop bound
-    // is rounded up to whole warps) so __match_any_sync sees the full warp
-    const long long start = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long nr = (n + 31) & ~31ll;
-    for (long long i = start; i < nr; i += stride) {
-        int bin = kBins;   // no bin
-        if (i < n) {
-            const T v = x[i];
-            if (first && v != v) ++nans;
-            const K key = key_of(v);
-            const bool match = hi >= kKeyBits ? true : (K)(key >> hi) == want;
-            if (match) bin = (int)((key >> shift) & dmask);
+    // each warp takes 128 consecutive keys per step (4 coalesced loads in
+    // flight per lane); the step index is uniform across the warp, so every
+    // __match_any_sync sees all 32 lanes
+    const long long warp_id = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long n_warps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long base = warp_id * 128; base < n; base += n_warps * 128) {
+        T v[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const long long i = base + k * 32 + lane;
+            v[k] = i < n ? x[i] : (T)0;
         }
-        const unsigned peers = __match_any_sync(0xFFFFFFFFu, bin);
-        if (bin < kBins && lane == __ffs(peers) - 1) atomicAdd(&sh[bin], (unsigned)__popc(peers));
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            int bin = kBins;   // no bin
+            if (base + k * 32 + lane < n) {
+                if (first && v[k] != v[k]) ++nans;
+                const K key = key_of(v[k]);
+                const bool match = hi >= kKeyBits ? true : (K)(key >> hi) == want;
+                if (match) bin = (int)((key >> shift) & dmask);
+            }
+            if (!__any_sync(0xFFFFFFFFu, bin < kBins)) continue;   // no lane inside the prefix range
+            const unsigned peers = __match_any_sync(0xFFFFFFFFu, bin);
+            if (bin < kBins && lane == __ffs(peers) - 1) atomicAdd(&sh[bin], (unsigned)__popc(peers));
+        }
     }
     if (first && nans) atomicAdd(&st->nan_count, nans);
     __syncthreads();
@@ -236,37 +245,47 @@ __global__ void __launch_bounds__(kThreads) k_sel_hist(const T* __restrict__ x, 
         if (sh[i]) atomicAdd(&st->hist[i], sh[i]);
 }
 
-// One warp: pick the bin holding rank k, fold it into the prefix, clear the histogram.
-__global__ void k_sel_scan(SelState* st, int shift, int width) {
-    const int lane = threadIdx.x;
+// One block of kBins / 2 threads: pick the bin holding rank k, fold it into
+// the prefix, clear the histogram.
+constexpr int kScanThreads = kBins / 2;
+
+__global__ void __launch_bounds__(kScanThreads) k_sel_scan(SelState* st, int shift, int width) {
+    __shared__ long long warp_sum[kScanThreads / 32];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int nb = 1 << width;
-    const int per = (nb + 31) / 32;
-    const int lo = lane * per, hi = min(lo + per, nb);
-    long long mine = 0;
-    for (int i = lo; i < hi; ++i) mine += st->hist[i];
+    const long long k = st->k;   // read by every thread before the owner rewrites it
+    const long long c0 = 2 * t < nb ? st->hist[2 * t] : 0;
+    const long long c1 = 2 * t + 1 < nb ? st->hist[2 * t + 1] : 0;
+    const long long mine = c0 + c1;
     long long incl = mine;
     for (int o = 1; o < 32; o <<= 1) {
-        const long long t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-        if (lane >= o) incl += t;
+        const long long v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += v;
     }
-    const long long excl = incl - mine;
-    const long long k = st->k;
-    const bool owner = k >= excl && k < incl;
-    if (owner) {
-        long long cum = excl;
-        int b = lo;
-        for (; b < hi - 1; ++b) {
-            const long long c = st->hist[b];
-            if (k < cum + c) break;
-            cum += c;
+    if (lane == 31) warp_sum[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        long long w = lane < kScanThreads / 32 ? warp_sum[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long v = __shfl_up_sync(0xFFFFFFFFu, w, o);
+            if (lane >= o) w += v;
         }
-        st->k = k - cum;
-        st->less += cum;
-        st->eq = st->hist[b];
+        if (lane < kScanThreads / 32) warp_sum[lane] = w;   // inclusive prefix over warps
+    }
+    __syncthreads();
+    incl += warp > 0 ? warp_sum[warp - 1] : 0;
+    const long long excl = incl - mine;
+    if (k >= excl && k < incl) {   // exactly one thread owns rank k
+        const int b = k < excl + c0 ? 2 * t : 2 * t + 1;
+        const long long below = k < excl + c0 ? excl : excl + c0;
+        st->k = k - below;
+        st->less += below;
+        st->eq = b == 2 * t ? c0 : c1;
         st->prefix |= (unsigned long long)b << shift;
     }
-    __syncwarp();
-    for (int i = lane; i < nb; i += 32) st->hist[i] = 0u;
+    __syncthreads();
+    if (2 * t < kBins) st->hist[2 * t] = 0u;
+    if (2 * t + 1 < kBins) st->hist[2 * t + 1] = 0u;
 }
 
 // Second rank (k1 = k0 + 1) when it lies past the run of key0: min{key > key0}.
@@ -278,7 +297,18 @@ __global__ void __launch_bounds__(kThreads) k_sel_min_above(const T* __restrict_
     const K key0 = (K)st->prefix;
     K best = (K)~(K)0;
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    for (; i + 3 * stride < n; i += 4 * stride) {   // 4 loads in flight
+        T v[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) v[k] = x[i + k * stride];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const K key = key_of(v[k]);
+            if (key > key0 && key < best) best = key;
+        }
+    }
+    for (; i < n; i += stride) {
         const K key = key_of(x[i]);
         if (key > key0 && key < best) best = key;
     }
@@ -371,51 +401,90 @@ __device__ __forceinline__ uint32_t quantise(T x, const QuantArgs& q) {
 
 struct FrameArgs {
     int nR, nA, nZ, n_u, n_v;
+    int v0, v1;      // window rows [v0, v1)
+    int u0, u1;      // window byte columns [u0, u1), multiples of the store width
+    int vec16;       // n_u % 16 == 0: 16-byte stores, else 4-byte stores
     const int* src_col;
     const int* src_row;
     QuantArgs q;
 };
 
+// Window tile of the frames: lane = frame row, warp = 16 frame columns.
+// Every load instruction of a warp reads 32 consecutive z of one sinogram row
+// (the rows of a frame are consecutive z); every lane stores 16 contiguous
+// bytes.  Rows / columns whose table entry is -1 (gaps between arrayed
+// copies, store-width padding at the window edge) get zeros.
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_frames(const T* __restrict__ sino, uint8_t* __restrict__ frames,
-                                                     const FrameArgs p) {
+__device__ __forceinline__ void frames_window_tile(const T* __restrict__ sino, uint8_t* __restrict__ frames,
+                                                   const FrameArgs& p, int a, int tile_v, int tile_u) {
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    const int v = blockIdx.y * 32 + lane;
-    const int u0 = (blockIdx.x * (kThreads / 32) + warp) * 32;
-    const int a = blockIdx.z;
-    if (u0 >= p.n_u) return;
-    const int z = v < p.n_v ? __ldg(p.src_row + v) : -1;
-    uint32_t word[8];
-#pragma unroll
-    for (int w = 0; w < 8; ++w) word[w] = 0u;
+    const int v = p.v0 + tile_v * 32 + lane;
+    const int u0 = p.u0 + (tile_u * (kThreads / 32) + warp) * 16;
+    if (u0 >= p.u1) return;
+    int z = v < p.v1 ? __ldg(p.src_row + v) : -1;
+    if (z >= p.nZ) z = -1;   // table entries outside the sinogram read as blank
+    uint32_t word[4] = {0u, 0u, 0u, 0u};
     // column indices are the same for all lanes: one broadcast load each
-    int r[32];
+    int r[16];
 #pragma unroll
-    for (int j = 0; j < 32; ++j) {
-        r[j] = (u0 + j < p.n_u) ? __ldg(p.src_col + u0 + j) : -1;
-        if (r[j] >= p.nR) r[j] = -1;   // table entries outside the sinogram read as blank
+    for (int j = 0; j < 16; ++j) {
+        r[j] = (u0 + j < p.u1) ? __ldg(p.src_col + u0 + j) : -1;
+        if (r[j] >= p.nR) r[j] = -1;
     }
-    if (z >= 0 && z < p.nZ) {
+    if (z >= 0) {
         const T* col = sino + (size_t)a * p.nZ + z;
         const size_t rs = (size_t)p.nA * p.nZ;
-        T x[32];
+        T x[16];
 #pragma unroll
-        for (int j = 0; j < 32; ++j) x[j] = r[j] >= 0 ? __ldg(col + (size_t)r[j] * rs) : (T)0;
+        for (int j = 0; j < 16; ++j) x[j] = r[j] >= 0 ? __ldg(col + (size_t)r[j] * rs) : (T)0;
 #pragma unroll
-        for (int j = 0; j < 32; ++j)
+        for (int j = 0; j < 16; ++j)
             if (r[j] >= 0) word[j >> 2] |= quantise(x[j], p.q) << (8 * (j & 3));
     }
-    if (v >= p.n_v) return;
+    if (v >= p.v1) return;
     uint8_t* dst = frames + ((size_t)a * p.n_v + v) * p.n_u + u0;
-    if (u0 + 32 <= p.n_u && (p.n_u & 15) == 0) {
-        reinterpret_cast<uint4*>(dst)[0] = make_uint4(word[0], word[1], word[2], word[3]);
-        reinterpret_cast<uint4*>(dst)[1] = make_uint4(word[4], word[5], word[6], word[7]);
+    if (p.vec16) {
+        *reinterpret_cast<uint4*>(dst) = make_uint4(word[0], word[1], word[2], word[3]);
     } else {
 #pragma unroll
-        for (int w = 0; w < 8; ++w)
-            if (u0 + 4 * w < p.n_u) reinterpret_cast<uint32_t*>(dst)[w] = word[w];
+        for (int w = 0; w < 4; ++w)
+            if (u0 + 4 * w < p.u1) reinterpret_cast<uint32_t*>(dst)[w] = word[w];
     }
+}
+
+// Frame row outside the window: zeros, contiguous 16-byte (4-byte when
+// n_u % 16 != 0) stores by one warp.
+__device__ __forceinline__ void frames_blank_row(uint8_t* __restrict__ frames, long long row, const FrameArgs& p) {
+    const int lane = threadIdx.x & 31;
+    const int v = (int)(row % p.n_v);
+    const bool in_rows = v >= p.v0 && v < p.v1;
+    uint8_t* dst = frames + row * p.n_u;
+    if (p.vec16) {
+        for (int u = lane * 16; u < p.n_u; u += 32 * 16)
+            if (!(in_rows && u >= p.u0 && u < p.u1)) *reinterpret_cast<uint4*>(dst + u) = make_uint4(0u, 0u, 0u, 0u);
+    } else {
+        for (int u = lane * 4; u < p.n_u; u += 32 * 4)
+            if (!(in_rows && u >= p.u0 && u < p.u1)) *reinterpret_cast<uint32_t*>(dst + u) = 0u;
+    }
+}
+
+// One grid for both parts, so the quantiser arithmetic of the window tiles
+// overlaps the store stream of the blank rows: blocks [0, n_win) are window
+// tiles (a, tile row, tile column), the rest take 8 blank frame rows each.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_frames(const T* __restrict__ sino, uint8_t* __restrict__ frames,
+                                                     const FrameArgs p, int tiles_u, int tiles_v, long long n_win,
+                                                     long long n_rows) {
+    const long long b = blockIdx.x;
+    if (b < n_win) {
+        const int tu = (int)(b % tiles_u);
+        const long long rest = b / tiles_u;
+        frames_window_tile<T>(sino, frames, p, (int)(rest / tiles_v), (int)(rest % tiles_v), tu);
+        return;
+    }
+    const long long row = (b - n_win) * (kThreads / 32) + (threadIdx.x >> 5);
+    if (row < n_rows) frames_blank_row(frames, row, p);
 }
 
 // ---------------------------------------------------------------------------
@@ -437,10 +506,27 @@ struct RebinArgs {
 };
 
 template <typename T>
+__device__ __forceinline__ double rebin_sample(const double (&x)[4], bool inb, double a0, double y0, double a1,
+                                               double y1, double dd, double tinv) {
+    double v = 0.0;
+    if (inb) {
+        v = dmul(dmul(x[0], a0), a1);
+        v = dadd(v, dmul(dmul(x[1], a0), y1));
+        v = dadd(v, dmul(dmul(x[2], y0), a1));
+        v = dadd(v, dmul(dmul(x[3], y0), y1));
+    }
+    return dmul(tinv, dmul(v, dd));
+}
+
+// One warp per output row (p, a), lanes along z, four z per lane in flight
+// (16 loads); eight rows per block.
+template <typename T>
 __global__ void __launch_bounds__(kThreads) k_rebin_fan(const T* __restrict__ in, T* __restrict__ out,
                                                         const RebinArgs p) {
-    const int row = blockIdx.x;   // pp * nA + a
-    const int pp = row / p.nA;
+    const int lane = threadIdx.x & 31;
+    const long long row = (long long)blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);   // pp * nA + a
+    if (row >= (long long)p.nP * p.nA) return;
+    const int pp = (int)(row / p.nA);
     const int i0 = __ldg(p.xi + pp), j0 = __ldg(p.ti + row);
     const double y0 = __ldg(p.xw + 4 * pp), a0 = __ldg(p.xw + 4 * pp + 1);
     const double dd = __ldg(p.xw + 4 * pp + 2), tinv = __ldg(p.xw + 4 * pp + 3);
@@ -452,18 +538,22 @@ __global__ void __launch_bounds__(kThreads) k_rebin_fan(const T* __restrict__ in
     const T* b00 = in + (size_t)(ok0 ? r0 : 0) * rs + (size_t)(inb ? j0 : 0) * p.nZ;
     const T* b10 = in + (size_t)(ok1 ? r1 : 0) * rs + (size_t)(inb ? j0 : 0) * p.nZ;
     T* o = out + (size_t)row * p.nZ;
-    for (int z = threadIdx.x; z < p.nZ; z += blockDim.x) {
-        double v = 0.0;
-        if (inb) {
-            const double x00 = ok0 ? ld(b00 + z) : 0.0, x01 = ok0 ? ld(b00 + p.nZ + z) : 0.0;
-            const double x10 = ok1 ? ld(b10 + z) : 0.0, x11 = ok1 ? ld(b10 + p.nZ + z) : 0.0;
-            v = dmul(dmul(x00, a0), a1);
-            v = dadd(v, dmul(dmul(x01, a0), y1));
-            v = dadd(v, dmul(dmul(x10, y0), a1));
-            v = dadd(v, dmul(dmul(x11, y0), y1));
+    for (int z0 = lane; z0 < p.nZ; z0 += 4 * 32) {
+        double x[4][4];
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+            const int z = z0 + h * 32;
+            const bool zin = z < p.nZ;
+            x[h][0] = ok0 && zin ? ld(b00 + z) : 0.0;
+            x[h][1] = ok0 && zin ? ld(b00 + p.nZ + z) : 0.0;
+            x[h][2] = ok1 && zin ? ld(b10 + z) : 0.0;
+            x[h][3] = ok1 && zin ? ld(b10 + p.nZ + z) : 0.0;
         }
-        v = dmul(tinv, dmul(v, dd));
-        o[z] = (T)v;
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+            const int z = z0 + h * 32;
+            if (z < p.nZ) o[z] = (T)rebin_sample<T>(x[h], inb, a0, y0, a1, y1, dd, tinv);
+        }
     }
 }
 
@@ -542,7 +632,7 @@ extern "C" int vam_select_pair(const void* x, int dtype, int64_t n, int64_t k0, 
             k_sel_hist<double><<<blocks, kThreads, 0, st>>>((const double*)x, n, s, shift, width, d == 0);
         else
             k_sel_hist<float><<<blocks, kThreads, 0, st>>>((const float*)x, n, s, shift, width, d == 0);
-        k_sel_scan<<<1, 32, 0, st>>>(s, shift, width);
+        k_sel_scan<<<1, kScanThreads, 0, st>>>(s, shift, width);
     }
     if (dtype == VAM_DTYPE_F64) {
         if (k1 != k0) k_sel_min_above<double><<<blocks, kThreads, 0, st>>>((const double*)x, n, s, k1);
@@ -570,12 +660,22 @@ extern "C" int vam_imageseq_frames(const void* sino, int dtype, int32_t nR, int3
                 "vam_imageseq_frames: bit_depth must be in [0, 32]");
     if (prm->has_norm) VAM_REQUIRE(prm->norm_dtype == VAM_DTYPE_F32 || prm->norm_dtype == VAM_DTYPE_F64,
                                    VAM_ERR_ARG, "vam_imageseq_frames: bad norm_dtype");
+    VAM_REQUIRE(prm->box_v0 >= 0 && prm->box_v0 <= prm->box_v1 && prm->box_v1 <= prm->n_v &&
+                prm->box_u0 >= 0 && prm->box_u0 <= prm->box_u1 && prm->box_u1 <= prm->n_u, VAM_ERR_ARG,
+                "vam_imageseq_frames: window box outside the frame");
     FrameArgs p;
     p.nR = nR;
     p.nA = nA;
     p.nZ = nZ;
     p.n_u = prm->n_u;
     p.n_v = prm->n_v;
+    p.vec16 = (prm->n_u % 16) == 0;
+    const int w = p.vec16 ? 16 : 4;
+    p.v0 = prm->box_v0;
+    p.v1 = prm->box_v1;
+    p.u0 = prm->box_u0 / w * w;
+    p.u1 = std::min((prm->box_u1 + w - 1) / w * w, prm->n_u);
+    if (p.v0 == p.v1 || p.u0 == p.u1) p.v0 = p.v1 = p.u0 = p.u1 = 0;   // empty window: all blank
     p.src_col = prm->src_col_dev;
     p.src_row = prm->src_row_dev;
     const double maxv = (double)((1ull << prm->bit_depth) - 1ull);
@@ -592,11 +692,22 @@ extern "C" int vam_imageseq_frames(const void* sino, int dtype, int32_t nR, int3
     q.max_d = maxv;
     q.max_f = (float)maxv;
     q.wide = prm->bit_depth > 16;
-    dim3 grid((prm->n_u + kThreads - 1) / kThreads, (prm->n_v + 31) / 32, nA);
-    if (dtype == VAM_DTYPE_F64)
-        k_frames<double><<<grid, kThreads, 0, (cudaStream_t)stream>>>((const double*)sino, frames, p);
-    else
-        k_frames<float><<<grid, kThreads, 0, (cudaStream_t)stream>>>((const float*)sino, frames, p);
+    cudaStream_t st = (cudaStream_t)stream;
+    const bool has_blank = !(p.v0 == 0 && p.v1 == prm->n_v && p.u0 == 0 && p.u1 == prm->n_u);
+    const long long n_rows = has_blank ? (long long)nA * prm->n_v : 0;
+    const int tiles_u = (p.u1 - p.u0 + (kThreads / 32) * 16 - 1) / ((kThreads / 32) * 16);
+    const int tiles_v = (p.v1 - p.v0 + 31) / 32;
+    const long long n_win = (long long)nA * tiles_u * tiles_v;
+    const long long blocks = n_win + (n_rows + kThreads / 32 - 1) / (kThreads / 32);
+    VAM_REQUIRE(blocks < (1ll << 31), VAM_ERR_SHAPE, "vam_imageseq_frames: too many frame rows");
+    if (blocks > 0) {
+        if (dtype == VAM_DTYPE_F64)
+            k_frames<double><<<(unsigned)blocks, kThreads, 0, st>>>((const double*)sino, frames, p, tiles_u,
+                                                                    tiles_v, n_win, n_rows);
+        else
+            k_frames<float><<<(unsigned)blocks, kThreads, 0, st>>>((const float*)sino, frames, p, tiles_u,
+                                                                   tiles_v, n_win, n_rows);
+    }
     VAM_CHECK_LAUNCH("vam_imageseq_frames");
     return VAM_OK;
 }
@@ -610,12 +721,11 @@ extern "C" int vam_rebin_fan(const void* in, int dtype, int32_t nR, int32_t nA, 
     VAM_REQUIRE(nR > 0 && nA > 0 && nZ > 0 && nP > 0, VAM_ERR_SHAPE, "vam_rebin_fan: empty shape");
     VAM_REQUIRE((int64_t)nP * nA < (1ll << 31), VAM_ERR_SHAPE, "vam_rebin_fan: nP * nA too large");
     RebinArgs p{nR, nA, nZ, nP, pad_lo, xi, xw, ti, tw};
-    const int threads = nZ >= kThreads ? kThreads : ((nZ + 31) / 32) * 32;
-    const unsigned rows = (unsigned)((int64_t)nP * nA);
+    const unsigned blocks = (unsigned)(((int64_t)nP * nA + kThreads / 32 - 1) / (kThreads / 32));
     if (dtype == VAM_DTYPE_F64)
-        k_rebin_fan<double><<<rows, threads, 0, (cudaStream_t)stream>>>((const double*)in, (double*)out, p);
+        k_rebin_fan<double><<<blocks, kThreads, 0, (cudaStream_t)stream>>>((const double*)in, (double*)out, p);
     else
-        k_rebin_fan<float><<<rows, threads, 0, (cudaStream_t)stream>>>((const float*)in, (float*)out, p);
+        k_rebin_fan<float><<<blocks, kThreads, 0, (cudaStream_t)stream>>>((const float*)in, (float*)out, p);
     VAM_CHECK_LAUNCH("vam_rebin_fan");
     return VAM_OK;
 }

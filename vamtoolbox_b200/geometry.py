@@ -231,7 +231,7 @@ def getInds(target):
     return np.logical_and(target > 0, circle), np.logical_and(target == 0, circle)
 
 
-def fan_beam_tables(angles, n_r, vial_width, N_screen, n_write, throw_ratio):
+def fan_beam_tables(angles, vial_width, N_screen, n_write, throw_ratio):
     """Sampling tables of rebinFanBeam (vamtoolbox/geometry.py:736-944), in float64.
 
     Follows the reference's formulas step by step: projector coordinate xp,
@@ -290,6 +290,32 @@ def grid_search(grid, x):
     return np.where(oob, -1, i).astype(np.int32), y
 
 
+_FAN_TABLES = {}
+
+
+def _fan_beam_device_tables(angles, vial_width, N_screen, n_write, throw_ratio, dev):
+    """Device copies of the rebinning tables, built once per geometry and device
+    (a projector setup converts many sinograms with the same tables)."""
+    import torch
+
+    key = (np.asarray(angles, dtype=np.float64).tobytes(), int(vial_width), tuple(int(v) for v in N_screen),
+           float(n_write), float(throw_ratio), str(dev))
+    hit = _FAN_TABLES.get(key)
+    if hit is not None:
+        return hit
+    xp, xv, theta_samp, dxv_dxp, T = fan_beam_tables(angles, vial_width, N_screen, n_write, throw_ratio)
+    xi, y0 = grid_search(xp, xv)
+    ti, y1 = grid_search(angles, theta_samp)
+    with np.errstate(divide="ignore"):
+        xw = np.stack([y0, 1 - y0, dxv_dxp, 1 / T], axis=1)
+    tw = np.stack([y1, 1 - y1], axis=2)
+    tabs = tuple(torch.from_numpy(np.ascontiguousarray(t)).to(dev) for t in (xi, xw, ti, tw))
+    if len(_FAN_TABLES) >= 16:
+        _FAN_TABLES.pop(next(iter(_FAN_TABLES)))
+    _FAN_TABLES[key] = tabs
+    return tabs
+
+
 def rebinFanBeam(sinogram, vial_width, N_screen, n_write, throw_ratio):
     """Rebin a parallel-beam sinogram for a non-telecentric projector and a
     vial that is not index matched (vamtoolbox/geometry.py:736-944; Orth et
@@ -313,18 +339,15 @@ def rebinFanBeam(sinogram, vial_width, N_screen, n_write, throw_ratio):
         raise ValueError(f"There are {n_a} point(s) in dimension 1, but method linear requires at least 2 points.")
     if not np.all(np.diff(angles) > 0):
         raise ValueError("The points in dimension 1 must be strictly ascending")
-    xp, xv, theta_samp, dxv_dxp, T = fan_beam_tables(angles, n_r, vial_width, N_screen, n_write, throw_ratio)
-
     pd = int((vial_width - n_r) / 2)
     if is_torch:
-        import torch.nn.functional as F
-
+        rows = n_r + 2 * max(pd, 0)
+        rows += 1 if rows < vial_width else 0
         padded = arr
-        if pd > 0:
-            padded = F.pad(padded.movedim(0, -1), (pd, pd)).movedim(-1, 0)
-        if padded.shape[0] < vial_width:
-            padded = F.pad(padded.movedim(0, -1), (0, 1)).movedim(-1, 0)
-        sinogram.array = padded.contiguous()
+        if rows != n_r:
+            padded = torch.zeros((rows, n_a, n_z), dtype=arr.dtype, device=arr.device)
+            padded[max(pd, 0):max(pd, 0) + n_r] = arr
+        sinogram.array = padded
     else:
         padded = arr
         if pd > 0:
@@ -336,10 +359,6 @@ def rebinFanBeam(sinogram, vial_width, N_screen, n_write, throw_ratio):
     if n_p != vial_width:
         raise ValueError(f"There are {vial_width} points and {n_p} values in dimension 0")
 
-    xi, y0 = grid_search(xp, xv)
-    ti, y1 = grid_search(angles, theta_samp)
-    xw = np.stack([y0, 1 - y0, dxv_dxp, 1 / T], axis=1)
-    tw = np.stack([y1, 1 - y1], axis=2)
     dt = arr.dtype
     if is_torch:
         dev = arr.device if arr.is_cuda else torch.device("cuda", torch.cuda.current_device())
@@ -355,10 +374,7 @@ def rebinFanBeam(sinogram, vial_width, N_screen, n_write, throw_ratio):
 
     code = _lib.DTYPE_F64 if np_dt == np.float64 else _lib.DTYPE_F32
     with torch.cuda.device(dev):
-        t_xi = torch.from_numpy(xi).to(dev)
-        t_xw = torch.from_numpy(np.ascontiguousarray(xw)).to(dev)
-        t_ti = torch.from_numpy(np.ascontiguousarray(ti)).to(dev)
-        t_tw = torch.from_numpy(np.ascontiguousarray(tw)).to(dev)
+        t_xi, t_xw, t_ti, t_tw = _fan_beam_device_tables(angles, vial_width, N_screen, n_write, throw_ratio, dev)
         out = torch.empty((n_p, n_a, n_z), dtype=src.dtype, device=dev)
         _lib.call("vam_rebin_fan", _lib.ptr(src), code, n_r, n_a, n_z, n_p, max(pd, 0), _lib.ptr(t_xi),
                   _lib.ptr(t_xw), _lib.ptr(t_ti), _lib.ptr(t_tw), _lib.ptr(out), _lib.stream_ptr())

@@ -101,19 +101,15 @@ def copy_offsets(cfg):
     return offsets
 
 
-def placement_tables(cfg, s_u, s_v, n_r, n_z, flip_r=False, flip_z=False):
-    """Frame column -> sinogram row and frame row -> sinogram z tables.
+def insert_boxes(cfg, s_u, s_v):
+    """Frame rectangles (u1, u2, v1, v2), one per inserted copy in insertion
+    order, of an s_v x s_u image (_insertImage, imagesequence.py:303-326).
 
-    The image of angle j is sino[:, j, :].T (s_v = z extent rows, s_u = r
-    extent columns), inserted at [v1:v2, u1:u2] by _insertImage
-    (imagesequence.py:303-326) once per copy; a later copy overwrites an
-    earlier one.  Raises the reference's exceptions for an image that does
-    not fit, and numpy's broadcast ValueError where the truncated bounds span
-    fewer pixels than the image.  Flips not applied by a plane transform are
-    folded in here (_invertU / _invertV, :358-365).  -1 marks blank pixels.
+    Raises the reference's exceptions for an image that does not fit, and
+    numpy's broadcast ValueError where the truncated bounds span fewer pixels
+    than the image.
     """
-    src_col = np.full(cfg.N_u, -1, dtype=np.int32)
-    src_row = np.full(cfg.N_v, -1, dtype=np.int32)
+    boxes = []
     for v_off in copy_offsets(cfg):
         u1 = int(cfg.N_u / 2 - cfg.u_offset - s_u / 2)
         u2 = int(cfg.N_u / 2 - cfg.u_offset + s_u / 2)
@@ -130,11 +126,36 @@ def placement_tables(cfg, s_u, s_v, n_r, n_z, flip_r=False, flip_z=False):
         if (v2 - v1, u2 - u1) != (s_v, s_u):
             raise ValueError(f"could not broadcast input array from shape ({s_v},{s_u}) into shape "
                              f"({v2 - v1},{u2 - u1})")
+        boxes.append((u1, u2, v1, v2))
+    return boxes
+
+
+def placement_tables(cfg, s_u, s_v, n_r, n_z, flip_r=False, flip_z=False):
+    """Frame column -> sinogram row and frame row -> sinogram z tables.
+
+    The image of angle j is sino[:, j, :].T (s_v = z extent rows, s_u = r
+    extent columns), inserted by _insertImage once per copy
+    (:func:`insert_boxes`); a later copy overwrites an earlier one.  Flips not
+    applied by a plane transform are folded in here (_invertU / _invertV,
+    imagesequence.py:358-365).  -1 marks blank pixels.
+    """
+    src_col = np.full(cfg.N_u, -1, dtype=np.int32)
+    src_row = np.full(cfg.N_v, -1, dtype=np.int32)
+    for u1, u2, v1, v2 in insert_boxes(cfg, s_u, s_v):
         cols = np.arange(s_u, dtype=np.int32)
         rows = np.arange(s_v, dtype=np.int32)
         src_col[u1:u2] = (n_r - 1 - cols) if flip_r else cols
         src_row[v1:v2] = (n_z - 1 - rows) if flip_z else rows
     return src_col, src_row
+
+
+def table_box(src_col, src_row):
+    """Bounding box (v0, v1, u0, u1) of the non-blank table entries."""
+    rows = np.flatnonzero(src_row >= 0)
+    cols = np.flatnonzero(src_col >= 0)
+    if rows.size == 0 or cols.size == 0:
+        return 0, 0, 0, 0
+    return int(rows[0]), int(rows[-1]) + 1, int(cols[0]), int(cols[-1]) + 1
 
 
 def percentile_ranks(n, p, dtype):
@@ -213,12 +234,12 @@ def _sinogram_array(sinogram):
     raise ArgumentError("sinogram not specified.")
 
 
-def device_frames(sinogram, cfg, device=None, stream=None):
-    """Run the frame pipeline on the GPU; returns the [nA][N_v][N_u] uint8 frames.
+class _Prepared:
+    """The sinogram after the plane transforms, on the device, with the
+    quantiser parameters of the frame kernel (everything but the tables)."""
 
-    ``sinogram``: numpy array, torch tensor (any device) or Sinogram, shape
-    [nR][nA][nZ], float32 or float64.
-    """
+
+def _prepare(sinogram, cfg, device=None, stream=None):
     import torch
 
     arr = _sinogram_array(sinogram)
@@ -239,6 +260,8 @@ def device_frames(sinogram, cfg, device=None, stream=None):
     if cur.dim() != 3:
         raise IndexError(f"too many indices for array: array is {cur.dim()}-dimensional, but 3 were indexed")
     _lib.load()
+    P = _Prepared()
+    P.dev = dev
     with torch.cuda.device(dev):
         st = _lib.stream_ptr(stream)
         cur_dt = np.dtype(np_dtype)
@@ -263,11 +286,10 @@ def device_frames(sinogram, cfg, device=None, stream=None):
             n_r, n_z = o_r, o_z
 
         prm = _lib.FrameParams()
-        prm.n_u, prm.n_v = int(cfg.N_u), int(cfg.N_v)
-        prm.bit_depth = int(cfg.bit_depth)
         _output_dtype(cfg.bit_depth)
         if not 0 <= cfg.bit_depth <= 32:
             raise ValueError(f"bit_depth {cfg.bit_depth} is outside 0..32")
+        prm.bit_depth = int(cfg.bit_depth)
         stage_dt = cur_dt
         if cfg.normalization_percentile is not None:
             n = cur.numel()
@@ -288,27 +310,51 @@ def device_frames(sinogram, cfg, device=None, stream=None):
             prm.has_scale = 1
             prm.intensity_scale = float(cfg.intensity_scale)
             prm.scale_is_f64 = int(scaled_dt == np.float64)
+    P.cur, P.cur_dt, P.shape, P.flips, P.prm, P.stream = cur, cur_dt, (n_r, n_a, n_z), (flip_r, flip_z), prm, st
+    return P
 
-        src_col, src_row = placement_tables(cfg, n_r, n_z, n_r, n_z, flip_r, flip_z)
-        col_d = torch.from_numpy(src_col).to(dev)
-        row_d = torch.from_numpy(src_row).to(dev)
+
+def _launch_frames(P, src_col, src_row, n_u, n_v, box, out):
+    import torch
+
+    prm = P.prm
+    prm.n_u, prm.n_v = int(n_u), int(n_v)
+    prm.box_v0, prm.box_v1, prm.box_u0, prm.box_u1 = box
+    with torch.cuda.device(P.dev):
+        col_d = torch.from_numpy(src_col).to(P.dev)
+        row_d = torch.from_numpy(src_row).to(P.dev)
         prm.src_col_dev = col_d.data_ptr()
         prm.src_row_dev = row_d.data_ptr()
-        frames = torch.empty((n_a, cfg.N_v, cfg.N_u), dtype=torch.uint8, device=dev)
+        n_r, n_a, n_z = P.shape
         if n_a > 0:
-            _lib.call("vam_imageseq_frames", _lib.ptr(cur), _dtype_code(cur_dt), n_r, n_a, n_z,
-                      ctypes.byref(prm), _lib.ptr(frames), st)
-    return frames
+            _lib.call("vam_imageseq_frames", _lib.ptr(P.cur), _dtype_code(P.cur_dt), n_r, n_a, n_z,
+                      ctypes.byref(prm), _lib.ptr(out), P.stream)
+    return out
+
+
+def device_frames(sinogram, cfg, device=None, stream=None):
+    """Run the frame pipeline on the GPU; returns the [nA][N_v][N_u] uint8 frames on the device.
+
+    ``sinogram``: numpy array, torch tensor (any device) or Sinogram, shape
+    [nR][nA][nZ], float32 or float64.
+    """
+    import torch
+
+    P = _prepare(sinogram, cfg, device, stream)
+    n_r, n_a, n_z = P.shape
+    src_col, src_row = placement_tables(cfg, n_r, n_z, n_r, n_z, *P.flips)
+    frames = torch.empty((n_a, cfg.N_v, cfg.N_u), dtype=torch.uint8, device=P.dev)
+    return _launch_frames(P, src_col, src_row, cfg.N_u, cfg.N_v, table_box(src_col, src_row), frames)
 
 
 class ImageSeq:
     """Sinogram converted to projector frames (imagesequence.py:85-284).
 
-    ``images`` is the reference's list of N_v x N_u uint8 arrays, one per
-    angle.  With ``keep_device_frames=True`` the frames also stay on the GPU
-    as ``frames_device`` ([nA][N_v][N_u] uint8), e.g. for a display pipeline
-    that never needs them on the host; with ``host_images=False`` the host
-    copy is skipped and ``images`` is None.
+    The frames are built on the GPU (:func:`device_frames`).  ``images`` is
+    the reference's list of N_v x N_u uint8 arrays, one per angle (views of
+    one page-locked [nA][N_v][N_u] host array).  ``keep_device_frames=True``
+    also keeps the device copy as ``frames_device``, e.g. for a display
+    pipeline; ``host_images=False`` skips the host copy (``images`` is None).
     """
 
     def __init__(self, image_config, sinogram, *, device=None, keep_device_frames=False, host_images=True):
@@ -316,10 +362,14 @@ class ImageSeq:
 
         self.file_extension = ".imgseq"
         self.image_config = image_config
-        frames = device_frames(sinogram, image_config, device=device)
-        self.frames_device = frames if keep_device_frames else None
+        self.frames_device = None
         self.images = None
+        frames = device_frames(sinogram, image_config, device=device)
+        if keep_device_frames:
+            self.frames_device = frames
         if host_images:
+            # one DMA into page-locked memory (torch's host caching allocator
+            # hands the block back for reuse once these images are released)
             host = torch.empty(frames.shape, dtype=torch.uint8, pin_memory=True)
             host.copy_(frames)
             arr = host.numpy()

@@ -3,16 +3,21 @@
     python -m vamtoolbox_b200.profile_case parallel --size 256 --angles 360 --calls 2
     python -m vamtoolbox_b200.profile_case parallel --size 512 --angles 720 --slices 1
     python -m vamtoolbox_b200.profile_case ray --size 96 --angles 120 --calls 1
+    python -m vamtoolbox_b200.profile_case formats --size 256 --angles 120 --calls 1
 
 ``parallel`` runs forward, reference-parity backprojection and the matched
 adjoint (after building its weight table) on a random N x N x N volume with
 ``angles`` equally spaced over 360 degrees; ``ray`` runs integrate and deposit
 of the curved-ray tracer through a graded-index, attenuating N^3 medium
-(physical path length, forward symplectic Euler), ``angles`` angles.  Each
+(physical path length, forward symplectic Euler), ``angles`` angles;
+``formats`` turns an N x angles x N float64 sinogram into 1920 x 1080 uint8
+projector frames (99.5th-percentile normalisation: select, then the frame
+kernel) and rebins it for a 300 px fan-beam vial.  Each
 kernel runs ``calls`` times; inputs are seeded; nothing is timed or printed
 but a one-line summary, so a profiler's launch filter (kernel name regex plus
 launch count) selects exactly the launches it wants.  The 256^3 x 360
-parallel case holds about 0.9 GB on the device, the 96^3 ray case about 0.1 GB.
+parallel case holds about 0.9 GB on the device, the 96^3 ray case about 0.1 GB,
+the 256 x 120 x 256 formats case about 0.4 GB.
 """
 from __future__ import annotations
 
@@ -96,9 +101,24 @@ def summarize_launches(path):
     return "\n".join(out)
 
 
+def run_formats(n, na, calls):
+    from . import geometry
+    from . import imagesequence as ims
+
+    g = torch.Generator(device="cuda").manual_seed(0)
+    sino = torch.rand((n, na, n), device="cuda", dtype=torch.float64, generator=g) ** 3 * 40.0
+    cfg = ims.ImageConfig((1920, 1080), normalization_percentile=99.5, invert_u=True)
+    pg = geometry.ProjectionGeometry(np.linspace(0, 360, na, endpoint=False))
+    for _ in range(calls):
+        frames = ims.device_frames(sino, cfg)
+        geometry.rebinFanBeam(geometry.Sinogram(sino, pg), 300, (1920, 1080), 1.5, 1.7)
+    torch.cuda.synchronize()
+    return f"formats {n} x {na} x {n} -> {tuple(frames.shape)} frames, fan-beam rebin to 300 px"
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
-    ap.add_argument("case", choices=["parallel", "ray", "summarize"])
+    ap.add_argument("case", choices=["parallel", "ray", "formats", "summarize"])
     ap.add_argument("csv", nargs="?", help="summarize: the ncu --csv launch list")
     ap.add_argument("--size", type=int, default=None)
     ap.add_argument("--angles", type=int, default=None)
@@ -113,6 +133,8 @@ def main(argv=None):
     if a.case == "parallel":
         tuning = dict((k, int(v)) for k, v in (kv.split("=") for kv in a.tuning.split(",") if kv))
         print(run_parallel(a.size or 256, a.angles or 360, a.calls, tuning, a.slices))
+    elif a.case == "formats":
+        print(run_formats(a.size or 256, a.angles or 120, a.calls))
     else:
         print(run_ray(a.size or 96, a.angles or 120, a.calls))
 
