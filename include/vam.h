@@ -356,6 +356,45 @@ int vam_append(const float* src_dev, int32_t n, float* arr_dev, int32_t* counter
                vam_stream_t stream);
 
 /* ======================================================================= */
+/* Vector-geometry parallel beam: the model of the reference's CUDA path    */
+/* (ASTRA parallel3d / parallel3d_vec, incl. inclined / laminography rays)  */
+/* ======================================================================= */
+
+typedef struct vam_vec_plan vam_vec_plan;
+
+typedef struct {
+    int32_t n_y, n_x, n_z;      /* target array [nY][nX][nZ] = ASTRA (col x, row y, slice z) */
+    int32_t n_angles;
+    int32_t det_cols, det_rows; /* detector nU x nV; the sinogram is [nU][nA][nV] */
+    const double* vectors;      /* host, n_angles x 12: ray direction, detector centre, u (pixel (0,0)->(0,1)),
+                                   v (pixel (0,0)->(1,0)), as the rows genVectorsAstra builds
+                                   (vamtoolbox/projector/genVectorsAstra.py:4-53) */
+    int32_t device;
+} vam_vec_geom;
+
+/* Per-angle affine sampling tables for the model of
+ * Projector3DParallelCUDAAstra (vamtoolbox/projector/Projector3DParallelCUDA.py:13-72):
+ * voxel (i, j, k) centred at (i + 0.5 - nY/2, j + 0.5 - nX/2, k + 0.5 - nZ/2),
+ * detector pixel (c, r) at d + (c - nU/2 + 0.5) u + (r - nV/2 + 0.5) v.
+ * VAM_ERR_ARG for a ray parallel to the detector plane. */
+int vam_vec_plan_create(const vam_vec_geom* geom, vam_vec_plan** out);
+int vam_vec_plan_destroy(vam_vec_plan* plan);
+/* Whether forward / backward use the slice-exact kernels (no inclination). */
+int vam_vec_plan_info(const vam_vec_plan* plan, int32_t* flat_forward, int32_t* flat_backward);
+
+/* Line integrals, Joseph-type: every ray sampled on each voxel plane across
+ * its dominant axis, bilinear in the plane (zero outside), times
+ * |ray| / |ray_dominant|; replaces astra.create_sino3d_gpu
+ * (Projector3DParallelCUDA.py:40-54).  vol [nY][nX][nZ] -> sino [nU][nA][nV]. */
+int vam_vec_forward(vam_vec_plan* plan, const float* vol_dev, float* sino_dev, vam_stream_t stream);
+
+/* Voxel-driven backprojection: each voxel centre carried along the ray onto
+ * the detector, the sinogram sampled there bilinearly (zero outside), summed
+ * over angles; replaces astra.creators.create_backprojection3d_gpu
+ * (Projector3DParallelCUDA.py:56-72). */
+int vam_vec_backward(vam_vec_plan* plan, const float* sino_dev, float* vol_dev, vam_stream_t stream);
+
+/* ======================================================================= */
 /* Output formats: projector frames (vamtoolbox/imagesequence.py) and      */
 /* fan-beam rebinning (vamtoolbox/geometry.py:736-944)                     */
 /* ======================================================================= */

@@ -374,8 +374,28 @@ def format_cases(vam):
     np.savez_compressed(OUT / "formats.npz", **out)
 
 
+VEC_CASES = [(np.linspace(0, 360, 12, endpoint=False), 0.0), (np.linspace(0, 360, 36, endpoint=False), 15.0),
+             (np.array([0.0, 33.3, 90.0, 181.0, 270.5]), -30.0), (np.linspace(0, 180, 8), 50.0)]
+
+
+def vecgeom_cases(vam):
+    """The reference's own genVectorsAstra rows (vamtoolbox/projector/genVectorsAstra.py:4-53): the
+    inclined (laminography) geometry its CUDA projector hands to ASTRA."""
+    import importlib
+
+    gv = importlib.import_module("vamtoolbox.projector.genVectorsAstra").genVectorsAstra
+    out = {}
+    for i, (ang, inc) in enumerate(VEC_CASES):
+        out[f"v{i}_angles"] = ang
+        out[f"v{i}_incline"] = np.array(inc)
+        out[f"v{i}_vectors"] = gv(ang, inc)
+    out["cone_vectors"] = gv(np.array([0.0, 45.0, 100.0]), 10.0, cone_angle=5.0, distance_origin_source=250.0)
+    np.savez_compressed(OUT / "vecgeom.npz", **out)
+
+
 GROUPS = {"parallel": parallel_cases, "ray": ray_cases, "algebraic": algebraic_cases,
-          "ray_autograd": ray_autograd_cases, "optim": optimizer_cases, "formats": format_cases}
+          "ray_autograd": ray_autograd_cases, "optim": optimizer_cases, "formats": format_cases,
+          "vecgeom": vecgeom_cases}
 
 
 def main():

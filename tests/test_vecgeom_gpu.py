@@ -1,0 +1,96 @@
+"""Vector-geometry (ASTRA-model) projector on the GPU (vam_vec_*) against the float64
+oracle, and its place behind projectorconstructor / optimize for inclined rays."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import vecgeom as V
+from tests.conftest import relL2
+from tests.test_vecgeom_golden import _smooth_phantom
+from vamtoolbox_b200 import geometry, optimize, projectorconstructor
+from vamtoolbox_b200.projector.Projector3DParallelCUDA import (Projector3DParallelCUDAAstra, VecPlan,
+                                                               genVectorsAstra, parallel3d_vectors)
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("incline,shape,n_ang", [(0.0, (40, 40, 12), 18), (15.0, (40, 40, 12), 18),
+                                                  (-30.0, (32, 32, 20), 12), (55.0, (24, 24, 24), 10)])
+def test_forward_backward_match_oracle(incline, shape, n_ang):
+    rng = np.random.default_rng(4)
+    vol = rng.random(shape)
+    ang = np.linspace(0, 360, n_ang, endpoint=False) + 3.0
+    vec = parallel3d_vectors(np.deg2rad(ang)) if incline == 0 else genVectorsAstra(ang, incline)
+    n_u, n_v = shape[1], shape[2]
+    plan = VecPlan(*shape, vec, n_u, n_v, "cuda")
+    assert plan.info()["flat_forward"] == (incline == 0) and plan.info()["flat_backward"] == (incline == 0)
+    f = plan.forward(torch.as_tensor(vol, dtype=torch.float32, device="cuda")).cpu().numpy()
+    assert relL2(f, V.forward(vol, vec, n_u, n_v)) < 2e-5
+    sino = rng.random((n_u, n_ang, n_v))
+    b = plan.backward(torch.as_tensor(sino, dtype=torch.float32, device="cuda")).cpu().numpy()
+    assert relL2(b, V.backward(sino, vec, shape)) < 2e-5
+
+
+def test_dominant_z_axis_geometry():
+    """Rays steeper than 45 degrees out of the plane step across z slices."""
+    vec = genVectorsAstra(np.array([45.0, 135.0]), 70.0)
+    assert (np.abs(vec[:, 2]) > np.abs(vec[:, :2]).max(1)).all()
+    shape = (20, 20, 16)
+    vol = _smooth_phantom(20, 16)
+    plan = VecPlan(*shape, vec, 20, 16, "cuda")
+    f = plan.forward(torch.as_tensor(vol, dtype=torch.float32, device="cuda")).cpu().numpy()
+    assert relL2(f, V.forward(vol, vec, 20, 16)) < 2e-5
+
+
+def _geo(n, nz, angles, **kw):
+    tg = geometry.TargetGeometry(target=_smooth_phantom(n, nz) > 0.8)
+    pg = geometry.ProjectionGeometry(angles, "parallel", CUDA=True, **kw)
+    return tg, pg
+
+
+def test_inclined_geometry_dispatches_to_vector_projector():
+    tg, pg = _geo(32, 8, np.linspace(0, 360, 20, endpoint=False), inclination_angle=20.0)
+    A = projectorconstructor.projectorconstructor(tg, pg)
+    assert isinstance(A, Projector3DParallelCUDAAstra)
+    x = np.array(tg.array, dtype=np.float64)
+    b = A.forward(x)
+    assert b.shape == (32, 20, 8) and b.dtype == np.float64
+    ref = V.forward(x, genVectorsAstra(pg.angles, 20.0), 32, 8)
+    assert relL2(b, ref) < 2e-5
+    back = A.backward(b.copy())
+    circle = np.asarray(__import__("vamtoolbox_b200.util.data", fromlist=["x"]).circle_inside_mask(32, 32))
+    assert not back[~circle].any()                        # clipped to the inscribed circle
+    tg2, pg2 = _geo(32, 8, np.linspace(0, 360, 20, endpoint=False))
+    assert not isinstance(projectorconstructor.projectorconstructor(tg2, pg2), Projector3DParallelCUDAAstra)
+    tg3, pg3 = _geo(32, 8, np.linspace(0, 360, 20, endpoint=False), parallel_model="astra")
+    assert isinstance(projectorconstructor.projectorconstructor(tg3, pg3), Projector3DParallelCUDAAstra)
+
+
+def test_forward_clips_input_in_place_and_backward_zeroes_zero_dose():
+    tg, pg = _geo(24, 4, np.linspace(0, 180, 6, endpoint=False), inclination_angle=10.0)
+    A = Projector3DParallelCUDAAstra(tg, pg)
+    x = np.ones((24, 24, 4))
+    A.forward(x)
+    assert x[0, 0, 0] == 0 and x[12, 12, 0] == 1          # the reference clips its argument in place
+    zd = np.zeros((24, 6, 4), dtype=bool)
+    zd[3, 2, 1] = True
+    pg.zero_dose_sino = zd
+    b = np.ones((24, 6, 4))
+    A.backward(b)
+    assert b[3, 2, 1] == 0 and b[4, 2, 1] == 1
+
+
+def test_device_tensors_stay_on_device():
+    tg, pg = _geo(24, 4, np.linspace(0, 180, 6, endpoint=False), inclination_angle=10.0)
+    A = Projector3DParallelCUDAAstra(tg, pg)
+    x = torch.rand((24, 24, 4), device="cuda")
+    b = A.forward(x)
+    assert b.is_cuda and tuple(b.shape) == (24, 6, 4)
+    assert A.backward(b).is_cuda
+
+
+@pytest.mark.parametrize("method", ["BCLP", "CAL"])
+def test_optimize_with_inclined_rays(method):
+    tg, pg = _geo(32, 8, np.linspace(0, 360, 24, endpoint=False), inclination_angle=12.0)
+    sino, recon, err = optimize.optimize(tg, pg, optimize.Options(method=method, n_iter=3, verbose=False))
+    assert np.isfinite(np.asarray(sino.array)).all() and np.asarray(sino.array).shape == (32, 24, 8)

@@ -77,6 +77,11 @@ class BclpParams(ctypes.Structure):
 
 
 # name -> (argtypes, restype)
+class VecGeom(ctypes.Structure):
+    _fields_ = [("n_y", _c_i32), ("n_x", _c_i32), ("n_z", _c_i32), ("n_angles", _c_i32),
+                ("det_cols", _c_i32), ("det_rows", _c_i32), ("vectors", ctypes.POINTER(_c_d)), ("device", _c_i32)]
+
+
 class FrameParams(ctypes.Structure):
     _fields_ = [("n_u", _c_i32), ("n_v", _c_i32), ("src_col_dev", _vp), ("src_row_dev", _vp),
                 ("bit_depth", _c_i32), ("has_norm", _c_i32), ("norm_value", _c_d), ("norm_dtype", _c_i32),
@@ -129,6 +134,11 @@ _SIGS = {
     "vam_scale_by_device": ([_vp, _vp, _c_i64, _c_int, _c_f, _vp], _c_int),
     "vam_osmo_model_update": ([_vp, _vp, _vp, _vp, _c_i64, _c_int, _c_f, _vp], _c_int),
     "vam_append": ([_vp, _c_i32, _vp, _vp, _c_i32, _vp], _c_int),
+    "vam_vec_plan_create": ([ctypes.POINTER(VecGeom), ctypes.POINTER(_vp)], _c_int),
+    "vam_vec_plan_destroy": ([_vp], _c_int),
+    "vam_vec_plan_info": ([_vp, ctypes.POINTER(_c_i32), ctypes.POINTER(_c_i32)], _c_int),
+    "vam_vec_forward": ([_vp, _vp, _vp, _vp], _c_int),
+    "vam_vec_backward": ([_vp, _vp, _vp, _vp], _c_int),
     "vam_sino_rotate": ([_vp, _c_int, _c_i32, _c_i32, _c_i32, _c_i32, _c_i32, ctypes.POINTER(_c_d), _vp, _c_i32,
                          _c_i32, _vp], _c_int),
     "vam_sino_resize": ([_vp, _c_int, _c_i32, _c_i32, _c_i32, _c_i32, _c_i32, _vp, _c_i32, _c_i32, _vp], _c_int),

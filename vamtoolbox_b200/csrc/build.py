@@ -21,7 +21,7 @@ PKG = CSRC.parent
 ROOT = PKG.parent
 OUT = PKG / "libvamcore.so"
 OBJ = PKG / "_build"
-SOURCES = ["capi.cu", "parallel.cu", "optim.cu", "raytrace.cu", "output.cu"]
+SOURCES = ["capi.cu", "parallel.cu", "optim.cu", "raytrace.cu", "output.cu", "vecgeom.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

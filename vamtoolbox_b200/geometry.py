@@ -38,6 +38,9 @@ class ProjectionGeometry:
         for k in _PROJ_KWARGS:
             setattr(self, k, kwargs.get(k, None))
         self.loading_path_for_matrix = kwargs.get("loading_path_for_matrix", True)
+        # "python" (default): the discretisation of the reference's Python projectors;
+        # "astra": the vector-geometry model of its CUDA path (always used for inclined rays)
+        self.parallel_model = kwargs.get("parallel_model", "python")
         self.absorption_mask = None
 
     def calcZeroDoseSinogram(self, A, target_geo):

@@ -183,6 +183,10 @@ class BCLPNorm:
         if plan is not None and hasattr(plan, "deposit"):
             return (lambda g, out: plan.deposit(g, out), lambda x, out: plan.integrate(x, out),
                     plan.grid_shape, (plan.num_rays,), P.device)
+        if plan is not None and hasattr(P, "backward_t") and hasattr(P, "forward_t"):
+            # vector-geometry (ASTRA-model) projector: its wrappers carry the circle clip and mask
+            return (lambda g, out: P.backward_t(g, out), lambda x, out: P.forward_t(x, out),
+                    plan.shape_vol, plan.shape_sino, P.device)
         raise TypeError("the device engine needs a vamtoolbox_b200 projector")
 
     def _table_ok(self):

@@ -256,7 +256,7 @@ class Projector3DParallel:
         return self.adjoint_t(b).double().cpu().numpy()
 
 
-# The reference's names for the same dispatch slots (projectorconstructor.py:74-160).
+# The reference's names for the same dispatch slots (projectorconstructor.py:74-160).  The
+# ASTRA-model CUDA class (vector geometry, inclined rays) is projector/Projector3DParallelCUDA.py.
 Projector3DParallelPython = Projector3DParallel
 Projector3DParallelAstra = Projector3DParallel
-Projector3DParallelCUDAAstra = Projector3DParallel

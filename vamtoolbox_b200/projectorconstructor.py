@@ -28,6 +28,14 @@ class CALopticalparams:
         raise NotImplementedError
 
 
+def _astra_model(proj_geo):
+    """Inclined rays (laminography) exist only in the reference's ASTRA path
+    (Projector3DParallelCUDA.py:27-38), so they select the vector-geometry
+    projector; ``parallel_model="astra"`` selects it for vertical rays too."""
+    incl = getattr(proj_geo, "inclination_angle", None)
+    return (incl is not None and incl != 0) or getattr(proj_geo, "parallel_model", None) == "astra"
+
+
 def projectorconstructor(target_geo, proj_geo, optical_params=None, **projector_kwargs):
     """Build the projector for ``target_geo`` / ``proj_geo``.
 
@@ -54,6 +62,12 @@ def projectorconstructor(target_geo, proj_geo, optical_params=None, **projector_
             from .projector.Projector2DParallel import Projector2DParallel
 
             A = Projector2DParallel(target_geo, proj_geo, **projector_kwargs)
+        elif _astra_model(proj_geo):
+            from .projector.Projector3DParallelCUDA import Projector3DParallelCUDAAstra
+
+            if getattr(proj_geo, "attenuation_field", None) is not None:
+                raise NotImplementedError("3D attenuation CUDA projector not yet implemented.")
+            A = Projector3DParallelCUDAAstra(target_geo, proj_geo, **projector_kwargs)
         else:
             from .projector.Projector3DParallel import Projector3DParallel
 
