@@ -62,6 +62,7 @@ def parse():
     ap.add_argument("--no-configs", action="store_true", help="skip the 2-D CAL / OSMO / grayscale BCLP legs")
     ap.add_argument("--no-algebraic", action="store_true", help="skip the propagation-matrix / SpMV leg")
     ap.add_argument("--no-formats", action="store_true", help="skip the projector-frame / fan-beam rebin leg")
+    ap.add_argument("--no-vec", action="store_true", help="skip the vector-geometry (inclined rays) projector leg")
     ap.add_argument("--ray-size", type=int, default=128)
     return ap.parse_args()
 
@@ -691,6 +692,61 @@ def run_formats(dev, n=256, n_angles=360, screen=(1920, 1080), reps=5, cpu=True)
     return out
 
 
+def run_vec_geometry(dev, n=256, n_angles=360, incline=15.0, reps=5, cpu=True):
+    """Vector-geometry (ASTRA-model) parallel projector, the reference's CUDA path: forward and
+    backprojection of an n^3 volume at n_angles angles with vertical rays (slice-exact kernels) and
+    rays inclined by `incline` degrees (laminography); the oracle's float64 numpy model beside it on
+    a sample of angles."""
+    import torch
+
+    from vamtoolbox_b200.projector.Projector3DParallelCUDA import VecPlan, genVectorsAstra, parallel3d_vectors
+
+    ang = np.linspace(0, 360, n_angles, endpoint=False)
+    st = torch.cuda.current_stream(dev)
+    g = torch.Generator(device=dev).manual_seed(0)
+    x = torch.rand((n, n, n), device=dev, generator=g)
+    b = torch.rand((n, n_angles, n), device=dev, generator=g)
+
+    def tim(fn):
+        fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / reps
+
+    out = {"workload": f"{n}^3 volume, {n_angles} angles, detector {n} x {n}"}
+    for name, vec in (("vertical", parallel3d_vectors(np.deg2rad(ang))), (f"inclined_{incline:g}deg",
+                                                                       genVectorsAstra(ang, incline))):
+        p = VecPlan(n, n, n, vec, n, n, dev)
+        ob, ox = torch.empty_like(b), torch.empty_like(x)
+        t_f = tim(lambda: p.forward(x, ob))
+        t_b = tim(lambda: p.backward(b, ox))
+        taps = 2 if p.info()["flat_forward"] else 4
+        out[name] = {"forward_ms": round(t_f, 4), "backward_ms": round(t_b, 4),
+                     "fwd_bwd_per_s": round(1000.0 / (t_f + t_b), 2),
+                     "forward_taps_GBs": round(4.0 * taps * n * n_angles * n * n / (t_f * 1e-3) / 1e9, 1),
+                     "hbm_bytes_per_call": 4 * (n ** 3 + n * n_angles * n)}
+        del p
+    if cpu:
+        from oracle import vecgeom as OV
+
+        k = 2
+        vol = x.cpu().double().numpy()
+        vec = genVectorsAstra(ang[:k], incline)
+        t0 = time.perf_counter()
+        OV.forward(vol, vec, n, n)
+        t_cpu = (time.perf_counter() - t0) * n_angles / k
+        out["cpu_baseline"] = {"value": round(1.0 / t_cpu, 5), "unit": "forward projections/s", "cores": 1,
+                               "kind": "port", "sample": f"{k} of {n_angles} inclined angles through the oracle's "
+                                                         "float64 numpy model, scaled to all angles",
+                               "forward_s": round(t_cpu, 2)}
+    return out
+
+
 def run_ours(args):
     import torch
 
@@ -894,6 +950,13 @@ def run_ours(args):
         except Exception as exc:  # report, never fail the headline number on it
             fmt = {"error": f"{type(exc).__name__}: {exc}"}
 
+    vecg = None
+    if ws_ == 1 and not args.no_vec:
+        try:
+            vecg = run_vec_geometry(dev, cpu=not args.no_cpu)
+        except Exception as exc:  # report, never fail the headline number on it
+            vecg = {"error": f"{type(exc).__name__}: {exc}"}
+
     ray = None
     if ws_ == 1 and not args.no_ray:
         try:
@@ -933,6 +996,7 @@ def run_ours(args):
             "ray_tracer": ray,
             "algebraic": algebraic,
             "output_formats": fmt,
+            "vector_geometry": vecg,
             "configs": configs,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm_peak, "unit": "GB/s",
                          "frac": round(achieved / hbm_peak, 5), "traffic": traffic, "peak_source": peak_src,

@@ -24,6 +24,7 @@
 
 #include <math.h>
 
+#include <algorithm>
 #include <vector>
 
 using vam::clear_error;
@@ -56,38 +57,40 @@ __device__ __forceinline__ float affine(const float (&q)[4], float a, float b, f
     return fmaf(q[3], c, fmaf(q[2], b, fmaf(q[1], a, q[0])));
 }
 
-// Bilinear tap helper on an [n0][n1] plane with strides s0, s1 (elements),
-// zero outside.  Returns the weighted sum.
-__device__ __forceinline__ float bilerp(const float* __restrict__ base, float f0, float f1, int n0, int n1,
-                                        size_t s0, size_t s1) {
+// Bilinear sample of an [n0][n1] plane (element strides s0, s1, 32-bit
+// offsets) at continuous indices (f0, f1), zero outside: interpolate along
+// axis 1 in the two axis-0 rows, then across them.
+__device__ __forceinline__ float bilerp(const float* __restrict__ base, float f0, float f1, int n0, int n1, int s0,
+                                        int s1) {
     const float g0 = floorf(f0), g1 = floorf(f1);
     const int i0 = (int)g0, i1 = (int)g1;
     const float t0 = f0 - g0, t1 = f1 - g1;
-    const bool a0 = i0 >= 0 && i0 < n0, b0 = i0 + 1 >= 0 && i0 + 1 < n0;
-    const bool a1 = i1 >= 0 && i1 < n1, b1 = i1 + 1 >= 0 && i1 + 1 < n1;
-    const float* p = base + (ptrdiff_t)i0 * (ptrdiff_t)s0 + (ptrdiff_t)i1 * (ptrdiff_t)s1;
-    const float x00 = (a0 && a1) ? __ldg(p) : 0.f;
-    const float x01 = (a0 && b1) ? __ldg(p + s1) : 0.f;
-    const float x10 = (b0 && a1) ? __ldg(p + s0) : 0.f;
-    const float x11 = (b0 && b1) ? __ldg(p + s0 + s1) : 0.f;
-    return (1.f - t0) * ((1.f - t1) * x00 + t1 * x01) + t0 * ((1.f - t1) * x10 + t1 * x11);
+    const bool a0 = (unsigned)i0 < (unsigned)n0, b0 = (unsigned)(i0 + 1) < (unsigned)n0;
+    const bool a1 = (unsigned)i1 < (unsigned)n1, b1 = (unsigned)(i1 + 1) < (unsigned)n1;
+    const int o = i0 * s0 + i1 * s1;
+    const float x00 = (a0 && a1) ? __ldg(base + o) : 0.f;
+    const float x01 = (a0 && b1) ? __ldg(base + o + s1) : 0.f;
+    const float x10 = (b0 && a1) ? __ldg(base + o + s0) : 0.f;
+    const float x11 = (b0 && b1) ? __ldg(base + o + s0 + s1) : 0.f;
+    const float r0 = fmaf(t1, x01 - x00, x00), r1 = fmaf(t1, x11 - x10, x10);
+    return fmaf(t0, r1 - r0, r0);
 }
 
-// Linear interpolation along one axis (slice-exact geometries: the other
-// in-plane coordinate is an integer voxel index on every sample).
-__device__ __forceinline__ float lerp1(const float* __restrict__ base, float f, int n, size_t s) {
+// Linear sample along one axis (slice-exact geometries: the other in-plane
+// coordinate is an integer voxel index on every sample).
+__device__ __forceinline__ float lerp1(const float* __restrict__ base, float f, int n, int s) {
     const float g = floorf(f);
     const int i0 = (int)g;
     const float t = f - g;
-    const float x0 = (i0 >= 0 && i0 < n) ? __ldg(base + (ptrdiff_t)i0 * (ptrdiff_t)s) : 0.f;
-    const float x1 = (i0 + 1 >= 0 && i0 + 1 < n) ? __ldg(base + (ptrdiff_t)(i0 + 1) * (ptrdiff_t)s) : 0.f;
-    return (1.f - t) * x0 + t * x1;
+    const float x0 = (unsigned)i0 < (unsigned)n ? __ldg(base + i0 * s) : 0.f;
+    const float x1 = (unsigned)(i0 + 1) < (unsigned)n ? __ldg(base + (i0 + 1) * s) : 0.f;
+    return fmaf(t, x1 - x0, x0);
 }
 
 // Forward: one thread per detector pixel (c, a, r), r fastest.  FLAT: every
 // ray stays in the slice k = r (no inclination), the in-plane z coordinate
 // is exact and only the horizontal axis is interpolated.
-template <bool FLAT>
+template <bool FLAT, bool HU>
 __global__ void __launch_bounds__(kThreads) k_vec_forward(const float* __restrict__ vol, float* __restrict__ sino,
                                                           const FwdAngle* __restrict__ ang, int nY, int nX, int nZ,
                                                           int nU, int nA, int nV) {
@@ -96,43 +99,110 @@ __global__ void __launch_bounds__(kThreads) k_vec_forward(const float* __restric
     const int c = blockIdx.z;
     if (r >= nV) return;
     const FwdAngle g = ang[a];
-    const size_t sI = (size_t)nX * nZ, sJ = (size_t)nZ, sK = 1;
+    const int sI = nX * nZ, sJ = nZ;
     const float fc = (float)c, fr = (float)r;
     float acc = 0.f;
-    if (g.axis == 0) {            // planes across i; in-plane (j, k)
-        const float j0 = affine(g.p0, fc, fr, 0.f), k0 = affine(g.p1, fc, fr, 0.f);
+    if (g.axis <= 1) {            // planes across i (axis 0) or j (axis 1); in-plane (other of i/j, k)
+        const int plane = g.axis == 0 ? sI : sJ, hs = g.axis == 0 ? sJ : sI, nh = g.axis == 0 ? nX : nY;
+        const int np = g.axis == 0 ? nY : nX;
+        // HU: the horizontal coordinate has no row term, so it is the same for
+        // every lane of the warp (computed from block indices and s only)
+        const float h0 = affine(g.p0, fc, HU ? 0.f : fr, 0.f), k0 = affine(g.p1, fc, fr, 0.f);
 #pragma unroll 4
-        for (int s = 0; s < nY; ++s) {
-            const float fj = fmaf(g.p0[3], (float)s, j0);
-            const float* pl = vol + (size_t)s * sI;
+        for (int s = 0; s < np; ++s) {
+            const float fh = fmaf(g.p0[3], (float)s, h0);
+            const float* pl = vol + s * plane;
             if (FLAT)
-                acc += lerp1(pl + (size_t)r * sK, fj, nX, sJ);
+                acc += lerp1(pl + r, fh, nh, hs);
             else
-                acc += bilerp(pl, fj, fmaf(g.p1[3], (float)s, k0), nX, nZ, sJ, sK);
-        }
-    } else if (g.axis == 1) {     // planes across j; in-plane (i, k)
-        const float i0 = affine(g.p0, fc, fr, 0.f), k0 = affine(g.p1, fc, fr, 0.f);
-#pragma unroll 4
-        for (int s = 0; s < nX; ++s) {
-            const float fi = fmaf(g.p0[3], (float)s, i0);
-            const float* pl = vol + (size_t)s * sJ;
-            if (FLAT)
-                acc += lerp1(pl + (size_t)r * sK, fi, nY, sI);
-            else
-                acc += bilerp(pl, fi, fmaf(g.p1[3], (float)s, k0), nY, nZ, sI, sK);
+                acc += bilerp(pl, fh, fmaf(g.p1[3], (float)s, k0), nh, nZ, hs, 1);
         }
     } else {                      // planes across k; in-plane (i, j)
         const float i0 = affine(g.p0, fc, fr, 0.f), j0 = affine(g.p1, fc, fr, 0.f);
+#pragma unroll 4
         for (int s = 0; s < nZ; ++s)
-            acc += bilerp(vol + (size_t)s * sK, fmaf(g.p0[3], (float)s, i0), fmaf(g.p1[3], (float)s, j0), nY, nX,
-                          sI, sJ);
+            acc += bilerp(vol + s, fmaf(g.p0[3], (float)s, i0), fmaf(g.p1[3], (float)s, j0), nY, nX, sI, sJ);
     }
-    sino[((size_t)c * nA + a) * nV + r] = acc * g.scale;
+    sino[(c * nA + a) * nV + r] = acc * g.scale;
+}
+
+__device__ __forceinline__ float4 ld4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+__device__ __forceinline__ void mix4(float4& acc, float4 x0, float4 x1, float t) {
+    acc.x += fmaf(t, x1.x - x0.x, x0.x);
+    acc.y += fmaf(t, x1.y - x0.y, x0.y);
+    acc.z += fmaf(t, x1.z - x0.z, x0.z);
+    acc.w += fmaf(t, x1.w - x0.w, x0.w);
+}
+
+// Slice-exact forward with four detector rows (= four slices) per lane: the
+// horizontal coordinate does not depend on the row, so one weight and two
+// 16-byte loads serve four samples.  nZ % 4 == 0, 16-byte aligned arrays.
+// Block = rows_per_block detector rows (c, a) x lanes_per_row lanes.
+__global__ void __launch_bounds__(kThreads) k_vec_forward_flat4(const float* __restrict__ vol,
+                                                                float* __restrict__ sino,
+                                                                const FwdAngle* __restrict__ ang, int nY, int nX,
+                                                                int nZ, int nU, int nA, int nV, int lanes_per_row) {
+    const int rows_per_block = blockDim.x / lanes_per_row;
+    const int row = blockIdx.x * rows_per_block + threadIdx.x / lanes_per_row;   // c * nA + a
+    const int r = (threadIdx.x % lanes_per_row) * 4;
+    if (row >= nU * nA || r >= nV) return;
+    const int c = row / nA, a = row - c * nA;
+    const FwdAngle g = ang[a];
+    const int sI = nX * nZ, sJ = nZ;
+    const int plane = g.axis == 0 ? sI : sJ, hs = g.axis == 0 ? sJ : sI, nh = g.axis == 0 ? nX : nY;
+    const int np = g.axis == 0 ? nY : nX;
+    const float h0 = affine(g.p0, (float)c, 0.f, 0.f);
+    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 acc = zero;
+#pragma unroll 4
+    for (int s = 0; s < np; ++s) {
+        const float fh = fmaf(g.p0[3], (float)s, h0);
+        const float gh = floorf(fh);
+        const int i0 = (int)gh;
+        const float t = fh - gh;
+        const float* pl = vol + s * plane + r;
+        const float4 x0 = (unsigned)i0 < (unsigned)nh ? ld4(pl + i0 * hs) : zero;
+        const float4 x1 = (unsigned)(i0 + 1) < (unsigned)nh ? ld4(pl + (i0 + 1) * hs) : zero;
+        mix4(acc, x0, x1, t);
+    }
+    const float sc = g.scale;
+    *reinterpret_cast<float4*>(sino + (c * nA + a) * nV + r) =
+        make_float4(acc.x * sc, acc.y * sc, acc.z * sc, acc.w * sc);
+}
+
+// Slice-exact backward with four slices per lane (the detector column does
+// not depend on k).
+__global__ void __launch_bounds__(kThreads) k_vec_backward_flat4(const float* __restrict__ sino,
+                                                                 float* __restrict__ vol,
+                                                                 const BwdAngle* __restrict__ ang, int nY, int nX,
+                                                                 int nZ, int nU, int nA, int nV, int lanes_per_row) {
+    const int rows_per_block = blockDim.x / lanes_per_row;
+    const int col = blockIdx.x * rows_per_block + threadIdx.x / lanes_per_row;   // i * nX + j
+    const int k = (threadIdx.x % lanes_per_row) * 4;
+    if (col >= nY * nX || k >= nZ) return;
+    const int i = col / nX, j = col - i * nX;
+    const float fi = (float)i, fj = (float)j;
+    const int sC = nA * nV;
+    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 acc = zero;
+#pragma unroll 4
+    for (int a = 0; a < nA; ++a) {
+        const BwdAngle g = ang[a];
+        const float fu = affine(g.u, fi, fj, 0.f);
+        const float gu = floorf(fu);
+        const int c0 = (int)gu;
+        const float t = fu - gu;
+        const float* pl = sino + a * nV + k;
+        const float4 x0 = (unsigned)c0 < (unsigned)nU ? ld4(pl + c0 * sC) : zero;
+        const float4 x1 = (unsigned)(c0 + 1) < (unsigned)nU ? ld4(pl + (c0 + 1) * sC) : zero;
+        mix4(acc, x0, x1, t);
+    }
+    *reinterpret_cast<float4*>(vol + (i * nX + j) * nZ + k) = acc;
 }
 
 // Backward: one thread per voxel (i, j, k), k fastest; angles looped.
 // FLAT: the detector row of voxel slice k is exactly k.
-template <bool FLAT>
+template <bool FLAT, bool HU>
 __global__ void __launch_bounds__(kThreads) k_vec_backward(const float* __restrict__ sino, float* __restrict__ vol,
                                                            const BwdAngle* __restrict__ ang, int nY, int nX, int nZ,
                                                            int nU, int nA, int nV) {
@@ -141,19 +211,19 @@ __global__ void __launch_bounds__(kThreads) k_vec_backward(const float* __restri
     const int i = blockIdx.z;
     if (k >= nZ) return;
     const float fi = (float)i, fj = (float)j, fk = (float)k;
-    const size_t sC = (size_t)nA * nV, sA = (size_t)nV;
+    const int sC = nA * nV;
     float acc = 0.f;
 #pragma unroll 4
     for (int a = 0; a < nA; ++a) {
         const BwdAngle g = ang[a];
-        const float fu = affine(g.u, fi, fj, fk);
-        const float* pl = sino + (size_t)a * sA;
+        const float fu = affine(g.u, fi, fj, HU ? 0.f : fk);   // HU: no k term, warp-uniform
+        const float* pl = sino + a * nV;
         if (FLAT)
             acc += lerp1(pl + k, fu, nU, sC);
         else
             acc += bilerp(pl, fu, affine(g.v, fi, fj, fk), nU, nV, sC, 1);
     }
-    vol[((size_t)i * nX + j) * nZ + k] = acc;
+    vol[(i * nX + j) * nZ + k] = acc;
 }
 
 }  // namespace
@@ -161,11 +231,20 @@ __global__ void __launch_bounds__(kThreads) k_vec_backward(const float* __restri
 struct vam_vec_plan {
     int nY, nX, nZ, nU, nA, nV, device;
     bool flat_fwd, flat_bwd;
+    bool hu_fwd, hu_bwd;     // horizontal coordinate independent of the detector row / voxel z
     FwdAngle* d_fwd;
     BwdAngle* d_bwd;
 };
 
 namespace {
+
+// Lanes per detector row (or voxel column) for the four-wide kernels: the
+// smallest power of two >= the float4 groups, at least one warp.
+int lanes_for(int groups) {
+    int l = 32;
+    while (l < groups) l <<= 1;
+    return l;
+}
 
 bool solve3(const double m[3][3], double inv[3][3]) {
     const double det = m[0][0] * (m[1][1] * m[2][2] - m[1][2] * m[2][1]) -
@@ -195,10 +274,17 @@ extern "C" int vam_vec_plan_create(const vam_vec_geom* geom, vam_vec_plan** out)
                 "vam_vec_plan_create: empty volume, detector or angle set");
     VAM_REQUIRE(nA <= 65535 && nU <= 65535 && nY <= 65535 && nX <= 65535, VAM_ERR_SHAPE,
                 "vam_vec_plan_create: dimension above 65535");
+    VAM_REQUIRE((int64_t)nY * nX * nZ < (1ll << 31) && (int64_t)nU * nA * nV < (1ll << 31), VAM_ERR_SHAPE,
+                "vam_vec_plan_create: volume or sinogram of 2^31 elements or more");
     const double cx = 0.5 - nY / 2.0, cy = 0.5 - nX / 2.0, cz = 0.5 - nZ / 2.0;   // voxel (0,0,0) centre
     std::vector<FwdAngle> fw(nA);
     std::vector<BwdAngle> bw(nA);
-    bool flat_f = true, flat_b = true;
+    bool flat_f = true, flat_b = true, hu_f = true, hu_b = true;
+    // coefficients whose effect over the whole index range stays below 1e-6
+    // voxel / pixel are rounding residue of an exact zero: snap them
+    auto snap = [](float& c, double extent) {
+        if (fabs((double)c) * extent < 1e-6) c = 0.f;
+    };
     for (int a = 0; a < nA; ++a) {
         const double* q = geom->vectors + 12 * a;
         for (int t = 0; t < 12; ++t)
@@ -228,7 +314,18 @@ extern "C" int vam_vec_plan_create(const vam_vec_geom* geom, vam_vec_plan** out)
             p[2] = (float)(v[b] - v[ax] * slope);
             p[3] = (float)slope;
         }
-        if (!(ax != 2 && g.p1[0] == 0.f && g.p1[1] == 0.f && g.p1[2] == 1.f && g.p1[3] == 0.f)) flat_f = false;
+        for (int w = 0; w < 2; ++w) {
+            float* p = w == 0 ? g.p0 : g.p1;
+            snap(p[0], 1.0);
+            snap(p[1], nU);
+            snap(p[2], nV);
+            snap(p[3], std::max(nY, std::max(nX, nZ)));   // per plane, over every plane
+        }
+        if (g.p0[2] != 0.f) hu_f = false;
+        // slice-exact: the z index of every sample is the detector row, and the
+        // horizontal coordinate does not depend on the row
+        if (!(ax != 2 && g.p1[0] == 0.f && g.p1[1] == 0.f && g.p1[2] == 1.f && g.p1[3] == 0.f && g.p0[2] == 0.f))
+            flat_f = false;
         // backward: solve p - d = U u + V v + t ray; column index = U + nU/2 - 0.5
         const double M[3][3] = {{u[0], v[0], ray[0]}, {u[1], v[1], ray[1]}, {u[2], v[2], ray[2]}};
         double Mi[3][3];
@@ -243,12 +340,21 @@ extern "C" int vam_vec_plan_create(const vam_vec_geom* geom, vam_vec_plan** out)
             p[2] = (float)row[1];
             p[3] = (float)row[2];
         }
-        if (!(h.v[0] == 0.f && h.v[1] == 0.f && h.v[2] == 0.f && h.v[3] == 1.f)) flat_b = false;
+        for (int w = 0; w < 2; ++w) {
+            float* p = w == 0 ? h.u : h.v;
+            snap(p[0], 1.0);
+            snap(p[1], nY);
+            snap(p[2], nX);
+            snap(p[3], nZ);
+        }
+        if (h.u[3] != 0.f) hu_b = false;
+        if (!(h.v[0] == 0.f && h.v[1] == 0.f && h.v[2] == 0.f && h.v[3] == 1.f && h.u[3] == 0.f)) flat_b = false;
     }
     if (nV != nZ) flat_f = flat_b = false;
     vam::DeviceGuard dg(geom->device);
     VAM_REQUIRE(dg.ok, VAM_ERR_CUDA, "vam_vec_plan_create: cannot select the device");
-    vam_vec_plan* p = new vam_vec_plan{nY, nX, nZ, nU, nA, nV, geom->device, flat_f, flat_b, nullptr, nullptr};
+    vam_vec_plan* p = new vam_vec_plan{nY, nX, nZ, nU, nA, nV, geom->device, flat_f, flat_b, hu_f, hu_b,
+                                       nullptr, nullptr};
     if (cudaMalloc(&p->d_fwd, sizeof(FwdAngle) * nA) != cudaSuccess ||
         cudaMalloc(&p->d_bwd, sizeof(BwdAngle) * nA) != cudaSuccess) {
         cudaFree(p->d_fwd);
@@ -288,13 +394,26 @@ extern "C" int vam_vec_forward(vam_vec_plan* p, const float* vol, float* sino, v
     clear_error();
     VAM_REQUIRE(p && vol && sino, VAM_ERR_ARG, "vam_vec_forward: null argument");
     vam::DeviceGuard dg(p->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (p->flat_fwd && p->nV % 4 == 0 && p->nV / 4 <= kThreads && ((uintptr_t)vol & 15u) == 0 &&
+        ((uintptr_t)sino & 15u) == 0) {
+        const int lanes = lanes_for(p->nV / 4);
+        const int rows = (int)((int64_t)p->nU * p->nA), per_block = kThreads / lanes;
+        k_vec_forward_flat4<<<(rows + per_block - 1) / per_block, kThreads, 0, st>>>(
+            vol, sino, p->d_fwd, p->nY, p->nX, p->nZ, p->nU, p->nA, p->nV, lanes);
+        VAM_CHECK_LAUNCH("vam_vec_forward");
+        return VAM_OK;
+    }
     dim3 grid((p->nV + kThreads - 1) / kThreads, p->nA, p->nU);
     if (p->flat_fwd)
-        k_vec_forward<true><<<grid, kThreads, 0, (cudaStream_t)stream>>>(vol, sino, p->d_fwd, p->nY, p->nX, p->nZ,
-                                                                        p->nU, p->nA, p->nV);
+        k_vec_forward<true, false><<<grid, kThreads, 0, st>>>(vol, sino, p->d_fwd, p->nY, p->nX, p->nZ, p->nU,
+                                                              p->nA, p->nV);
+    else if (p->hu_fwd)
+        k_vec_forward<false, true><<<grid, kThreads, 0, st>>>(vol, sino, p->d_fwd, p->nY, p->nX, p->nZ, p->nU,
+                                                              p->nA, p->nV);
     else
-        k_vec_forward<false><<<grid, kThreads, 0, (cudaStream_t)stream>>>(vol, sino, p->d_fwd, p->nY, p->nX, p->nZ,
-                                                                         p->nU, p->nA, p->nV);
+        k_vec_forward<false, false><<<grid, kThreads, 0, st>>>(vol, sino, p->d_fwd, p->nY, p->nX, p->nZ, p->nU,
+                                                               p->nA, p->nV);
     VAM_CHECK_LAUNCH("vam_vec_forward");
     return VAM_OK;
 }
@@ -303,13 +422,26 @@ extern "C" int vam_vec_backward(vam_vec_plan* p, const float* sino, float* vol, 
     clear_error();
     VAM_REQUIRE(p && vol && sino, VAM_ERR_ARG, "vam_vec_backward: null argument");
     vam::DeviceGuard dg(p->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (p->flat_bwd && p->nZ % 4 == 0 && p->nZ / 4 <= kThreads && ((uintptr_t)vol & 15u) == 0 &&
+        ((uintptr_t)sino & 15u) == 0) {
+        const int lanes = lanes_for(p->nZ / 4);
+        const int cols = (int)((int64_t)p->nY * p->nX), per_block = kThreads / lanes;
+        k_vec_backward_flat4<<<(cols + per_block - 1) / per_block, kThreads, 0, st>>>(
+            sino, vol, p->d_bwd, p->nY, p->nX, p->nZ, p->nU, p->nA, p->nV, lanes);
+        VAM_CHECK_LAUNCH("vam_vec_backward");
+        return VAM_OK;
+    }
     dim3 grid((p->nZ + kThreads - 1) / kThreads, p->nX, p->nY);
     if (p->flat_bwd)
-        k_vec_backward<true><<<grid, kThreads, 0, (cudaStream_t)stream>>>(sino, vol, p->d_bwd, p->nY, p->nX, p->nZ,
-                                                                         p->nU, p->nA, p->nV);
+        k_vec_backward<true, false><<<grid, kThreads, 0, st>>>(sino, vol, p->d_bwd, p->nY, p->nX, p->nZ, p->nU,
+                                                               p->nA, p->nV);
+    else if (p->hu_bwd)
+        k_vec_backward<false, true><<<grid, kThreads, 0, st>>>(sino, vol, p->d_bwd, p->nY, p->nX, p->nZ, p->nU,
+                                                               p->nA, p->nV);
     else
-        k_vec_backward<false><<<grid, kThreads, 0, (cudaStream_t)stream>>>(sino, vol, p->d_bwd, p->nY, p->nX, p->nZ,
-                                                                          p->nU, p->nA, p->nV);
+        k_vec_backward<false, false><<<grid, kThreads, 0, st>>>(sino, vol, p->d_bwd, p->nY, p->nX, p->nZ, p->nU,
+                                                                p->nA, p->nV);
     VAM_CHECK_LAUNCH("vam_vec_backward");
     return VAM_OK;
 }

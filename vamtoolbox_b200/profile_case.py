@@ -4,6 +4,7 @@
     python -m vamtoolbox_b200.profile_case parallel --size 512 --angles 720 --slices 1
     python -m vamtoolbox_b200.profile_case ray --size 96 --angles 120 --calls 1
     python -m vamtoolbox_b200.profile_case formats --size 256 --angles 120 --calls 1
+    python -m vamtoolbox_b200.profile_case vec --size 128 --angles 90 --incline 15
 
 ``parallel`` runs forward, reference-parity backprojection and the matched
 adjoint (after building its weight table) on a random N x N x N volume with
@@ -12,7 +13,9 @@ of the curved-ray tracer through a graded-index, attenuating N^3 medium
 (physical path length, forward symplectic Euler), ``angles`` angles;
 ``formats`` turns an N x angles x N float64 sinogram into 1920 x 1080 uint8
 projector frames (99.5th-percentile normalisation: select, then the frame
-kernel) and rebins it for a 300 px fan-beam vial.  Each
+kernel) and rebins it for a 300 px fan-beam vial; ``vec`` runs the
+vector-geometry (ASTRA-model) forward and backprojection of an N^3 volume
+with rays inclined by ``incline`` degrees.  Each
 kernel runs ``calls`` times; inputs are seeded; nothing is timed or printed
 but a one-line summary, so a profiler's launch filter (kernel name regex plus
 launch count) selects exactly the launches it wants.  The 256^3 x 360
@@ -116,14 +119,31 @@ def run_formats(n, na, calls):
     return f"formats {n} x {na} x {n} -> {tuple(frames.shape)} frames, fan-beam rebin to 300 px"
 
 
+def run_vec(n, na, calls, incline):
+    from .projector.Projector3DParallelCUDA import VecPlan, genVectorsAstra, parallel3d_vectors
+
+    ang = np.linspace(0, 360, na, endpoint=False)
+    vec = parallel3d_vectors(np.deg2rad(ang)) if incline == 0 else genVectorsAstra(ang, incline)
+    p = VecPlan(n, n, n, vec, n, n, "cuda")
+    g = torch.Generator(device="cuda").manual_seed(0)
+    x = torch.rand((n, n, n), device="cuda", generator=g)
+    b = torch.rand((n, na, n), device="cuda", generator=g)
+    for _ in range(calls):
+        p.forward(x)
+        p.backward(b)
+    torch.cuda.synchronize()
+    return f"vec {n}^3 x {na} incline {incline}: {p.info()}"
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
-    ap.add_argument("case", choices=["parallel", "ray", "formats", "summarize"])
+    ap.add_argument("case", choices=["parallel", "ray", "formats", "vec", "summarize"])
     ap.add_argument("csv", nargs="?", help="summarize: the ncu --csv launch list")
     ap.add_argument("--size", type=int, default=None)
     ap.add_argument("--angles", type=int, default=None)
     ap.add_argument("--calls", type=int, default=1)
     ap.add_argument("--slices", type=int, default=None, help="parallel case: nZ (default: size; 1 = a 2-D slice)")
+    ap.add_argument("--incline", type=float, default=15.0, help="vec case: ray inclination in degrees")
     ap.add_argument("--tuning", default="", help="comma list key=value of launch shapes (parallel case)")
     a = ap.parse_args(argv)
     if a.case == "summarize":
@@ -133,6 +153,8 @@ def main(argv=None):
     if a.case == "parallel":
         tuning = dict((k, int(v)) for k, v in (kv.split("=") for kv in a.tuning.split(",") if kv))
         print(run_parallel(a.size or 256, a.angles or 360, a.calls, tuning, a.slices))
+    elif a.case == "vec":
+        print(run_vec(a.size or 128, a.angles or 90, a.calls, a.incline))
     elif a.case == "formats":
         print(run_formats(a.size or 256, a.angles or 120, a.calls))
     else:
