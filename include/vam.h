@@ -394,6 +394,21 @@ int vam_vec_forward(vam_vec_plan* plan, const float* vol_dev, float* sino_dev, v
  * (Projector3DParallelCUDA.py:56-72). */
 int vam_vec_backward(vam_vec_plan* plan, const float* sino_dev, float* vol_dev, vam_stream_t stream);
 
+/* 2-D "line" model of the reference's Projector2DParallelCUDAAstra
+ * (vamtoolbox/projector/Projector2DParallelCUDA.py:7-45, ASTRA's "line"
+ * projector): the weight of a (ray, pixel) pair is the length of the ray, a
+ * zero-width line, inside the unit pixel.  ASTRA's 2-D frame: pixel (i, j) of
+ * [nY][nX] at (j - nX/2 + 1/2, nY/2 - i - 1/2), detector bin d at offset
+ * d - nT/2 + 1/2 along (cos a, sin a), rays along (sin a, -cos a).  The
+ * backward is the forward's exact transpose (astra create_backprojection with
+ * that projector).  img [nY][nX], sino [nT][nA]. */
+typedef struct vam_line2d_plan vam_line2d_plan;
+int vam_line2d_plan_create(int32_t n_y, int32_t n_x, int32_t n_angles, const double* angles_deg, int32_t det_count,
+                           int32_t device, vam_line2d_plan** out);
+int vam_line2d_plan_destroy(vam_line2d_plan* plan);
+int vam_line2d_forward(vam_line2d_plan* plan, const float* img_dev, float* sino_dev, vam_stream_t stream);
+int vam_line2d_backward(vam_line2d_plan* plan, const float* sino_dev, float* img_dev, vam_stream_t stream);
+
 /* ======================================================================= */
 /* Output formats: projector frames (vamtoolbox/imagesequence.py) and      */
 /* fan-beam rebinning (vamtoolbox/geometry.py:736-944)                     */

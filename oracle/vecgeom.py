@@ -77,3 +77,55 @@ def backward(sino, vectors, vol_shape):
         fv = sol[1] + n_v / 2 - 0.5
         out += _bilinear(sino[:, a, :], fu, fv)
     return out
+
+
+# ---------------------------------------------------------------------------
+# 2-D "line" model (vamtoolbox/projector/Projector2DParallelCUDA.py:7-45)
+# ---------------------------------------------------------------------------
+
+def _segment_in_square(p0, d, cx, cy):
+    """Length of the line p0 + s d (|d| = 1) inside the unit square centred at (cx, cy)
+    (Liang-Barsky clipping of an unbounded line)."""
+    lo, hi = -np.inf * np.ones(np.broadcast(cx, cy).shape), np.inf * np.ones(np.broadcast(cx, cy).shape)
+    for k, c in ((0, cx), (1, cy)):
+        if abs(d[k]) < 1e-15:
+            inside = np.abs(p0[k] - c) <= 0.5
+            lo = np.where(inside, lo, np.inf)
+            hi = np.where(inside, hi, -np.inf)
+        else:
+            s1 = (c - 0.5 - p0[k]) / d[k]
+            s2 = (c + 0.5 - p0[k]) / d[k]
+            lo = np.maximum(lo, np.minimum(s1, s2))
+            hi = np.minimum(hi, np.maximum(s1, s2))
+    return np.maximum(hi - lo, 0.0)
+
+
+def line2d_matrix(n_y, n_x, angles_deg, n_t):
+    """Dense system matrix [nT * nA][nY * nX] of the line model: row (d, a) holds the
+    intersection lengths of ray (d, a) with every pixel, ASTRA's 2-D frame
+    (pixel (i, j) at (j - nX/2 + 1/2, nY/2 - i - 1/2), bin d at d - nT/2 + 1/2 along
+    (cos a, sin a), rays along (sin a, -cos a))."""
+    ii, jj = np.meshgrid(np.arange(n_y), np.arange(n_x), indexing="ij")
+    cx = (jj - n_x / 2 + 0.5).ravel()
+    cy = (n_y / 2 - ii - 0.5).ravel()
+    th = np.deg2rad(np.asarray(angles_deg, dtype=np.float64))
+    M = np.zeros((n_t * th.size, n_y * n_x))
+    for a, t in enumerate(th):
+        u = np.array([np.cos(t), np.sin(t)])
+        ray = np.array([np.sin(t), -np.cos(t)])
+        for d in range(n_t):
+            p0 = u * (d - n_t / 2 + 0.5)
+            M[d * th.size + a] = _segment_in_square(p0, ray, cx, cy)
+    return M
+
+
+def line2d_forward(img, angles_deg, n_t):
+    img = np.asarray(img, dtype=np.float64)
+    M = line2d_matrix(img.shape[0], img.shape[1], angles_deg, n_t)
+    return (M @ img.ravel()).reshape(n_t, -1)
+
+
+def line2d_backward(sino, angles_deg, shape):
+    sino = np.asarray(sino, dtype=np.float64)
+    M = line2d_matrix(shape[0], shape[1], angles_deg, sino.shape[0])
+    return (M.T @ sino.ravel()).reshape(shape)

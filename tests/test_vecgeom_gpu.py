@@ -94,3 +94,41 @@ def test_optimize_with_inclined_rays(method):
     tg, pg = _geo(32, 8, np.linspace(0, 360, 24, endpoint=False), inclination_angle=12.0)
     sino, recon, err = optimize.optimize(tg, pg, optimize.Options(method=method, n_iter=3, verbose=False))
     assert np.isfinite(np.asarray(sino.array)).all() and np.asarray(sino.array).shape == (32, 24, 8)
+
+
+@pytest.mark.parametrize("shape,n_ang", [((40, 40), 36), ((33, 33), 17), ((64, 48), 20)])
+def test_line2d_matches_oracle_and_is_a_transpose(shape, n_ang):
+    from vamtoolbox_b200.projector.Projector2DParallelCUDA import Line2DPlan
+
+    rng = np.random.default_rng(8)
+    ang = np.sort(rng.uniform(0, 360, n_ang))
+    ang[:4] = [0.0, 45.0, 90.0, 135.0]                     # axis-aligned and diagonal rays included
+    n_t = shape[1]
+    plan = Line2DPlan(*shape, ang, n_t, "cuda")
+    img = rng.random(shape)
+    f = plan.forward(img).cpu().numpy()
+    assert relL2(f, V.line2d_forward(img, ang, n_t)) < 1e-5
+    sino = rng.random((n_t, ang.size))
+    b = plan.backward(sino).cpu().numpy()
+    assert relL2(b, V.line2d_backward(sino, ang, shape)) < 1e-5
+    lhs = float((f.astype(np.float64) * sino).sum())
+    rhs = float((img * b.astype(np.float64)).sum())
+    assert abs(lhs - rhs) / abs(lhs) < 1e-6                # <A x, y> = <x, A^T y>
+
+
+def test_line2d_dispatch():
+    from vamtoolbox_b200.projector.Projector2DParallelCUDA import Projector2DParallelCUDAAstra
+
+    tg = geometry.TargetGeometry(target=_smooth_phantom(48, 3) > 0.8)
+    tg.segmentZ(1)
+    pg = geometry.ProjectionGeometry(np.linspace(0, 180, 60, endpoint=False), "parallel", CUDA=True,
+                                     parallel_model="astra")
+    A = projectorconstructor.projectorconstructor(tg, pg)
+    assert isinstance(A, Projector2DParallelCUDAAstra)
+    x = np.ones((48, 48))
+    b = A.forward(x)
+    assert b.shape == (48, 60) and b.dtype == np.float64
+    assert x[0, 0] == 0 and x[24, 24] == 1                 # the input is clipped in place
+    back = A.backward(b.copy())
+    from vamtoolbox_b200.util.data import circle_inside_mask
+    assert back.shape == (48, 48) and not back[~circle_inside_mask(48, 48)].any()

@@ -226,7 +226,180 @@ __global__ void __launch_bounds__(kThreads) k_vec_backward(const float* __restri
     vol[(i * nX + j) * nZ + k] = acc;
 }
 
+// ---------------------------------------------------------------------------
+// 2-D "line" model (the projector the reference's Projector2DParallelCUDAAstra
+// builds, vamtoolbox/projector/Projector2DParallelCUDA.py:7-45): the weight of
+// a (ray, pixel) pair is the length of the ray -- a zero-width line -- inside
+// the unit pixel square.  ASTRA's 2-D frame: pixel (i, j) of an [nY][nX]
+// image at (j - nX/2 + 1/2, nY/2 - i - 1/2) (row 0 on top), detector bin d at
+// offset d - nT/2 + 1/2 along u = (cos a, sin a), rays along (sin a, -cos a).
+// For a line at signed normal distance t from the pixel centre the chord is
+// 1/A for |t| <= (A-B)/2, ((A+B)/2 - |t|) / (A B) up to (A+B)/2, then 0, with
+// A = max(|cos|, |sin|), B = min.  Forward and backward evaluate the same t
+// (fmaf(y, s, x c) - t_d) for a (ray, pixel) pair, so the backward is the
+// forward's exact transpose.
+// ---------------------------------------------------------------------------
+struct LineAngle {
+    float c, s;          // cos, sin
+    float half_diff;     // (A - B) / 2
+    float half_sum;      // (A + B) / 2
+    float full;          // 1 / A
+    float inv_ab;        // 1 / (A B), 0 when B == 0
+    int along_x;         // |sin| >= |cos|: rays run mostly along x, one band per column
+    int pad;
+};
+
+__device__ __forceinline__ float chord(float t, const LineAngle& g) {
+    const float at = fabsf(t);
+    if (at <= g.half_diff) return g.full;
+    if (at >= g.half_sum) return 0.f;
+    return (g.half_sum - at) * g.inv_ab;
+}
+
+__global__ void __launch_bounds__(kThreads) k_line2d_forward(const float* __restrict__ img, float* __restrict__ sino,
+                                                             const LineAngle* __restrict__ ang, int nY, int nX,
+                                                             int nT, int nA) {
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;   // a * nT + d (bins of one angle adjacent)
+    if (gid >= nA * nT) return;
+    const int a = gid / nT, d = gid - a * nT;
+    const LineAngle g = ang[a];
+    const float td = (float)d - 0.5f * (float)nT + 0.5f;
+    const float x0 = 0.5f - 0.5f * (float)nX, y0 = 0.5f * (float)nY - 0.5f;   // centre of pixel (0, 0)
+    float acc = 0.f;
+    if (g.along_x) {
+        for (int j = 0; j < nX; ++j) {
+            const float x = x0 + (float)j;
+            const float y = (td - x * g.c) / g.s;          // crossing of the column centre line
+            const int ic = __float2int_rn(y0 - y);
+#pragma unroll
+            for (int q = -1; q <= 1; ++q) {
+                const int i = ic + q;
+                if ((unsigned)i >= (unsigned)nY) continue;
+                const float yi = y0 - (float)i;
+                const float w = chord(fmaf(yi, g.s, x * g.c) - td, g);
+                if (w != 0.f) acc = fmaf(w, __ldg(img + i * nX + j), acc);
+            }
+        }
+    } else {
+        for (int i = 0; i < nY; ++i) {
+            const float y = y0 - (float)i;
+            const float x = (td - y * g.s) / g.c;          // crossing of the row centre line
+            const int jc = __float2int_rn(x - x0);
+#pragma unroll
+            for (int q = -1; q <= 1; ++q) {
+                const int j = jc + q;
+                if ((unsigned)j >= (unsigned)nX) continue;
+                const float xj = x0 + (float)j;
+                const float w = chord(fmaf(y, g.s, xj * g.c) - td, g);
+                if (w != 0.f) acc = fmaf(w, __ldg(img + i * nX + j), acc);
+            }
+        }
+    }
+    sino[d * nA + a] = acc;
+}
+
+__global__ void __launch_bounds__(kThreads) k_line2d_backward(const float* __restrict__ sino, float* __restrict__ img,
+                                                              const LineAngle* __restrict__ ang, int nY, int nX,
+                                                              int nT, int nA) {
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;   // i * nX + j
+    if (gid >= nY * nX) return;
+    const int i = gid / nX, j = gid - i * nX;
+    const float x = 0.5f - 0.5f * (float)nX + (float)j, y = 0.5f * (float)nY - 0.5f - (float)i;
+    const float dofs = 0.5f * (float)nT - 0.5f;
+    float acc = 0.f;
+    for (int a = 0; a < nA; ++a) {
+        const LineAngle g = ang[a];
+        const float tp = fmaf(y, g.s, x * g.c);
+        const int dc = __float2int_rn(tp + dofs);
+#pragma unroll
+        for (int q = -1; q <= 1; ++q) {
+            const int d = dc + q;
+            if ((unsigned)d >= (unsigned)nT) continue;
+            const float td = (float)d - 0.5f * (float)nT + 0.5f;
+            const float w = chord(tp - td, g);
+            if (w != 0.f) acc = fmaf(w, __ldg(sino + d * nA + a), acc);
+        }
+    }
+    img[gid] = acc;
+}
+
 }  // namespace
+
+struct vam_line2d_plan {
+    int nY, nX, nT, nA, device;
+    LineAngle* d_ang;
+};
+
+extern "C" int vam_line2d_plan_create(int32_t n_y, int32_t n_x, int32_t n_angles, const double* angles_deg,
+                                      int32_t det_count, int32_t device, vam_line2d_plan** out) {
+    clear_error();
+    VAM_REQUIRE(angles_deg && out, VAM_ERR_ARG, "vam_line2d_plan_create: null argument");
+    VAM_REQUIRE(n_y > 0 && n_x > 0 && n_angles > 0 && det_count > 0, VAM_ERR_SHAPE,
+                "vam_line2d_plan_create: empty image, detector or angle set");
+    VAM_REQUIRE((int64_t)n_y * n_x < (1ll << 31) && (int64_t)det_count * n_angles < (1ll << 31), VAM_ERR_SHAPE,
+                "vam_line2d_plan_create: image or sinogram of 2^31 elements or more");
+    std::vector<LineAngle> h(n_angles);
+    for (int a = 0; a < n_angles; ++a) {
+        VAM_REQUIRE(isfinite(angles_deg[a]), VAM_ERR_ARG, "vam_line2d_plan_create: non-finite angle");
+        const double th = angles_deg[a] * 3.14159265358979323846 / 180.0;
+        const double c = cos(th), sn = sin(th);
+        const double A = fmax(fabs(c), fabs(sn)), B = fmin(fabs(c), fabs(sn));
+        LineAngle& g = h[a];
+        g.c = (float)c;
+        g.s = (float)sn;
+        g.half_diff = (float)((A - B) / 2.0);
+        g.half_sum = (float)((A + B) / 2.0);
+        g.full = (float)(1.0 / A);
+        g.inv_ab = B > 1e-12 ? (float)(1.0 / (A * B)) : 0.f;
+        g.along_x = fabs(sn) >= fabs(c);
+        g.pad = 0;
+    }
+    vam::DeviceGuard dg(device);
+    VAM_REQUIRE(dg.ok, VAM_ERR_CUDA, "vam_line2d_plan_create: cannot select the device");
+    vam_line2d_plan* p = new vam_line2d_plan{n_y, n_x, det_count, n_angles, device, nullptr};
+    if (cudaMalloc(&p->d_ang, sizeof(LineAngle) * n_angles) != cudaSuccess) {
+        delete p;
+        return set_error(VAM_ERR_NOMEM, "vam_line2d_plan_create: cudaMalloc failed");
+    }
+    if (cudaMemcpy(p->d_ang, h.data(), sizeof(LineAngle) * n_angles, cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaFree(p->d_ang);
+        delete p;
+        return set_error(VAM_ERR_CUDA, "vam_line2d_plan_create: table upload failed");
+    }
+    *out = p;
+    return VAM_OK;
+}
+
+extern "C" int vam_line2d_plan_destroy(vam_line2d_plan* p) {
+    clear_error();
+    if (!p) return VAM_OK;
+    vam::DeviceGuard dg(p->device);
+    cudaFree(p->d_ang);
+    delete p;
+    return VAM_OK;
+}
+
+extern "C" int vam_line2d_forward(vam_line2d_plan* p, const float* img, float* sino, vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(p && img && sino, VAM_ERR_ARG, "vam_line2d_forward: null argument");
+    vam::DeviceGuard dg(p->device);
+    const int n = p->nA * p->nT;
+    k_line2d_forward<<<(n + kThreads - 1) / kThreads, kThreads, 0, (cudaStream_t)stream>>>(img, sino, p->d_ang, p->nY,
+                                                                                        p->nX, p->nT, p->nA);
+    VAM_CHECK_LAUNCH("vam_line2d_forward");
+    return VAM_OK;
+}
+
+extern "C" int vam_line2d_backward(vam_line2d_plan* p, const float* sino, float* img, vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(p && img && sino, VAM_ERR_ARG, "vam_line2d_backward: null argument");
+    vam::DeviceGuard dg(p->device);
+    const int n = p->nY * p->nX;
+    k_line2d_backward<<<(n + kThreads - 1) / kThreads, kThreads, 0, (cudaStream_t)stream>>>(sino, img, p->d_ang,
+                                                                                         p->nY, p->nX, p->nT, p->nA);
+    VAM_CHECK_LAUNCH("vam_line2d_backward");
+    return VAM_OK;
+}
 
 struct vam_vec_plan {
     int nY, nX, nZ, nU, nA, nV, device;

@@ -58,7 +58,11 @@ def projectorconstructor(target_geo, proj_geo, optical_params=None, **projector_
 
         A = PyTorchRayTracingPropagator(target_geo, proj_geo, **projector_kwargs)
     elif proj_geo.ray_type in ("parallel", None):
-        if target_geo.n_dim == 2:
+        if target_geo.n_dim == 2 and getattr(proj_geo, "parallel_model", None) == "astra":
+            from .projector.Projector2DParallelCUDA import Projector2DParallelCUDAAstra
+
+            A = Projector2DParallelCUDAAstra(target_geo, proj_geo, **projector_kwargs)
+        elif target_geo.n_dim == 2:
             from .projector.Projector2DParallel import Projector2DParallel
 
             A = Projector2DParallel(target_geo, proj_geo, **projector_kwargs)
