@@ -732,6 +732,25 @@ def run_vec_geometry(dev, n=256, n_angles=360, incline=15.0, reps=5, cpu=True):
                      "forward_taps_GBs": round(4.0 * taps * n * n_angles * n * n / (t_f * 1e-3) / 1e9, 1),
                      "hbm_bytes_per_call": 4 * (n ** 3 + n * n_angles * n)}
         del p
+    # 2-D line model (ASTRA "line" projector of the reference's 2-D CUDA class): 512^2 image, 720 angles
+    from vamtoolbox_b200.projector.Projector2DParallelCUDA import Line2DPlan
+
+    n2, a2 = 512, 720
+    ang2 = np.linspace(0, 180, a2, endpoint=False)
+    lp = Line2DPlan(n2, n2, ang2, n2, dev)
+    img = torch.rand((n2, n2), device=dev, generator=g)
+    s2 = torch.rand((n2, a2), device=dev, generator=g)
+    t_lf = tim(lambda: lp.forward(img))
+    t_lb = tim(lambda: lp.backward(s2))
+    out["line_2d"] = {"workload": f"{n2}^2 image, {a2} angles, {n2} bins", "forward_ms": round(t_lf, 4),
+                      "backward_ms": round(t_lb, 4)}
+    if cpu:
+        from oracle import vecgeom as OV
+
+        t0 = time.perf_counter()
+        OV.line2d_forward(img.cpu().double().numpy(), ang2[:1], n2)
+        out["line_2d"]["cpu_forward_s"] = round((time.perf_counter() - t0) * a2, 1)
+        out["line_2d"]["cpu_sample"] = "1 of 720 angles through the oracle's ray-clipping numpy model, scaled"
     if cpu:
         from oracle import vecgeom as OV
 

@@ -119,13 +119,32 @@ def line2d_matrix(n_y, n_x, angles_deg, n_t):
     return M
 
 
+def _line2d_rows(n_y, n_x, angles_deg, n_t):
+    """Yield (d, a, lengths over all pixels) for every ray, one row of line2d_matrix at a time."""
+    ii, jj = np.meshgrid(np.arange(n_y), np.arange(n_x), indexing="ij")
+    cx = (jj - n_x / 2 + 0.5).ravel()
+    cy = (n_y / 2 - ii - 0.5).ravel()
+    for a, t in enumerate(np.deg2rad(np.asarray(angles_deg, dtype=np.float64))):
+        u = np.array([np.cos(t), np.sin(t)])
+        ray = np.array([np.sin(t), -np.cos(t)])
+        for d in range(n_t):
+            yield d, a, _segment_in_square(u * (d - n_t / 2 + 0.5), ray, cx, cy)
+
+
 def line2d_forward(img, angles_deg, n_t):
+    """Sinogram [nT][nA] of img [nY][nX] under the line model (rows streamed, no dense matrix)."""
     img = np.asarray(img, dtype=np.float64)
-    M = line2d_matrix(img.shape[0], img.shape[1], angles_deg, n_t)
-    return (M @ img.ravel()).reshape(n_t, -1)
+    flat = img.ravel()
+    out = np.zeros((n_t, np.size(angles_deg)))
+    for d, a, row in _line2d_rows(img.shape[0], img.shape[1], angles_deg, n_t):
+        out[d, a] = row @ flat
+    return out
 
 
 def line2d_backward(sino, angles_deg, shape):
+    """Transpose of line2d_forward: sino [nT][nA] -> image of `shape`."""
     sino = np.asarray(sino, dtype=np.float64)
-    M = line2d_matrix(shape[0], shape[1], angles_deg, sino.shape[0])
-    return (M.T @ sino.ravel()).reshape(shape)
+    out = np.zeros(shape[0] * shape[1])
+    for d, a, row in _line2d_rows(shape[0], shape[1], angles_deg, sino.shape[0]):
+        out += sino[d, a] * row
+    return out.reshape(shape)
