@@ -394,6 +394,13 @@ int vam_vec_forward(vam_vec_plan* plan, const float* vol_dev, float* sino_dev, v
  * (Projector3DParallelCUDA.py:56-72). */
 int vam_vec_backward(vam_vec_plan* plan, const float* sino_dev, float* vol_dev, vam_stream_t stream);
 
+/* Exact transpose of vam_vec_forward (<A x, y> = <x, A^T y> up to float
+ * summation order): every ray adds its value times the forward's weights to
+ * the voxels the forward read (float atomics).  No counterpart in the
+ * reference (ASTRA's backprojection above is voxel-driven); used for
+ * gradients. */
+int vam_vec_adjoint(vam_vec_plan* plan, const float* sino_dev, float* vol_dev, vam_stream_t stream);
+
 /* 2-D "line" model of the reference's Projector2DParallelCUDAAstra
  * (vamtoolbox/projector/Projector2DParallelCUDA.py:7-45, ASTRA's "line"
  * projector): the weight of a (ray, pixel) pair is the length of the ray, a

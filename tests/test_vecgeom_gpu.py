@@ -132,3 +132,44 @@ def test_line2d_dispatch():
     back = A.backward(b.copy())
     from vamtoolbox_b200.util.data import circle_inside_mask
     assert back.shape == (48, 48) and not back[~circle_inside_mask(48, 48)].any()
+
+
+@pytest.mark.parametrize("incline", [0.0, 15.0, 60.0])
+def test_vec_adjoint_is_the_transpose(incline):
+    shape = (28, 28, 16)
+    ang = np.linspace(0, 360, 14, endpoint=False) + 2.0
+    vec = parallel3d_vectors(np.deg2rad(ang)) if incline == 0 else genVectorsAstra(ang, incline)
+    plan = VecPlan(*shape, vec, 28, 16, "cuda")
+    g = torch.Generator(device="cuda").manual_seed(3)
+    x = torch.rand(shape, device="cuda", generator=g)
+    y = torch.rand(plan.shape_sino, device="cuda", generator=g)
+    lhs = float((plan.forward(x).double() * y.double()).sum())
+    rhs = float((x.double() * plan.adjoint(y).double()).sum())
+    assert abs(lhs - rhs) / abs(lhs) < 1e-5
+
+
+def test_autograd_vec_and_line2d():
+    from vamtoolbox_b200 import autograd as AG
+    from vamtoolbox_b200.projector.Projector2DParallelCUDA import Line2DPlan
+
+    vec = genVectorsAstra(np.linspace(0, 360, 10, endpoint=False), 20.0)
+    plan = VecPlan(20, 20, 12, vec, 20, 12, "cuda")
+    x = torch.rand((20, 20, 12), device="cuda", requires_grad=True)
+    w = torch.rand(plan.shape_sino, device="cuda")
+    (AG.vec_forward(x, plan) * w).sum().backward()
+    assert torch.allclose(x.grad, plan.adjoint(w), rtol=1e-5, atol=1e-6)
+
+    lp = Line2DPlan(24, 24, np.linspace(0, 180, 16, endpoint=False), 24, "cuda")
+    x2 = torch.rand((24, 24), device="cuda", dtype=torch.float32, requires_grad=True)
+    w2 = torch.rand((24, 16), device="cuda")
+    (AG.line2d_forward(x2, lp) * w2).sum().backward()
+    assert torch.allclose(x2.grad, lp.backward(w2), rtol=1e-6, atol=1e-6)
+    b2 = torch.rand((24, 16), device="cuda", requires_grad=True)
+    w3 = torch.rand((24, 24), device="cuda")
+    (AG.line2d_backward(b2, lp) * w3).sum().backward()
+    assert torch.allclose(b2.grad, lp.forward(w3), rtol=1e-6, atol=1e-6)
+    # a linear map: a central difference along a random direction equals the directional derivative
+    d = torch.rand((24, 24), device="cuda")
+    xd = x2.detach().double()
+    fd = ((lp.forward((xd + 0.5 * d).float()).double() - lp.forward((xd - 0.5 * d).float()).double()) * w2).sum()
+    assert abs(float(fd) - float((x2.grad * d).sum())) / abs(float(fd)) < 1e-4

@@ -139,6 +139,7 @@ _SIGS = {
     "vam_vec_plan_info": ([_vp, ctypes.POINTER(_c_i32), ctypes.POINTER(_c_i32)], _c_int),
     "vam_vec_forward": ([_vp, _vp, _vp, _vp], _c_int),
     "vam_vec_backward": ([_vp, _vp, _vp, _vp], _c_int),
+    "vam_vec_adjoint": ([_vp, _vp, _vp, _vp], _c_int),
     "vam_line2d_plan_create": ([_c_i32, _c_i32, _c_i32, ctypes.POINTER(_c_d), _c_i32, _c_i32, ctypes.POINTER(_vp)],
                                _c_int),
     "vam_line2d_plan_destroy": ([_vp], _c_int),

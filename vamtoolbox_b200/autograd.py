@@ -9,9 +9,13 @@
   (R5, its exact transpose), d/dalpha recomputes every ray's path
   (vam_ray_grad_alpha) instead of storing it.
 * :func:`ray_deposit` -- R5; backward is R6.
+* :func:`vec_forward` -- the vector-geometry (ASTRA-model) forward; backward is
+  its exact transpose (vam_vec_adjoint), not ASTRA's voxel-driven backprojection.
+* :func:`line2d_forward` / :func:`line2d_backward` -- the 2-D line model and
+  its exact transpose, each the other's gradient.
 
 Plans are the objects of :mod:`vamtoolbox_b200.projector` (``ParallelPlan``,
-``RayPlan``); inputs are float32 CUDA tensors of the plan's shapes.
+``RayPlan``, ``VecPlan``, ``Line2DPlan``); inputs are float32 CUDA tensors of the plan's shapes.
 """
 from __future__ import annotations
 
@@ -100,3 +104,51 @@ class _RayDeposit(torch.autograd.Function):
 def ray_deposit(g, plan):
     """Dose deposited by ray energies g (differentiable)."""
     return _RayDeposit.apply(g, plan)
+
+
+class _VecForward(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, x, plan):
+        ctx.plan = plan
+        return plan.forward(x.contiguous())
+
+    @staticmethod
+    def backward(ctx, gb):
+        return ctx.plan.adjoint(gb.contiguous()), None
+
+
+def vec_forward(x, plan):
+    """Vector-geometry sinogram of x (differentiable; gradient by the exact transpose)."""
+    return _VecForward.apply(x, plan)
+
+
+class _Line2DForward(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, x, plan):
+        ctx.plan = plan
+        return plan.forward(x)
+
+    @staticmethod
+    def backward(ctx, gb):
+        return ctx.plan.backward(gb.contiguous()), None
+
+
+class _Line2DBackward(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, b, plan):
+        ctx.plan = plan
+        return plan.backward(b)
+
+    @staticmethod
+    def backward(ctx, gx):
+        return ctx.plan.forward(gx.contiguous()), None
+
+
+def line2d_forward(x, plan):
+    """2-D line-model sinogram of x (differentiable)."""
+    return _Line2DForward.apply(x, plan)
+
+
+def line2d_backward(b, plan):
+    """Exact transpose of line2d_forward applied to b (differentiable)."""
+    return _Line2DBackward.apply(b, plan)

@@ -200,6 +200,50 @@ __global__ void __launch_bounds__(kThreads) k_vec_backward_flat4(const float* __
     *reinterpret_cast<float4*>(vol + (i * nX + j) * nZ + k) = acc;
 }
 
+// Exact transpose of the forward (for gradients; ASTRA's backprojection is
+// voxel-driven and is not): every ray walks the forward's samples and adds
+// g * scale * weight to the taps it read.  Float atomics: exact up to the
+// order of the additions.
+__device__ __forceinline__ void scatter_bilerp(float* __restrict__ base, float f0, float f1, int n0, int n1, int s0,
+                                               int s1, float v) {
+    const float g0 = floorf(f0), g1 = floorf(f1);
+    const int i0 = (int)g0, i1 = (int)g1;
+    const float t0 = f0 - g0, t1 = f1 - g1;
+    const bool a0 = (unsigned)i0 < (unsigned)n0, b0 = (unsigned)(i0 + 1) < (unsigned)n0;
+    const bool a1 = (unsigned)i1 < (unsigned)n1, b1 = (unsigned)(i1 + 1) < (unsigned)n1;
+    const int o = i0 * s0 + i1 * s1;
+    const float r0 = v * (1.f - t0), r1 = v * t0;
+    if (a0 && a1) atomicAdd(base + o, r0 * (1.f - t1));
+    if (a0 && b1) atomicAdd(base + o + s1, r0 * t1);
+    if (b0 && a1) atomicAdd(base + o + s0, r1 * (1.f - t1));
+    if (b0 && b1) atomicAdd(base + o + s0 + s1, r1 * t1);
+}
+
+__global__ void __launch_bounds__(kThreads) k_vec_adjoint(const float* __restrict__ sino, float* __restrict__ vol,
+                                                          const FwdAngle* __restrict__ ang, int nY, int nX, int nZ,
+                                                          int nU, int nA, int nV) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const int a = blockIdx.y;
+    const int c = blockIdx.z;
+    if (r >= nV) return;
+    const FwdAngle g = ang[a];
+    const float v = sino[(c * nA + a) * nV + r] * g.scale;
+    if (v == 0.f) return;
+    const int sI = nX * nZ, sJ = nZ;
+    const float fc = (float)c, fr = (float)r;
+    if (g.axis <= 1) {
+        const int plane = g.axis == 0 ? sI : sJ, hs = g.axis == 0 ? sJ : sI, nh = g.axis == 0 ? nX : nY;
+        const int np = g.axis == 0 ? nY : nX;
+        const float h0 = affine(g.p0, fc, fr, 0.f), k0 = affine(g.p1, fc, fr, 0.f);
+        for (int s = 0; s < np; ++s)
+            scatter_bilerp(vol + s * plane, fmaf(g.p0[3], (float)s, h0), fmaf(g.p1[3], (float)s, k0), nh, nZ, hs, 1, v);
+    } else {
+        const float i0 = affine(g.p0, fc, fr, 0.f), j0 = affine(g.p1, fc, fr, 0.f);
+        for (int s = 0; s < nZ; ++s)
+            scatter_bilerp(vol + s, fmaf(g.p0[3], (float)s, i0), fmaf(g.p1[3], (float)s, j0), nY, nX, sI, sJ, v);
+    }
+}
+
 // Backward: one thread per voxel (i, j, k), k fastest; angles looped.
 // FLAT: the detector row of voxel slice k is exactly k.
 template <bool FLAT, bool HU>
@@ -588,6 +632,18 @@ extern "C" int vam_vec_forward(vam_vec_plan* p, const float* vol, float* sino, v
         k_vec_forward<false, false><<<grid, kThreads, 0, st>>>(vol, sino, p->d_fwd, p->nY, p->nX, p->nZ, p->nU,
                                                                p->nA, p->nV);
     VAM_CHECK_LAUNCH("vam_vec_forward");
+    return VAM_OK;
+}
+
+extern "C" int vam_vec_adjoint(vam_vec_plan* p, const float* sino, float* vol, vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(p && vol && sino, VAM_ERR_ARG, "vam_vec_adjoint: null argument");
+    vam::DeviceGuard dg(p->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    VAM_TRY_CUDA(cudaMemsetAsync(vol, 0, sizeof(float) * (size_t)p->nY * p->nX * p->nZ, st));
+    dim3 grid((p->nV + kThreads - 1) / kThreads, p->nA, p->nU);
+    k_vec_adjoint<<<grid, kThreads, 0, st>>>(sino, vol, p->d_fwd, p->nY, p->nX, p->nZ, p->nU, p->nA, p->nV);
+    VAM_CHECK_LAUNCH("vam_vec_adjoint");
     return VAM_OK;
 }
 

@@ -110,6 +110,16 @@ class VecPlan:
                       _lib.stream_ptr(torch.cuda.current_stream(self.device)))
         return out
 
+    def adjoint(self, sino, out=None):
+        """Exact transpose of ``forward`` (float atomics; for gradients)."""
+        self._check(sino, self.shape_sino, "adjoint input")
+        out = torch.empty(self.shape_vol, dtype=torch.float32, device=self.device) if out is None else out
+        self._check(out, self.shape_vol, "adjoint output")
+        with torch.cuda.device(self.device):
+            _lib.call("vam_vec_adjoint", self._h, _lib.ptr(sino), _lib.ptr(out),
+                      _lib.stream_ptr(torch.cuda.current_stream(self.device)))
+        return out
+
     def backward(self, sino, out=None):
         self._check(sino, self.shape_sino, "backward input")
         out = torch.empty(self.shape_vol, dtype=torch.float32, device=self.device) if out is None else out
