@@ -479,7 +479,7 @@ typedef struct {
  * np.minimum(., max), astype(uint8/16/32) and the store into a uint8 frame
  * (low byte) is replayed in the reference's dtypes; the insertion offsets,
  * array copies and flips of _insertImage / _arrayInsertImage (:303-355) are
- * carried by the two tables.  nA <= 65535.  The blank area outside the box
+ * carried by the two tables.  The blank area outside the box
  * is written with contiguous zero stores, the box by the gather kernel; a
  * box equal to the frame makes it one gather pass (used to fetch just the
  * image window, frame = window). */

@@ -651,8 +651,7 @@ extern "C" int vam_imageseq_frames(const void* sino, int dtype, int32_t nR, int3
     VAM_REQUIRE(sino && prm && frames && prm->src_col_dev && prm->src_row_dev, VAM_ERR_ARG,
                 "vam_imageseq_frames: null argument");
     VAM_REQUIRE(dtype_ok(dtype), VAM_ERR_ARG, "vam_imageseq_frames: dtype must be VAM_DTYPE_F32 or VAM_DTYPE_F64");
-    VAM_REQUIRE(nR > 0 && nA > 0 && nZ > 0 && nA <= 65535, VAM_ERR_SHAPE,
-                "vam_imageseq_frames: need nR, nZ > 0 and 0 < nA <= 65535");
+    VAM_REQUIRE(nR > 0 && nA > 0 && nZ > 0, VAM_ERR_SHAPE, "vam_imageseq_frames: empty sinogram");
     VAM_REQUIRE(prm->n_u > 0 && prm->n_v > 0 && prm->n_u % 4 == 0, VAM_ERR_SHAPE,
                 "vam_imageseq_frames: frame width must be a positive multiple of 4");
     VAM_REQUIRE(((uintptr_t)frames & 15u) == 0, VAM_ERR_ARG, "vam_imageseq_frames: frames not 16-byte aligned");
