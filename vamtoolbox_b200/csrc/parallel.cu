@@ -1282,7 +1282,9 @@ struct Item {
     long long tstart;  // first ticket of the call inside a batch
     long long cost;    // samples the call evaluates (batch ordering and ticket sizes)
     unsigned chunk;    // blocks of the call's grid per ticket
-    int family;        // 1 forward, 2 backward_ref, 4 adjoint
+    int family;        // body family (k_batch instances)
+    unsigned ntk;      // tickets of the call: ticket j covers blocks j, j + ntk, j + 2 ntk, ...
+    unsigned pad_;
     // pre-pass of the fast forward in mask mode: pre_out = mask * pre_in
     const float* pre_in;
     const float* pre_mask;
@@ -1410,9 +1412,15 @@ int describe(vam_parallel_plan* plan, Op op, const float* in, float* out, Item& 
 template <int FAM, int VZ, bool OCC, int ABS>
 __device__ __forceinline__ void gen_body(const Item& it, unsigned bx, unsigned by) {
     const Args a = it.a;
-    if constexpr ((FAM & 1) != 0) if (it.kind == KF_GEN) k_forward_body<VZ, OCC, ABS>(a, bx, by);
-    if constexpr ((FAM & 2) != 0) if (it.kind == KB_GEN) k_backward_ref_body<VZ, OCC, ABS>(a, bx, by);
+    if constexpr ((FAM & 16) != 0) if (it.kind == KF_GEN) k_forward_body<VZ, OCC, ABS>(a, bx, by);
+    if constexpr ((FAM & 8) != 0) if (it.kind == KB_GEN) k_backward_ref_body<VZ, OCC, ABS>(a, bx, by);
     if constexpr ((FAM & 4) != 0) if (it.kind == KA_GEN) k_adjoint_body<VZ, OCC, ABS>(a, bx, by);
+}
+
+template <int FAM, int VZ, int ABS>
+__device__ __forceinline__ void lean_gen_body(const Item& it, const Args& a, unsigned bx, unsigned by) {
+    if constexpr (FAM == 32) if (it.kind == KF_GEN) k_forward_body<VZ, false, ABS>(a, bx, by);
+    if constexpr (FAM == 64) if (it.kind == KB_GEN) k_backward_ref_body<VZ, false, ABS>(a, bx, by);
 }
 
 template <int FAM, int VZ, bool OCC>
@@ -1434,7 +1442,7 @@ __device__ __forceinline__ void fast_body(const Item& it, unsigned bx, unsigned 
             k_forward_2d_body<RAY>(a, bx, by);
         }
     }
-    if constexpr ((FAM & 2) != 0) {
+    if constexpr ((FAM & 8) != 0 || ((FAM & 2) != 0 && !RAY)) {
         if (it.kind == KB_2D) {
             const Args a = it.a;
             k_backward_2d_body<RAY>(a, bx, by);
@@ -1458,14 +1466,31 @@ __device__ __forceinline__ void fast_body(const Item& it, unsigned bx, unsigned 
     }
 }
 
-// FAM: the op families (1 forward, 2 backward_ref, 4 adjoint) this instance
-// carries; a batch launches the narrowest instance covering its calls, so a
-// forward-only batch is not compiled around the backprojectors' registers.
+// FAM: the body families this instance carries -- 1 the fast and 2-D
+// forwards, 2 the fast, batched and 2-D backprojections without per-ray
+// absorption, 4 adjoint, 8 the other backprojections (generic with occlusion
+// or per-ray absorption, fast with per-ray absorption), 16 the generic forward
+// with occlusion or per-ray absorption, 32 / 64 the generic forward /
+// backprojection without either; a batch launches one instance per family
+// present, so no body is compiled around the registers of rarer ones and each
+// keeps about its direct kernel's occupancy.
 template <int FAM>
 __device__ __forceinline__ void item_body(const Item& it, unsigned bx, unsigned by) {
     if (it.kind == KF_GEN || it.kind == KB_GEN || it.kind == KA_GEN) {
-        if (it.vz == 4) { if (it.occ) gen_body_fam<FAM, 4, true>(it, bx, by); else gen_body_fam<FAM, 4, false>(it, bx, by); }
-        else { if (it.occ) gen_body_fam<FAM, 1, true>(it, bx, by); else gen_body_fam<FAM, 1, false>(it, bx, by); }
+        if constexpr (FAM == 32 || FAM == 64) {
+            // the lean generic families: no occlusion, no per-ray absorption
+            const Args a = it.a;
+            if (it.absm == VAM_ABS_MASK) {
+                if (it.vz == 4) lean_gen_body<FAM, 4, VAM_ABS_MASK>(it, a, bx, by);
+                else lean_gen_body<FAM, 1, VAM_ABS_MASK>(it, a, bx, by);
+            } else {
+                if (it.vz == 4) lean_gen_body<FAM, 4, VAM_ABS_NONE>(it, a, bx, by);
+                else lean_gen_body<FAM, 1, VAM_ABS_NONE>(it, a, bx, by);
+            }
+        } else if constexpr ((FAM & (4 | 8 | 16)) != 0) {
+            if (it.vz == 4) { if (it.occ) gen_body_fam<FAM, 4, true>(it, bx, by); else gen_body_fam<FAM, 4, false>(it, bx, by); }
+            else { if (it.occ) gen_body_fam<FAM, 1, true>(it, bx, by); else gen_body_fam<FAM, 1, false>(it, bx, by); }
+        }
     } else if (it.kind == KA_TABLE) {
         if constexpr ((FAM & 4) != 0) {
             const Args a = it.a;
@@ -1473,7 +1498,7 @@ __device__ __forceinline__ void item_body(const Item& it, unsigned bx, unsigned 
             else k_adjoint_table_body<4>(a, it.table, bx, by);
         }
     } else if (it.ray) {
-        fast_body<FAM, true>(it, bx, by);
+        if constexpr (FAM != 2) fast_body<FAM, true>(it, bx, by);   // nor a per-ray absorption body
     } else {
         fast_body<FAM, false>(it, bx, by);
     }
@@ -1580,10 +1605,12 @@ struct BatchParams {
 };
 static_assert(sizeof(BatchParams) < 32000, "batch parameters must fit the 32 KB kernel parameter space");
 
-// The forward bodies fit 64 registers, so the forward-only instance asks for
-// four resident CTAs per SM; the others keep the backprojectors' 80.
+// The lean backprojections fit 48 registers, the fast and 2-D forwards and
+// the lean generic backprojection 64, so those instances ask for five and
+// four resident CTAs per SM; the others keep 80 (no spills).
 template <int FAM>
-__global__ void __launch_bounds__(256, FAM == 1 ? 4 : 3) k_batch(const __grid_constant__ BatchParams P) {
+__global__ void __launch_bounds__(256, FAM == 2 ? 5 : (FAM == 1 || FAM == 64 ? 4 : 3))
+    k_batch(const __grid_constant__ BatchParams P) {
     __shared__ long long s_t;
     __shared__ int s_idx;
     for (;;) {
@@ -1605,13 +1632,11 @@ __global__ void __launch_bounds__(256, FAM == 1 ? 4 : 3) k_batch(const __grid_co
         if (t >= P.total) return;  // uniform: every thread read the same s_t
         const Item& it = P.items[idx];
         const unsigned gx = it.gx, nb = it.gx * it.gy;  // a call's grid has < 2^32 blocks
-        const unsigned b0 = (unsigned)(t - it.tstart) * it.chunk;
-        const unsigned n = min(it.chunk, nb - b0);
-        unsigned bx = b0 % gx, by = b0 / gx;
-        for (unsigned k = 0; k < n; ++k) {
-            item_body<FAM>(it, bx, by);
+        // strided blocks: the CTAs holding consecutive tickets work on neighbouring blocks of the
+        // call's grid at any moment, as a direct launch's resident blocks do (L2 reuse)
+        for (unsigned b = (unsigned)(t - it.tstart); b < nb; b += it.ntk) {
+            item_body<FAM>(it, b % gx, b / gx);
             if (it.smem) __syncthreads();  // the next block restages the body's shared memory
-            if (++bx == gx) { bx = 0; ++by; }
         }
     }
 }
@@ -1622,7 +1647,11 @@ BatchKernel batch_kernel(int fam) {
         case 1: return k_batch<1>;
         case 2: return k_batch<2>;
         case 4: return k_batch<4>;
-        default: return k_batch<7>;
+        case 8: return k_batch<8>;
+        case 16: return k_batch<16>;
+        case 32: return k_batch<32>;
+        case 64: return k_batch<64>;
+        default: return k_batch<127>;
     }
 }
 
@@ -1867,15 +1896,30 @@ extern "C" int vam_parallel_adjoint(vam_parallel_plan* p, const float* sino, flo
 // ---------------------------------------------------------------------------
 // batches
 // ---------------------------------------------------------------------------
+// launches (ticket counters) one list may need: 48 calls per launch, and one
+// more launch at each of the <= 6 changes of body family
+constexpr int kBatchMaxLaunches = 80;
+
+// dynamic shared-memory sizes the batch kernels' residency is tabulated for
+constexpr unsigned kSmemBuckets[4] = {0u, 16u * 1024, 40u * 1024, 48u * 1024};
+
+inline int smem_bucket(unsigned smem) {
+    int k = 0;
+    while (k < 3 && kSmemBuckets[k] < smem) ++k;
+    return k;
+}
+
 struct vam_batch {
     int device;
     unsigned long long* d_counter;
     int sms;
-    int per_sm[8];             // resident CTAs per SM of k_batch<fam> (fam 1, 2, 4, 7)
+    int per_sm[128][4];        // resident CTAs per SM of k_batch<fam> (fam 1 .. 64, 127) per
+                               // dynamic shared-memory bucket (kSmemBuckets)
     std::vector<Item> host;    // the described calls of the last list, in queue order
     std::vector<int> group;    // first call of each launch (kBatchMaxItems calls per launch)
     std::vector<long long> tickets;  // tickets of each launch
-    std::vector<int> fam;      // op families of each launch
+    std::vector<int> fam;      // body family of each launch
+    std::vector<unsigned> gsmem;  // dynamic shared memory of each launch (its calls' largest)
     long long blocks;          // blocks of all calls' grids
     unsigned smem;
     int any_pre;
@@ -1890,26 +1934,28 @@ extern "C" int vam_batch_create(int32_t device, vam_batch** out) {
     VAM_REQUIRE(g.ok, VAM_ERR_CUDA, "vam_batch_create: cannot select device");
     int sms = 0;
     VAM_TRY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-    int per_sm[8] = {0};
-    // residency with the largest dynamic shared memory a call may ask for (48 KB, the batched
-    // backprojection's trig table), so a list never needs a runtime query (which would not be
-    // allowed during graph capture); the opt-in limit is raised first, as 48 KB plus the
-    // kernel's static shared memory exceeds the default
-    for (int fam : {1, 2, 4, 7}) {
+    int per_sm[128][4] = {};
+    // residency for each dynamic shared-memory bucket up to the largest a call may ask for (48 KB,
+    // the batched backprojection's trig table), queried once here, so a list never needs a
+    // runtime query (which would not be allowed during graph capture); the opt-in limit is
+    // raised first, as 48 KB plus the kernel's static shared memory exceeds the default
+    for (int fam : {1, 2, 4, 8, 16, 32, 64, 127}) {
         VAM_TRY_CUDA(cudaFuncSetAttribute(batch_kernel(fam), cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
-        VAM_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[fam], batch_kernel(fam),
-                                                                   kWarpsPerBlock * kWarp, 48 * 1024));
-        VAM_REQUIRE(per_sm[fam] > 0, VAM_ERR_NOTSUP, "vam_batch_create: the batch kernel cannot be resident");
+        for (int k = 0; k < 4; ++k) {
+            VAM_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[fam][k], batch_kernel(fam),
+                                                                       kWarpsPerBlock * kWarp, kSmemBuckets[k]));
+            VAM_REQUIRE(per_sm[fam][k] > 0, VAM_ERR_NOTSUP, "vam_batch_create: the batch kernel cannot be resident");
+        }
     }
     auto* b = new vam_batch();
     b->device = device;
     b->sms = sms;
-    for (int i = 0; i < 8; ++i) b->per_sm[i] = per_sm[i];
+    std::memcpy(b->per_sm, per_sm, sizeof(per_sm));
     b->blocks = 0;
     b->smem = 0;
     b->any_pre = 0;
     b->ctas = 0;
-    const cudaError_t e = cudaMalloc(&b->d_counter, sizeof(unsigned long long) * 64);
+    const cudaError_t e = cudaMalloc(&b->d_counter, sizeof(unsigned long long) * kBatchMaxLaunches);
     if (e != cudaSuccess) {
         delete b;
         return set_error(VAM_ERR_NOMEM, std::string("vam_batch_create: ") + cudaGetErrorString(e));
@@ -1959,31 +2005,45 @@ int batch_prepare(vam_batch* b, const vam_work* work, int32_t n) {
         const Op op = w.op == VAM_OP_FORWARD ? Op::Forward : (w.op == VAM_OP_BACKWARD_REF ? Op::BackwardRef : Op::Adjoint);
         const int rc = describe(w.plan, op, w.in, w.out, items[i], "vam_batch");
         if (rc != VAM_OK) return rc;
+        const Item& d = items[i];
+        // generic bodies with occlusion or per-ray absorption, and per-ray fast backprojections, go
+        // to the heavy families (8 backward, 16 forward)
+        const bool gen_heavy = d.occ || d.absm == VAM_ABS_RAY;
+        if (d.kind == KB_GEN) items[i].family = gen_heavy ? 8 : 64;
+        else if (d.family == 2 && d.ray) items[i].family = 8;
+        if (d.kind == KF_GEN) items[i].family = gen_heavy ? 16 : 32;
         VAM_REQUIRE((long long)items[i].gx * items[i].gy < (1LL << 32), VAM_ERR_SHAPE, "vam_batch: call grid too large");
         items[i].cost = (long long)std::llround((double)items[i].cost * time_weight(items[i]));
     }
-    // largest call first, so the small ones fill the tail of the queue
-    std::stable_sort(items.begin(), items.end(), [](const Item& x, const Item& y) { return x.cost > y.cost; });
+    // one launch per body family (each with the narrowest instance and its occupancy), and
+    // within a family the largest call first, so the small ones fill the tail of the queue
+    std::stable_sort(items.begin(), items.end(), [](const Item& x, const Item& y) {
+        return x.family != y.family ? x.family < y.family : x.cost > y.cost;
+    });
     b->group.clear();
     b->tickets.clear();
     b->fam.clear();
+    b->gsmem.clear();
     b->smem = 0;
     b->any_pre = 0;
     b->blocks = 0;
-    for (int g0 = 0; g0 < n; g0 += kBatchMaxItems) {
-        const int g1 = std::min(n, g0 + kBatchMaxItems);
+    for (int g0 = 0, g1 = 0; g0 < n; g0 = g1) {
+        g1 = g0 + 1;
+        while (g1 < n && g1 - g0 < kBatchMaxItems && items[g1].family == items[g0].family) ++g1;
         int fam = 0;
         long long cost = 0;
+        unsigned gsmem = 0;
         for (int i = g0; i < g1; ++i) {
             fam |= items[i].family;
             cost += std::max(items[i].cost, 1LL);
-            b->smem = std::max(b->smem, items[i].smem);
+            gsmem = std::max(gsmem, items[i].smem);
             b->any_pre |= items[i].pre_in != nullptr;
         }
-        if (fam != 1 && fam != 2 && fam != 4) fam = 7;
+        b->smem = std::max(b->smem, gsmem);
+        if (fam != 1 && fam != 2 && fam != 4 && fam != 8 && fam != 16 && fam != 32 && fam != 64) fam = 127;
         // tickets: about 8 per resident CTA over the launch, each call's share proportional to
-        // its samples; a ticket is a run of consecutive blocks of one call
-        const double want = 8.0 * b->sms * b->per_sm[fam];
+        // its samples; a ticket is every ntk-th block of one call from its index on
+        const double want = 8.0 * b->sms * b->per_sm[fam][smem_bucket(gsmem)];
         long long total = 0;
         for (int i = g0; i < g1; ++i) {
             Item& it = items[i];
@@ -1992,6 +2052,7 @@ int batch_prepare(vam_batch* b, const vam_work* work, int32_t n) {
             tk = std::max(1LL, std::min(tk, nb));
             it.chunk = (unsigned)((nb + tk - 1) / tk);
             tk = (nb + it.chunk - 1) / it.chunk;
+            it.ntk = (unsigned)tk;
             it.tstart = total;
             total += tk;
             b->blocks += nb;
@@ -1999,7 +2060,9 @@ int batch_prepare(vam_batch* b, const vam_work* work, int32_t n) {
         b->group.push_back(g0);
         b->tickets.push_back(total);
         b->fam.push_back(fam);
+        b->gsmem.push_back(gsmem);
     }
+    VAM_REQUIRE((int)b->group.size() <= kBatchMaxLaunches, VAM_ERR_SHAPE, "vam_batch: too many launches for one list");
     b->host.swap(items);
     return VAM_OK;
 }
@@ -2041,9 +2104,10 @@ extern "C" int vam_batch_submit(vam_batch* b, const vam_work* work, int32_t n, v
             VAM_CHECK_LAUNCH("k_batch_premask");
         }
         const int fam = b->fam[k];
-        const long long ctas = std::min<long long>((long long)b->sms * b->per_sm[fam], P.total);
+        const unsigned gsmem = b->gsmem[k];
+        const long long ctas = std::min<long long>((long long)b->sms * b->per_sm[fam][smem_bucket(gsmem)], P.total);
         b->ctas = (int)ctas;
-        batch_kernel(fam)<<<(unsigned)ctas, kWarpsPerBlock * kWarp, b->smem, st>>>(P);
+        batch_kernel(fam)<<<(unsigned)ctas, kWarpsPerBlock * kWarp, gsmem, st>>>(P);
         VAM_CHECK_LAUNCH("k_batch");
     }
     return VAM_OK;
