@@ -124,8 +124,10 @@ int vam_parallel_set_tuning(vam_parallel_plan* plan, const vam_parallel_tuning* 
 int vam_parallel_get_tuning(vam_parallel_plan* plan, vam_parallel_tuning* tuning);
 
 /* Batched calls over many plans (targets of uneven size, different angle
- * counts, 2-D slices next to 3-D volumes) in ONE persistent launch fed by a
- * device work queue.  Each work item is one forward / backward_ref / adjoint
+ * counts, 2-D slices next to 3-D volumes) in persistent launches fed by
+ * device work queues: one launch per kernel-body family present in the list,
+ * each compiled with only that family's bodies (their registers, their
+ * occupancy).  Each work item is one forward / backward_ref / adjoint
  * call exactly as the single-plan entry points describe it, and produces
  * bit-identical results; items run concurrently, so no item may read another
  * item's output or write another item's input or output.  A fast forward in
@@ -133,7 +135,8 @@ int vam_parallel_get_tuning(vam_parallel_plan* plan, vam_parallel_tuning* tuning
  * per batch with VAM_OP_FORWARD.
  *
  * The calls' descriptions travel by value in the launch's parameters (48
- * calls per launch; longer lists become consecutive launches), so a submit
+ * calls per launch; longer lists and further families become consecutive
+ * launches on the stream), so a submit
  * makes no CUDA call but a counter reset and the launches: it is stream
  * ordered, allocates nothing and may be captured in a CUDA graph with any
  * list.  A batch object (its queue counters) is driven from one stream at a

@@ -1,8 +1,9 @@
-"""Many projector calls over many plans in one persistent launch.
+"""Many projector calls over many plans in persistent launches.
 
 ``ProjectionBatch`` binds ``vam_batch_*``: a list of (plan, op, input, output)
 calls -- targets of uneven size, 2-D slices next to 3-D volumes, different
-angle counts -- runs as ONE persistent kernel whose CTAs take the calls'
+angle counts -- runs as one persistent kernel per kernel-body family present
+(each compiled with only that family's bodies), whose CTAs take the calls'
 blocks from a device work queue, largest call first.  Each call computes
 exactly what the plan's own forward / backward_ref / adjoint computes
 (bit-identical), so a batch is a drop-in for running the targets one at a

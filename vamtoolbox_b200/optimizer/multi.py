@@ -4,7 +4,7 @@
 geometry, angle count, absorption and response options, exactly as
 ``BCLPNorm`` (vamtoolbox/optimizer/BCLP.py:277-534) runs it -- but issues the
 projections of all targets together: every iteration is one batched
-backprojection (all targets' g -> dose in one persistent launch), the
+backprojection (all targets' g -> dose in persistent launches), the
 per-target fused dose passes, one batched forward (all operands -> gradients),
 and the per-target clamped updates, all captured once in a CUDA graph.  Each
 target's sequence of operations is the one its own ``DeviceIteration`` issues,
