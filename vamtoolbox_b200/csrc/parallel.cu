@@ -2098,9 +2098,15 @@ extern "C" int vam_batch_submit(vam_batch* b, const vam_work* work, int32_t n, v
         P.counter = b->d_counter + k;
         std::memcpy(P.items, b->host.data() + g0, sizeof(Item) * (size_t)(g1 - g0));
         bool pre = false;
-        for (int i = 0; i < P.n; ++i) pre |= P.items[i].pre_in != nullptr;
+        long long pre_max = 0;
+        for (int i = 0; i < P.n; ++i) {
+            pre |= P.items[i].pre_in != nullptr;
+            if (P.items[i].pre_in) pre_max = std::max(pre_max, P.items[i].pre_npix * P.items[i].pre_nz);
+        }
         if (pre) {
-            k_batch_premask<<<dim3(64, (unsigned)P.n), 256, 0, st>>>(P);
+            // about 8 elements per thread for the largest call (blockIdx.y = call)
+            const long long gx = std::min<long long>(std::max<long long>((pre_max + 2047) / 2048, 1), 4096);
+            k_batch_premask<<<dim3((unsigned)gx, (unsigned)P.n), 256, 0, st>>>(P);
             VAM_CHECK_LAUNCH("k_batch_premask");
         }
         const int fam = b->fam[k];
