@@ -1279,12 +1279,9 @@ struct Item {
     unsigned gx, gy;  // the call's own grid (blocks of kWarpsPerBlock warps)
     unsigned smem;    // dynamic shared memory of the body
     int pre_nz;
-    long long tstart;  // first ticket of the call inside a batch
-    long long cost;    // samples the call evaluates (batch ordering and ticket sizes)
-    unsigned chunk;    // blocks of the call's grid per ticket
-    int family;        // body family (k_batch instances)
-    unsigned ntk;      // tickets of the call: ticket j covers blocks j, j + ntk, j + 2 ntk, ...
-    unsigned pad_;
+    long long tstart;  // first ticket (virtual block) of the call inside a batch launch
+    long long cost;    // estimated time of the call (batch ordering)
+    int family;        // body family (k_batch instances): a bit of the FAM mask
     // pre-pass of the fast forward in mask mode: pre_out = mask * pre_in
     const float* pre_in;
     const float* pre_mask;
@@ -1330,6 +1327,7 @@ int describe(vam_parallel_plan* plan, Op op, const float* in, float* out, Item& 
                 a.mask = nullptr;
             }
             it.kind = KF_2D;
+            it.family = 128;
             it.gx = (unsigned)((plan->nX + k2J - 1) / k2J);
             it.gy = (unsigned)plan->nA;
             it.smem = k2Smem;
@@ -1437,7 +1435,10 @@ __device__ __forceinline__ void fast_body(const Item& it, unsigned bx, unsigned 
             const FastArgs f = it.f;
             if (it.vz == 8) k_forward_fast_body<8, RAY>(f, bx, by);
             else k_forward_fast_body<4, RAY>(f, bx, by);
-        } else if (it.kind == KF_2D) {
+        }
+    }
+    if constexpr ((FAM & 128) != 0) {
+        if (it.kind == KF_2D) {
             const Args a = it.a;
             k_forward_2d_body<RAY>(a, bx, by);
         }
@@ -1466,8 +1467,8 @@ __device__ __forceinline__ void fast_body(const Item& it, unsigned bx, unsigned 
     }
 }
 
-// FAM: the body families this instance carries -- 1 the fast and 2-D
-// forwards, 2 the fast, batched and 2-D backprojections without per-ray
+// FAM: the body families this instance carries -- 1 the fast forward, 128
+// the 2-D forward, 2 the fast, batched and 2-D backprojections without per-ray
 // absorption, 4 adjoint, 8 the other backprojections (generic with occlusion
 // or per-ray absorption, fast with per-ray absorption), 16 the generic forward
 // with occlusion or per-ray absorption, 32 / 64 the generic forward /
@@ -1587,10 +1588,15 @@ int run(vam_parallel_plan* plan, Op op, const float* in, float* out, cudaStream_
 // Every call of a batch keeps its own grid; the calls' blocks are numbered
 // consecutively (largest call first) into virtual blocks, and each resident
 // CTA takes the next virtual block from a device counter (the work queue),
-// finds its call by binary search, copies the call's description into shared
-// memory and runs the call's body for that block.  Calls of uneven size (2-D
-// slices next to 3-D volumes, different angle counts) therefore fill the
-// device together instead of one after another.
+// finds its call by binary search and runs the call's body for that block.
+// Calls of uneven size (2-D slices next to 3-D volumes, different angle
+// counts) therefore fill the device together instead of one after another.
+// A ticket is one block, as in a direct launch: the resident CTAs work on one
+// window of consecutive blocks, whose sinogram or volume footprint stays in
+// L2 (tickets of several blocks spread over a call's grid multiplied the DRAM
+// reads of a 160^3 x 720 backprojection by 6.6); while at least two tickets
+// per CTA remain, each CTA fetches its next ticket while its current block
+// runs, which hides the counter's latency.
 // ---------------------------------------------------------------------------
 // The calls of one launch travel by value in the kernel's parameter space
 // (__grid_constant__, up to 32 KB): a CTA reads its call's description through
@@ -1599,45 +1605,58 @@ int run(vam_parallel_plan* plan, Op op, const float* in, float* out, cudaStream_
 constexpr int kBatchMaxItems = 48;
 struct BatchParams {
     int n;
-    long long total;  // tickets
-    unsigned long long* counter;
+    unsigned total;  // tickets (virtual blocks) of the launch, < 2^31
+    unsigned* counter;
     Item items[kBatchMaxItems];
 };
+
+// the last call of a launch whose first ticket is <= t
+__device__ __forceinline__ int batch_find(const BatchParams& P, unsigned t) {
+    int lo = 0, hi = P.n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (P.items[mid].tstart <= (long long)t) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
 static_assert(sizeof(BatchParams) < 32000, "batch parameters must fit the 32 KB kernel parameter space");
 
-// The lean backprojections fit 48 registers, the fast and 2-D forwards and
-// the lean generic backprojection 64, so those instances ask for five and
-// four resident CTAs per SM; the others keep 80 (no spills).
+// Resident CTAs per SM each instance asks for, i.e. its register cap: the
+// lean generic backprojection fits 40 registers (six CTAs, as its direct
+// kernel: a 160^3 x 720 call ran 1.36x longer at four), the fast and 2-D
+// backprojections and the 2-D forward 48 (five), the fast forward and the
+// lean generic forward 64 (four); the heavy instances keep 80.
 template <int FAM>
-__global__ void __launch_bounds__(256, FAM == 2 ? 5 : (FAM == 1 || FAM == 64 ? 4 : 3))
+__global__ void __launch_bounds__(256, FAM == 64 ? 6 : (FAM == 2 || FAM == 128 ? 5 : (FAM == 1 || FAM == 32 ? 4 : 3)))
     k_batch(const __grid_constant__ BatchParams P) {
-    __shared__ long long s_t;
-    __shared__ int s_idx;
-    for (;;) {
-        if (threadIdx.x == 0) {
-            const long long t = (long long)atomicAdd(P.counter, 1ULL);
-            int lo = 0, hi = P.n - 1;  // the last call whose first ticket is <= t
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (P.items[mid].tstart <= t) lo = mid;
-                else hi = mid - 1;
-            }
-            s_t = t;
-            s_idx = lo;
-        }
-        __syncthreads();
-        const long long t = s_t;
-        const int idx = s_idx;
-        __syncthreads();  // s_t / s_idx are rewritten next round
+    __shared__ unsigned s_t[2];
+    __shared__ int s_idx[2];
+    if (threadIdx.x == 0) {
+        const unsigned t = atomicAdd(P.counter, 1u);
+        s_t[0] = t;
+        s_idx[0] = t < P.total ? batch_find(P, t) : 0;
+    }
+    __syncthreads();
+    // s_t / s_idx alternate between two slots: slot s is read at the top of a round, slot s ^ 1 is
+    // written at its end, and the barrier closing the round orders both
+    for (int s = 0;; s ^= 1) {
+        const unsigned t = s_t[s];
         if (t >= P.total) return;  // uniform: every thread read the same s_t
-        const Item& it = P.items[idx];
-        const unsigned gx = it.gx, nb = it.gx * it.gy;  // a call's grid has < 2^32 blocks
-        // strided blocks: the CTAs holding consecutive tickets work on neighbouring blocks of the
-        // call's grid at any moment, as a direct launch's resident blocks do (L2 reuse)
-        for (unsigned b = (unsigned)(t - it.tstart); b < nb; b += it.ntk) {
-            item_body<FAM>(it, b % gx, b / gx);
-            if (it.smem) __syncthreads();  // the next block restages the body's shared memory
+        // the next ticket is fetched while the block runs, except near the end of the queue, where
+        // a CTA holding two tickets would run both blocks back to back while others find none
+        const bool early = t + 2u * gridDim.x < P.total;
+        unsigned next = 0;
+        if (threadIdx.x == 0 && early) next = atomicAdd(P.counter, 1u);
+        const Item& it = P.items[s_idx[s]];
+        const unsigned b = t - (unsigned)it.tstart;  // a call's grid has < 2^31 blocks
+        item_body<FAM>(it, b % it.gx, b / it.gx);
+        if (threadIdx.x == 0) {
+            if (!early) next = atomicAdd(P.counter, 1u);
+            s_t[s ^ 1] = next;
+            s_idx[s ^ 1] = next < P.total ? batch_find(P, next) : 0;
         }
+        __syncthreads();  // also: the next block restages the body's shared memory
     }
 }
 
@@ -1651,7 +1670,8 @@ BatchKernel batch_kernel(int fam) {
         case 16: return k_batch<16>;
         case 32: return k_batch<32>;
         case 64: return k_batch<64>;
-        default: return k_batch<127>;
+        case 128: return k_batch<128>;
+        default: return k_batch<255>;
     }
 }
 
@@ -1897,7 +1917,7 @@ extern "C" int vam_parallel_adjoint(vam_parallel_plan* p, const float* sino, flo
 // batches
 // ---------------------------------------------------------------------------
 // launches (ticket counters) one list may need: 48 calls per launch, and one
-// more launch at each of the <= 6 changes of body family
+// more launch at each of the <= 7 changes of body family
 constexpr int kBatchMaxLaunches = 80;
 
 // dynamic shared-memory sizes the batch kernels' residency is tabulated for
@@ -1911,9 +1931,9 @@ inline int smem_bucket(unsigned smem) {
 
 struct vam_batch {
     int device;
-    unsigned long long* d_counter;
+    unsigned* d_counter;
     int sms;
-    int per_sm[128][4];        // resident CTAs per SM of k_batch<fam> (fam 1 .. 64, 127) per
+    int per_sm[256][4];        // resident CTAs per SM of k_batch<fam> (fam 1 .. 128, 255) per
                                // dynamic shared-memory bucket (kSmemBuckets)
     std::vector<Item> host;    // the described calls of the last list, in queue order
     std::vector<int> group;    // first call of each launch (kBatchMaxItems calls per launch)
@@ -1934,12 +1954,12 @@ extern "C" int vam_batch_create(int32_t device, vam_batch** out) {
     VAM_REQUIRE(g.ok, VAM_ERR_CUDA, "vam_batch_create: cannot select device");
     int sms = 0;
     VAM_TRY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-    int per_sm[128][4] = {};
+    int per_sm[256][4] = {};
     // residency for each dynamic shared-memory bucket up to the largest a call may ask for (48 KB,
     // the batched backprojection's trig table), queried once here, so a list never needs a
     // runtime query (which would not be allowed during graph capture); the opt-in limit is
     // raised first, as 48 KB plus the kernel's static shared memory exceeds the default
-    for (int fam : {1, 2, 4, 8, 16, 32, 64, 127}) {
+    for (int fam : {1, 2, 4, 8, 16, 32, 64, 128, 255}) {
         VAM_TRY_CUDA(cudaFuncSetAttribute(batch_kernel(fam), cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
         for (int k = 0; k < 4; ++k) {
             VAM_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[fam][k], batch_kernel(fam),
@@ -1955,7 +1975,7 @@ extern "C" int vam_batch_create(int32_t device, vam_batch** out) {
     b->smem = 0;
     b->any_pre = 0;
     b->ctas = 0;
-    const cudaError_t e = cudaMalloc(&b->d_counter, sizeof(unsigned long long) * kBatchMaxLaunches);
+    const cudaError_t e = cudaMalloc(&b->d_counter, sizeof(unsigned) * kBatchMaxLaunches);
     if (e != cudaSuccess) {
         delete b;
         return set_error(VAM_ERR_NOMEM, std::string("vam_batch_create: ") + cudaGetErrorString(e));
@@ -1976,8 +1996,8 @@ namespace vam {
 namespace {
 // Relative time per sample of each body (fast forward = 1), measured on
 // B200: the generic kernels gather fewer samples per second than the fast
-// ones, and a single slice (nZ = 1) far fewer, so tickets are sized in
-// estimated time, not in samples.
+// ones, and a single slice (nZ = 1) far fewer, so a batch orders its calls
+// (longest first) by estimated time, not by samples.
 double time_weight(const Item& it) {
     const bool slice = it.a.nZ == 1 || it.f.nZ == 1;
     switch (it.kind) {
@@ -1993,7 +2013,7 @@ double time_weight(const Item& it) {
     }
 }
 
-// describe every call, order the queue, size the tickets; no CUDA call
+// describe every call, order the queue, number the tickets; no CUDA call
 int batch_prepare(vam_batch* b, const vam_work* work, int32_t n) {
     VAM_REQUIRE(n <= kBatchMaxItems * 64, VAM_ERR_SHAPE, "vam_batch: at most 3072 calls per list");
     std::vector<Item> items((size_t)n);
@@ -2012,7 +2032,7 @@ int batch_prepare(vam_batch* b, const vam_work* work, int32_t n) {
         if (d.kind == KB_GEN) items[i].family = gen_heavy ? 8 : 64;
         else if (d.family == 2 && d.ray) items[i].family = 8;
         if (d.kind == KF_GEN) items[i].family = gen_heavy ? 16 : 32;
-        VAM_REQUIRE((long long)items[i].gx * items[i].gy < (1LL << 32), VAM_ERR_SHAPE, "vam_batch: call grid too large");
+        VAM_REQUIRE((long long)items[i].gx * items[i].gy < (1LL << 31), VAM_ERR_SHAPE, "vam_batch: call grid too large");
         items[i].cost = (long long)std::llround((double)items[i].cost * time_weight(items[i]));
     }
     // one launch per body family (each with the narrowest instance and its occupancy), and
@@ -2031,32 +2051,24 @@ int batch_prepare(vam_batch* b, const vam_work* work, int32_t n) {
         g1 = g0 + 1;
         while (g1 < n && g1 - g0 < kBatchMaxItems && items[g1].family == items[g0].family) ++g1;
         int fam = 0;
-        long long cost = 0;
         unsigned gsmem = 0;
         for (int i = g0; i < g1; ++i) {
             fam |= items[i].family;
-            cost += std::max(items[i].cost, 1LL);
             gsmem = std::max(gsmem, items[i].smem);
             b->any_pre |= items[i].pre_in != nullptr;
         }
         b->smem = std::max(b->smem, gsmem);
-        if (fam != 1 && fam != 2 && fam != 4 && fam != 8 && fam != 16 && fam != 32 && fam != 64) fam = 127;
-        // tickets: about 8 per resident CTA over the launch, each call's share proportional to
-        // its samples; a ticket is every ntk-th block of one call from its index on
-        const double want = 8.0 * b->sms * b->per_sm[fam][smem_bucket(gsmem)];
+        if (fam & (fam - 1)) fam = 255;  // one family per launch; the all-bodies instance otherwise
+        // tickets: one per block of each call's grid, the calls one after another
         long long total = 0;
         for (int i = g0; i < g1; ++i) {
             Item& it = items[i];
             const long long nb = (long long)it.gx * it.gy;
-            long long tk = (long long)std::llround(want * (double)std::max(it.cost, 1LL) / (double)cost);
-            tk = std::max(1LL, std::min(tk, nb));
-            it.chunk = (unsigned)((nb + tk - 1) / tk);
-            tk = (nb + it.chunk - 1) / it.chunk;
-            it.ntk = (unsigned)tk;
             it.tstart = total;
-            total += tk;
+            total += nb;
             b->blocks += nb;
         }
+        VAM_REQUIRE(total < (1LL << 31), VAM_ERR_SHAPE, "vam_batch: more than 2^31 blocks in one launch");
         b->group.push_back(g0);
         b->tickets.push_back(total);
         b->fam.push_back(fam);
@@ -2085,7 +2097,7 @@ extern "C" int vam_batch_submit(vam_batch* b, const vam_work* work, int32_t n, v
     const int rc = batch_prepare(b, work, n);
     if (rc != VAM_OK) return rc;
     const int groups = (int)b->group.size();
-    VAM_TRY_CUDA(cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long) * groups, st));
+    VAM_TRY_CUDA(cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned) * groups, st));
     static BatchParams P;  // 15 KB: too large for the stack of every caller thread
     static std::mutex mu;
     std::lock_guard<std::mutex> lock(mu);
@@ -2094,7 +2106,7 @@ extern "C" int vam_batch_submit(vam_batch* b, const vam_work* work, int32_t n, v
         const int g1 = k + 1 < groups ? b->group[k + 1] : n;
         std::memset(&P, 0, sizeof(P));
         P.n = g1 - g0;
-        P.total = b->tickets[k];
+        P.total = (unsigned)b->tickets[k];
         P.counter = b->d_counter + k;
         std::memcpy(P.items, b->host.data() + g0, sizeof(Item) * (size_t)(g1 - g0));
         bool pre = false;
