@@ -128,6 +128,39 @@ def test_batch_long_list_spans_launches():
         assert torch.equal(rb, ox) and torch.equal(ra, oa)
 
 
+def test_batch_large_calls_bitwise():
+    """Calls large enough for the 2-D tile bodies (forward from 192 px, backprojection from 320 px), the
+    generic 3-D bodies at nZ = 160 and the fast ones, with more blocks than resident CTAs, so the CTAs
+    fetch their next ticket while a block runs and switch to one ticket at a time near the end."""
+    rng = np.random.default_rng(7)
+    plans = []
+    for shape, na, mode in [((256, 256, 1), 90, "mask"), ((352, 352, 1), 60, None),
+                            ((96, 96, 160), 40, "mask"), ((64, 64, 96), 120, None)]:
+        p = ParallelPlan(shape[0], shape[1], shape[2], np.linspace(0, 360, na, endpoint=False))
+        if mode == "mask":
+            p.set_absorption("mask", mask=rng.uniform(0.3, 1.0, shape[:2]))
+        x = torch.as_tensor(rng.uniform(0, 1, shape), dtype=torch.float32, device="cuda")
+        b = torch.as_tensor(rng.uniform(0, 1, p.shape_sino), dtype=torch.float32, device="cuda")
+        plans.append((p, x, b))
+    ref = [(p.forward(x), p.backward_ref(b)) for p, x, b in plans]
+    batch = ProjectionBatch()
+    work, outs = [], []
+    for p, x, b in plans:
+        ob, ox = torch.full_like(b, np.nan), torch.full_like(x, np.nan)
+        work += [(p, "forward", x, ob), (p, "backward_ref", b, ox)]
+        outs.append((ob, ox))
+    for _ in range(2):  # a resubmission reuses the prepared list
+        batch.submit(work)
+        torch.cuda.synchronize()
+        for (rf, rb), (of, ob) in zip(ref, outs):
+            assert torch.equal(rf, of)
+            assert torch.equal(rb, ob)
+        for o in outs:
+            for t in o:
+                t.fill_(np.nan)
+    assert batch.info()["virtual_blocks"] > 2 * 148 * 6
+
+
 def test_batch_rejects_bad_work():
     plans = make_plans(3)
     batch = ProjectionBatch()
