@@ -135,12 +135,15 @@ int vam_parallel_get_tuning(vam_parallel_plan* plan, vam_parallel_tuning* tuning
  * per batch with VAM_OP_FORWARD.
  *
  * The calls' descriptions travel by value in the launch's parameters (48
- * calls per launch; longer lists and further families become consecutive
- * launches on the stream), so a submit
- * makes no CUDA call but a counter reset and the launches: it is stream
- * ordered, allocates nothing and may be captured in a CUDA graph with any
- * list.  A batch object (its queue counters) is driven from one stream at a
- * time.
+ * calls per launch; longer lists and further families become further
+ * launches), so a submit makes no CUDA call but a counter reset, the launches
+ * and an event fork / join: the launches after the first run on up to three
+ * streams the batch owns, forked from the caller's stream and joined back to
+ * it before the submit returns, so each launch fills the SMs the previous
+ * one's tail frees.  A submit is therefore ordered on the caller's stream,
+ * allocates nothing and may be captured in a CUDA graph with any list.  A
+ * batch object (its queue counters and streams) is driven from one stream at
+ * a time.
  *
  * Replaces running the reference's per-target projector calls one target at a
  * time (vamtoolbox/projector/Projector3DParallel.py:113-207 per target). */

@@ -1923,6 +1923,10 @@ constexpr int kBatchMaxLaunches = 80;
 // dynamic shared-memory sizes the batch kernels' residency is tabulated for
 constexpr unsigned kSmemBuckets[4] = {0u, 16u * 1024, 40u * 1024, 48u * 1024};
 
+// streams of a batch besides the caller's: the launches of one list run on up to
+// kBatchSide + 1 streams, forked from and joined to the caller's stream
+constexpr int kBatchSide = 3;
+
 inline int smem_bucket(unsigned smem) {
     int k = 0;
     while (k < 3 && kSmemBuckets[k] < smem) ++k;
@@ -1944,7 +1948,20 @@ struct vam_batch {
     unsigned smem;
     int any_pre;
     int ctas;                  // persistent CTAs of the last launch
+    cudaStream_t side[kBatchSide];  // non-blocking streams for the launches after the first
+    cudaEvent_t fork;               // recorded on the caller's stream before the launches
+    cudaEvent_t join[kBatchSide];   // recorded on each side stream after its launches
 };
+
+static void batch_release(vam_batch* b) {
+    for (int s = 0; s < kBatchSide; ++s) {
+        if (b->side[s]) cudaStreamDestroy(b->side[s]);
+        if (b->join[s]) cudaEventDestroy(b->join[s]);
+    }
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->d_counter) cudaFree(b->d_counter);
+    delete b;
+}
 
 extern "C" int vam_batch_create(int32_t device, vam_batch** out) {
     clear_error();
@@ -1975,10 +1992,22 @@ extern "C" int vam_batch_create(int32_t device, vam_batch** out) {
     b->smem = 0;
     b->any_pre = 0;
     b->ctas = 0;
-    const cudaError_t e = cudaMalloc(&b->d_counter, sizeof(unsigned) * kBatchMaxLaunches);
+    b->d_counter = nullptr;
+    b->fork = nullptr;
+    for (int s = 0; s < kBatchSide; ++s) b->side[s] = nullptr, b->join[s] = nullptr;
+    cudaError_t e = cudaMalloc(&b->d_counter, sizeof(unsigned) * kBatchMaxLaunches);
     if (e != cudaSuccess) {
-        delete b;
+        batch_release(b);
         return set_error(VAM_ERR_NOMEM, std::string("vam_batch_create: ") + cudaGetErrorString(e));
+    }
+    e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+    for (int s = 0; s < kBatchSide && e == cudaSuccess; ++s) {
+        e = cudaStreamCreateWithFlags(&b->side[s], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join[s], cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) {
+        batch_release(b);
+        return set_error(VAM_ERR_CUDA, std::string("vam_batch_create: ") + cudaGetErrorString(e));
     }
     *out = b;
     return VAM_OK;
@@ -1987,8 +2016,7 @@ extern "C" int vam_batch_create(int32_t device, vam_batch** out) {
 extern "C" int vam_batch_destroy(vam_batch* b) {
     if (!b) return VAM_OK;
     DeviceGuard g(b->device);
-    cudaFree(b->d_counter);
-    delete b;
+    batch_release(b);
     return VAM_OK;
 }
 
@@ -2088,20 +2116,15 @@ extern "C" int vam_batch_prepare(vam_batch* b, const vam_work* work, int32_t n, 
     return batch_prepare(b, work, n);
 }
 
-extern "C" int vam_batch_submit(vam_batch* b, const vam_work* work, int32_t n, vam_stream_t stream) {
-    clear_error();
-    VAM_REQUIRE(b && work && n > 0, VAM_ERR_ARG, "vam_batch_submit: null argument or empty work list");
-    DeviceGuard g(b->device);
-    VAM_REQUIRE(g.ok, VAM_ERR_CUDA, "vam_batch_submit: cannot select device");
-    cudaStream_t st = (cudaStream_t)stream;
-    const int rc = batch_prepare(b, work, n);
-    if (rc != VAM_OK) return rc;
+namespace vam {
+namespace {
+int batch_launch(vam_batch* b, int n, cudaStream_t st0, int lanes) {
     const int groups = (int)b->group.size();
-    VAM_TRY_CUDA(cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned) * groups, st));
     static BatchParams P;  // 15 KB: too large for the stack of every caller thread
     static std::mutex mu;
     std::lock_guard<std::mutex> lock(mu);
     for (int k = 0; k < groups; ++k) {
+        cudaStream_t st = k % lanes == 0 ? st0 : b->side[k % lanes - 1];
         const int g0 = b->group[k];
         const int g1 = k + 1 < groups ? b->group[k + 1] : n;
         std::memset(&P, 0, sizeof(P));
@@ -2129,6 +2152,35 @@ extern "C" int vam_batch_submit(vam_batch* b, const vam_work* work, int32_t n, v
         VAM_CHECK_LAUNCH("k_batch");
     }
     return VAM_OK;
+}
+}  // namespace
+}  // namespace vam
+
+extern "C" int vam_batch_submit(vam_batch* b, const vam_work* work, int32_t n, vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(b && work && n > 0, VAM_ERR_ARG, "vam_batch_submit: null argument or empty work list");
+    DeviceGuard g(b->device);
+    VAM_REQUIRE(g.ok, VAM_ERR_CUDA, "vam_batch_submit: cannot select device");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int rc = batch_prepare(b, work, n);
+    if (rc != VAM_OK) return rc;
+    const int groups = (int)b->group.size();
+    VAM_TRY_CUDA(cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned) * groups, st));
+    // Launch k runs on stream k mod lanes (the caller's stream, then the batch's own ones), forked
+    // from and joined to the caller's stream: the calls of a list are independent, so the next
+    // launch's CTAs take the SMs that the previous one's tail frees instead of waiting for its end.
+    const int lanes = std::min(groups, kBatchSide + 1);
+    if (lanes > 1) {
+        VAM_TRY_CUDA(cudaEventRecord(b->fork, st));
+        for (int s = 0; s + 1 < lanes; ++s) VAM_TRY_CUDA(cudaStreamWaitEvent(b->side[s], b->fork, 0));
+    }
+    const int rc_launch = batch_launch(b, n, st, lanes);
+    // joined even after a failed launch, so a stream capture never ends with a side stream forked
+    for (int s = 0; s + 1 < lanes; ++s) {
+        VAM_TRY_CUDA(cudaEventRecord(b->join[s], b->side[s]));
+        VAM_TRY_CUDA(cudaStreamWaitEvent(st, b->join[s], 0));
+    }
+    return rc_launch;
 }
 
 extern "C" int vam_batch_info(vam_batch* b, int64_t* virtual_blocks, int32_t* ctas) {

@@ -24,8 +24,10 @@ class MultiTargetBCLP:
 
     schedule:
       "persistent" -- per iteration one batched backprojection and one batched
-                      forward, each a single persistent launch over all targets
-                      (vam_batch_submit), with the per-target fused passes between;
+                      forward over all targets (vam_batch_submit: a persistent
+                      launch per kernel-body family, the families on forked
+                      streams), with the per-target fused passes between, each
+                      on its target's stream;
       "streams"    -- each target's whole iteration chain on its own stream inside
                       the graph, so the hardware interleaves the targets' own
                       specialised kernels with no barrier between phases;
@@ -59,17 +61,25 @@ class MultiTargetBCLP:
             self.schedule = self._pick()
 
     # -- persistent schedule: phases over all targets
+    # (the per-target passes between the batched launches run on the targets' own streams, so
+    # the small ones overlap instead of queueing one after another)
     def state(self):
         self.back.submit(self.back_work)
-        for it in self.its:
-            it.ws.bclp_dose_pass(it.dose, it.fT, it.prm, it.mapped, it.operand, it.stats)
-            it.ws.append(it.stats, it.log, it.counter)
+        self._fork_join(self._dose)
 
     def update(self):
         self.fwd.submit(self.fwd_work)
-        for it in self.its:
-            b = it.bclp
-            it.ws.bclp_update(it.g, it.grad, b.learning_rate, b.p, b.q, b.glb, b.gub, it.stats)
+        self._fork_join(self._update)
+
+    @staticmethod
+    def _dose(it):
+        it.ws.bclp_dose_pass(it.dose, it.fT, it.prm, it.mapped, it.operand, it.stats)
+        it.ws.append(it.stats, it.log, it.counter)
+
+    @staticmethod
+    def _update(it):
+        b = it.bclp
+        it.ws.bclp_update(it.g, it.grad, b.learning_rate, b.p, b.q, b.glb, b.gub, it.stats)
 
     # -- streams schedule: one chain per target, forked from and joined to the current stream
     def _fork_join(self, fn):
