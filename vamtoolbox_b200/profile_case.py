@@ -5,6 +5,7 @@
     python -m vamtoolbox_b200.profile_case ray --size 96 --angles 120 --calls 1
     python -m vamtoolbox_b200.profile_case formats --size 256 --angles 120 --calls 1
     python -m vamtoolbox_b200.profile_case vec --size 128 --angles 90 --incline 15
+    python -m vamtoolbox_b200.profile_case batch --calls 1 --direct
 
 ``parallel`` runs forward, reference-parity backprojection and the matched
 adjoint (after building its weight table) on a random N x N x N volume with
@@ -15,12 +16,16 @@ of the curved-ray tracer through a graded-index, attenuating N^3 medium
 projector frames (99.5th-percentile normalisation: select, then the frame
 kernel) and rebins it for a 300 px fan-beam vial; ``vec`` runs the
 vector-geometry (ASTRA-model) forward and backprojection of an N^3 volume
-with rays inclined by ``incline`` degrees.  Each
+with rays inclined by ``incline`` degrees; ``batch`` submits the backprojections,
+then the forwards, of 16 uneven calls (8 slices of 128^2-512^2 and 8 volumes
+of 64^3-160^3, 180 / 360 / 720 angles, mask absorption) as two
+batched lists (vam_batch_submit), and with ``--direct`` then runs the same
+calls one by one.  Each
 kernel runs ``calls`` times; inputs are seeded; nothing is timed or printed
 but a one-line summary, so a profiler's launch filter (kernel name regex plus
 launch count) selects exactly the launches it wants.  The 256^3 x 360
 parallel case holds about 0.9 GB on the device, the 96^3 ray case about 0.1 GB,
-the 256 x 120 x 256 formats case about 0.4 GB.
+the 256 x 120 x 256 formats case about 0.4 GB, the batch case about 0.5 GB.
 """
 from __future__ import annotations
 
@@ -135,9 +140,45 @@ def run_vec(n, na, calls, incline):
     return f"vec {n}^3 x {na} incline {incline}: {p.info()}"
 
 
+def run_batch(calls, direct, seed=5):
+    """The shapes and angle counts of the 16-target multi-target workload (the same seeded draws), with
+    random inputs and a random absorption mask per call (every target of that workload absorbs)."""
+    from .batch import ProjectionBatch
+    from .projector.Projector3DParallel import ParallelPlan
+
+    rng = np.random.default_rng(seed)
+    g = torch.Generator(device="cuda").manual_seed(0)
+    back, fwd = [], []
+    for k in range(16):
+        two_d = k < 8
+        n = int(rng.choice([128, 256, 384, 512] if two_d else [64, 96, 128, 160]))
+        na = int(rng.choice([180, 360, 720]))
+        alpha = float(rng.uniform(0.0, 1.0 / n))  # per pixel: up to e^-1 across the container
+        rng.uniform()  # binary / grayscale draw of the workload (no effect on the projections)
+        nz = 1 if two_d else n
+        p = ParallelPlan(n, n, nz, np.linspace(0, 360, na, endpoint=False))
+        mrng = np.random.default_rng(100 + k)
+        p.set_absorption("mask", mask=np.exp(-alpha * mrng.uniform(0.0, n, (n, n))))
+        x = torch.rand((n, n, nz), device="cuda", generator=g)
+        b = torch.rand((n, na, nz), device="cuda", generator=g)
+        back.append((p, "backward_ref", b, torch.empty_like(x)))
+        fwd.append((p, "forward", x, torch.empty_like(b)))
+    bb, bf = ProjectionBatch(), ProjectionBatch()
+    for _ in range(calls):
+        bb.submit(back)
+        bf.submit(fwd)
+        if direct:
+            for p, _, i, o in back:
+                p.backward_ref(i, o)
+            for p, _, i, o in fwd:
+                p.forward(i, o)
+    torch.cuda.synchronize()
+    return f"batch: 16 uneven calls x (backward_ref, forward), {calls} submit(s){', then direct' if direct else ''}"
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
-    ap.add_argument("case", choices=["parallel", "ray", "formats", "vec", "summarize"])
+    ap.add_argument("case", choices=["parallel", "ray", "formats", "vec", "batch", "summarize"])
     ap.add_argument("csv", nargs="?", help="summarize: the ncu --csv launch list")
     ap.add_argument("--size", type=int, default=None)
     ap.add_argument("--angles", type=int, default=None)
@@ -145,6 +186,7 @@ def main(argv=None):
     ap.add_argument("--slices", type=int, default=None, help="parallel case: nZ (default: size; 1 = a 2-D slice)")
     ap.add_argument("--incline", type=float, default=15.0, help="vec case: ray inclination in degrees")
     ap.add_argument("--tuning", default="", help="comma list key=value of launch shapes (parallel case)")
+    ap.add_argument("--direct", action="store_true", help="batch case: also run every call on its own")
     a = ap.parse_args(argv)
     if a.case == "summarize":
         print(summarize_launches(a.csv))
@@ -155,6 +197,8 @@ def main(argv=None):
         print(run_parallel(a.size or 256, a.angles or 360, a.calls, tuning, a.slices))
     elif a.case == "vec":
         print(run_vec(a.size or 128, a.angles or 90, a.calls, a.incline))
+    elif a.case == "batch":
+        print(run_batch(a.calls, a.direct))
     elif a.case == "formats":
         print(run_formats(a.size or 256, a.angles or 120, a.calls))
     else:
