@@ -106,3 +106,110 @@ def test_lost_rank_surfaces_as_error_not_hang():
     for p in procs:
         p.join(timeout=60)
     assert out != "completed"
+
+
+# ---------------------------------------------------------------------------
+# ray tracer: angle shards (every rank traces a block of angles, sums its deposit)
+# ---------------------------------------------------------------------------
+def _ray_case():
+    """A small graded-index, attenuating 3-D medium on the reference's coordinate grid."""
+    n, nz = 10, 4
+    xv = np.linspace(-(n - 1) / 2, (n - 1) / 2, n) * 0.002
+    zv = np.linspace(-(nz - 1) / 2, (nz - 1) / 2, nz) * 0.002
+    xg, yg, zg = np.meshgrid(xv, xv, zv, indexing="ij")
+    r2 = (xg ** 2 + yg ** 2) / (xv.max() ** 2)
+    nfield = 1.5 + 0.02 * r2 + 0.003 * np.sin(7 * xg / xv.max() + 3 * zg / zv.max())
+    alpha = 40.0 * (1 + 0.3 * np.cos(5 * yg / xv.max()))
+    angles = np.linspace(0, 360, 7, endpoint=False)
+    kw = dict(step_size=(xv[1] - xv[0]) / 2, max_num_step=3 * n, n_kind=1, n_grid=nfield, a_kind=3,
+              a_grid=alpha, absorb=alpha)
+    return dict(xv=xv, yv=xv, zv=zv), angles, kw
+
+
+def _ray_worker(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        from oracle import oracle as O
+        from vamtoolbox_b200.distributed import angle_range, dose_allreduce, ray_indices
+
+        grid, angles, kw = _ray_case()
+        a0, a1 = angle_range(angles.size, world, rank)
+        x0, v0, shape = O.setup_rays_parallel(grid["xv"], grid["yv"], grid["zv"], angles[a0:a1])
+        n_rays = shape[0] * angles.size * shape[2]
+        idx = ray_indices(shape[0], angles.size, shape[2], a0, a1)
+        g_all = np.random.default_rng(3).uniform(0, 1, n_rays).astype(np.float32)
+        f = np.random.default_rng(4).uniform(0, 1, (grid["xv"].size, grid["yv"].size, grid["zv"].size))
+        rows, _ = O.ray_trace("integrate", grid, x0, v0, 1.0, f=f, **kw)  # this rank's sinogram rows
+        dose, _ = O.ray_trace("deposit", grid, x0, v0, 1.0, g=g_all[idx], **kw)
+        dt = torch.as_tensor(dose)
+        dose_allreduce(dt)
+        q.put((rank, x0, idx, rows, dt.numpy()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_angle_shards_cover_every_ray_once():
+    from vamtoolbox_b200.distributed import angle_range, ray_indices
+
+    for n_det, na, nz in ((5, 7, 3), (8, 360, 1), (4, 3, 6)):
+        for world in (1, 2, 3):
+            if world > na:
+                continue
+            got = np.concatenate([ray_indices(n_det, na, nz, *angle_range(na, world, r)) for r in range(world)])
+            assert np.array_equal(np.sort(got), np.arange(n_det * na * nz))
+
+
+def test_two_rank_ray_shards_equal_single_process():
+    """Each rank's rays and integrated sinogram rows are the single-process ones at ray_indices, and the
+    summed partial deposits equal the single-process deposit (float64 oracle)."""
+    from oracle import oracle as O
+
+    world = 2
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_ray_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=180) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    grid, angles, kw = _ray_case()
+    x0, v0, shape = O.setup_rays_parallel(grid["xv"], grid["yv"], grid["zv"], angles)
+    n_rays = shape[0] * angles.size * shape[2]
+    g_all = np.random.default_rng(3).uniform(0, 1, n_rays).astype(np.float32)
+    f = np.random.default_rng(4).uniform(0, 1, (grid["xv"].size, grid["yv"].size, grid["zv"].size))
+    sino, _ = O.ray_trace("integrate", grid, x0, v0, 1.0, f=f, **kw)
+    dose, _ = O.ray_trace("deposit", grid, x0, v0, 1.0, g=g_all, **kw)
+    assert dose.max() > 0
+    for _, x0_r, idx, rows, dose_sum in res:
+        assert np.array_equal(x0_r, x0[idx])
+        assert np.array_equal(rows, sino[idx])
+        assert np.allclose(dose_sum, dose, rtol=1e-12, atol=1e-14)
+
+
+def test_target_shards_balance_and_cover():
+    from vamtoolbox_b200.distributed import target_shards
+
+    rng = np.random.default_rng(5)
+    costs = rng.choice([64 ** 3, 96 ** 3, 128 ** 3, 160 ** 3], 16) * rng.choice([180, 360, 720], 16)
+    for world in (1, 2, 3, 8):
+        shards = target_shards(costs, world)
+        assert sorted(i for s in shards for i in s) == list(range(16))
+        loads = [sum(costs[i] for i in s) for s in shards]
+        # longest-processing-time first: within 4/3 of the ideal share or one target of it
+        assert max(loads) <= max(4 / 3 * sum(costs) / world, max(costs)) + 1e-9
+        assert shards == target_shards(costs, world)  # deterministic
+
+
+def test_shard_angles_splits_the_geometry():
+    from vamtoolbox_b200 import geometry
+    from vamtoolbox_b200.distributed import shard_angles
+
+    pg = geometry.ProjectionGeometry(np.linspace(0, 360, 9, endpoint=False), "ray_trace", CUDA=True)
+    parts = [shard_angles(pg, 2, r) for r in range(2)]
+    assert np.array_equal(np.concatenate([p.angles for p in parts]), pg.angles)
+    assert [p.n_angles for p in parts] == [5, 4]
+    assert pg.n_angles == 9 and parts[0] is not pg
