@@ -520,8 +520,10 @@ __device__ __forceinline__ double rebin_sample(const double (&x)[4], bool inb, d
 
 // One warp per output row (p, a), lanes along z, four z per lane in flight
 // (16 loads); eight rows per block.
+// four resident CTAs per SM (64 registers, a few spilled bytes; three at 72-75): 0.083 -> 0.076 ms for
+// a float64 256 x 120 x 256 sinogram, identical results
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_rebin_fan(const T* __restrict__ in, T* __restrict__ out,
+__global__ void __launch_bounds__(kThreads, 4) k_rebin_fan(const T* __restrict__ in, T* __restrict__ out,
                                                         const RebinArgs p) {
     const int lane = threadIdx.x & 31;
     const long long row = (long long)blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);   // pp * nA + a
