@@ -122,3 +122,16 @@ def test_angle_shards_reproduce_the_full_run(golden):
         assert np.array_equal(Pr.forward_t(f).cpu().numpy(), full_rows[idx])
         dose += Pr.backward_t(w[torch.as_tensor(idx, device="cuda")]).double()
     assert float((dose - full_dose).norm() / full_dose.norm()) < 1e-5
+
+
+def test_integrate_is_bitwise_repeatable(golden):
+    """The integrate has no atomics (one thread per ray, fixed sample order): repeated calls, and a
+    call after a deposit has reused the plan's scratch field, give identical bits."""
+    R = golden["raytrace"]
+    P = make_prop(R, "r3")
+    f = torch.as_tensor(np.random.default_rng(8).uniform(size=P.plan.grid_shape), device="cuda", dtype=torch.float32)
+    first = P.forward_t(f).clone()
+    for _ in range(3):
+        assert torch.equal(P.forward_t(f), first)
+    P.backward_t(torch.ones(P.plan.num_rays, device="cuda"))
+    assert torch.equal(P.forward_t(f), first)
