@@ -70,6 +70,25 @@ def test_disk_sinogram_known_answer():
     assert np.allclose(b[:, 0], b[:, 2], rtol=0, atol=1e-12)
 
 
+def test_ray_absorption_disk_known_answer():
+    """Straight-ray transmission: with the per-ray weight exp(-alpha (s - s_entry)), s_entry =
+    -sqrt(R^2 - t^2), a centred uniform disk of radius rho projects to
+    exp(-alpha sqrt(R^2 - t^2)) 2 sinh(alpha sqrt(rho^2 - t^2)) / alpha."""
+    n, rho, R, alpha = 128, 40.0, 56.0, 0.02
+    yy, xx = np.mgrid[:n, :n] - n // 2
+    disk = np.zeros((n, n))
+    for dy in np.linspace(-0.5, 0.5, 8, endpoint=False) + 1 / 16:
+        for dx in np.linspace(-0.5, 0.5, 8, endpoint=False) + 1 / 16:
+            disk += ((xx + dx) ** 2 + (yy + dy) ** 2 <= rho ** 2)
+    disk /= 64
+    b = O.parallel_forward(disk[:, :, None], np.array([0.0, 37.0, 90.0, 211.0]), absorption=("ray", alpha, R))[:, :, 0]
+    t = np.arange(n) - n // 2
+    inner = np.abs(t) < rho - 2
+    Lr, Lc = np.sqrt(np.clip(R ** 2 - t ** 2.0, 0, None)), np.sqrt(np.clip(rho ** 2 - t ** 2.0, 0, None))
+    want = np.exp(-alpha * Lr) * 2 * np.sinh(alpha * Lc) / alpha
+    assert np.max(np.abs(b[inner] - want[inner, None]) / want[inner, None]) < 0.01
+
+
 def test_ray_oracle_matches_reference(golden):
     R = golden["raytrace"]
     for tag in ("r3", "r2"):

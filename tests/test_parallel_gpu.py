@@ -283,3 +283,33 @@ def test_single_slice_paths_against_oracle(n, na, absn, path):
         p.set_tuning({"forward_vz": 4, "backward_vz": 4})  # tiles at every size
     assert relL2(p.forward(dev(x)).cpu().numpy(), O.parallel_forward(x, ang, absorption=oabs)) < TOL
     assert relL2(p.backward_ref(dev(b)).cpu().numpy(), O.parallel_backward_ref(b, ang, absorption=oabs)) < TOL
+
+
+@pytest.mark.parametrize("nz", [1, 8])
+def test_ray_absorption_disk_known_answer(nz):
+    """Per-ray absorption, centred uniform disk of radius rho inside a container of radius R: the
+    weight exp(-alpha (s - s_entry)), s_entry = -sqrt(R^2 - t^2), integrates over the disk's chord
+    to b(t) = exp(-alpha sqrt(R^2 - t^2)) 2 sinh(alpha sqrt(rho^2 - t^2)) / alpha (straight-ray
+    transmission); with alpha -> 0 it is the chord 2 sqrt(rho^2 - t^2)."""
+    from vamtoolbox_b200.projector.Projector3DParallel import ParallelPlan
+
+    n, rho, R, alpha = 128, 40.0, 56.0, 0.02
+    yy, xx = np.mgrid[:n, :n] - n // 2
+    disk = np.zeros((n, n))
+    for dy in np.linspace(-0.5, 0.5, 8, endpoint=False) + 1 / 16:
+        for dx in np.linspace(-0.5, 0.5, 8, endpoint=False) + 1 / 16:
+            disk += ((xx + dx) ** 2 + (yy + dy) ** 2 <= rho ** 2)
+    disk /= 64
+    angles = np.array([0.0, 37.0, 90.0, 211.0])
+    p = ParallelPlan(n, n, nz, angles)
+    p.set_absorption("ray", alpha_per_px=alpha, radius_px=R)
+    x = torch.as_tensor(np.repeat(disk[:, :, None], nz, axis=2), dtype=torch.float32, device="cuda").contiguous()
+    b = p.forward(x).cpu().numpy().astype(np.float64)
+    t = np.arange(n) - n // 2
+    inner = np.abs(t) < rho - 2
+    Lr, Lc = np.sqrt(np.clip(R ** 2 - t ** 2.0, 0, None)), np.sqrt(np.clip(rho ** 2 - t ** 2.0, 0, None))
+    want = np.exp(-alpha * Lr) * 2 * np.sinh(alpha * Lc) / alpha
+    rel = np.abs(b[inner] - want[inner, None, None]) / want[inner, None, None]
+    assert rel.max() < 0.01
+    for k in range(1, nz):
+        assert np.array_equal(b[:, :, k], b[:, :, 0])
