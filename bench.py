@@ -18,7 +18,8 @@ Reported beside the headline:
   plain       the reference's numpy loop calling the projector per step with host
               arrays (engine="host"), the plain per-call GPU path;
   fwd_adj     forward + reference-parity backprojection pairs per second;
-  roofline    of the dominant kernel (forward projector), HBM bytes it must move;
+  roofline    of the dominant kernel of the step (the projector with the larger share of the
+              measured kernel time), HBM bytes it must move, and its on-chip gathered taps;
   cpu_baseline the reference's algorithm (oracle/vamoracle.c, OpenMP) on a bounded
               z-slab sample on this host's cores, extrapolated to the full volume.
 `--impl reference` prints the CPU reference arm's line instead.
@@ -940,7 +941,7 @@ def run_ours(args):
         torch.cuda.synchronize(dev)
         plain = args.plain_steps / (time.perf_counter() - t0 - 0.0)
 
-    # ---- roofline of the dominant kernel (forward projector)
+    # ---- roofline of the dominant kernel: the projector with the larger share of the step
     peaks = {}
     try:
         peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
@@ -952,16 +953,28 @@ def run_ours(args):
     ny = nx = n
     vol_bytes = ny * nx * n * 4
     sino_bytes = ny * na * n * 4
-    fwd_ms = kmean["forward"]
-    achieved = (vol_bytes + sino_bytes) / (fwd_ms * 1e-3) / 1e9
-    # taps the kernel gathers: 4 x 4 B per lattice sample and slice; angle pairs (a, a+180) share one
-    # lattice of (N+1)^2 samples (even N), unpaired angles use N^2
-    pairs = count_angle_pairs(np.linspace(0, 360, na, endpoint=False))
-    lattice = pairs * (n + 1 - n % 2) ** 2 + (na - 2 * pairs) * n * n
-    tap_bytes = 16.0 * lattice * n
+    dom = "backward_ref" if kmean["backward_ref"] > kmean["forward"] else "forward"
+    dom_ms = kmean[dom]
+    achieved = (vol_bytes + sino_bytes) / (dom_ms * 1e-3) / 1e9
+    if dom == "forward":
+        # taps the kernel gathers: 4 x 4 B per lattice sample and slice; angle pairs (a, a+180) share
+        # one lattice of (N+1)^2 samples (even N), unpaired angles use N^2; the reference's warp
+        # samples N^2 points per angle
+        pairs = count_angle_pairs(np.linspace(0, 360, na, endpoint=False))
+        lattice = pairs * (n + 1 - n % 2) ** 2 + (na - 2 * pairs) * n * n
+        tap_bytes, ref_tap_bytes = 16.0 * lattice * n, 16.0 * n * n * na * n
+        dom_name = "forward projector (R1)"
+    else:
+        # 2 detector rows x 4 B per (pixel, angle, slice): the kernel reads them for the pixels inside
+        # the clip circle, the reference's np.interp for every pixel
+        from vamtoolbox_b200.util.data import circle_inside_mask
+
+        inside = int(circle_inside_mask(ny, nx).sum())
+        tap_bytes, ref_tap_bytes = 8.0 * inside * na * n, 8.0 * ny * nx * na * n
+        dom_name = "reference-parity backprojection (R2)"
     onchip_peak = 148 * 128 * 1.965e9 / 1e9     # L1/shared load bandwidth, nominal
     traffic = None
-    tf = ROOT / "profiles" / "forward_traffic.json"
+    tf = ROOT / "profiles" / ("forward_traffic.json" if dom == "forward" else "backward_traffic.json")
     if tf.exists():
         try:
             tr = json.loads(tf.read_text())
@@ -1044,11 +1057,11 @@ def run_ours(args):
             "configs": configs,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm_peak, "unit": "GB/s",
                          "frac": round(achieved / hbm_peak, 5), "traffic": traffic, "peak_source": peak_src,
-                         "kernel": "forward projector (R1)",
-                         "onchip": {"gathered_tap_bytes": tap_bytes, "reference_tap_bytes": 16.0 * n * n * na * n,
-                                    "achieved_GBs": round(tap_bytes / (fwd_ms * 1e-3) / 1e9, 1),
+                         "kernel": dom_name, "kernel_ms": round(dom_ms, 4),
+                         "onchip": {"gathered_tap_bytes": tap_bytes, "reference_tap_bytes": ref_tap_bytes,
+                                    "achieved_GBs": round(tap_bytes / (dom_ms * 1e-3) / 1e9, 1),
                                     "nominal_peak_GBs": round(onchip_peak, 1),
-                                    "frac": round(tap_bytes / (fwd_ms * 1e-3) / 1e9 / onchip_peak, 4)}},
+                                    "frac": round(tap_bytes / (dom_ms * 1e-3) / 1e9 / onchip_peak, 4)}},
             "cpu_baseline": cpu,
             "clocks": clk,
         }
