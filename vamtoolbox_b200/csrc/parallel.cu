@@ -1626,7 +1626,9 @@ int run(vam_parallel_plan* plan, Op op, const float* in, float* out, cudaStream_
 }
 
 // ---------------------------------------------------------------------------
-// Batched calls: one persistent launch over the virtual blocks of many calls.
+// Batched calls: persistent launches over the virtual blocks of many calls,
+// one per kernel-body family (and per 48 calls), on streams forked from and
+// joined to the caller's.
 //
 // Every call of a batch keeps its own grid; the calls' blocks are numbered
 // consecutively (largest call first) into virtual blocks, and each resident
