@@ -143,6 +143,72 @@ def parallel_backward_ref(b, angles_deg, occlusion=None, absorption=None):
     return x
 
 
+def occlusion_sinogram_2d(occlusion, angles_deg):
+    """Projector2DParallelPython.generateOccSinogram (vamtoolbox/projector/Projector2DParallel.py:70-143):
+    per angle, the pixels' detector coordinate t = x cos - y sin is binned with np.digitize over the
+    sorted detector axis (a coordinate below the first bin index -1, i.e. the last bin's value), and
+    each bin holding occluded pixels gets the least s = x sin + y cos among them; other bins are NaN.
+    The values are assigned to the sorted unique bin indices in ascending order of the bins' values,
+    as the reference's np.split / np.unique steps do.  occlusion: boolean [n, n].  Returns [n, nA]."""
+    occ = np.asarray(occlusion, dtype=bool)
+    n = occ.shape[0]
+    C = n // 2
+    y, x = np.mgrid[:n, :n] - C
+    proj_t = np.arange(n) - C
+    ang = np.deg2rad(np.asarray(angles_deg, dtype=np.float64))
+    out = np.zeros((n, ang.size))
+    bins = np.sort(proj_t)
+    for i, a in enumerate(ang):
+        c, s_ = np.cos(a), np.sin(a)
+        t = x * c - y * s_
+        s = x * s_ + y * c
+        k = np.digitize(t, bins=bins) - 1
+        td = proj_t[k]
+        t_occ, s_occ = td[occ], s[occ]
+        order = np.argsort(t_occ)  # stable for the grouping below: groups need only their members
+        t_sorted, s_sorted = t_occ[order], s_occ[order]
+        starts = np.unique(t_sorted, return_index=True)[1]
+        mins = [np.min(g) for g in np.split(s_sorted, starts[1:])] if t_sorted.size else []
+        col = np.full(n, np.nan)
+        col[np.unique(k[occ])] = mins
+        out[:, i] = col
+    return out
+
+
+def parallel_forward_2d_occluded(x, angles_deg, occ_sinogram):
+    """Projector2DParallelPython.forward with an occlusion (Projector2DParallel.py:145-186): the input
+    clipped to the circle, rotated, samples with y > occ[j] (the detector column's least occluded s)
+    zeroed, columns summed.  The same shadow rule as the 3-D forward, applied at every angle."""
+    occ = _f64(occ_sinogram)[:, :, None]
+    flag = np.ones((occ.shape[1], 1), dtype=np.uint8)
+    return parallel_forward(clip_to_circle(x)[:, :, None], angles_deg, occlusion=(occ, flag))[:, :, 0]
+
+
+def parallel_backward_2d_occluded(b, angles_deg, occ_sinogram):
+    """Projector2DParallelPython.backward with an occlusion (Projector2DParallel.py:188-233 and its
+    getOccShadow :240-247): per angle np.interp of the projection at t (left = right = 0), zeroed where
+    s exceeds the occlusion value of t's np.digitize bin (no shadow where that value is NaN), summed
+    over angles and clipped to the circle."""
+    b = _f64(b)
+    n, na = b.shape
+    C = n // 2
+    y, x = np.mgrid[:n, :n] - C
+    proj_t = np.arange(n) - C
+    bins = np.sort(proj_t)
+    occ = _f64(occ_sinogram)
+    out = np.zeros((n, n))
+    for i, a in enumerate(np.deg2rad(np.asarray(angles_deg, dtype=np.float64))):
+        c, s_ = np.cos(a), np.sin(a)
+        t = x * c - y * s_
+        s = x * s_ + y * c
+        back = np.interp(t, proj_t, b[:, i], left=0, right=0)
+        td = proj_t[np.digitize(t, bins=bins) - 1]
+        with np.errstate(invalid="ignore"):
+            shadow = s > np.interp(td, proj_t, occ[:, i], left=np.nan, right=np.nan)
+        out += back * np.logical_not(shadow)
+    return clip_to_circle(out)
+
+
 # --------------------------------------------------------------------------
 # ray tracer
 # --------------------------------------------------------------------------

@@ -37,4 +37,5 @@ def golden():
     import numpy as np
 
     d = ROOT / "tests" / "golden"
-    return {k: np.load(d / f"{k}.npz") for k in ("parallel", "raytrace", "optim", "ray_autograd", "algebraic", "formats", "vecgeom")}
+    return {k: np.load(d / f"{k}.npz") for k in ("parallel", "raytrace", "optim", "ray_autograd", "algebraic", "formats", "vecgeom",
+                                                 "occ2d")}

@@ -393,9 +393,40 @@ def vecgeom_cases(vam):
     np.savez_compressed(OUT / "vecgeom.npz", **out)
 
 
+def occ2d_cases(vam):
+    """Projector2DParallelPython with a digitised occlusion (Projector2DParallel.py:70-143, 145-247):
+    the occlusion sinogram, forward and backward, for an even and an odd slice with occluders whose
+    detector coordinates stay on the detector (np.digitize never wraps to the last bin)."""
+    geo = vam.geometry
+    P2 = vam.projector.Projector2DParallel.Projector2DParallelPython
+    rng = np.random.default_rng(4321)
+    out = {}
+    for tag, n, na, boxes in (("even", 20, 12, ((8, 12, 11, 15), (5, 7, 6, 9))),
+                              ("odd", 21, 9, ((9, 13, 4, 7),))):
+        occ = np.zeros((n, n), dtype=bool)
+        for r0, r1, c0, c1 in boxes:
+            occ[r0:r1, c0:c1] = True
+        x = rng.uniform(0, 1, (n, n))
+        ang = np.linspace(0, 360, na, endpoint=False) + 0.7
+        tg = geo.TargetGeometry(target=x.copy(), clip_to_circle=False)
+        tg.segmentZ(0)
+        tg.target = tg.array  # Projector2DParallel.py:205 reads target_geo.target (see parallel_cases)
+        pg = geo.ProjectionGeometry(ang, "parallel", CUDA=False, occlusion=occ.copy())
+        A2 = P2(tg, pg)
+        b = rng.uniform(0, 1, (n, na))
+        out[f"{tag}_occ"] = occ
+        out[f"{tag}_x"] = x
+        out[f"{tag}_angles"] = ang
+        out[f"{tag}_sino"] = A2.occ_sinogram
+        out[f"{tag}_fwd"] = A2.forward(x.copy())
+        out[f"{tag}_b"] = b
+        out[f"{tag}_bwd"] = A2.backward(b.copy())
+    np.savez_compressed(OUT / "occ2d.npz", **out)
+
+
 GROUPS = {"parallel": parallel_cases, "ray": ray_cases, "algebraic": algebraic_cases,
           "ray_autograd": ray_autograd_cases, "optim": optimizer_cases, "formats": format_cases,
-          "vecgeom": vecgeom_cases}
+          "vecgeom": vecgeom_cases, "occ2d": occ2d_cases}
 
 
 def main():
