@@ -165,7 +165,7 @@ def occlusion_sinogram_2d(occlusion, angles_deg):
         k = np.digitize(t, bins=bins) - 1
         td = proj_t[k]
         t_occ, s_occ = td[occ], s[occ]
-        order = np.argsort(t_occ)  # stable for the grouping below: groups need only their members
+        order = np.argsort(t_occ)  # any order within a bin: only each bin's minimum is kept
         t_sorted, s_sorted = t_occ[order], s_occ[order]
         starts = np.unique(t_sorted, return_index=True)[1]
         mins = [np.min(g) for g in np.split(s_sorted, starts[1:])] if t_sorted.size else []
