@@ -96,6 +96,11 @@ def build_problem(n, n_angles, seed):
     return tg, pg
 
 
+def workload_name(n, n_angles):
+    """The workload string both bench arms print."""
+    return f"BCLP iteration, parallel beam, {n}^3 x {n_angles} angles, radial absorption mask e^-1"
+
+
 def bclp_options(n_iter):
     from vamtoolbox_b200.optimize import Options
 
@@ -218,8 +223,18 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-# CPU reference algorithm (oracle) on a z-slab sample
+# CPU reference algorithm (oracle): timed baseline and parity at the timed size
 # ---------------------------------------------------------------------------
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def rel_err(a, b):
+    return float(abs(float(a) - float(b)) / max(abs(float(b)), 1e-300))
+
+
 def cpu_bclp_sample(tg, pg, g0, opts, n_slices, steps=1):
     """Time `steps` BCLP iterations of the reference's algorithm on n_slices z-slices."""
     from oracle import oracle as O
@@ -245,18 +260,59 @@ def cpu_bclp_sample(tg, pg, g0, opts, n_slices, steps=1):
     return (time.perf_counter() - t0) / steps
 
 
-def cpu_baseline(tg, pg, g0, opts, n_total, budget_s):
+def device_bclp_step(it):
+    """One eager BCLP iteration of the device engine from its current g; returns host float64 copies of
+    the input g and of every product of the step (dose, mapped dose, forward of the operand, the 9 loss /
+    norm sums, updated g)."""
+    import torch
+
+    g_in = it.g.double().cpu().numpy()
+    it.step()
+    torch.cuda.synchronize(it.device)
+    h = lambda t: t.double().cpu().numpy()
+    return {"g": g_in, "dose": h(it.dose), "mapped": h(it.mapped), "fwd": h(it.grad), "stats": h(it.stats),
+            "g_new": h(it.g)}
+
+
+def bclp_parity(dev_out, ref):
+    """relL2 of the device iteration's products against the float64 oracle's, same input g."""
+    st, rs = dev_out["stats"], ref["stats"]
+    return {"dose": rel_l2(dev_out["dose"], ref["dose"]), "mapped_dose": rel_l2(dev_out["mapped"], ref["mapped"]),
+            "forward_of_operand": rel_l2(dev_out["fwd"], ref["fwd"]), "g_new": rel_l2(dev_out["g_new"], ref["g_new"]),
+            "loss_sum": rel_err(st[0], rs[0]), "l1_norm": rel_err(st[3], rs[3]), "linf_norm": rel_err(st[7], rs[7])}
+
+
+def oracle_bclp_iteration(tg, pg, opts, g):
+    """The float64 oracle's BCLP iteration (whole volume, all angles) from sinogram g, and its time."""
+    from oracle import iterations as OI
+
+    rm = opts.response_model
+    tables = (rm.interp_f_0, rm.interp_map_0, rm.interp_dmapdf_0)
+    mask = np.asarray(pg.absorption_mask)[:, :, 0] if pg.absorption_mask is not None else None
+    t0 = time.perf_counter()
+    ref = OI.bclp_iteration(g, np.asarray(tg.array, np.float64), np.asarray(pg.angles, np.float64), mask, tables,
+                            opts.eps, opts.weight, opts.p, opts.q, opts.learning_rate, opts.blb, opts.bub)
+    return ref, time.perf_counter() - t0
+
+
+def cpu_baseline_and_parity(it, tg, pg, opts):
+    """One full BCLP iteration of the reference's algorithm (float64 C oracle, OpenMP on all host
+    threads) from the device engine's current sinogram: its time is the CPU baseline (no extrapolation:
+    every z-slice and angle), its products are the parity reference for the device iteration run from
+    the same sinogram."""
     from oracle import oracle as O
 
+    dev_out = device_bclp_step(it)
+    ref, t = oracle_bclp_iteration(tg, pg, opts, dev_out["g"])
     cores = O.num_threads()
-    t1 = cpu_bclp_sample(tg, pg, g0, opts, 1)
-    n = int(max(1, min(n_total, budget_s / max(t1, 1e-6))))
-    n = max(1, min(n, 64))
-    t = cpu_bclp_sample(tg, pg, g0, opts, n)
-    per_iter = t * n_total / n
-    return {"value": 1.0 / per_iter, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{n} of {n_total} z-slices x {pg.n_angles} angles, 1 BCLP iteration (float64 C oracle, "
-                      f"OpenMP {cores} threads), extrapolated linearly over z-slices ({t:.2f} s measured)"}
+    n = tg.array.shape
+    cpu = {"value": 1.0 / t, "unit": UNIT, "cores": cores, "kind": "port",
+           "sample": f"1 BCLP iteration over the whole {n[0]}x{n[1]}x{n[2]} volume x {pg.n_angles} angles "
+                     f"(float64 C oracle, OpenMP {cores} threads), {t:.2f} s measured, not extrapolated"}
+    par = {"reference": "float64 oracle (restated reference projectors + numpy BCLP body), same input g",
+           "workload": f"one BCLP iteration, {n[0]}^3 x {pg.n_angles} angles, radial absorption mask, whole volume",
+           "relL2": bclp_parity(dev_out, ref), "tolerance": {"projector products": 1e-5, "optimizer state": 1e-4}}
+    return cpu, par
 
 
 # ---------------------------------------------------------------------------
@@ -449,7 +505,40 @@ def run_ray_bclp(dev, n=128, n_angles=360, steps=5, warmup=2, cpu=True):
             out["cpu_baseline"] = ray_cpu_sample(cv, nx, ax, n_angles)
         except Exception as exc:
             out["cpu_baseline"] = {"error": f"{type(exc).__name__}: {exc}"}
+        try:
+            out["parity"] = ray_chunk_parity(plan, cv, nx, ax, np.linspace(0, 360, n_angles, endpoint=False))
+        except Exception as exc:
+            out["parity"] = {"error": f"{type(exc).__name__}: {exc}"}
     return out
+
+
+def ray_chunk_parity(plan, cv, nx, ax, angles, first=0, count=16, seed=11):
+    """Integrate and deposit at the full workload size against the float64 oracle tracer on one block of
+    `count` angles: the device traces every ray (integrate of a seeded field; deposit of seeded energies
+    on the block's rays, zero elsewhere), the oracle traces the block's rays."""
+    import torch
+
+    from oracle import iterations as OI
+
+    n0, na, nz = plan.sino_shape
+    rng = np.random.default_rng(seed)
+    f = rng.uniform(0.0, 1.0, plan.grid_shape)
+    g_rows = rng.uniform(0.0, 1.0, (n0, count, nz)).astype(np.float32)
+    g_all = np.zeros((n0, na, nz), np.float32)
+    g_all[:, first:first + count] = g_rows
+    dev = plan.device
+    integral = plan.integrate(torch.as_tensor(f, dtype=torch.float32, device=dev)).reshape(n0, na, nz)
+    dose = plan.deposit(torch.as_tensor(g_all, device=dev))
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    ri, rd, act = OI.ray_chunk(cv, nx, ax, angles, first, count, f, g_rows, plan.step_size, plan.max_num_step)
+    t = time.perf_counter() - t0
+    return {"reference": "float64 oracle tracer (float32 ray state, as the reference), one block of angles",
+            "sample": f"angles {first}..{first + count - 1} of {na} ({n0 * count * nz} rays), step cap "
+                      f"{plan.max_num_step}", "oracle_s": round(t, 2),
+            "relL2": {"integrate": rel_l2(integral[:, first:first + count].double().cpu().numpy(), ri),
+                      "deposit": rel_l2(dose.double().cpu().numpy(), rd)},
+            "tolerance": 1e-4, "oracle_rays_active_at_cap": int(act)}
 
 
 def _time_optimize(make, n_iter):
@@ -472,46 +561,126 @@ def _time_optimize(make, n_iter):
             "iter_s": round(1000.0 / ms, 3) if ms else None}
 
 
-def run_configs():
-    """The reference's other headline workloads, each through optimize(target, proj, Options(...)) on
-    the device engine: 2-D CAL 256^2 padded to a 363-bin detector with 360 angles; OSMO 256^3 with e^-1
-    absorption and 360 angles; grayscale BCLP 192^3 with 720 angles and a generalised-logistic response."""
+def config_cal_2d(n_iter):
+    """2-D CAL: a 256^2 ellipse target zero-padded to 363^2 (the 363-bin detector), 360 angles, lr 0.4,
+    d_h 0.5."""
+    from vamtoolbox_b200 import geometry, synthetic
+    from vamtoolbox_b200.optimize import Options
+
+    t = synthetic.ellipses_2d(256, seed=1)
+    t = np.pad(t, ((53, 54), (53, 54)))
+    tg = geometry.TargetGeometry(target=t)
+    pg = geometry.ProjectionGeometry(np.linspace(0, 360, 360, endpoint=False), "parallel", CUDA=True)
+    return tg, pg, Options(method="CAL", n_iter=n_iter, learning_rate=0.4, d_h=0.5)
+
+
+def config_osmo(n_iter):
+    """OSMO at 256^3 x 360 angles with e^-1 radial absorption."""
+    from vamtoolbox_b200.optimize import Options
+
+    tg, pg = build_problem(256, 360, seed=2)
+    return tg, pg, Options(method="OSMO", n_iter=n_iter)
+
+
+def config_gray_bclp(n_iter, p=2, n=192, n_angles=720):
+    """Grayscale BCLP: 192^3 smoothed-noise 3-level target with a ramp, 720 angles, generalised-logistic
+    response table (M 0.6, B 12), eps 0.05, weights 1 inside / 0.5 outside, Lp norm p, q 1."""
     from vamtoolbox_b200 import geometry, response, synthetic
     from vamtoolbox_b200.optimize import Options
 
+    t = synthetic.grayscale_3d(n, seed=3)
+    tg = geometry.TargetGeometry(target=t)
+    pg = geometry.ProjectionGeometry(np.linspace(0, 360, n_angles, endpoint=False), "parallel", CUDA=True)
+    rm = response.ResponseModel(type="interpolation", form="gen_log_fun", M=0.6, B=12)
+    w = np.where(t > 0, 1.0, 0.5)
+    return tg, pg, Options(method="BCLP", n_iter=n_iter, response_model=rm, eps=0.05, weight=w, p=p, q=1,
+                           learning_rate=1e-3)
+
+
+def cal_parity(tg, pg, opts):
+    """One CAL iteration of the device engine against the float64 oracle's from the same state."""
+    import torch
+
+    from oracle import iterations as OI
+    from vamtoolbox_b200.optimizer.CAL import CALDevice
+    from vamtoolbox_b200.projectorconstructor import projectorconstructor
+
+    c = CALDevice(tg, pg, opts, projectorconstructor(tg, pg))
+    x0, b0 = c.x.double().cpu().numpy(), c.b.double().cpu().numpy()
+    c.step(1)
+    torch.cuda.synchronize()
+    xd = c.x.double().cpu().numpy()
+    xd = xd / xd.max()
+    t0 = time.perf_counter()
+    xr, br, ver = OI.cal_step(x0, b0, np.atleast_3d(tg.array), np.atleast_3d(tg.gel_inds),
+                              np.atleast_3d(tg.void_inds), np.asarray(pg.angles, np.float64), opts.d_h,
+                              opts.sigmoid, opts.learning_rate)
+    n = np.sum(tg.gel_inds) + np.sum(tg.void_inds)
+    return {"reference": "float64 oracle, one CAL iteration from the device state", "oracle_s": round(time.perf_counter() - t0, 2),
+            "relL2": {"sinogram": rel_l2(c.b.double().cpu().numpy(), br), "reconstruction": rel_l2(xd, xr)},
+            "ver": float(c.ver.item()), "ver_oracle": float(ver),
+            "ver_voxels_apart": float(abs(float(c.ver.item()) - ver) * n)}
+
+
+def osmo_parity(tg, pg, opts):
+    """The first OSMO half step (void voxels) of the device engine against the float64 oracle's from the
+    same model and reconstruction, whole volume."""
+    import torch
+
+    from oracle import iterations as OI
+    from vamtoolbox_b200.optimizer.OSMO import OSMODevice
+    from vamtoolbox_b200.projectorconstructor import projectorconstructor
+
+    it = OSMODevice(tg, pg, opts, projectorconstructor(tg, pg))
+    x0, xm0 = it.x.double().cpu().numpy(), it.xm.double().cpu().numpy()
+    it.half(False)
+    torch.cuda.synchronize()
+    mask = np.asarray(pg.absorption_mask)[:, :, 0] if pg.absorption_mask is not None else None
+    t0 = time.perf_counter()
+    xr, br, xmr = OI.osmo_half(x0, xm0, tg.gel_inds, tg.void_inds, False, opts.d_l,
+                               np.asarray(pg.angles, np.float64), mask, opts.inhibition)
+    return {"reference": "float64 oracle, one OSMO half step from the device state, whole volume",
+            "oracle_s": round(time.perf_counter() - t0, 2),
+            "relL2": {"model": rel_l2(it.xm.double().cpu().numpy(), xmr), "sinogram": rel_l2(it.b.double().cpu().numpy(), br),
+                      "reconstruction": rel_l2(it.x.double().cpu().numpy(), xr)}}
+
+
+def gray_bclp_parity(tg, pg, opts):
+    """One grayscale BCLP iteration (response table, weights) of the device engine against the float64
+    oracle's from the same sinogram, whole volume."""
+    from vamtoolbox_b200.optimizer.BCLP import BCLPNorm
+
+    dev_out = device_bclp_step(BCLPNorm(tg, pg, opts).device_iteration())
+    ref, t = oracle_bclp_iteration(tg, pg, opts, dev_out["g"])
+    return {"reference": "float64 oracle, one BCLP iteration from the same g, whole volume", "oracle_s": round(t, 2),
+            "relL2": bclp_parity(dev_out, ref)}
+
+
+def run_configs(parity=True):
+    """The reference's other headline workloads, each through optimize(target, proj, Options(...)) on
+    the device engine: 2-D CAL 256^2 padded to a 363-bin detector with 360 angles; OSMO 256^3 with e^-1
+    absorption and 360 angles; grayscale BCLP 192^3 with 720 angles and a generalised-logistic response.
+    With parity, each also runs one iteration from the same state on the device and in the float64
+    oracle and reports the relL2 of the products."""
     out = {}
-
-    def c1(n):
-        t = synthetic.ellipses_2d(256, seed=1)
-        t = np.pad(t, ((53, 54), (53, 54)))  # 363-bin detector: the target zero-padded to 363^2
-        tg = geometry.TargetGeometry(target=t)
-        pg = geometry.ProjectionGeometry(np.linspace(0, 360, 360, endpoint=False), "parallel", CUDA=True)
-        return tg, pg, Options(method="CAL", n_iter=n, learning_rate=0.4, d_h=0.5)
-
-    def c2(n):
-        tg, pg = build_problem(256, 360, seed=2)
-        return tg, pg, Options(method="OSMO", n_iter=n)
-
-    def c3(n):
-        t = synthetic.grayscale_3d(192, seed=3)
-        tg = geometry.TargetGeometry(target=t)
-        pg = geometry.ProjectionGeometry(np.linspace(0, 360, 720, endpoint=False), "parallel", CUDA=True)
-        rm = response.ResponseModel(type="interpolation", form="gen_log_fun", M=0.6, B=12)
-        w = np.where(t > 0, 1.0, 0.5)
-        return tg, pg, Options(method="BCLP", n_iter=n, response_model=rm, eps=0.05, weight=w, p=2, q=1,
-                               learning_rate=1e-3)
-
-    for key, make, n_iter, desc in (
-            ("cal_2d_256_363x360", c1, 20, "2-D CAL, 256^2 target padded to 363^2, 360 angles, lr 0.4, d_h 0.5"),
-            ("osmo_256cube_360_absorbing", c2, 30, "OSMO, 256^3, 360 angles, e^-1 radial absorption"),
-            ("bclp_gray_192cube_720", c3, 40, "grayscale BCLP, 192^3, 720 angles, response M 0.6 B 12, eps 0.05, "
-                                              "weights 1 / 0.5, p 2, q 1")):
+    for key, make, n_iter, desc, par in (
+            ("cal_2d_256_363x360", config_cal_2d, 20, "2-D CAL, 256^2 target padded to 363^2, 360 angles, lr 0.4, d_h 0.5",
+             cal_parity),
+            ("osmo_256cube_360_absorbing", config_osmo, 30, "OSMO, 256^3, 360 angles, e^-1 radial absorption", osmo_parity),
+            ("bclp_gray_192cube_720", config_gray_bclp, 40, "grayscale BCLP, 192^3, 720 angles, response M 0.6 B 12, eps 0.05, "
+                                              "weights 1 / 0.5, p 2, q 1", gray_bclp_parity)):
         try:
             r = _time_optimize(make, n_iter)
             r["workload"] = desc
             out[key] = r
         except Exception as exc:  # report, never fail the headline number on it
             out[key] = {"error": f"{type(exc).__name__}: {exc}"}
+            continue
+        if parity:
+            try:
+                r["parity"] = par(*make(n_iter))
+            except Exception as exc:  # report, never fail the headline number on it
+                r["parity"] = {"error": f"{type(exc).__name__}: {exc}"}
     out["unit"] = "iter/s of the device engine's iteration loop; optimize_call_s is the whole call"
     return out
 
@@ -991,7 +1160,7 @@ def run_ours(args):
 
     configs = None
     if ws_ == 1 and not args.no_configs:
-        configs = run_configs()
+        configs = run_configs(parity=not args.no_cpu)
 
     algebraic = None
     if ws_ == 1 and not args.no_algebraic:
@@ -1021,12 +1190,13 @@ def run_ours(args):
         except Exception as exc:  # report, never fail the headline number on it
             ray = {"error": f"{type(exc).__name__}: {exc}"}
 
-    cpu = None
+    cpu, parity = None, None
     if rank == 0 and not args.no_cpu:
         try:
-            cpu = cpu_baseline(tg, pg, bclp.g0, opts, n, args.cpu_seconds)
+            # a fresh iteration state (g = g0) with no cross-rank hook: only rank 0 runs it
+            cpu, parity = cpu_baseline_and_parity(bclp.device_iteration(), tg, pg, opts)
         except Exception as exc:  # report, never fail the GPU number on it
-            cpu = {"value": None, "unit": UNIT, "error": str(exc)}
+            cpu = {"value": None, "unit": UNIT, "error": f"{type(exc).__name__}: {exc}"}
 
     if rank == 0:
         line = {
@@ -1034,8 +1204,8 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": round(ms_max, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ellipsoid/cylinder target, "
             "shapes of the 256^3 x 360 absorbing OSMO/BCLP configuration)",
-            "config": {"workload": f"BCLP iteration, parallel beam, {n}^3 x {na} angles per GPU, radial absorption "
-                                   f"mask e^-1, z-slab per rank", "global_batch": ws_, "target": [n, n, n * ws_],
+            "config": {"workload": workload_name(n, na), "per_rank": f"{n}^3 z-slab of the target per GPU",
+                       "global_batch": ws_, "target": [n, n, n * ws_],
                        "angles": na, "parallelism": f"z-slab x{ws_}" if ws_ > 1 else "single GPU",
                        "l2": "inputs larger than L2 (working set ~450 MB per iteration)",
                        "graph": dist is None, "launch_shapes": tuning},
@@ -1063,6 +1233,7 @@ def run_ours(args):
                                     "nominal_peak_GBs": round(onchip_peak, 1),
                                     "frac": round(tap_bytes / (dom_ms * 1e-3) / 1e9 / onchip_peak, 4)}},
             "cpu_baseline": cpu,
+            "parity": parity,
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)
@@ -1103,7 +1274,8 @@ def run_reference(args):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws_, "steps": len(ts), "warmup": args.warmup,
             "ms_per_step": per * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": f"BCLP iteration, parallel beam, {n}^3 x {na} angles, radial absorption mask"},
+            "config": {"workload": workload_name(n, na), "per_rank": f"{n}^3 z-slab of the target per GPU",
+                       "global_batch": ws_, "target": [n, n, n * ws_], "angles": na},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": f"{n_slice} of {n} z-slices per step, float64 C restatement of the reference's "
                                        f"projectors + numpy BCLP body, extrapolated over z"},

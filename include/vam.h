@@ -299,10 +299,13 @@ int vam_reduce(const float* x_dev, int64_t n, int op, float* out_dev, void* work
  * partial per 2048 inputs, so n is limited to 8388608 elements (larger n:
  * VAM_ERR_SHAPE, nothing launched).  Allocates nothing and calls no
  * allocating routine.  The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress); make that first call before any stream
- * capture.  All calls share the one array: calls that overlap on the GPU
- * (different streams, no ordering) race; each call writes every partial it
- * reads, so nothing carries over between calls. */
+ * address (cudaGetSymbolAddress) and loads the entry point's kernels for every
+ * op; make that first call before any stream capture.  The address is cached
+ * per device ordinal for the life of the process: after cudaDeviceReset on a
+ * device the cached address is stale, so do not call this entry point on a
+ * device that was reset after its first call.  All calls share the one array:
+ * calls that overlap on the GPU (different streams, no ordering) race; each
+ * call writes every partial it reads, so nothing carries over between calls. */
 int vam_reduce_noalloc(const float* x_dev, int64_t n, int op, float* out_dev, vam_stream_t stream);
 
 /* Volumetric error rate (vamtoolbox/metrics.py:47-87): out_dev[0] =

@@ -1,11 +1,11 @@
 """Small, self-contained runs of one hot-path kernel, for profilers.
 
-    python -m vamtoolbox_b200.profile_case parallel --size 256 --angles 360 --calls 2
-    python -m vamtoolbox_b200.profile_case parallel --size 512 --angles 720 --slices 1
-    python -m vamtoolbox_b200.profile_case ray --size 96 --angles 120 --calls 1
-    python -m vamtoolbox_b200.profile_case formats --size 256 --angles 120 --calls 1
-    python -m vamtoolbox_b200.profile_case vec --size 128 --angles 90 --incline 15
-    python -m vamtoolbox_b200.profile_case batch --calls 1 --direct
+    python profile_case.py parallel --size 256 --angles 360 --calls 2
+    python profile_case.py parallel --size 512 --angles 720 --slices 1
+    python profile_case.py ray --size 96 --angles 120 --calls 1
+    python profile_case.py formats --size 256 --angles 120 --calls 1
+    python profile_case.py vec --size 128 --angles 90 --incline 15
+    python profile_case.py batch --calls 1 --direct
 
 ``parallel`` runs forward, reference-parity backprojection and the matched
 adjoint (after building its weight table) on a random N x N x N volume with
@@ -36,7 +36,7 @@ import torch
 
 
 def run_parallel(n, na, calls, tuning, nz=None):
-    from .projector.Projector3DParallel import ParallelPlan
+    from vamtoolbox_b200.projector.Projector3DParallel import ParallelPlan
 
     nz = n if nz is None else nz
     p = ParallelPlan(n, n, nz, np.linspace(0, 360, na, endpoint=False))
@@ -56,8 +56,8 @@ def run_parallel(n, na, calls, tuning, nz=None):
 
 
 def run_ray(n, na, calls):
-    from . import geometry, medium, synthetic
-    from .projector.pyTorchRayTrace import PyTorchRayTracingPropagator
+    from vamtoolbox_b200 import geometry, medium, synthetic
+    from vamtoolbox_b200.projector.pyTorchRayTrace import PyTorchRayTracingPropagator
 
     tg = geometry.TargetGeometry(target=np.zeros((n, n, n)))
     cv = tg.constructCoordVec()
@@ -110,8 +110,8 @@ def summarize_launches(path):
 
 
 def run_formats(n, na, calls):
-    from . import geometry
-    from . import imagesequence as ims
+    from vamtoolbox_b200 import geometry
+    from vamtoolbox_b200 import imagesequence as ims
 
     g = torch.Generator(device="cuda").manual_seed(0)
     sino = torch.rand((n, na, n), device="cuda", dtype=torch.float64, generator=g) ** 3 * 40.0
@@ -125,7 +125,7 @@ def run_formats(n, na, calls):
 
 
 def run_vec(n, na, calls, incline):
-    from .projector.Projector3DParallelCUDA import VecPlan, genVectorsAstra, parallel3d_vectors
+    from vamtoolbox_b200.projector.Projector3DParallelCUDA import VecPlan, genVectorsAstra, parallel3d_vectors
 
     ang = np.linspace(0, 360, na, endpoint=False)
     vec = parallel3d_vectors(np.deg2rad(ang)) if incline == 0 else genVectorsAstra(ang, incline)
@@ -143,8 +143,8 @@ def run_vec(n, na, calls, incline):
 def run_batch(calls, direct, seed=5):
     """The shapes and angle counts of the 16-target multi-target workload (the same seeded draws), with
     random inputs and a random absorption mask per call (every target of that workload absorbs)."""
-    from .batch import ProjectionBatch
-    from .projector.Projector3DParallel import ParallelPlan
+    from vamtoolbox_b200.batch import ProjectionBatch
+    from vamtoolbox_b200.projector.Projector3DParallel import ParallelPlan
 
     rng = np.random.default_rng(seed)
     g = torch.Generator(device="cuda").manual_seed(0)

@@ -6,9 +6,10 @@ memory before a print starts and must not trigger cudaMalloc's implicit
 synchronisation during exposure.  This entry point keeps its scratch in a
 static device array inside the library instead of a caller workspace.  The
 test calls it through the C ABI and checks it against the workspace-based
-vam_reduce, twice in a row on different data (the shared scratch keeps the
-previous call's contents), and checks that sizes above its stated maximum are
-rejected before anything is launched.  It lives in a file pytest collects last.
+vam_reduce and against a float64 numpy reduction of the same data, twice in
+a row on different data (the shared scratch keeps the previous call's
+contents), and checks that sizes above its stated maximum are rejected before
+anything is launched.  It lives in a file pytest collects last.
 """
 import ctypes
 
@@ -34,7 +35,10 @@ def test_noalloc_reduce_matches_workspace_reduce_on_two_calls(n):
     work = torch.empty(int(lib.vam_reduce_workspace_bytes(n)), dtype=torch.uint8, device="cuda")
     rng = np.random.default_rng(n)
     for call in range(2):
-        x = torch.as_tensor(rng.standard_normal(n).astype(np.float32), device="cuda")
+        xh = rng.standard_normal(n).astype(np.float32)
+        x = torch.as_tensor(xh, device="cuda")
+        x64 = xh.astype(np.float64)
+        exact = {_lib.RED_MAX: float(x64.max()), _lib.RED_MIN: float(x64.min()), _lib.RED_SUM: float(x64.sum())}
         for op in (_lib.RED_MAX, _lib.RED_MIN, _lib.RED_SUM):
             ref = torch.full((1,), float("nan"), device="cuda")
             got = torch.full((1,), float("nan"), device="cuda")
@@ -45,6 +49,12 @@ def test_noalloc_reduce_matches_workspace_reduce_on_two_calls(n):
             r, g = float(ref.item()), float(got.item())
             assert np.isfinite(g)
             assert abs(g - r) <= 1e-6 * max(1.0, abs(r)), (call, op, g, r)
+            # independent check: max and min are exact; the sum is accumulated in float64 and rounded
+            # once to float32, so it lies within one float32 ulp of numpy's float64 sum
+            if op == _lib.RED_SUM:
+                assert abs(g - exact[op]) <= 2 ** -23 * max(abs(exact[op]), 1.0), (call, g, exact[op])
+            else:
+                assert g == exact[op], (call, op, g, exact[op])
 
 
 def test_noalloc_reduce_rejects_sizes_above_its_maximum():

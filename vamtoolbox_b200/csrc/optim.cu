@@ -404,7 +404,9 @@ double* g_noalloc_addr[kNoAllocMaxDevices] = {};
 
 // Device address of g_noalloc_partials on the current device.  In host code
 // the symbol is only a host-side stand-in, never a device pointer, so the
-// address is looked up once per device and cached.
+// address is looked up once per device and cached.  The same first call also
+// loads the six reduction kernels this entry point launches (CUDA loads
+// kernels lazily, on first use), so no later call of any op loads a module.
 int noalloc_scratch(double** out) {
     int dev = -1;
     VAM_TRY_CUDA(cudaGetDevice(&dev));
@@ -415,6 +417,15 @@ int noalloc_scratch(double** out) {
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
         if (e != cudaSuccess || !p)
             return set_error(VAM_ERR_CUDA, std::string("vam_reduce_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        const void* kernels[] = {(const void*)k_reduce_partial<VAM_RED_MAX>, (const void*)k_reduce_final<VAM_RED_MAX>,
+                                 (const void*)k_reduce_partial<VAM_RED_MIN>, (const void*)k_reduce_final<VAM_RED_MIN>,
+                                 (const void*)k_reduce_partial<VAM_RED_SUM>, (const void*)k_reduce_final<VAM_RED_SUM>};
+        for (const void* k : kernels) {
+            cudaFuncAttributes fa;
+            e = cudaFuncGetAttributes(&fa, k);
+            if (e != cudaSuccess)
+                return set_error(VAM_ERR_CUDA, std::string("vam_reduce_noalloc: loading its kernels: ") + cudaGetErrorString(e));
+        }
         g_noalloc_addr[dev] = static_cast<double*>(p);
     }
     *out = g_noalloc_addr[dev];

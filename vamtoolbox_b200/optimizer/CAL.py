@@ -72,6 +72,54 @@ def _cal_host(target_geo, proj_geo, options, A=None):
     return (geometry.Sinogram(b_opt, proj_geo, options), geometry.Reconstruction(x_opt, proj_geo, options), err)
 
 
+class CALDevice:
+    """Device state and fused kernels of the CAL loop (CAL.py:147-195).
+
+    The reconstruction x is kept unnormalised with max(x) as a device
+    scalar.  ``step(it)`` issues one iteration on the current stream: the
+    sigmoid threshold of x / max(x) against the target, the forward
+    projection of the residual, the (momentum) sinogram update clipped at
+    zero, the backprojection, its maximum, VER and the log append.  Nothing
+    is allocated and nothing syncs, so a step is captured once as a CUDA
+    graph when the momentum is zero.
+    """
+
+    def __init__(self, target_geo, proj_geo, options, A):
+        self.options = options
+        dev = self.device = A.device
+        ws = self.ws = Workspace(dev)
+        plan = self.plan = A.plan
+        vs, ss = plan.shape_vol, plan.shape_sino
+        self.tgt = torch.as_tensor(np.ascontiguousarray(np.atleast_3d(target_geo.array), dtype=np.float32),
+                                   device=dev)
+        self.mask = torch.as_tensor(metrics.region_mask(target_geo).reshape(vs), device=dev)
+        n_iter = options.n_iter
+        self.err_log = torch.full((max(n_iter, 1),), float("nan"), dtype=torch.float32, device=dev)
+        self.counter = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.ver, self.xmax = ws.scalar(), ws.scalar()
+        # initial sinogram: forward, filter (cuFFT), clip
+        b = plan.forward(self.tgt)
+        self.b = udata.filterSinogram_t(b, options.filter).clamp_(min=0).contiguous()
+        self.x = plan.backward_ref(self.b)
+        ws.max(self.x, self.xmax)
+        ws.ver(self.x, self.mask, self.ver)
+        ws.append(self.ver, self.err_log, self.counter)
+        self.xt = torch.empty(vs, dtype=torch.float32, device=dev)
+        self.db = torch.empty(ss, dtype=torch.float32, device=dev)
+        self.db_prev = torch.zeros(ss, dtype=torch.float32, device=dev)
+        self.m, self.lr = float(options.momentum), float(options.learning_rate)
+
+    def step(self, it):
+        o, ws, plan = self.options, self.ws, self.plan
+        ws.cal_threshold(self.x, self.xmax, self.tgt, o.d_h, o.sigmoid, self.xt)
+        plan.forward(self.xt, self.db)
+        ws.cal_update(self.b, self.db, self.db_prev if self.m != 0 else None, self.lr, self.m, it)
+        plan.backward_ref(self.b, self.x)
+        ws.max(self.x, self.xmax)
+        ws.ver(self.x, self.mask, self.ver)
+        ws.append(self.ver, self.err_log, self.counter)
+
+
 def minimizeCAL(target_geo, proj_geo, options):
     from ..projector.Projector3DParallel import Projector3DParallel
 
@@ -79,44 +127,14 @@ def minimizeCAL(target_geo, proj_geo, options):
     if (getattr(options, "engine", "device") == "host" or options.d_h is None or options.bit_depth is not None
             or not isinstance(A, Projector3DParallel)):
         return _cal_host(target_geo, proj_geo, options, A)
-    dev = A.device
-    ws = Workspace(dev)
-    plan = A.plan
-    vs, ss = plan.shape_vol, plan.shape_sino
-    tgt = torch.as_tensor(np.ascontiguousarray(np.atleast_3d(target_geo.array), dtype=np.float32), device=dev)
-    mask = torch.as_tensor(metrics.region_mask(target_geo).reshape(vs), device=dev)
-    n_iter = options.n_iter
-    err_log = torch.full((max(n_iter, 1),), float("nan"), dtype=torch.float32, device=dev)
-    counter = torch.zeros(1, dtype=torch.int32, device=dev)
-    ver = ws.scalar()
-    xmax = ws.scalar()
-    # initial sinogram: forward, filter (cuFFT), clip
-    b = plan.forward(tgt)
-    b = udata.filterSinogram_t(b, options.filter).clamp_(min=0).contiguous()
-    x = plan.backward_ref(b)
-    ws.max(x, xmax)
-    ws.ver(x, mask, ver)
-    ws.append(ver, err_log, counter)
-    xt = torch.empty(vs, dtype=torch.float32, device=dev)
-    db = torch.empty(ss, dtype=torch.float32, device=dev)
-    db_prev = torch.zeros(ss, dtype=torch.float32, device=dev)
-    m, lr = float(options.momentum), float(options.learning_rate)
-
-    def step(it):
-        ws.cal_threshold(x, xmax, tgt, options.d_h, options.sigmoid, xt)
-        plan.forward(xt, db)
-        ws.cal_update(b, db, db_prev if m != 0 else None, lr, m, it)
-        plan.backward_ref(b, x)
-        ws.max(x, xmax)
-        ws.ver(x, mask, ver)
-        ws.append(ver, err_log, counter)
-
+    c = CALDevice(target_geo, proj_geo, options, A)
+    dev, ws, plan, n_iter, m = c.device, c.ws, c.plan, options.n_iter, c.m
     st = torch.cuda.current_stream(dev)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     done = 0
     graphable = m == 0 and options.bit_depth is None and options.exit_param is None
     if graphable and n_iter > 2:
-        gr = capture(lambda: step(1), dev)
+        gr = capture(lambda: c.step(1), dev)
         ev0.record(st)
         for _ in range(1, n_iter):
             gr.replay()
@@ -125,14 +143,15 @@ def minimizeCAL(target_geo, proj_geo, options):
     else:
         ev0.record(st)
         for it in range(1, n_iter):
-            step(it)
+            c.step(it)
             done += 1
             if m != 0:
-                db_prev.copy_(db)
-            if options.exit_param is not None and float(ver.item()) <= options.exit_param:
+                c.db_prev.copy_(c.db)
+            if options.exit_param is not None and float(c.ver.item()) <= options.exit_param:
                 break
         ev1.record(st)
     # final positivity / normalisation / reconstruction (CAL.py:197-208)
+    b, xmax = c.b, c.xmax
     bmax = ws.scalar()
     b.clamp_(min=0)
     ws.max(b, bmax)
@@ -140,8 +159,8 @@ def minimizeCAL(target_geo, proj_geo, options):
     x_opt = plan.backward_ref(b)
     ws.max(x_opt, xmax)
     ws.scale(x_opt, xmax)
-    err = err_log.double().cpu().numpy()
-    err = np.where(np.arange(err.size) < int(counter.item()), err, np.nan)
+    err = c.err_log.double().cpu().numpy()
+    err = np.where(np.arange(err.size) < int(c.counter.item()), err, np.nan)
     # device time per iteration of the loop (CUDA events on the engine's stream)
     options.device_iteration_ms = ev0.elapsed_time(ev1) / done if done else None
     return (geometry.Sinogram(b.double().cpu().numpy(), proj_geo, options),

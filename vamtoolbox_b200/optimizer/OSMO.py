@@ -58,6 +58,60 @@ def _osmo_host(target_geo, proj_geo, options, A):
     return geometry.Sinogram(b_opt, proj_geo, options), geometry.Reconstruction(x, proj_geo, options), err
 
 
+class OSMODevice:
+    """Device state and fused kernels of the OSMO loop (OSMO.py:36-109, 141-147).
+
+    ``half(gel)`` issues one half step on the current stream: the model
+    update on void (gel False) or gel voxels, the forward projection, its
+    device-side maximum and the normalisation floored at the inhibition
+    level, the backprojection, its maximum and the normalisation floored at
+    zero.  ``step()`` is one OSMO iteration (void half, gel half, VER, log
+    append).  Nothing is allocated and nothing syncs, so ``capture()``
+    records a step once as a CUDA graph.
+    """
+
+    def __init__(self, target_geo, proj_geo, options, A):
+        self.options = options
+        self.A = A
+        dev = self.device = A.device
+        plan = self.plan = A.plan
+        ws = self.ws = Workspace(dev)
+        vs = plan.shape_vol
+        self.mask = torch.as_tensor(metrics.region_mask(target_geo).reshape(vs), device=dev)
+        n_iter = options.n_iter
+        self.err_log = torch.full((max(n_iter, 1),), float("nan"), dtype=torch.float32, device=dev)
+        self.counter = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.ver, self.xmax, self.bmax = ws.scalar(), ws.scalar(), ws.scalar()
+        tgt = torch.as_tensor(np.ascontiguousarray(target_geo.array, dtype=np.float64), device=dev)
+        self.xm = udata.filterTargetOSMO_t(tgt, options.filter).to(torch.float32).reshape(vs).contiguous()
+        self.b = plan.forward(self.xm).clamp_(min=0)
+        self.x = plan.backward_ref(self.b)
+        ws.max(self.x, self.xmax)
+        ws.scale(self.x, self.xmax)
+        ws.ver(self.x, self.mask, self.ver)
+        ws.append(self.ver, self.err_log, self.counter)
+        self.inh = float(options.inhibition)
+
+    def half(self, gel):
+        o, ws, plan = self.options, self.ws, self.plan
+        ws.osmo_model(self.xm, self.x, None, self.mask, gel, o.d_h if gel else o.d_l)
+        plan.forward(self.xm, self.b)
+        ws.max(self.b, self.bmax)
+        ws.scale(self.b, self.bmax, floor=self.inh)
+        plan.backward_ref(self.b, self.x)
+        ws.max(self.x, self.xmax)
+        ws.scale(self.x, self.xmax, floor=0.0)
+
+    def step(self):
+        self.half(False)
+        self.half(True)
+        self.ws.ver(self.x, self.mask, self.ver)
+        self.ws.append(self.ver, self.err_log, self.counter)
+
+    def capture(self):
+        return capture(self.step, self.device)
+
+
 def minimizeOSMO(target_geo, proj_geo, options):
     from ..projector.Projector3DParallel import Projector3DParallel
 
@@ -65,45 +119,13 @@ def minimizeOSMO(target_geo, proj_geo, options):
     if (getattr(options, "engine", "device") == "host" or not isinstance(A, Projector3DParallel)
             or options.bit_depth is not None):
         return _osmo_host(target_geo, proj_geo, options, A)
-    dev = A.device
-    plan = A.plan
-    ws = Workspace(dev)
-    vs, ss = plan.shape_vol, plan.shape_sino
-    mask = torch.as_tensor(metrics.region_mask(target_geo).reshape(vs), device=dev)
-    n_iter = options.n_iter
-    err_log = torch.full((max(n_iter, 1),), float("nan"), dtype=torch.float32, device=dev)
-    counter = torch.zeros(1, dtype=torch.int32, device=dev)
-    ver, xmax, bmax = ws.scalar(), ws.scalar(), ws.scalar()
-    tgt = torch.as_tensor(np.ascontiguousarray(target_geo.array, dtype=np.float64), device=dev)
-    xm = udata.filterTargetOSMO_t(tgt, options.filter).to(torch.float32).reshape(vs).contiguous()
-    b = plan.forward(xm).clamp_(min=0)
-    x = plan.backward_ref(b)
-    ws.max(x, xmax)
-    ws.scale(x, xmax)
-    ws.ver(x, mask, ver)
-    ws.append(ver, err_log, counter)
-    inh = float(options.inhibition)
-
-    def half(gel):
-        ws.osmo_model(xm, x, None, mask, gel, options.d_h if gel else options.d_l)
-        plan.forward(xm, b)
-        ws.max(b, bmax)
-        ws.scale(b, bmax, floor=inh)
-        plan.backward_ref(b, x)
-        ws.max(x, xmax)
-        ws.scale(x, xmax, floor=0.0)
-
-    def step():
-        half(False)
-        half(True)
-        ws.ver(x, mask, ver)
-        ws.append(ver, err_log, counter)
-
+    it = OSMODevice(target_geo, proj_geo, options, A)
+    dev, n_iter = it.device, options.n_iter
     st = torch.cuda.current_stream(dev)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     done = 0
     if options.exit_param is None and n_iter > 2:
-        gr = capture(step, dev)
+        gr = it.capture()
         ev0.record(st)
         for _ in range(1, n_iter):
             gr.replay()
@@ -112,14 +134,14 @@ def minimizeOSMO(target_geo, proj_geo, options):
     else:
         ev0.record(st)
         for _ in range(1, n_iter):
-            step()
+            it.step()
             done += 1
-            if options.exit_param is not None and float(ver.item()) <= options.exit_param:
+            if options.exit_param is not None and float(it.ver.item()) <= options.exit_param:
                 break
         ev1.record(st)
-    err = err_log.double().cpu().numpy()
+    err = it.err_log.double().cpu().numpy()
     # device time per iteration of the loop (CUDA events on the engine's stream)
     options.device_iteration_ms = ev0.elapsed_time(ev1) / done if done else None
-    err = np.where(np.arange(err.size) < int(counter.item()), err, np.nan)
-    return (geometry.Sinogram(b.double().cpu().numpy(), proj_geo, options),
-            geometry.Reconstruction(x.double().cpu().numpy(), proj_geo, options), err)
+    err = np.where(np.arange(err.size) < int(it.counter.item()), err, np.nan)
+    return (geometry.Sinogram(it.b.double().cpu().numpy(), proj_geo, options),
+            geometry.Reconstruction(it.x.double().cpu().numpy(), proj_geo, options), err)
