@@ -82,6 +82,23 @@ int vam_parallel_set_absorption(vam_parallel_plan* plan, int mode, const float* 
  * on the device; later forward/backward_ref/adjoint calls apply the shadow
  * (Projector3DParallel.py:147-153, 192-201, 209-216). */
 int vam_parallel_set_occlusion(vam_parallel_plan* plan, const float* insert_dev, vam_stream_t stream);
+/* The 2-D class's digitised occlusion (Projector2DParallelPython.generateOccSinogram,
+ * Projector2DParallel.py:70-143) for a plan with n_z == 1: occlusion_dev is
+ * [nY][nX] bytes, nonzero = occluded.  Per angle each occluded pixel's
+ * detector coordinate t = x cos - y sin is binned with np.digitize over the
+ * detector axis and each bin keeps its least s = x sin + y cos, assigned to
+ * the bins in the reference's order (a coordinate below the first bin counts
+ * as the last bin's value).  Later forward / adjoint calls zero samples past
+ * the bin's minimum (Projector2DParallel.py:145-186); backward_ref zeroes
+ * pixels whose s exceeds the minimum of t's bin (getOccShadow, :235-247).
+ * Reads back an error flag, so it synchronises the stream.  VAM_ERR_SHAPE
+ * where the reference raises ValueError: an empty occlusion, or occluded
+ * pixels below the first bin and in the last bin at one angle. */
+int vam_parallel_set_occlusion_2d(vam_parallel_plan* plan, const uint8_t* occlusion_dev, vam_stream_t stream);
+/* Copies the float64 bin minima of the digitised 2-D occlusion ([nY][nA], NaN
+ * where a bin holds no occluded pixel: the reference's occ_sinogram) into
+ * out_dev.  VAM_ERR_ARG unless vam_parallel_set_occlusion_2d succeeded. */
+int vam_parallel_get_occlusion_sinogram_2d(vam_parallel_plan* plan, double* out_dev, vam_stream_t stream);
 int vam_parallel_clear_occlusion(vam_parallel_plan* plan);
 /* Copies the occlusion sinogram ([nR][nA][nZ], NaN where a column has no
  * occluder) into out_dev.  VAM_ERR_ARG if no occlusion is set. */
@@ -99,6 +116,12 @@ int vam_parallel_forward(vam_parallel_plan* plan, const float* vol_dev, float* s
  * (Projector3DParallel.py:158-207).  Not the transpose of R1. */
 int vam_parallel_backward_ref(vam_parallel_plan* plan, const float* sino_dev, float* vol_dev,
                               vam_stream_t stream);
+
+/* R2 without the inscribed-circle clip: Projector2DParallelPython.backward(b,
+ * clipping=False) (Projector2DParallel.py:188, 230-231).  The first call
+ * allocates the plan's all-ones pixel table. */
+int vam_parallel_backward_ref_noclip(vam_parallel_plan* plan, const float* sino_dev, float* vol_dev,
+                                     vam_stream_t stream);
 
 /* Matched transpose of R1 (<A x, y> == <x, A^T y>), gather form, no atomics.
  * No counterpart in the reference (its backward is R2); used for autograd. */
@@ -313,13 +336,30 @@ int vam_reduce_noalloc(const float* x_dev, int64_t n, int op, float* out_dev, va
 int vam_metric_ver(const float* x_dev, const uint8_t* mask_dev, int64_t n, float* out_dev,
                    void* work_dev, size_t work_bytes, vam_stream_t stream);
 
+/* In-part dose range (vamtoolbox/metrics.py:130-156, layerwise=False): out_dev[0] =
+ * max(x[gel]) - min(x[gel]).  mask_dev as for vam_metric_ver.  With no gel voxel
+ * out_dev[0] is NaN (the reference's np.min raises on the empty selection). */
+int vam_metric_ipdr(const float* x_dev, const uint8_t* mask_dev, int64_t n, float* out_dev,
+                    void* work_dev, size_t work_bytes, vam_stream_t stream);
+
+/* Response model of the BCLP dose pass (vamtoolbox/response.py:12-399). */
+enum vam_response_kind {
+    VAM_RESP_TABLE = 0,     /* type="interpolation": np.interp on the table, nearest-value extrapolation */
+    VAM_RESP_GLF = 1,       /* type="analytical", form="gen_log_fun": A + (K-A) / (1 + exp(-B(f-M)))^(1/nu) */
+    VAM_RESP_LINEAR = 2,    /* type="analytical", form="linear": M f + C */
+    VAM_RESP_IDENTITY = 3   /* type="analytical", form="identity": f */
+};
+
 /* BCLP state update, one pass over the dose (vamtoolbox/optimizer/BCLP.py:277-437):
- * mapped = response(dose) (interpolation table), e = mapped - f_T,
+ * mapped = response(dose), e = mapped - f_T,
  * eb = |e| - eps, v = eb > 0, operand = v*w*|eb|^(p-1)*sign(e)*dresponse(dose).
  * stats_dev[0..8] = { sum v*w*|eb|^p, l0, l0_eps0, l1, l1_eps0, l2^2, l2_eps0^2, lf, lf_eps0 }.
- * Scalars: eps / weight are arrays when eps_dev / weight_dev are non-null. */
+ * Scalars: eps / weight are arrays when eps_dev / weight_dev are non-null.
+ * The response is the table (VAM_RESP_TABLE) or a closed form evaluated in
+ * float64 per voxel (response.py:191-279: _map_glf / _dmapdf_glf, _map_lin /
+ * _dmapdf_lin, _map_id / _dmapdf_id). */
 typedef struct {
-    const float* table_f;       /* device, n_table sample points (uniformly spaced) */
+    const float* table_f;       /* device, n_table strictly increasing sample points */
     const float* table_map;     /* device, response at the sample points */
     const float* table_dmap;    /* device, derivative at the sample points */
     int32_t n_table;
@@ -328,6 +368,9 @@ typedef struct {
     float eps, weight, p;
     const float* eps_dev;       /* optional per-voxel eps */
     const float* weight_dev;    /* optional per-voxel weight */
+    int32_t response;           /* vam_response_kind; the table fields are unused unless VAM_RESP_TABLE */
+    double resp_A, resp_K, resp_B, resp_M, resp_nu;  /* VAM_RESP_GLF; VAM_RESP_LINEAR uses resp_M */
+    double resp_C;              /* VAM_RESP_LINEAR offset */
 } vam_bclp_params;
 
 int vam_bclp_dose_pass(const float* dose_dev, const float* target_dev, int64_t n,

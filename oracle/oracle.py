@@ -184,11 +184,12 @@ def parallel_forward_2d_occluded(x, angles_deg, occ_sinogram):
     return parallel_forward(clip_to_circle(x)[:, :, None], angles_deg, occlusion=(occ, flag))[:, :, 0]
 
 
-def parallel_backward_2d_occluded(b, angles_deg, occ_sinogram):
+def parallel_backward_2d_occluded(b, angles_deg, occ_sinogram, clipping=True):
     """Projector2DParallelPython.backward with an occlusion (Projector2DParallel.py:188-233 and its
     getOccShadow :240-247): per angle np.interp of the projection at t (left = right = 0), zeroed where
     s exceeds the occlusion value of t's np.digitize bin (no shadow where that value is NaN), summed
-    over angles and clipped to the circle."""
+    over angles and, with clipping, clipped to the circle (the reference clips after every angle, which
+    equals one clip at the end)."""
     b = _f64(b)
     n, na = b.shape
     C = n // 2
@@ -206,7 +207,7 @@ def parallel_backward_2d_occluded(b, angles_deg, occ_sinogram):
         with np.errstate(invalid="ignore"):
             shadow = s > np.interp(td, proj_t, occ[:, i], left=np.nan, right=np.nan)
         out += back * np.logical_not(shadow)
-    return clip_to_circle(out)
+    return clip_to_circle(out) if clipping else out
 
 
 # --------------------------------------------------------------------------

@@ -421,12 +421,140 @@ def occ2d_cases(vam):
         out[f"{tag}_fwd"] = A2.forward(x.copy())
         out[f"{tag}_b"] = b
         out[f"{tag}_bwd"] = A2.backward(b.copy())
+        out[f"{tag}_bwd_noclip"] = A2.backward(b.copy(), clipping=False)
+    # occluders in the corners: at some angles their detector coordinate falls below the first bin, where
+    # np.digitize gives index -1 (the last bin's value); the reference then pairs its per-bin minima with
+    # the bins in a shifted order ("wrap", kept), or raises when the last bin is occupied too ("clash")
+    for tag, boxes in (("wrap", ((0, 3, 0, 3), (9, 12, 9, 11))), ("clash", ((0, 3, 0, 3), (17, 20, 17, 20)))):
+        n, na = 20, 16
+        occ = np.zeros((n, n), dtype=bool)
+        for r0, r1, c0, c1 in boxes:
+            occ[r0:r1, c0:c1] = True
+        x = rng.uniform(0, 1, (n, n))
+        ang = np.linspace(0, 360, na, endpoint=False) + 0.3
+        tg = geo.TargetGeometry(target=x.copy(), clip_to_circle=False)
+        tg.segmentZ(0)
+        tg.target = tg.array
+        pg = geo.ProjectionGeometry(ang, "parallel", CUDA=False, occlusion=occ.copy())
+        out[f"{tag}_occ"], out[f"{tag}_x"], out[f"{tag}_angles"] = occ, x, ang
+        try:
+            A2 = P2(tg, pg)
+        except ValueError as exc:
+            out[f"{tag}_error"] = np.array(str(exc))
+            continue
+        b = rng.uniform(0, 1, (n, na))
+        out[f"{tag}_sino"] = A2.occ_sinogram
+        out[f"{tag}_fwd"] = A2.forward(x.copy())
+        out[f"{tag}_b"] = b
+        out[f"{tag}_bwd"] = A2.backward(b.copy())
     np.savez_compressed(OUT / "occ2d.npz", **out)
+
+
+def _ray_run(vam, tg, im, am, ab, ang, param, solver, rng):
+    """Integrate a seeded field and deposit seeded energies through the reference's tracer."""
+    geo = vam.geometry
+    RT = vam.projector.pyTorchRayTrace
+    pg = geo.ProjectionGeometry(ang, "ray_trace", CUDA=False, index_model=im, attenuation_model=am,
+                                absorption_model=ab, ray_trace_method="eikonal", eikonal_parametrization=param,
+                                ray_trace_ode_solver=solver, ray_trace_ray_config="parallel", inclination_angle=0.0,
+                                ray_density=1)
+    P = RT.PyTorchRayTracingPropagator(tg, pg)
+    f = rng.uniform(0, 1, tg.array.shape)
+    g = P.forward(f.copy())
+    gin = rng.uniform(0, 1, g.shape).astype(np.float32)
+    return f, np.asarray(g), gin, np.asarray(P.backward(gin.copy()))
+
+
+def option_cases(vam):
+    """Every selectable integrator x parametrisation of the reference's tracer on a graded-index grid
+    medium, the analytic Luneburg-lens index (n_sur 1 and 1.2), the analytic homogeneous-ball
+    attenuation, and the reference's dose metrics (calcVER / calcIPDR / calcPW / calcCV) on a seeded
+    dose."""
+    import torch
+
+    geo, med = vam.geometry, vam.medium
+    out = {}
+    rng = np.random.default_rng(2024)
+    n, nz = 12, 6
+    tg = geo.TargetGeometry(target=rng.uniform(0, 1, (n, n, nz)))
+    cv = tg.constructCoordVec()
+    xg, yg, _ = np.meshgrid(*cv, indexing="ij")
+    R = np.amax(cv[0])
+    n_x = 1.30 + 0.05 * (xg ** 2 + yg ** 2) / R ** 2 + 0.01 * rng.uniform(-1, 1, xg.shape)
+    alpha_x = 20.0 * (1 + 0.3 * rng.uniform(-1, 1, xg.shape))
+    ang = np.linspace(0, 360, 5, endpoint=False)
+    out["xv"], out["yv"], out["zv"] = cv
+    out["n"], out["alpha"], out["angles"] = n_x, alpha_x, ang
+    for param in ("physical_path_length", "canonical", "optical_path_length"):
+        for solver in ("forward_symplectic_euler", "forward_euler", "leapfrog"):
+            am = med.AttenuationModel(cv, type="interpolation", form="freeform", alpha_x=torch.as_tensor(alpha_x))
+            if solver == "leapfrog":
+                # the reference's leapfrog start-up step stores the index gradient into the float32 ray state
+                # without a cast (pyTorchRayTrace.py:816-828): with an interpolated (float64) index field it
+                # raises, so its leapfrog runs here through the analytic Luneburg lens (float32 gradient)
+                im = med.IndexModel(cv, type="analytical", form="luneburg_lens", R=0.9, p=2, n_sur=1.2)
+            else:
+                im = med.IndexModel(cv, type="interpolation", form="freeform", n_x=torch.as_tensor(n_x))
+            key = f"{param}__{solver}"
+            f, g, gin, dose = _ray_run(vam, tg, im, am, am, ang, param, solver, rng)
+            out[key + "_f"], out[key + "_fwd"], out[key + "_g"], out[key + "_bwd"] = f, g, gin, dose
+    # analytic Luneburg lens (p = 2, radius 0.9 of the domain) with an absorbing cylinder
+    for tag, n_sur in (("lune1", 1.0), ("lune12", 1.2)):
+        im = med.IndexModel(cv, type="analytical", form="luneburg_lens", R=0.9, p=2, n_sur=n_sur)
+        am = med.AttenuationModel(cv, type="analytical", form="homogeneous_cylinder", R=1, alpha_internal=15.0)
+        f, g, gin, dose = _ray_run(vam, tg, im, am, am, ang, "physical_path_length", "forward_symplectic_euler", rng)
+        out[tag + "_f"], out[tag + "_fwd"], out[tag + "_g"], out[tag + "_bwd"] = f, g, gin, dose
+        out[tag + "_params"] = np.array([0.9, 2.0, n_sur])
+    # analytic homogeneous ball attenuation (radius 0.8 of the domain) in a homogeneous index
+    im = med.IndexModel(cv, type="analytical", form="homogeneous", n_sur=1.0)
+    am = med.AttenuationModel(cv, type="analytical", form="homogeneous_ball", R=0.8, alpha_internal=25.0)
+    f, g, gin, dose = _ray_run(vam, tg, im, am, am, ang, "physical_path_length", "forward_symplectic_euler", rng)
+    out["ball_f"], out["ball_fwd"], out["ball_g"], out["ball_bwd"] = f, g, gin, dose
+    out["ball_params"] = np.array([0.8, 25.0])
+    # dose metrics on a seeded target and dose
+    t = ellipses_target(20, 3, rng)
+    tg2 = geo.TargetGeometry(target=t.copy())
+    dose = rng.uniform(0, 1, t.shape) + 0.5 * t
+    out["m_target"], out["m_dose"] = t, dose
+    M = vam.metrics
+    # (the reference's layerwise=True branches index a 2-D slice with the 3-D gel / void masks and raise
+    # IndexError, metrics.py:78-90, 118-127, 158-166, so only the whole-volume values are stored)
+    out["m_ver"], out["m_ipdr"], out["m_pw"] = M.calcVER(tg2, dose), M.calcIPDR(tg2, dose), M.calcPW(tg2, dose)
+    out["m_cv"] = M.calcCV(tg2, dose)
+    np.savez_compressed(OUT / "options.npz", **out)
+
+
+def analytic_response_cases(vam):
+    """BCLP with the reference's analytical generalised-logistic response model (evaluated in closed
+    form, not by the interpolation table), p = 2 and p = 4 with weights."""
+    geo = vam.geometry
+    out = {}
+    rng = np.random.default_rng(31)
+    n, nz = 24, 2
+    t = ellipses_target(n, nz, rng)
+    # the analytical inverse map is -inf at a response of 0 (and the filtered initial sinogram NaN), so the
+    # target's responses stay inside (0, 1), with no circle clip to zero the corners
+    tgray = 0.05 + 0.9 * np.clip(t * 0.8 + 0.1 * rng.uniform(0, 1, t.shape), 0, 1)
+    ang = np.linspace(0, 360, 18, endpoint=False)
+    out["target"], out["angles"] = tgray, ang
+    w = np.where(tgray > 0.15, 1.0, 0.5)
+    out["weight"] = w
+    for p, wt, lr in ((2, 1, 0.002), (4, w, 0.02)):
+        rm = vam.response.ResponseModel(type="analytical", form="gen_log_fun", B=12, M=0.6)
+        tg = geo.TargetGeometry(target=tgray.copy(), clip_to_circle=False)
+        pg = geo.ProjectionGeometry(ang, "parallel", CUDA=False, attenuation_field=np.zeros((n, n, nz)))
+        opts = refload.fresh_options(vam, method="BCLP", n_iter=4, p=p, q=1, eps=0.05, weight=wt, learning_rate=lr,
+                                     response_model=rm, filter="ram-lak")
+        sino, dose, mapped, logs = vam.optimize.optimize(tg, pg, opts, output="full")
+        out[f"p{p}_sino"], out[f"p{p}_dose"], out[f"p{p}_mapped"] = sino.array, dose.array, mapped.array
+        out[f"p{p}_loss"] = logs.loss
+    np.savez_compressed(OUT / "analytic_bclp.npz", **out)
 
 
 GROUPS = {"parallel": parallel_cases, "ray": ray_cases, "algebraic": algebraic_cases,
           "ray_autograd": ray_autograd_cases, "optim": optimizer_cases, "formats": format_cases,
-          "vecgeom": vecgeom_cases, "occ2d": occ2d_cases}
+          "vecgeom": vecgeom_cases, "occ2d": occ2d_cases, "options": option_cases,
+          "analytic_bclp": analytic_response_cases}
 
 
 def main():

@@ -159,3 +159,60 @@ def test_device_filters_match_reference(golden):
         x = np.random.default_rng(1).uniform(size=(20, 20, 3))
         assert np.allclose(udata.filterTargetOSMO_t(torch.as_tensor(x, device="cuda"), name).cpu().numpy(),
                            udata.filterTargetOSMO(x, name), atol=1e-10), name
+
+
+@pytest.mark.parametrize("engine", ["device", "host"])
+@pytest.mark.parametrize("p", [2, 4])
+def test_bclp_analytic_response_matches_reference(golden, engine, p):
+    """BCLP with ResponseModel(type="analytical", form="gen_log_fun"): the fused device pass evaluates the
+    generalised logistic and its derivative in closed form (float64 per voxel), no table."""
+    from vamtoolbox_b200.optimize import optimize
+    from vamtoolbox_b200.response import ResponseModel
+
+    from vamtoolbox_b200 import geometry
+
+    A = golden["analytic_bclp"]
+    tg = geometry.TargetGeometry(target=A["target"].copy(), clip_to_circle=False)
+    pg = geometry.ProjectionGeometry(A["angles"], "parallel", CUDA=True)
+    rm = ResponseModel(type="analytical", form="gen_log_fun", B=12, M=0.6)
+    w, lr = (1, 0.002) if p == 2 else (A["weight"], 0.02)
+    sino, dose, mapped, logs = optimize(tg, pg, opts(method="BCLP", n_iter=4, p=p, q=1, eps=0.05, weight=w,
+                                                     learning_rate=lr, response_model=rm, filter="ram-lak",
+                                                     engine=engine), output="full")
+    assert relL2(sino.array, A[f"p{p}_sino"]) < 1e-4
+    assert relL2(dose.array, A[f"p{p}_dose"]) < 1e-4
+    assert relL2(mapped.array, A[f"p{p}_mapped"]) < 1e-4
+    assert np.allclose(logs.loss, A[f"p{p}_loss"], rtol=1e-4)
+
+
+@pytest.mark.parametrize("form,kw", [("linear", {"M": 0.8, "C": 0.05}), ("identity", {})])
+def test_bclp_closed_form_linear_identity_match_host_engine(form, kw):
+    """The linear and identity closed forms on the device against the reference's numpy loop (host engine)."""
+    from vamtoolbox_b200.optimize import optimize
+    from vamtoolbox_b200.response import ResponseModel
+
+    rng = np.random.default_rng(8)
+    t = np.clip(rng.uniform(size=(24, 24, 4)), 0, 1)
+    ang = np.linspace(0, 360, 18, endpoint=False)
+    res = []
+    for engine in ("device", "host"):
+        tg, pg = geo(t, ang)
+        rm = ResponseModel(type="analytical", form=form, **kw)
+        res.append(optimize(tg, pg, opts(method="BCLP", n_iter=3, p=2, q=1, eps=0.05, learning_rate=0.002,
+                                         response_model=rm, engine=engine), output="full"))
+    assert relL2(res[0][0].array, res[1][0].array) < 1e-4
+    assert relL2(res[0][2].array, res[1][2].array) < 1e-4
+
+
+def test_device_metrics_match_reference(golden):
+    """calcVER / calcIPDR of a CUDA tensor (fused device reductions) against the reference's values."""
+    import torch
+
+    from vamtoolbox_b200 import geometry, metrics
+
+    G = golden["options"]
+    tg = geometry.TargetGeometry(target=G["m_target"].copy())
+    d = torch.as_tensor(G["m_dose"], device="cuda")
+    n = np.sum(tg.gel_inds) + np.sum(tg.void_inds)
+    assert abs(metrics.calcVER(tg, d) - G["m_ver"]) * n <= 1.0 + 1e-9
+    assert abs(metrics.calcIPDR(tg, d) - G["m_ipdr"]) <= 1e-6 * abs(G["m_ipdr"])

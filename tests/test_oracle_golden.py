@@ -172,13 +172,20 @@ def test_occlusion_2d_digitised_matches_reference(golden):
     """The 2-D class's digitised occlusion (np.digitize bins, least occluded s per bin) and its shadowed
     forward and backward: the oracle's restatement gives the reference's outputs exactly."""
     G = golden["occ2d"]
-    for tag in ("even", "odd"):
+    for tag in ("even", "odd", "wrap"):
         occ, x, ang = G[f"{tag}_occ"], G[f"{tag}_x"], G[f"{tag}_angles"]
         sino = O.occlusion_sinogram_2d(occ, ang)
         assert np.array_equal(sino, G[f"{tag}_sino"], equal_nan=True)
         assert np.isfinite(sino).any() and np.isnan(sino).any()
         assert relL2(O.parallel_forward_2d_occluded(x, ang, sino), G[f"{tag}_fwd"]) < 1e-14
         assert relL2(O.parallel_backward_2d_occluded(G[f"{tag}_b"], ang, sino), G[f"{tag}_bwd"]) < 1e-14
+        if tag != "wrap":
+            assert relL2(O.parallel_backward_2d_occluded(G[f"{tag}_b"], ang, sino, clipping=False),
+                         G[f"{tag}_bwd_noclip"]) < 1e-14
         # the shadow matters: without it the forward differs
         free = O.parallel_forward(O.clip_to_circle(x)[:, :, None], ang)[:, :, 0]
         assert relL2(free, G[f"{tag}_fwd"]) > 0.1
+    # the corner occluder of "clash" fills the last bin and wraps onto it: the reference raises
+    with pytest.raises(ValueError, match="shape mismatch"):
+        O.occlusion_sinogram_2d(G["clash_occ"], G["clash_angles"])
+    assert "shape mismatch" in str(G["clash_error"])

@@ -37,6 +37,7 @@ class VamError(RuntimeError):
     def __init__(self, func, code, msg):
         super().__init__(f"{func} failed with {_STATUS.get(code, code)}: {msg}")
         self.code = code
+        self.message = msg
 
 
 class ParallelGeom(ctypes.Structure):
@@ -73,7 +74,12 @@ class Work(ctypes.Structure):
 class BclpParams(ctypes.Structure):
     _fields_ = [("table_f", _vp), ("table_map", _vp), ("table_dmap", _vp), ("n_table", _c_i32),
                 ("table_f0", _c_f), ("table_inv_step", _c_f),
-                ("eps", _c_f), ("weight", _c_f), ("p", _c_f), ("eps_dev", _vp), ("weight_dev", _vp)]
+                ("eps", _c_f), ("weight", _c_f), ("p", _c_f), ("eps_dev", _vp), ("weight_dev", _vp),
+                ("response", _c_i32), ("resp_A", _c_d), ("resp_K", _c_d), ("resp_B", _c_d), ("resp_M", _c_d),
+                ("resp_nu", _c_d), ("resp_C", _c_d)]
+
+
+RESP_TABLE, RESP_GLF, RESP_LINEAR, RESP_IDENTITY = 0, 1, 2, 3
 
 
 # name -> (argtypes, restype)
@@ -99,10 +105,13 @@ _SIGS = {
     "vam_parallel_plan_destroy": ([_vp], _c_int),
     "vam_parallel_set_absorption": ([_vp, _c_int, _vp, _c_f, _c_f, _vp], _c_int),
     "vam_parallel_set_occlusion": ([_vp, _vp, _vp], _c_int),
+    "vam_parallel_set_occlusion_2d": ([_vp, _vp, _vp], _c_int),
+    "vam_parallel_get_occlusion_sinogram_2d": ([_vp, _vp, _vp], _c_int),
     "vam_parallel_clear_occlusion": ([_vp], _c_int),
     "vam_parallel_get_occlusion_sinogram": ([_vp, _vp, _vp], _c_int),
     "vam_parallel_forward": ([_vp, _vp, _vp, _vp], _c_int),
     "vam_parallel_backward_ref": ([_vp, _vp, _vp, _vp], _c_int),
+    "vam_parallel_backward_ref_noclip": ([_vp, _vp, _vp, _vp], _c_int),
     "vam_parallel_adjoint": ([_vp, _vp, _vp, _vp], _c_int),
     "vam_parallel_prepare_adjoint": ([_vp, _vp], _c_int),
     "vam_parallel_set_tuning": ([_vp, ctypes.POINTER(ParallelTuning)], _c_int),
@@ -126,6 +135,7 @@ _SIGS = {
     "vam_reduce": ([_vp, _c_i64, _c_int, _vp, _vp, ctypes.c_size_t, _vp], _c_int),
     "vam_reduce_noalloc": ([_vp, _c_i64, _c_int, _vp, _vp], _c_int),
     "vam_metric_ver": ([_vp, _vp, _c_i64, _vp, _vp, ctypes.c_size_t, _vp], _c_int),
+    "vam_metric_ipdr": ([_vp, _vp, _c_i64, _vp, _vp, ctypes.c_size_t, _vp], _c_int),
     "vam_bclp_dose_pass": ([_vp, _vp, _c_i64, ctypes.POINTER(BclpParams), _vp, _vp, _vp, _vp, ctypes.c_size_t, _vp],
                            _c_int),
     "vam_bclp_sino_update": ([_vp, _vp, _c_i64, _c_f, _c_f, _c_f, _c_f, _c_f, _c_int, _vp, _vp], _c_int),

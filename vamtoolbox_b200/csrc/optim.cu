@@ -134,6 +134,32 @@ __global__ void __launch_bounds__(kThreads) k_ver_final(const double* __restrict
 }
 
 // ---------------------------------------------------------------------------
+// IPDR (metrics.py:130-156): max - min over gel voxels
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_ipdr_partial(const float* __restrict__ x, const uint8_t* __restrict__ m,
+                                                           int64_t n, double* __restrict__ part) {
+    double mn = INFINITY, mx = -INFINITY;
+    for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads) {
+        if (m[i] == 1) {
+            const double v = (double)x[i];
+            mn = fmin(mn, v);
+            mx = fmax(mx, v);
+        }
+    }
+    mn = block_reduce<double, VAM_RED_MIN>(mn);
+    mx = block_reduce<double, VAM_RED_MAX>(mx);
+    if (threadIdx.x == 0) { part[blockIdx.x] = mn; part[kMaxBlocks + blockIdx.x] = mx; }
+}
+
+__global__ void __launch_bounds__(kThreads) k_ipdr_final(const double* __restrict__ part, int nb, float* __restrict__ out) {
+    double mn = INFINITY, mx = -INFINITY;
+    for (int i = threadIdx.x; i < nb; i += kThreads) { mn = fmin(mn, part[i]); mx = fmax(mx, part[kMaxBlocks + i]); }
+    mn = block_reduce<double, VAM_RED_MIN>(mn);
+    mx = block_reduce<double, VAM_RED_MAX>(mx);
+    if (threadIdx.x == 0) out[0] = (mn <= mx) ? (float)(mx - mn) : __int_as_float(0x7fc00000);
+}
+
+// ---------------------------------------------------------------------------
 // BCLP dose pass (BCLP.py:293-437)
 // ---------------------------------------------------------------------------
 struct TableRef {
@@ -142,6 +168,8 @@ struct TableRef {
     const float* dm;
     int n;
     float f0, inv_step;
+    int kind;                            // vam_response_kind
+    double A, K, B, M, nu, C;            // closed-form parameters
 };
 
 // np.interp(d, f, y, left=y[0], right=y[-1]) on a uniformly spaced table
@@ -162,6 +190,33 @@ __device__ __forceinline__ void table_interp(const TableRef& t, float d, float& 
     out_dm = fmaf(w, t.dm[j + 1] - t.dm[j], t.dm[j]);
 }
 
+// Closed-form response models in float64, in the reference's operation order
+// (response.py:191-218 _map_glf / _dmapdf_glf, :239-250 linear, :252-262 identity).
+__device__ __forceinline__ void response_eval(const TableRef& t, float d, float& out_m, float& out_dm) {
+    if (t.kind == VAM_RESP_TABLE) {
+        table_interp(t, d, out_m, out_dm);
+        return;
+    }
+    if (t.kind == VAM_RESP_LINEAR) {
+        out_m = (float)(t.M * (double)d + t.C);
+        out_dm = (float)t.M;
+        return;
+    }
+    if (t.kind == VAM_RESP_IDENTITY) {
+        out_m = d;
+        out_dm = 1.f;
+        return;
+    }
+    const double e = exp(-t.B * ((double)d - t.M));
+    const double onep = 1.0 + e;
+    const double m = t.A + (t.K - t.A) / (t.nu == 1.0 ? onep : pow(onep, 1.0 / t.nu));
+    const double c1 = t.nu == 1.0 ? 1.0 / (t.K - t.A) : pow(1.0 / (t.K - t.A), t.nu);
+    const double y = m - t.A;
+    const double c3 = t.nu == 1.0 ? y * y : pow(y, t.nu + 1.0);
+    out_m = (float)m;
+    out_dm = (float)(c1 * (t.B / t.nu) * c3 * e);
+}
+
 __device__ __forceinline__ float powabs(float a, float p) {
     if (p == 2.f) return a * a;
     if (p == 1.f) return a;
@@ -180,7 +235,7 @@ struct DoseStats {
 __device__ __forceinline__ void dose_voxel(const TableRef& tab, float d, float tgt, float ep, float w, float p,
                                            float& mp, float& op, DoseStats& S) {
     float dmp;
-    table_interp(tab, d, mp, dmp);
+    response_eval(tab, d, mp, dmp);
     const float e = mp - tgt;
     const float ae = fabsf(e);
     const float eb = ae - ep;
@@ -467,6 +522,21 @@ extern "C" int vam_reduce_noalloc(const float* x, int64_t n, int op, float* out,
     return VAM_OK;
 }
 
+extern "C" int vam_metric_ipdr(const float* x, const uint8_t* mask, int64_t n, float* out, void* work,
+                               size_t work_bytes, vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(x && mask && out && work, VAM_ERR_ARG, "vam_metric_ipdr: null argument");
+    VAM_REQUIRE(n > 0, VAM_ERR_SHAPE, "vam_metric_ipdr: empty input");
+    VAM_REQUIRE(work_bytes >= kWorkBytes, VAM_ERR_ARG, "vam_metric_ipdr: workspace too small");
+    const int nb = blocks_for(n);
+    cudaStream_t st = (cudaStream_t)stream;
+    double* part = (double*)work;
+    k_ipdr_partial<<<nb, kThreads, 0, st>>>(x, mask, n, part);
+    k_ipdr_final<<<1, kThreads, 0, st>>>(part, nb, out);
+    VAM_CHECK_LAUNCH("vam_metric_ipdr");
+    return VAM_OK;
+}
+
 extern "C" int vam_metric_ver(const float* x, const uint8_t* mask, int64_t n, float* out, void* work,
                               size_t work_bytes, vam_stream_t stream) {
     clear_error();
@@ -489,16 +559,24 @@ extern "C" int vam_bclp_dose_pass(const float* dose, const float* target, int64_
                                   vam_stream_t stream) {
     clear_error();
     VAM_REQUIRE(dose && target && prm && operand && stats && work, VAM_ERR_ARG, "vam_bclp_dose_pass: null argument");
-    VAM_REQUIRE(prm->table_f && prm->table_map && prm->table_dmap && prm->n_table >= 2, VAM_ERR_ARG,
-                "vam_bclp_dose_pass: response table needs >= 2 points");
+    VAM_REQUIRE(prm->response >= VAM_RESP_TABLE && prm->response <= VAM_RESP_IDENTITY, VAM_ERR_ARG,
+                "vam_bclp_dose_pass: unknown response kind");
+    VAM_REQUIRE(prm->response != VAM_RESP_TABLE ||
+                    (prm->table_f && prm->table_map && prm->table_dmap && prm->n_table >= 2),
+                VAM_ERR_ARG, "vam_bclp_dose_pass: response table needs >= 2 points");
+    VAM_REQUIRE(prm->response != VAM_RESP_GLF || (prm->resp_K != prm->resp_A && prm->resp_nu != 0.0),
+                VAM_ERR_ARG, "vam_bclp_dose_pass: generalised logistic needs K != A and nu != 0");
     VAM_REQUIRE(n > 0, VAM_ERR_SHAPE, "vam_bclp_dose_pass: empty input");
     VAM_REQUIRE(work_bytes >= kWorkBytes, VAM_ERR_ARG, "vam_bclp_dose_pass: workspace too small");
     VAM_REQUIRE(std::isfinite(prm->p) && prm->p > 0.f, VAM_ERR_ARG, "vam_bclp_dose_pass: p must be > 0");
-    // The table is uniform (np.linspace): table_f0 / table_inv_step seed the bin
-    // search, which is then corrected against the table values themselves.
+    // table_f0 / table_inv_step seed the bin search as if the table were uniform
+    // (np.linspace); the search then walks to the bin against the table values
+    // themselves, so any strictly increasing table gives np.interp's bin.
     TableRef t;
     t.f = prm->table_f; t.m = prm->table_map; t.dm = prm->table_dmap; t.n = prm->n_table;
     t.f0 = prm->table_f0; t.inv_step = prm->table_inv_step;
+    t.kind = prm->response;
+    t.A = prm->resp_A; t.K = prm->resp_K; t.B = prm->resp_B; t.M = prm->resp_M; t.nu = prm->resp_nu; t.C = prm->resp_C;
     const int nb = blocks_for(n);
     cudaStream_t st = (cudaStream_t)stream;
     double* part = (double*)work;

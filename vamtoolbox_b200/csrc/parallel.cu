@@ -67,9 +67,11 @@ struct Args {
     const float* mask;
     const float* occ;
     const uint8_t* occ_flag;
+    const double* occ64;  // occ_mode 1: float64 minima [nR][nA] of the digitised 2-D occlusion
     int nY, nX, nZ, nA, C;
     int lz_shift, zvec, zchunks;
     float alpha, R;  // VAM_ABS_RAY
+    int occ_mode, pad_;
 };
 
 template <int VZ>
@@ -1096,10 +1098,17 @@ __device__ __forceinline__ void k_backward_ref_body(const Args& a, unsigned bx, 
             }
             if (OCC && zok) {
                 const double sv = __dadd_rn(__dmul_rn(X, tr.y), __dmul_rn(Y, tr.x));
+                if (a.occ_mode == 1) {
+                    // 2-D class (getOccShadow, Projector2DParallel.py:235-247): s against the minimum of t's
+                    // np.digitize bin, which for t inside the detector is the interpolation bin j0; NaN
+                    // (no occluder) compares false
+                    if (sv > a.occ64[(size_t)j0 * a.nA + th]) v[0] = 0.f;
+                } else {
 #pragma unroll
-                for (int e = 0; e < VZ; ++e) {
-                    const double o = interp_nan(t, ft, j0, a.nY, a.C, a.occ + (size_t)th * a.nZ + z0 + e, rs);
-                    if (sv > floor(o)) v[e] = 0.f;
+                    for (int e = 0; e < VZ; ++e) {
+                        const double o = interp_nan(t, ft, j0, a.nY, a.C, a.occ + (size_t)th * a.nZ + z0 + e, rs);
+                        if (sv > floor(o)) v[e] = 0.f;
+                    }
                 }
             }
             if (ABS == VAM_ABS_RAY) {
@@ -1287,6 +1296,82 @@ __global__ void k_occ_flag(const float* __restrict__ occ, uint8_t* __restrict__ 
     flag[idx] = f;
 }
 
+// ---------------------------------------------------------------------------
+// The 2-D class's digitised occlusion sinogram (Projector2DParallel.py:70-143).
+// Per angle every occluded pixel's detector coordinate t = x cos - y sin goes to
+// its np.digitize bin over proj_t (index -1, i.e. the last bin's value, below
+// the first bin), and each bin keeps the least s = x sin + y cos of its pixels.
+// Slots: [nA][n + 1], slot 0 the wrapped index -1, slot 1 + k bin k; minima by
+// atomicMin on an order-preserving integer key of the float64 s (exact and
+// independent of the order of the atomics).
+// ---------------------------------------------------------------------------
+constexpr unsigned long long kOccEmpty = ~0ull;
+
+__device__ __forceinline__ unsigned long long occ_key(double v) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+}
+
+__device__ __forceinline__ double occ_value(unsigned long long k) {
+    const unsigned long long b = (k & 0x8000000000000000ull) ? (k & 0x7fffffffffffffffull) : ~k;
+    return __longlong_as_double((long long)b);
+}
+
+__global__ void __launch_bounds__(256) k_occ2d_bin(const uint8_t* __restrict__ occlusion,
+                                                   const double4* __restrict__ trig,
+                                                   unsigned long long* __restrict__ slots, int n, int nA, int C) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;  // over (angle, pixel)
+    if (idx >= (long long)nA * n * n) return;
+    const int p = (int)(idx % ((long long)n * n));
+    const int th = (int)(idx / ((long long)n * n));
+    if (!occlusion[p]) return;
+    const double X = (double)(p % n - C), Y = (double)(p / n - C);
+    const double4 tr = trig[th];
+    const double t = __dsub_rn(__dmul_rn(X, tr.x), __dmul_rn(Y, tr.y));
+    const double s = __dadd_rn(__dmul_rn(X, tr.y), __dmul_rn(Y, tr.x));
+    const int k = t < (double)(-C) ? 0 : 1 + min((int)floor(t) + C, n - 1);
+    atomicMin(slots + (size_t)th * (n + 1) + k, occ_key(s));
+}
+
+// One thread per angle: the reference pairs the sorted unique bin indices with the per-bin minima
+// sorted by bin value.  Without a wrapped index that is each bin's own minimum; with one (index -1,
+// valued as the last bin) the minima shift by one bin, and if the last bin is occupied as well the
+// two lists differ in length and the reference raises (flag bit 1).  An empty occlusion makes the
+// reference take the minimum of an empty group (flag bit 2).
+__global__ void k_occ2d_assign(const unsigned long long* __restrict__ slots, double* __restrict__ occ64,
+                               float* __restrict__ occ, uint8_t* __restrict__ flag, int* __restrict__ err, int n,
+                               int nA) {
+    const int th = blockIdx.x * blockDim.x + threadIdx.x;
+    if (th >= nA) return;
+    const unsigned long long* sl = slots + (size_t)th * (n + 1);
+    const double qnan = __longlong_as_double(0x7ff8000000000000LL);
+    for (int j = 0; j < n; ++j) occ64[(size_t)j * nA + th] = qnan;
+    const unsigned long long wrap = sl[0];
+    bool any = wrap != kOccEmpty;
+    if (wrap == kOccEmpty) {
+        for (int j = 0; j < n; ++j)
+            if (sl[1 + j] != kOccEmpty) { occ64[(size_t)j * nA + th] = occ_value(sl[1 + j]); any = true; }
+    } else if (sl[n] != kOccEmpty) {
+        atomicOr(err, 1);
+    } else {
+        int prev = n - 1;
+        for (int j = 0; j < n - 1; ++j) {
+            if (sl[1 + j] == kOccEmpty) continue;
+            occ64[(size_t)prev * nA + th] = occ_value(sl[1 + j]);
+            prev = j;
+        }
+        occ64[(size_t)prev * nA + th] = occ_value(wrap);
+    }
+    if (!any) atomicOr(err, 2);
+    // the forward's shadow test compares the integer sample coordinate k - C with the minimum:
+    // k - C > v <=> k - C > floor(v), so the forward table holds floor(v) (exact in float32)
+    for (int j = 0; j < n; ++j) {
+        const double v = occ64[(size_t)j * nA + th];
+        occ[(size_t)j * nA + th] = isnan(v) ? __double2float_rn(v) : (float)floor(v);
+    }
+    flag[th] = 1;
+}
+
 enum class Op { Forward, BackwardRef, Adjoint };
 
 // Slices per lane of the fast kernels for nZ slices (0 = use the generic
@@ -1335,8 +1420,10 @@ struct Item {
 };
 static_assert(sizeof(Item) % 8 == 0, "Item is copied to shared memory in 8-byte words");
 
-int describe(vam_parallel_plan* plan, Op op, const float* in, float* out, Item& it, const char* name) {
+int describe(vam_parallel_plan* plan, Op op, const float* in, float* out, Item& it, const char* name,
+             bool noclip = false) {
     VAM_REQUIRE(plan && in && out, VAM_ERR_ARG, std::string(name) + ": null argument");
+    VAM_REQUIRE(!noclip || plan->d_ones, VAM_ERR_ARG, std::string(name) + ": no all-ones circle table");
     std::memset(&it, 0, sizeof(it));
     it.cost = (long long)plan->nY * plan->nX * plan->nZ * plan->nA;
     it.family = op == Op::Forward ? 1 : (op == Op::BackwardRef ? 2 : 4);
@@ -1353,7 +1440,7 @@ int describe(vam_parallel_plan* plan, Op op, const float* in, float* out, Item& 
     // 2-D slice: shared-memory tiles when tuned to them (any width but 1), or automatically for
     // slices wide enough to fill the device with tiles (forward from 192, backprojection from 320 px)
     const bool tiles_2d = want == 0 ? plan->nX >= (op == Op::Forward ? 192 : 320) : want != 1;
-    if (plan->nZ == 1 && !plan->has_occ && op != Op::Adjoint && tiles_2d) {
+    if (plan->nZ == 1 && !plan->has_occ && op != Op::Adjoint && tiles_2d && !noclip) {
         Args& a = it.a;
         a.in = in; a.out = out; a.trig = plan->d_trig; a.circle = plan->d_circle;
         a.mask = plan->abs_mode == VAM_ABS_MASK ? plan->d_mask : nullptr;
@@ -1401,7 +1488,8 @@ int describe(vam_parallel_plan* plan, Op op, const float* in, float* out, Item& 
         it.gy = (unsigned)(ray ? plan->nA : plan->n_tasks_paired);
         return VAM_OK;
     }
-    if (op != Op::Forward && !plan->has_occ && vzf && (long long)plan->nY * plan->nA * plan->nZ < (1LL << 31)) {
+    if (op != Op::Forward && !plan->has_occ && vzf && !noclip &&
+        (long long)plan->nY * plan->nA * plan->nZ < (1LL << 31)) {
         Args& a = it.a;
         a.in = in; a.out = out; a.trig = plan->d_trig; a.circle = plan->d_circle;
         a.mask = plan->abs_mode == VAM_ABS_MASK ? plan->d_mask : nullptr;
@@ -1432,8 +1520,9 @@ int describe(vam_parallel_plan* plan, Op op, const float* in, float* out, Item& 
     const bool aligned = (((uintptr_t)in | (uintptr_t)out) & 15) == 0;
     Layout L = choose_layout(plan->nZ, aligned);
     Args& a = it.a;
-    a.in = in; a.out = out; a.trig = plan->d_trig; a.circle = plan->d_circle;
+    a.in = in; a.out = out; a.trig = plan->d_trig; a.circle = noclip ? plan->d_ones : plan->d_circle;
     a.mask = plan->d_mask; a.occ = plan->d_occ; a.occ_flag = plan->d_occ_flag;
+    a.occ64 = plan->d_occ64; a.occ_mode = plan->has_occ ? plan->occ_mode : 0;
     a.nY = plan->nY; a.nX = plan->nX; a.nZ = plan->nZ; a.nA = plan->nA; a.C = plan->C;
     a.lz_shift = L.lz_shift; a.zvec = L.zvec; a.zchunks = L.zchunks;
     a.alpha = plan->abs_alpha; a.R = plan->abs_R;
@@ -1615,12 +1704,13 @@ int launch_item(const Item& it, cudaStream_t st, const char* name) {
     return VAM_OK;
 }
 
-int run(vam_parallel_plan* plan, Op op, const float* in, float* out, cudaStream_t st, const char* name) {
+int run(vam_parallel_plan* plan, Op op, const float* in, float* out, cudaStream_t st, const char* name,
+        bool noclip = false) {
     VAM_REQUIRE(plan, VAM_ERR_ARG, std::string(name) + ": null argument");
     DeviceGuard g(plan->device);
     VAM_REQUIRE(g.ok, VAM_ERR_CUDA, std::string(name) + ": cannot select device");
     Item it;
-    const int rc = describe(plan, op, in, out, it, name);
+    const int rc = describe(plan, op, in, out, it, name, noclip);
     if (rc != VAM_OK) return rc;
     return launch_item(it, st, name);
 }
@@ -1831,6 +1921,8 @@ extern "C" int vam_parallel_plan_destroy(vam_parallel_plan* p) {
     cudaFree(p->d_mask);
     cudaFree(p->d_occ);
     cudaFree(p->d_occ_flag);
+    cudaFree(p->d_occ64);
+    cudaFree(p->d_ones);
     cudaFree(p->d_tasks_paired);
     cudaFree(p->d_tasks_single);
     cudaFree(p->d_vol_scratch);
@@ -1879,6 +1971,48 @@ extern "C" int vam_parallel_set_occlusion(vam_parallel_plan* p, const float* ins
     k_occ_flag<<<(unsigned)((nf + 255) / 256), 256, 0, st>>>(p->d_occ, p->d_occ_flag, p->nX, p->nA, p->nZ);
     VAM_CHECK_LAUNCH("k_occ_flag");
     p->has_occ = 1;
+    p->occ_mode = 0;
+    return VAM_OK;
+}
+
+extern "C" int vam_parallel_set_occlusion_2d(vam_parallel_plan* p, const uint8_t* occlusion_dev, vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(p && occlusion_dev, VAM_ERR_ARG, "vam_parallel_set_occlusion_2d: null argument");
+    VAM_REQUIRE(p->nZ == 1, VAM_ERR_SHAPE, "vam_parallel_set_occlusion_2d: the digitised occlusion is for 2-D plans (n_z == 1)");
+    DeviceGuard g(p->device);
+    const int n = p->nY;
+    const size_t ns = (size_t)n * p->nA;
+    if (!p->d_occ) VAM_TRY_CUDA(cudaMalloc(&p->d_occ, sizeof(float) * ns));
+    if (!p->d_occ_flag) VAM_TRY_CUDA(cudaMalloc(&p->d_occ_flag, (size_t)p->nA));
+    if (!p->d_occ64) VAM_TRY_CUDA(cudaMalloc(&p->d_occ64, sizeof(double) * ns));
+    cudaStream_t st = (cudaStream_t)stream;
+    unsigned long long* slots = nullptr;
+    int* d_err = nullptr;
+    const size_t nslots = (size_t)(n + 1) * p->nA;
+    VAM_TRY_CUDA(cudaMalloc(&slots, sizeof(unsigned long long) * nslots + 256));
+    d_err = reinterpret_cast<int*>(reinterpret_cast<char*>(slots) + sizeof(unsigned long long) * nslots);
+    int h_err = 0;
+    cudaError_t e = cudaMemsetAsync(slots, 0xff, sizeof(unsigned long long) * nslots, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_err, 0, sizeof(int), st);
+    if (e == cudaSuccess) {
+        const long long np = (long long)p->nA * n * n;
+        k_occ2d_bin<<<(unsigned)((np + 255) / 256), 256, 0, st>>>(occlusion_dev, p->d_trig, slots, n, p->nA, p->C);
+        k_occ2d_assign<<<(unsigned)((p->nA + 127) / 128), 128, 0, st>>>(slots, p->d_occ64, p->d_occ, p->d_occ_flag,
+                                                                        d_err, n, p->nA);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(slots);
+    if (e != cudaSuccess) return set_error(VAM_ERR_CUDA, std::string("vam_parallel_set_occlusion_2d: ") + cudaGetErrorString(e));
+    if (h_err & 2)
+        return set_error(VAM_ERR_SHAPE, "vam_parallel_set_occlusion_2d: zero-size array to reduction operation minimum "
+                                        "which has no identity (the occlusion is empty)");
+    if (h_err & 1)
+        return set_error(VAM_ERR_SHAPE, "vam_parallel_set_occlusion_2d: shape mismatch: occluded pixels below the "
+                                        "first detector bin and in the last bin at the same angle");
+    p->has_occ = 1;
+    p->occ_mode = 1;
     return VAM_OK;
 }
 
@@ -1886,6 +2020,17 @@ extern "C" int vam_parallel_clear_occlusion(vam_parallel_plan* p) {
     clear_error();
     VAM_REQUIRE(p, VAM_ERR_ARG, "vam_parallel_clear_occlusion: null plan");
     p->has_occ = 0;
+    return VAM_OK;
+}
+
+extern "C" int vam_parallel_get_occlusion_sinogram_2d(vam_parallel_plan* p, double* out_dev, vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(p && out_dev, VAM_ERR_ARG, "vam_parallel_get_occlusion_sinogram_2d: null argument");
+    VAM_REQUIRE(p->has_occ && p->occ_mode == 1, VAM_ERR_ARG,
+                "vam_parallel_get_occlusion_sinogram_2d: no digitised 2-D occlusion set");
+    DeviceGuard g(p->device);
+    VAM_TRY_CUDA(cudaMemcpyAsync(out_dev, p->d_occ64, sizeof(double) * (size_t)p->nY * p->nA, cudaMemcpyDeviceToDevice,
+                                 (cudaStream_t)stream));
     return VAM_OK;
 }
 
@@ -1951,6 +2096,19 @@ extern "C" int vam_parallel_forward(vam_parallel_plan* p, const float* vol, floa
 extern "C" int vam_parallel_backward_ref(vam_parallel_plan* p, const float* sino, float* vol, vam_stream_t stream) {
     clear_error();
     return run(p, Op::BackwardRef, sino, vol, (cudaStream_t)stream, "vam_parallel_backward_ref");
+}
+
+extern "C" int vam_parallel_backward_ref_noclip(vam_parallel_plan* p, const float* sino, float* vol,
+                                                vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(p, VAM_ERR_ARG, "vam_parallel_backward_ref_noclip: null plan");
+    if (!p->d_ones) {
+        DeviceGuard g(p->device);
+        const size_t np = (size_t)p->nY * p->nX;
+        VAM_TRY_CUDA(cudaMalloc(&p->d_ones, np));
+        VAM_TRY_CUDA(cudaMemsetAsync(p->d_ones, 1, np, (cudaStream_t)stream));
+    }
+    return run(p, Op::BackwardRef, sino, vol, (cudaStream_t)stream, "vam_parallel_backward_ref_noclip", true);
 }
 
 extern "C" int vam_parallel_adjoint(vam_parallel_plan* p, const float* sino, float* vol, vam_stream_t stream) {

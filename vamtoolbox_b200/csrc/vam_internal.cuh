@@ -69,6 +69,12 @@ struct vam_parallel_plan {
     float* d_occ;           // [nR][nA][nZ] occlusion sinogram, NaN = none
     uint8_t* d_occ_flag;    // [nA][nZ] forward shadow gate
     int has_occ;
+    // 0: the 3-D class's occlusion (Projector3DParallel.py:77-111, 192-201); 1: the 2-D class's
+    // digitised occlusion (Projector2DParallel.py:70-143, 235-247), nZ == 1 only, whose
+    // backprojection compares s against the float64 minima in d_occ64 ([nR][nA])
+    int occ_mode;
+    double* d_occ64;
+    uint8_t* d_ones;        // [nY][nX] all ones: the circle table of a backprojection without clipping
     // angle tasks of the fast forward: (a, b) with b the angle 180 degrees from a
     // (both sampled from a's lattice), or b = -1 for an unpaired angle
     int2* d_tasks_paired;

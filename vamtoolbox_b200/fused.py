@@ -78,12 +78,29 @@ class Workspace:
 
 
 def bclp_params(response_model, eps, weight, p, device, keep):
-    """vam_bclp_params for an interpolation response model (tables on device)."""
-    f, m, dm, f0, inv_step = response_model.device_tables(device)
+    """vam_bclp_params for a response model: interpolation tables on the device, or the closed form
+    of an analytical generalised-logistic / linear / identity model (evaluated in float64 per voxel)."""
     prm = _lib.BclpParams()
-    prm.table_f, prm.table_map, prm.table_dmap = f.data_ptr(), m.data_ptr(), dm.data_ptr()
-    prm.n_table = f.numel()
-    prm.table_f0, prm.table_inv_step = f0, inv_step
+    rm = response_model
+    if rm.type == "interpolation":
+        f, m, dm, f0, inv_step = rm.device_tables(device)
+        prm.table_f, prm.table_map, prm.table_dmap = f.data_ptr(), m.data_ptr(), dm.data_ptr()
+        prm.n_table = f.numel()
+        prm.table_f0, prm.table_inv_step = f0, inv_step
+        prm.response = _lib.RESP_TABLE
+        keep += [f, m, dm]
+    elif rm.form == "gen_log_fun":
+        q = rm.params
+        prm.response = _lib.RESP_GLF
+        prm.resp_A, prm.resp_K, prm.resp_B = float(q["A"]), float(q["K"]), float(q["B"])
+        prm.resp_M, prm.resp_nu = float(q["M"]), float(q["nu"])
+    elif rm.form == "linear":
+        prm.response = _lib.RESP_LINEAR
+        prm.resp_M, prm.resp_C = float(rm.params["M"]), float(rm.params["C"])
+    elif rm.form == "identity":
+        prm.response = _lib.RESP_IDENTITY
+    else:
+        raise NotImplementedError(f"response model {rm.type}/{rm.form} has no device form")
     prm.p = float(p)
     if isinstance(eps, torch.Tensor):
         keep.append(eps)
@@ -95,7 +112,6 @@ def bclp_params(response_model, eps, weight, p, device, keep):
         prm.weight_dev, prm.weight = weight.data_ptr(), 0.0
     else:
         prm.weight = float(weight)
-    keep += [f, m, dm]
     return prm
 
 

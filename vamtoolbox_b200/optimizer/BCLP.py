@@ -189,8 +189,8 @@ class BCLPNorm:
                     plan.shape_vol, plan.shape_sino, P.device)
         raise TypeError("the device engine needs a vamtoolbox_b200 projector")
 
-    def _table_ok(self):
-        return getattr(self.response_model, "has_uniform_table", lambda: False)()
+    def _device_response_ok(self):
+        return getattr(self.response_model, "has_device_form", lambda: False)()
 
     def device_iteration(self, reduce_stats=None):
         """A :class:`DeviceIteration` holding this problem's device state (g = g0)."""
@@ -282,10 +282,10 @@ class DeviceIteration:
         self.log = torch.full((n_iter + 1, 9), float("nan"), dtype=torch.float32, device=dev)
         self.counter = torch.zeros(1, dtype=torch.int32, device=dev)
         self._keep = []
-        if not bclp._table_ok():
+        if not bclp._device_response_ok():
             raise NotImplementedError(
-                "the fused BCLP pass evaluates interpolation response models (the default); "
-                "use engine='host' for analytical or non-uniform response tables")
+                "the fused BCLP pass evaluates interpolation tables with increasing sample points and the "
+                "analytical gen_log_fun / linear / identity forms; use engine='host' for other response models")
         eps = f32(bclp.eps).reshape(vol_shape) if np.ndim(bclp.eps) else bclp.eps
         weight = f32(bclp.weight).reshape(vol_shape) if np.ndim(bclp.weight) else bclp.weight
         self.prm = bclp_params(bclp.response_model, eps, weight, bclp.p, dev, self._keep)

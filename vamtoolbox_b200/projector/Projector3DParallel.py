@@ -132,6 +132,32 @@ class ParallelPlan:
             torch.cuda.current_stream(self.device).synchronize()
         self.has_occlusion = True
 
+    def set_occlusion_2d(self, occlusion):
+        """The 2-D class's digitised occlusion (Projector2DParallel.py:70-143) from a boolean [nY, nX]
+        mask.  Raises ValueError where the reference's generateOccSinogram raises (an empty mask; occluded
+        pixels both below the first detector bin and in the last bin at one angle)."""
+        if self.shape_vol[2] != 1:
+            raise ValueError("the digitised occlusion is defined for 2-D (single-slice) plans")
+        occ = np.asarray(occlusion).reshape(-1)
+        if occ.size != self.shape_vol[0] * self.shape_vol[1]:
+            raise ValueError(f"occlusion must be {self.shape_vol[:2]}, got {np.shape(occlusion)}")
+        m = torch.as_tensor(np.ascontiguousarray(occ != 0, dtype=np.uint8), device=self.device)
+        with torch.cuda.device(self.device):
+            try:
+                _lib.call("vam_parallel_set_occlusion_2d", self._h, _lib.ptr(m), self._stream())
+            except _lib.VamError as exc:
+                if exc.code == _lib.VAM_ERR_SHAPE:
+                    raise ValueError(exc.message) from exc
+                raise
+        self.has_occlusion = True
+
+    def occlusion_sinogram_2d(self):
+        """The float64 bin minima of the digitised 2-D occlusion, [nY, n_angles], NaN for empty bins."""
+        out = torch.empty(self.shape_sino[:2], dtype=torch.float64, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.call("vam_parallel_get_occlusion_sinogram_2d", self._h, _lib.ptr(out), self._stream())
+        return out
+
     def occlusion_sinogram(self):
         out = torch.empty(self.shape_sino, dtype=torch.float32, device=self.device)
         with torch.cuda.device(self.device):
@@ -162,6 +188,16 @@ class ParallelPlan:
         self._check(out, self.shape_vol, "backward output")
         with torch.cuda.device(self.device):
             _lib.call("vam_parallel_backward_ref", self._h, _lib.ptr(sino), _lib.ptr(out), self._stream())
+        return out
+
+    def backward_ref_noclip(self, sino, out=None):
+        """backward_ref without the inscribed-circle clip (Projector2DParallel.py:188, 230-231)."""
+        self._check(sino, self.shape_sino, "backward input")
+        if out is None:
+            out = torch.empty(self.shape_vol, dtype=torch.float32, device=self.device)
+        self._check(out, self.shape_vol, "backward output")
+        with torch.cuda.device(self.device):
+            _lib.call("vam_parallel_backward_ref_noclip", self._h, _lib.ptr(sino), _lib.ptr(out), self._stream())
         return out
 
     def adjoint(self, sino, out=None):

@@ -4,7 +4,9 @@ Same constructor and methods as vamtoolbox/response.py:12-399 (generalised
 logistic / linear / identity / freeform forms, analytical or 512-point
 interpolation evaluation).  ``device_tables`` exposes the interpolation
 tables to the fused BCLP kernel (vam_bclp_dose_pass), which evaluates map and
-dmap/df with np.interp semantics (nearest-value extrapolation).
+dmap/df with np.interp semantics (nearest-value extrapolation); analytical
+generalised-logistic, linear and identity models are evaluated by the same
+kernel in closed form, in float64 per voxel.
 """
 from __future__ import annotations
 
@@ -144,6 +146,16 @@ class ResponseModel:
             return False
         d = np.diff(f)
         return bool(np.all(d > 0) and np.allclose(d, d[0], rtol=1e-9, atol=0))
+
+    def has_device_form(self):
+        """True when the fused BCLP dose pass evaluates this model on the device: an interpolation
+        table with strictly increasing sample points (np.interp's requirement; its bins are found by a
+        search seeded as if uniform), or an analytical generalised-logistic / linear / identity form
+        in closed form."""
+        if self.type == "analytical":
+            return self.form in ("gen_log_fun", "linear", "identity")
+        f = np.asarray(self.interp_f_0, dtype=np.float64)
+        return bool(f.size >= 2 and np.all(np.diff(f) > 0) and np.asarray(self.interp_map_0).shape == f.shape)
 
     def device_tables(self, device):
         """float32 (f, map, dmap) tables on `device` for the fused BCLP kernel."""
