@@ -66,6 +66,7 @@ def parse():
     ap.add_argument("--no-formats", action="store_true", help="skip the projector-frame / fan-beam rebin leg")
     ap.add_argument("--no-vec", action="store_true", help="skip the vector-geometry (inclined rays) projector leg")
     ap.add_argument("--ray-size", type=int, default=128)
+    ap.add_argument("--e2e-iters", type=int, default=40, help="iterations of the timed optimize() call (e2e)")
     return ap.parse_args()
 
 
@@ -539,6 +540,53 @@ def ray_chunk_parity(plan, cv, nx, ax, angles, first=0, count=16, seed=11):
             "relL2": {"integrate": rel_l2(integral[:, first:first + count].double().cpu().numpy(), ri),
                       "deposit": rel_l2(dose.double().cpu().numpy(), rd)},
             "tolerance": 1e-4, "oracle_rays_active_at_cap": int(act)}
+
+
+def time_optimize_e2e(n, n_angles, n_iter=40, seed=1000):
+    """The headline workload through the public call a user makes: optimize(target_geo, proj_geo,
+    Options(method="BCLP", n_iter)) on numpy inputs, returning numpy outputs (sinogram, dose, loss log).
+    One untimed call warms the plan, cuFFT and allocator caches; the second call is timed on the wall
+    clock between two device synchronisations (projector plan, absorption mask upload, device set-up of
+    g0, the captured iterations and the float64 downloads all inside)."""
+    import torch
+
+    from vamtoolbox_b200 import optimize as vopt
+
+    out = None
+    for _ in range(2):
+        tg, pg = build_problem(n, n_angles, seed=seed)
+        opts = bclp_options(n_iter)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sino, recon, loss = vopt.optimize(tg, pg, opts)
+        torch.cuda.synchronize()
+        t = time.perf_counter() - t0
+        assert isinstance(sino.array, np.ndarray) and isinstance(recon.array, np.ndarray)
+        out = {"call_s": t, "device_ms_per_iteration": getattr(opts, "device_iteration_ms", None),
+               "h2d": int(np.asarray(tg.array).size * 8), "d2h": int(sino.array.nbytes + recon.array.nbytes),
+               "finite": bool(np.isfinite(sino.array).all() and np.isfinite(recon.array).all())}
+        del sino, recon, loss  # a caller done with one result before the next call
+    out["n_iter"] = n_iter
+    return out
+
+
+def e2e_line(opt, replay, device_value):
+    """The contract's e2e object: the whole optimize() call (iterations per second of the call, set-up
+    and transfers included) when it was measured, else the graph replay with per-step host copies."""
+    if not opt or "call_s" not in opt:
+        line = dict(replay)
+        if opt:
+            line["optimize"] = opt
+        return line
+    n = opt["n_iter"]
+    return {"value": round(n / opt["call_s"], 4), "unit": UNIT, "h2d_bytes_per_step": opt["h2d"] / n,
+            "d2h_bytes_per_step": opt["d2h"] / n,
+            "path": f"vamtoolbox_b200.optimize.optimize(target_geo, proj_geo, Options(method='BCLP', n_iter={n})): "
+                    "numpy float64 target in; numpy float64 sinogram, dose and loss log out; one call timed whole",
+            "n_iter": n, "call_s": round(opt["call_s"], 5),
+            "device_ms_per_iteration": round(opt["device_ms_per_iteration"], 4) if opt["device_ms_per_iteration"] else None,
+            "fraction_of_device_loop": round(n / opt["call_s"] / device_value, 4), "outputs_finite": opt["finite"],
+            "graph_replay": replay}
 
 
 def _time_optimize(make, n_iter):
@@ -1093,6 +1141,18 @@ def run_ours(args):
         e2e_ms = float(t.item())
     h2d = g_host.numel() * 4
     d2h = s_out.numel() * 4
+    e2e_replay = {"value": round(1000.0 * ws_ / e2e_ms, 4), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                  "d2h_bytes_per_step": d2h,
+                  "path": "captured iteration graph replayed per step; each step's g copied in from pinned host "
+                          "memory (double-buffered on a copy stream) and its 9 loss / norm sums copied out"}
+
+    # ---- end to end through the public drop-in call: optimize() with numpy in and numpy out
+    e2e_opt = None
+    if ws_ == 1:
+        try:
+            e2e_opt = time_optimize_e2e(n, na, n_iter=args.e2e_iters)
+        except Exception as exc:  # report, never fail the headline number on it
+            e2e_opt = {"error": f"{type(exc).__name__}: {exc}"}
 
     # ---- plain per-call GPU path (reference numpy loop, host arrays)
     plain = None
@@ -1209,8 +1269,7 @@ def run_ours(args):
                        "angles": na, "parallelism": f"z-slab x{ws_}" if ws_ > 1 else "single GPU",
                        "l2": "inputs larger than L2 (working set ~450 MB per iteration)",
                        "graph": dist is None, "launch_shapes": tuning},
-            "e2e": {"value": round(1000.0 * ws_ / e2e_ms, 4), "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
+            "e2e": e2e_line(e2e_opt, e2e_replay, value / ws_),
             "plain_gpu": {"value": plain, "unit": UNIT, "path": "reference numpy BCLP loop, projector per call with "
                                                                  "host arrays"},
             "fused_vs_plain": (value / ws_ / plain) if plain else None,

@@ -312,6 +312,23 @@ enum vam_reduce_op { VAM_RED_MAX = 0, VAM_RED_MIN = 1, VAM_RED_SUM = 2 };
 int vam_reduce(const float* x_dev, int64_t n, int op, float* out_dev, void* work_dev,
                size_t work_bytes, vam_stream_t stream);
 
+/* Sinogram filtering along the detector axis (vamtoolbox/util/data.py:302-370,
+ * filterSinogram: zero-pad each detector column to a power of two >= 2 nR,
+ * multiply its spectrum by the real filter of _get_fourier_filter, :373-438,
+ * invert, crop).  The transforms are cuFFT's real-to-complex / complex-to-real
+ * pair over the padded axis; these two kernels are the steps around them.
+ * vam_spectrum_scale: spectrum_dev complex128 [n_freq][m] (re, im pairs),
+ * row k multiplied in place by filter_dev[k] (float64). */
+int vam_spectrum_scale(void* spectrum_dev, const double* filter_dev, int64_t n_freq, int64_t m,
+                       vam_stream_t stream);
+/* out_dev[r][j] = clip(scale * y_dev[r][j], lo, hi) as float32 for the first
+ * n_rows rows of y_dev ([>= n_rows][m], float64): the crop of the padded
+ * inverse transform, the reference's normalisations (BCLP's pi / (2 n_angles))
+ * and constraints (clip at 0 / the bounds) in one pass.  has_lo / has_hi
+ * select the bounds. */
+int vam_filter_epilogue(const double* y_dev, int64_t n_rows, int64_t m, double scale, int has_lo, double lo,
+                        int has_hi, double hi, float* out_dev, vam_stream_t stream);
+
 /* Same reduction as vam_reduce for callers that cannot allocate device memory
  * (code running between cudaStreamBeginCapture and EndCapture in global
  * capture mode, where cudaMalloc is not permitted, or a host that reserves

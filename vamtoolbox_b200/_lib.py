@@ -136,6 +136,8 @@ _SIGS = {
     "vam_reduce_noalloc": ([_vp, _c_i64, _c_int, _vp, _vp], _c_int),
     "vam_metric_ver": ([_vp, _vp, _c_i64, _vp, _vp, ctypes.c_size_t, _vp], _c_int),
     "vam_metric_ipdr": ([_vp, _vp, _c_i64, _vp, _vp, ctypes.c_size_t, _vp], _c_int),
+    "vam_spectrum_scale": ([_vp, _vp, _c_i64, _c_i64, _vp], _c_int),
+    "vam_filter_epilogue": ([_vp, _c_i64, _c_i64, _c_d, _c_int, _c_d, _c_int, _c_d, _vp, _vp], _c_int),
     "vam_bclp_dose_pass": ([_vp, _vp, _c_i64, ctypes.POINTER(BclpParams), _vp, _vp, _vp, _vp, ctypes.c_size_t, _vp],
                            _c_int),
     "vam_bclp_sino_update": ([_vp, _vp, _c_i64, _c_f, _c_f, _c_f, _c_f, _c_f, _c_int, _vp, _vp], _c_int),

@@ -444,6 +444,64 @@ extern "C" int vam_reduce(const float* x, int64_t n, int op, float* out, void* w
 }
 
 // ---------------------------------------------------------------------------
+// Sinogram filter (util/data.py:302-370) around cuFFT's real transforms along the
+// detector axis: the half spectrum times the real filter, and the epilogue that
+// crops the padded inverse transform, scales, clips and converts to float32.
+// ---------------------------------------------------------------------------
+namespace vam {
+namespace {
+
+// X[k][m] *= h[k], X complex128 [nk][m] (row k = frequency k of every column)
+__global__ void __launch_bounds__(kThreads) k_spectrum_scale(double2* __restrict__ X, const double* __restrict__ h,
+                                                             int64_t m) {
+    const double hk = h[blockIdx.y];
+    double2* row = X + (int64_t)blockIdx.y * m;
+    for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < m; i += (int64_t)gridDim.x * kThreads) {
+        double2 v = row[i];
+        v.x *= hk;
+        v.y *= hk;
+        row[i] = v;
+    }
+}
+
+// out[r][m] = clip(scale * y[r][m], lo, hi) as float32, rows r < n_rows of y [>= n_rows][m]
+__global__ void __launch_bounds__(kThreads) k_filter_epilogue(const double* __restrict__ y, int64_t n, double scale,
+                                                              int has_lo, double lo, int has_hi, double hi,
+                                                              float* __restrict__ out) {
+    for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads) {
+        double v = y[i] * scale;
+        if (has_lo) v = fmax(v, lo);
+        if (has_hi) v = fmin(v, hi);
+        out[i] = (float)v;
+    }
+}
+
+}  // namespace
+}  // namespace vam
+
+extern "C" int vam_spectrum_scale(void* spectrum, const double* filter, int64_t n_freq, int64_t m, vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(spectrum && filter, VAM_ERR_ARG, "vam_spectrum_scale: null argument");
+    VAM_REQUIRE(n_freq > 0 && m > 0 && n_freq < 65536, VAM_ERR_SHAPE, "vam_spectrum_scale: 0 < n_freq < 65536, m > 0");
+    const int64_t bx = std::min<int64_t>((m + kThreads - 1) / kThreads, 1024);
+    k_spectrum_scale<<<dim3((unsigned)bx, (unsigned)n_freq), kThreads, 0, (cudaStream_t)stream>>>(
+        static_cast<double2*>(spectrum), filter, m);
+    VAM_CHECK_LAUNCH("vam_spectrum_scale");
+    return VAM_OK;
+}
+
+extern "C" int vam_filter_epilogue(const double* y, int64_t n_rows, int64_t m, double scale, int has_lo, double lo,
+                                   int has_hi, double hi, float* out, vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(y && out, VAM_ERR_ARG, "vam_filter_epilogue: null argument");
+    VAM_REQUIRE(n_rows > 0 && m > 0, VAM_ERR_SHAPE, "vam_filter_epilogue: empty input");
+    const int64_t n = n_rows * m;
+    k_filter_epilogue<<<blocks_for(n), kThreads, 0, (cudaStream_t)stream>>>(y, n, scale, has_lo, lo, has_hi, hi, out);
+    VAM_CHECK_LAUNCH("vam_filter_epilogue");
+    return VAM_OK;
+}
+
+// ---------------------------------------------------------------------------
 // No-allocation reduction: scratch in a static device array
 // ---------------------------------------------------------------------------
 namespace vam {

@@ -26,7 +26,7 @@ import numpy as np
 import torch
 
 from .. import geometry
-from ..fused import Workspace, bclp_params, capture
+from ..fused import Workspace, bclp_params, capture, to_host_f64
 from ..projectorconstructor import projectorconstructor
 from ..util import data as udata
 
@@ -90,8 +90,14 @@ class BCLPNorm:
         self.exit_param = options.exit_param
         self.verbose = options.verbose
         self.test_alternate_handling = getattr(options, "test_alternate_handling", False)
-        self.dose = self.mapped_dose = None
+        self.dose = None
+        self._mapped_dose = None
+        self.mapped_t = None
+        self.g0_t = self.fT_t = None
         self.P = projectorconstructor(self.target_geo, self.proj_geo)
+        if self._device_init_ok():
+            self._init_device()
+            return
         if self.response_model.checkResponseTarget(self.target_geo.array) is False:
             warnings.warn("Target is either out of range of response function over non-negative real dose input, "
                           "or contains inf/nan.")
@@ -108,6 +114,54 @@ class BCLPNorm:
         self.g0 = np.asarray(self.g0)
         self.g0_shape = self.g0.shape
         self.g0 = self.imposeSinogramConstraints(self.g0)
+
+    # -- device-resident set-up (engine="device", parallel beam) -------------------
+    def _device_init_ok(self):
+        """The target, the initial sinogram and the constraints stay on the device when the device engine
+        runs a parallel-beam plan with a device response form and no bit-depth quantisation."""
+        return (getattr(self.options, "engine", "device") == "device" and self.bit_depth is None
+                and hasattr(getattr(self.P, "plan", None), "backward_ref") and self._device_response_ok()
+                and getattr(self.response_model, "device_map_inv_ok", lambda: False)())
+
+    def _init_device(self):
+        """BCLP.py's set-up (response-target check, g0 = filter(forward(map_inv(f_T))) * pi / (2 n_angles),
+        imposeSinogramConstraints) on the device: the float64 target is uploaded once, the checks reduce
+        on the device, and g0 is filtered, scaled and clipped into a float32 device tensor (no host
+        round trip of the 3-D arrays)."""
+        dev = self.P.device
+        tgt = torch.as_tensor(np.ascontiguousarray(self.target_geo.array, dtype=np.float64)).to(dev)
+        if self.response_model.checkResponseTarget_t(tgt) is False:
+            warnings.warn("Target is either out of range of response function over non-negative real dose input, "
+                          "or contains inf/nan.")
+        self.fT_t = tgt.to(torch.float32)
+        n_angles = self.proj_geo.n_angles
+        if self.g0 is None:
+            f0 = self.response_model.map_inv_t(tgt)
+            b = self.P.forward_t(f0)
+            g0 = udata.filterSinogram_t(b, self.options.filter, scale=np.pi / (2 * n_angles), lo=self.glb, hi=self.gub)
+        else:
+            g0 = torch.as_tensor(np.asarray(self.g0)).to(dev, torch.float32).reshape(self.P.plan.shape_sino)
+            if self.glb is not None or self.gub is not None:
+                g0 = g0.clamp(min=self.glb, max=self.gub)
+        self.g0_t = g0.contiguous()
+        self.g0_shape = tuple(self.g0_t.shape)
+        self.g0 = None  # the host copy is made on demand (host_g0)
+
+    def host_g0(self):
+        """The initial sinogram as a host float64 array (a download when it lives on the device)."""
+        if self.g0 is None and self.g0_t is not None:
+            self.g0 = self.g0_t.double().cpu().numpy()
+        return self.g0
+
+    @property
+    def mapped_dose(self):
+        if self._mapped_dose is None and self.mapped_t is not None:
+            self._mapped_dose = self.mapped_t.double().cpu().numpy()
+        return self._mapped_dose
+
+    @mapped_dose.setter
+    def mapped_dose(self, value):
+        self._mapped_dose = value
 
     # -- shared helpers (BCLP.py:528-590) ------------------------------------
     def imposeSinogramConstraints(self, g):
@@ -152,7 +206,7 @@ class BCLPNorm:
         L.lf[i], L.lf_eps0[i] = np.amax(v * np.abs(eb)), np.amax(v0 * np.abs(e))
 
     def gradientDescentHost(self):
-        g = self.checkSinogramShape(self.g0, "flattened")
+        g = self.checkSinogramShape(self.host_g0(), "flattened")
         for _ in range(self.logs.options.n_iter):
             dose, mapped, e, eb, v, loss = self._host_state(g)
             self.logs.loss[self.logs.curr_iter] = loss
@@ -242,9 +296,9 @@ class BCLPNorm:
             self.logs.iter_times[k] = iter_times[k]
         tshape = self.target_geo.array.shape
         self.dose_t, self.mapped_t, self.g_t = it.dose.reshape(tshape), it.mapped.reshape(tshape), it.g
-        self.dose = self.dose_t.double().cpu().numpy()
-        self.mapped_dose = self.mapped_t.double().cpu().numpy()
-        return it.g.double().cpu().numpy().reshape(-1)
+        self._mapped_dose = None  # downloaded on first use (output="full" / "components")
+        self.dose, g = to_host_f64(self.dose_t, it.g)
+        return g.reshape(-1)
 
     def gradientDescent(self):
         if getattr(self.options, "engine", "device") == "host":
@@ -272,8 +326,14 @@ class DeviceIteration:
         n_iter = bclp.logs.options.n_iter
         self.ws = Workspace(dev)
         f32 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float32), device=dev)
-        self.fT = f32(bclp.target_geo.array).reshape(vol_shape).contiguous()
-        self.g = f32(bclp.g0).reshape(sino_shape).contiguous()
+        if bclp.fT_t is not None:
+            self.fT = bclp.fT_t.reshape(vol_shape).contiguous()
+        else:
+            self.fT = f32(bclp.target_geo.array).reshape(vol_shape).contiguous()
+        if bclp.g0_t is not None:
+            self.g = bclp.g0_t.reshape(sino_shape).clone()
+        else:
+            self.g = f32(bclp.host_g0()).reshape(sino_shape).contiguous()
         self.dose = torch.empty(vol_shape, dtype=torch.float32, device=dev)
         self.mapped = torch.empty(vol_shape, dtype=torch.float32, device=dev)
         self.operand = torch.empty(vol_shape, dtype=torch.float32, device=dev)

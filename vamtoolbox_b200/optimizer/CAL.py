@@ -15,7 +15,7 @@ import numpy as np
 import torch
 
 from .. import geometry, metrics
-from ..fused import Workspace, capture
+from ..fused import Workspace, capture, to_host_f64
 from ..projectorconstructor import projectorconstructor
 from ..util import data as udata
 
@@ -99,7 +99,7 @@ class CALDevice:
         self.ver, self.xmax = ws.scalar(), ws.scalar()
         # initial sinogram: forward, filter (cuFFT), clip
         b = plan.forward(self.tgt)
-        self.b = udata.filterSinogram_t(b, options.filter).clamp_(min=0).contiguous()
+        self.b = udata.filterSinogram_t(b, options.filter, lo=0.0)
         self.x = plan.backward_ref(self.b)
         ws.max(self.x, self.xmax)
         ws.ver(self.x, self.mask, self.ver)
@@ -163,5 +163,5 @@ def minimizeCAL(target_geo, proj_geo, options):
     err = np.where(np.arange(err.size) < int(c.counter.item()), err, np.nan)
     # device time per iteration of the loop (CUDA events on the engine's stream)
     options.device_iteration_ms = ev0.elapsed_time(ev1) / done if done else None
-    return (geometry.Sinogram(b.double().cpu().numpy(), proj_geo, options),
-            geometry.Reconstruction(x_opt.double().cpu().numpy(), proj_geo, options), err)
+    b_h, x_h = to_host_f64(b, x_opt)
+    return geometry.Sinogram(b_h, proj_geo, options), geometry.Reconstruction(x_h, proj_geo, options), err

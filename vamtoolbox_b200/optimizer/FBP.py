@@ -13,7 +13,7 @@ def minimizeFBP(target_geo, proj_geo, options):
     A = projectorconstructor(target_geo, proj_geo)
     err = np.full(options.n_iter, np.nan)
     if hasattr(getattr(A, "plan", None), "backward_ref"):  # parallel beam: cuFFT filter on the device
-        b = udata.filterSinogram_t(A.forward_t(target_geo.array).to(torch.float64), options.filter).cpu().numpy()
+        b = udata.filterSinogram_t(A.forward_t(target_geo.array), options.filter).double().cpu().numpy()
     else:
         b = udata.filterSinogram(A.forward(target_geo.array), options.filter)
     if getattr(options, "offset", False):

@@ -14,7 +14,7 @@ import numpy as np
 import torch
 
 from .. import geometry, metrics
-from ..fused import Workspace, capture
+from ..fused import Workspace, capture, to_host_f64
 from ..projectorconstructor import projectorconstructor
 from ..util import data as udata
 
@@ -143,5 +143,5 @@ def minimizeOSMO(target_geo, proj_geo, options):
     # device time per iteration of the loop (CUDA events on the engine's stream)
     options.device_iteration_ms = ev0.elapsed_time(ev1) / done if done else None
     err = np.where(np.arange(err.size) < int(it.counter.item()), err, np.nan)
-    return (geometry.Sinogram(it.b.double().cpu().numpy(), proj_geo, options),
-            geometry.Reconstruction(it.x.double().cpu().numpy(), proj_geo, options), err)
+    b_h, x_h = to_host_f64(it.b, it.x)
+    return geometry.Sinogram(b_h, proj_geo, options), geometry.Reconstruction(x_h, proj_geo, options), err

@@ -157,6 +157,52 @@ class ResponseModel:
         f = np.asarray(self.interp_f_0, dtype=np.float64)
         return bool(f.size >= 2 and np.all(np.diff(f) > 0) and np.asarray(self.interp_map_0).shape == f.shape)
 
+    # -- device forms of the set-up steps (torch float64, same values as the numpy methods) -------
+    def device_map_inv_ok(self):
+        """map_inv has a device form: the closed forms, or np.interp on an increasing map table."""
+        if self.type == "analytical":
+            return self.form in ("gen_log_fun", "linear", "identity")
+        m = np.asarray(self.interp_map_0, dtype=np.float64)
+        return bool(m.size >= 2 and np.all(np.diff(m) > 0))
+
+    def map_inv_t(self, mapped):
+        """map_inv of a float64 CUDA tensor (response.py:220-237, 281-290)."""
+        import torch
+
+        if self.type == "analytical":
+            p = self.params
+            if self.form == "gen_log_fun":
+                num = -torch.log(((p["K"] - p["A"]) / (mapped - p["A"])) ** p["nu"] - 1)
+                return num / p["B"] + p["M"]
+            if self.form == "linear":
+                return (mapped - p["C"]) / p["M"]
+            return mapped.clone()
+        return _interp_t(mapped, torch.as_tensor(np.asarray(self.interp_map_0, np.float64), device=mapped.device),
+                         torch.as_tensor(np.asarray(self.interp_f_0, np.float64), device=mapped.device))
+
+    def checkResponseTarget_t(self, f_T):
+        """checkResponseTarget of a CUDA tensor: the four reductions on the device, one read-back."""
+        import torch
+
+        lo, hi = torch.aminmax(f_T)
+        flags = torch.stack([lo, hi, torch.isinf(f_T).any().to(f_T.dtype), torch.isnan(f_T).any().to(f_T.dtype)]).cpu()
+        lo, hi, has_inf, has_nan = (float(v) for v in flags)
+        ok = True
+        if self.form == "gen_log_fun" and hi > self.params["K"]:
+            warnings.warn("Maximum response target is greater than right asymptotic value of response function.")
+            ok = False
+        m0 = self.map(0)
+        if (lo < m0) and ~(np.isclose(lo, m0, atol=0.01 * hi)):
+            warnings.warn("Minimum response target is lower than response at zero optical dose.")
+            ok = False
+        if has_inf:
+            warnings.warn("Response target contains infinite value(s).")
+            ok = False
+        if has_nan:
+            warnings.warn("Response target contains nan value(s).")
+            ok = False
+        return ok
+
     def device_tables(self, device):
         """float32 (f, map, dmap) tables on `device` for the fused BCLP kernel."""
         import torch
@@ -171,3 +217,18 @@ class ResponseModel:
 
     def __repr__(self):
         return str(self.params)
+
+
+def _interp_t(x, xp, fp):
+    """np.interp(x, xp, fp) with nearest-value extrapolation (left = fp[0], right = fp[-1]) for an
+    increasing xp, on CUDA float64 tensors: bin by searchsorted, then fp[j] + slope (x - xp[j])."""
+    import torch
+
+    n = xp.numel()
+    j = (torch.searchsorted(xp, x, right=True) - 1).clamp_(0, n - 2)
+    x0, x1, y0, y1 = xp[j], xp[j + 1], fp[j], fp[j + 1]
+    y = (y1 - y0) / (x1 - x0) * (x - x0) + y0
+    y = torch.where(x == x0, y0, y)
+    y = torch.where(x < xp[0], fp[0], y)
+    y = torch.where(x >= xp[-1], fp[-1], y)
+    return torch.where(torch.isnan(x), x, y)

@@ -138,20 +138,55 @@ def filterSinogram(sinogram, filter_name):
     return out
 
 
-def filterSinogram_t(sino, filter_name):
-    """Device version of filterSinogram for a [nR, nA, nZ] (or [nR, nA]) torch tensor."""
+_FILTER_CACHE = {}
+
+
+def _device_filter_half(size, filter_name, device):
+    """The first size // 2 + 1 values of the real, even filter (the half spectrum of a real transform),
+    float64 on the device, cached per (size, name, device)."""
     import torch
 
+    key = (size, filter_name, str(device))
+    if key not in _FILTER_CACHE:
+        f = _get_fourier_filter(size, filter_name)[: size // 2 + 1, 0]
+        _FILTER_CACHE[key] = torch.as_tensor(np.ascontiguousarray(f), device=device, dtype=torch.float64)
+    return _FILTER_CACHE[key]
+
+
+def filterSinogram_t(sino, filter_name, scale=1.0, lo=None, hi=None, out=None):
+    """Device version of filterSinogram for a [nR, nA, nZ] (or [nR, nA]) torch tensor, followed by
+    ``clip(scale * filtered, lo, hi)`` and returned as float32 (``out`` if given).
+
+    The filter is real and even, so the reference's complex FFT of the zero-padded real columns times the
+    filter, inverted and cropped to its real part, equals cuFFT's real-to-complex transform along the
+    padded detector axis, the half spectrum times the filter's first size // 2 + 1 values
+    (vam_spectrum_scale), the complex-to-real inverse and the crop; the crop, scale, clip and float32
+    conversion are one pass (vam_filter_epilogue)."""
+    import torch
+
+    from .. import _lib
+
     if filter_name is None or filter_name.lower() == "none":
-        return sino
-    if filter_name.lower() not in _SINO_FILTERS:
-        raise ValueError("Unknown filter: %s" % filter_name)
-    pX = sino.shape[0]
-    size = max(64, int(2 ** np.ceil(np.log2(2 * pX))))
-    filt = torch.as_tensor(_get_fourier_filter(size, filter_name)[:, 0], device=sino.device, dtype=torch.float64)
-    shape = (size,) + (1,) * (sino.ndim - 1)
-    spec = torch.fft.fft(sino.to(torch.float64), n=size, dim=0) * filt.reshape(shape)
-    return torch.fft.ifft(spec, dim=0).real[:pX].to(sino.dtype).contiguous()
+        x = sino.to(torch.float64)
+    else:
+        if filter_name.lower() not in _SINO_FILTERS:
+            raise ValueError("Unknown filter: %s" % filter_name)
+        pX = sino.shape[0]
+        size = max(64, int(2 ** np.ceil(np.log2(2 * pX))))
+        m = sino[0].numel()
+        spec = torch.fft.rfft(sino.to(torch.float64).reshape(pX, m), n=size, dim=0).contiguous()
+        filt = _device_filter_half(size, filter_name, sino.device)
+        st = _lib.stream_ptr(torch.cuda.current_stream(sino.device))
+        _lib.call("vam_spectrum_scale", _lib.ptr(spec), _lib.ptr(filt), spec.shape[0], m, st)
+        x = torch.fft.irfft(spec, n=size, dim=0)
+    if out is None:
+        out = torch.empty(sino.shape, dtype=torch.float32, device=sino.device)
+    pX, m = sino.shape[0], sino[0].numel()
+    x = x.contiguous()
+    _lib.call("vam_filter_epilogue", _lib.ptr(x), pX, m, float(scale), int(lo is not None),
+              float(lo if lo is not None else 0.0), int(hi is not None), float(hi if hi is not None else 0.0),
+              _lib.ptr(out), _lib.stream_ptr(torch.cuda.current_stream(sino.device)))
+    return out
 
 
 def discretize(x, bit_depth, range, output_dtype=float):
