@@ -353,10 +353,12 @@ def multi_target_problems(seed=5, n_iter=25):
 
 
 def run_multi_target(dev, n_iter=25):
-    """Aggregate BCLP iter/s of 16 uneven targets, three ways, each a captured graph replayed n_iter
-    times after 3 warm-up replays: all targets per iteration in two persistent work-queue launches
-    (vam_batch_submit), every target's chain on its own stream in one graph, and each target's own
-    graph replayed on its own, one target after another."""
+    """Aggregate BCLP iter/s of 16 uneven targets, four ways, each a captured graph replayed n_iter
+    times after 3 warm-up replays: all targets per iteration in two persistent work-queue batches
+    (vam_batch_submit; all backprojections, then all forwards), the same with the targets in two halves
+    half an iteration apart (each batch mixes one half's backprojections with the other's forwards),
+    every target's chain on its own stream in one graph, and each target's own graph replayed on its
+    own, one target after another."""
     import torch
 
     from vamtoolbox_b200.fused import graph_kernel_nodes
@@ -386,7 +388,7 @@ def run_multi_target(dev, n_iter=25):
            "metric": "aggregate BCLP iterations/s over 16 uneven targets (target-iterations per second)"}
     total = len(probs) * n_iter
     launches = {}
-    for sched in ("persistent", "streams"):
+    for sched in ("persistent", "streams", "phased"):
         multi.schedule = sched
         g = multi.capture()
         launches[sched] = graph_kernel_nodes(g)
@@ -399,8 +401,8 @@ def run_multi_target(dev, n_iter=25):
     t_seq = timed([gr.replay for gr in graphs])
     del graphs
     out["one_at_a_time_iter_s"] = round(total / (t_seq / 1e3), 2)
-    out["speedup_persistent"] = round(out["persistent_iter_s"] / out["one_at_a_time_iter_s"], 3)
-    out["speedup_streams"] = round(out["streams_iter_s"] / out["one_at_a_time_iter_s"], 3)
+    for sched in ("persistent", "streams", "phased"):
+        out[f"speedup_{sched}"] = round(out[f"{sched}_iter_s"] / out["one_at_a_time_iter_s"], 3)
     out["launches_per_iteration"] = launches
     return out
 

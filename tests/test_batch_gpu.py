@@ -173,7 +173,7 @@ def test_batch_rejects_bad_work():
     assert h.vam_batch_submit(batch._h, None, 0, None) == _lib.VAM_ERR_ARG
 
 
-@pytest.mark.parametrize("schedule", ["persistent", "streams", "auto"])
+@pytest.mark.parametrize("schedule", ["persistent", "streams", "phased", "auto"])
 def test_multi_target_bclp_matches_one_at_a_time(schedule):
     from vamtoolbox_b200 import geometry
     from vamtoolbox_b200.optimize import Options

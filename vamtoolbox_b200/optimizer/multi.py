@@ -31,11 +31,18 @@ class MultiTargetBCLP:
       "streams"    -- each target's whole iteration chain on its own stream inside
                       the graph, so the hardware interleaves the targets' own
                       specialised kernels with no barrier between phases;
-      "auto"       -- time one captured iteration of each and keep the faster.
+      "phased"     -- the targets in two halves (A, B, alternating by cost) with B
+                      half an iteration ahead: each persistent batch holds A's
+                      backprojections with B's forwards, then A's forwards with
+                      B's backprojections, so both kernel-body families share the
+                      device in every phase; every target still runs back, dose
+                      pass, forward, update in its own order (B's first state is
+                      computed before the loop, A's last one after it);
+      "auto"       -- time one captured iteration of each and keep the fastest.
     """
 
     def __init__(self, problems, schedule="auto"):
-        if schedule not in ("auto", "persistent", "streams"):
+        if schedule not in ("auto", "persistent", "streams", "phased"):
             raise ValueError(f"unknown schedule {schedule!r}")
         self.solvers = [BCLPNorm(tg, pg, o) for tg, pg, o in problems]
         if not self.solvers:
@@ -55,6 +62,18 @@ class MultiTargetBCLP:
         self.streams = [torch.cuda.Stream(device=self.device) for _ in self.its]
         self.fork = torch.cuda.Event()
         self.joins = [torch.cuda.Event() for _ in self.its]
+        # phased schedule: halves by cost (largest first, alternating), their mixed batch lists
+        cost = [it.g.numel() * it.dose.shape[-1] for it in self.its]
+        order = sorted(range(len(self.its)), key=lambda k: -cost[k])
+        self.half_a = [self.its[k] for k in order[0::2]]
+        self.half_b = [self.its[k] for k in order[1::2]]
+        self.phase1 = ProjectionBatch(self.device)
+        self.phase2 = ProjectionBatch(self.device)
+        back = lambda it: (it.bclp.P.plan, "backward_ref", it.g, it.dose)
+        fwd = lambda it: (it.bclp.P.plan, "forward", it.operand, it.grad)
+        self.phase1_work = [back(it) for it in self.half_a] + [fwd(it) for it in self.half_b]
+        self.phase2_work = [fwd(it) for it in self.half_a] + [back(it) for it in self.half_b]
+        self._b_primed = False
         self.schedule = schedule
         self.timings = None
         if schedule == "auto":
@@ -93,25 +112,78 @@ class MultiTargetBCLP:
         for ev in self.joins:
             main.wait_event(ev)
 
+    def _fork_join_over(self, its, fn):
+        main = torch.cuda.current_stream(self.device)
+        self.fork.record(main)
+        for k, it in enumerate(its):
+            s, ev = self.streams[k], self.joins[k]
+            s.wait_event(self.fork)
+            with torch.cuda.stream(s):
+                fn(it)
+            ev.record(s)
+        for ev in self.joins[:len(its)]:
+            main.wait_event(ev)
+
+    def prime(self):
+        """Phased schedule: half B's first backprojection and dose pass (its state for iteration 0),
+        issued once before the loop; a no-op when already issued."""
+        if self._b_primed or not self.half_b:
+            self._b_primed = True
+            return
+        for it in self.half_b:
+            it.back(it.g, it.dose)
+        self._fork_join_over(self.half_b, self._dose)
+        self._b_primed = True
+
     def step(self):
         if self.schedule == "persistent":
             self.state()
             self.update()
+        elif self.schedule == "phased":
+            self.phase1.submit(self.phase1_work)
+            self._fork_join_over(self.half_a, self._dose)
+            self._fork_join_over(self.half_b, self._update)
+            self.phase2.submit(self.phase2_work)
+            self._fork_join_over(self.half_a, self._update)
+            self._fork_join_over(self.half_b, self._dose)
         else:
             self._fork_join(lambda it: it.step())
 
+    def finish_state(self):
+        """The final dose of every target after the loop: all targets' (persistent / streams) or half
+        A's (phased: half B's is the last phase of the loop)."""
+        if self.schedule == "phased":
+            for it in self.half_a:
+                it.back(it.g, it.dose)
+            self._fork_join_over(self.half_a, self._dose)
+        else:
+            self.state()
+
     def capture(self):
-        """The whole multi-target iteration as one CUDA graph (lists validated first, nothing run)."""
+        """The whole multi-target iteration as one CUDA graph (lists validated first, nothing run).
+        The phased schedule's half B is primed on the current stream first (outside the graph)."""
         self.back.prepare(self.back_work)
         self.fwd.prepare(self.fwd_work)
+        if self.schedule == "phased":
+            self.phase1.prepare(self.phase1_work)
+            self.phase2.prepare(self.phase2_work)
+            self.prime()
         return capture(self.step, self.device)
 
+    def reset(self, saved):
+        """Restore every target's sinogram and log (and the phased schedule's priming) to a saved start."""
+        for it, g in zip(self.its, saved):
+            it.g.copy_(g)
+            it.counter.zero_()
+            it.log.fill_(float("nan"))
+        self._b_primed = False
+
     def _pick(self, reps=3):
-        """Time both schedules on captured iterations from the same starting sinograms; keep the faster."""
+        """Time the schedules on captured iterations from the same starting sinograms; keep the fastest."""
         saved = [it.g.clone() for it in self.its]
         st = torch.cuda.current_stream(self.device)
         times = {}
-        for sched in ("persistent", "streams"):
+        for sched in ("persistent", "streams", "phased"):
             self.schedule = sched
             gr = self.capture()
             gr.replay()
@@ -123,10 +195,7 @@ class MultiTargetBCLP:
             e1.synchronize()
             times[sched] = e0.elapsed_time(e1) / reps
             del gr
-            for it, g in zip(self.its, saved):
-                it.g.copy_(g)
-                it.counter.zero_()
-                it.log.fill_(float("nan"))
+            self.reset(saved)
         torch.cuda.synchronize(self.device)
         self.timings = times
         return min(times, key=times.get)
@@ -142,6 +211,8 @@ class MultiTargetBCLP:
         st = torch.cuda.current_stream(self.device)
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(n_iter + 1)]
         ev[0].record(st)
+        if self.schedule == "phased":
+            self.prime()
         if graph:
             gr = self.capture()
             for k in range(n_iter):
@@ -152,7 +223,7 @@ class MultiTargetBCLP:
             for k in range(n_iter):
                 self.step()
                 ev[k + 1].record(st)
-        self.state()  # the final dose of every target (persistent schedule's first phase)
+        self.finish_state()  # the final dose of every target
         torch.cuda.synchronize(self.device)
         times = [ev[0].elapsed_time(ev[k + 1]) / 1e3 for k in range(n_iter)]
         out = []
