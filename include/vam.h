@@ -104,6 +104,15 @@ int vam_parallel_clear_occlusion(vam_parallel_plan* plan);
  * occluder) into out_dev.  VAM_ERR_ARG if no occlusion is set. */
 int vam_parallel_get_occlusion_sinogram(vam_parallel_plan* plan, float* out_dev, vam_stream_t stream);
 
+/* Builds the plan's backprojection bin table: for every pixel inside the clip
+ * circle and every angle, np.interp's bin of t = x cos - y sin (float64, the
+ * reference's expression) as a row offset and its float32 weight, 8 bytes per
+ * pixel and angle (147 MB at 256^3 x 360).  Later eight-slice backprojections
+ * read the table instead of evaluating the float64 bins (identical results).
+ * Allocates: call before any stream capture.  VAM_ERR_NOTSUP when the plan's
+ * sinogram has 2^31 elements or more. */
+int vam_parallel_prepare_backward(vam_parallel_plan* plan, vam_stream_t stream);
+
 /* R1 forward: rotate-and-sum Radon transform with bilinear sampling, zero
  * outside the image, detector width nY.  Replaces
  * Projector3DParallelPython.forward (Projector3DParallel.py:113-156). */
@@ -142,6 +151,8 @@ typedef struct {
     int32_t forward_vz, backward_vz, adjoint_vz;
     int32_t backward_batch;
     int32_t adjoint_table;
+    int32_t backward_table;  /* 1: the eight-slice backprojection reads its bins from the plan's table
+                                (vam_parallel_prepare_backward) when it is built; 0: computes them */
 } vam_parallel_tuning;
 int vam_parallel_set_tuning(vam_parallel_plan* plan, const vam_parallel_tuning* tuning);
 int vam_parallel_get_tuning(vam_parallel_plan* plan, vam_parallel_tuning* tuning);

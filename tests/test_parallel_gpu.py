@@ -216,9 +216,10 @@ def test_adjoint_without_weight_table(absn):
     assert not p._adj_ready
 
 
-TUNINGS = [dict(forward_vz=fv, backward_vz=bv, backward_batch=bb, adjoint_vz=av, adjoint_table=at)
-           for fv, (bv, bb), (av, at) in [(4, (4, 1), (4, 1)), (8, (8, 1), (8, 1)), (4, (4, 2), (4, 0)),
-                                          (8, (8, 2), (8, 0)), (4, (4, 4), (8, 1)), (1, (1, 1), (1, 0))]]
+TUNINGS = [dict(forward_vz=fv, backward_vz=bv, backward_batch=bb, adjoint_vz=av, adjoint_table=at, backward_table=bt)
+           for fv, (bv, bb, bt), (av, at) in [(4, (4, 1, 0), (4, 1)), (8, (8, 1, 0), (8, 1)), (4, (4, 2, 0), (4, 0)),
+                                              (8, (8, 2, 0), (8, 0)), (4, (4, 4, 0), (8, 1)), (1, (1, 1, 0), (1, 0)),
+                                              (8, (8, 2, 1), (8, 1))]]
 
 
 @pytest.mark.parametrize("tuning", TUNINGS, ids=lambda t: "-".join(str(v) for v in t.values()))

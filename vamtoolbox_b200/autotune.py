@@ -23,7 +23,8 @@ from . import _lib
 
 # slices per lane: 1 = the generic kernel, 4 / 8 = the fast kernels (nZ % 4 == 0)
 FORWARD_VZ = (1, 4, 8)
-BACKWARD = ((1, 1), (4, 1), (8, 1), (4, 2), (8, 2), (4, 4))  # (slices per lane, angles per batch)
+# (slices per lane, angles per batch, bin table): the table serves eight slices per lane
+BACKWARD = ((1, 1, 0), (4, 1, 0), (8, 1, 0), (4, 2, 0), (8, 2, 0), (4, 4, 0), (8, 2, 1))
 ADJOINT = ((1, 0), (4, 1), (8, 1), (4, 0), (8, 0))           # (slices per lane, weight table on)
 
 _lock = threading.Lock()
@@ -91,9 +92,11 @@ def measure(plan, reps=3, warm=1, ops=("forward", "backward", "adjoint")):
         for vz in FORWARD_VZ if "forward" in ops else ():
             plan.set_tuning(dict(base, forward_vz=vz))
             times["forward"][str(vz)] = _time(lambda: plan.forward(x, ob), reps, warm)
-        for vz, bt in BACKWARD if "backward" in ops else ():
-            plan.set_tuning(dict(base, backward_vz=vz, backward_batch=bt))
-            times["backward"][f"{vz},{bt}"] = _time(lambda: plan.backward_ref(b, ox), reps, warm)
+        for vz, bt, tb in BACKWARD if "backward" in ops else ():
+            if tb and not getattr(plan, "has_backward_table", False):
+                continue
+            plan.set_tuning(dict(base, backward_vz=vz, backward_batch=bt, backward_table=tb))
+            times["backward"][f"{vz},{bt},{tb}"] = _time(lambda: plan.backward_ref(b, ox), reps, warm)
         for vz, tb in ADJOINT if "adjoint" in ops else ():
             if tb and not table:
                 continue
@@ -104,7 +107,8 @@ def measure(plan, reps=3, warm=1, ops=("forward", "backward", "adjoint")):
     if times["forward"]:
         best["forward_vz"] = int(min(times["forward"], key=times["forward"].get))
     if times["backward"]:
-        best["backward_vz"], best["backward_batch"] = map(int, min(times["backward"], key=times["backward"].get).split(","))
+        best["backward_vz"], best["backward_batch"], best["backward_table"] = map(
+            int, min(times["backward"], key=times["backward"].get).split(","))
     if times["adjoint"]:
         best["adjoint_vz"], best["adjoint_table"] = map(int, min(times["adjoint"], key=times["adjoint"].get).split(","))
     return best, times

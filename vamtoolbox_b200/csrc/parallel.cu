@@ -807,6 +807,130 @@ __global__ void __launch_bounds__(256, 6) k_backward_batched8(Args a) {
 }
 
 // ---------------------------------------------------------------------------
+// R2 backprojection from the plan's bin table.
+//
+// k_bwd_table evaluates, once per plan, for every pixel inside the clip circle
+// and every angle the same float64 t = x cos - y sin, floor and float32 weight
+// as the batched kernel, stored as (j0 * nA * nZ + angle * nZ, weight bits),
+// or (-1, 0) where t falls outside the detector (np.interp left = right = 0:
+// no contribution).  At the detector's last bin (t == xp[-1], weight 0) the
+// entry is (row nY - 2, weight 1), which adds the same single row with the
+// same rounding.  k_backward_tab8 then runs, per pixel and z chunk, one table
+// entry per angle (streamed: the table is read once per call), two 16-byte
+// loads per detector row and packed f32x2 FMAs (two fmaf roundings each), so
+// its sums are bit-identical to k_backward_batched8's for finite data.  One
+// angle per step with the next entry prefetched, 48 registers, five CTAs per
+// SM: 1.52 -> 1.32 ms at 256^3 x 360 (A/B in one process; two angles in flight
+// at 64 registers 1.43 ms, a six- or eight-CTA register cap 1.41 / 1.44 ms).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_bwd_table(const double4* __restrict__ trig, const int* __restrict__ plist,
+                                                   int2* __restrict__ tab, int npc, int nA, int nA_pad, int nY,
+                                                   int nX, int nZ, int C) {
+    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;  // over (in-circle pixel, angle), angle fastest
+    if (idx >= (long)npc * nA_pad) return;
+    const int th = (int)(idx % nA_pad);
+    const int pc = (int)(idx / nA_pad);
+    if (th >= nA) { tab[idx] = make_int2(-1, 0); return; }
+    const int p = plist[pc];
+    const double X = (double)(p % nX - C), Y = (double)(p / nX - C);
+    const double4 tr = trig[th];
+    const double t = __dsub_rn(__dmul_rn(X, tr.x), __dmul_rn(Y, tr.y));
+    if (!(t >= (double)(-C) && t <= (double)(nY - 1 - C))) { tab[idx] = make_int2(-1, 0); return; }
+    const double ft = floor(t);
+    const int j0 = (int)ft + C;
+    const int rs = nA * nZ;
+    if (j0 == nY - 1) tab[idx] = make_int2((nY - 2) * rs + th * nZ, __float_as_int(1.f));
+    else tab[idx] = make_int2(j0 * rs + th * nZ, __float_as_int((float)(t - ft)));
+}
+
+__device__ __forceinline__ unsigned long long pk_pair(float lo, float hi) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+
+__device__ __forceinline__ void fma_pair(unsigned long long& acc, unsigned long long w2, float a, float b) {
+    asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc) : "l"(w2), "l"(pk_pair(a, b)));
+}
+
+// acc (slice pairs) += w0 * row r0 + w1 * row r1, eight slices per lane (q1: the lane's second vector)
+__device__ __forceinline__ void tab_rows(unsigned long long (&acc)[4], const float* __restrict__ p0, int rs, float w,
+                                         bool q1) {
+    const float4 a0 = __ldg(reinterpret_cast<const float4*>(p0));
+    const float4 a2 = __ldg(reinterpret_cast<const float4*>(p0 + rs));
+    float4 a1 = make_float4(0.f, 0.f, 0.f, 0.f), a3 = a1;
+    if (q1) {
+        a1 = __ldg(reinterpret_cast<const float4*>(p0 + 128));
+        a3 = __ldg(reinterpret_cast<const float4*>(p0 + rs + 128));
+    }
+    const unsigned long long w0 = pk_pair(1.f - w, 1.f - w), w1 = pk_pair(w, w);
+    fma_pair(acc[0], w0, a0.x, a0.y); fma_pair(acc[1], w0, a0.z, a0.w);
+    fma_pair(acc[2], w0, a1.x, a1.y); fma_pair(acc[3], w0, a1.z, a1.w);
+    fma_pair(acc[0], w1, a2.x, a2.y); fma_pair(acc[1], w1, a2.z, a2.w);
+    fma_pair(acc[2], w1, a3.x, a3.y); fma_pair(acc[3], w1, a3.z, a3.w);
+}
+
+// FULL: nZ a multiple of 256, every lane's two vectors inside the volume (no load predicates)
+template <bool FULL>
+__device__ __forceinline__ void k_backward_tab_body(const Args& a, const int2* __restrict__ tab,
+                                                    const int* __restrict__ cidx, int nA_pad, unsigned bx) {
+    const int lane = threadIdx.x & 31;
+    const long item = (long)bx * kWarpsPerBlock + (threadIdx.x >> 5);
+    const int zc = (int)(item % a.zchunks);
+    const long p = item / a.zchunks;
+    if (p >= (long)a.nY * a.nX) return;
+    int z0, qn;
+    lane_z<8>(zc, lane, a.nZ, z0, qn);
+    if (qn == 0) return;
+    const bool q1 = FULL || qn == 2;
+    unsigned long long acc[4] = {0ull, 0ull, 0ull, 0ull};
+    const int pc = cidx[p];
+    if (pc >= 0) {
+        const int rs = a.nA * a.nZ;
+        const float* __restrict__ bz = a.in + z0;
+        const int2* __restrict__ e = tab + (size_t)pc * nA_pad;
+        int2 q = __ldcs(e);
+#pragma unroll 1
+        for (int k = 0; k < a.nA; ++k) {
+            const int2 nq = __ldcs(e + min(k + 1, nA_pad - 1));  // the next angle's entry in flight
+            if (q.x >= 0) {
+                if (FULL) {
+                    const float* pa = bz + q.x;
+                    const float4 a0 = __ldg(reinterpret_cast<const float4*>(pa));
+                    const float4 a1 = __ldg(reinterpret_cast<const float4*>(pa + 128));
+                    const float4 a2 = __ldg(reinterpret_cast<const float4*>(pa + rs));
+                    const float4 a3 = __ldg(reinterpret_cast<const float4*>(pa + rs + 128));
+                    const float w = __int_as_float(q.y);
+                    const unsigned long long w0 = pk_pair(1.f - w, 1.f - w), w1 = pk_pair(w, w);
+                    fma_pair(acc[0], w0, a0.x, a0.y); fma_pair(acc[1], w0, a0.z, a0.w);
+                    fma_pair(acc[2], w0, a1.x, a1.y); fma_pair(acc[3], w0, a1.z, a1.w);
+                    fma_pair(acc[0], w1, a2.x, a2.y); fma_pair(acc[1], w1, a2.z, a2.w);
+                    fma_pair(acc[2], w1, a3.x, a3.y); fma_pair(acc[3], w1, a3.z, a3.w);
+                } else {
+                    tab_rows(acc, bz + q.x, rs, __int_as_float(q.y), q1);
+                }
+            }
+            q = nq;
+        }
+    }
+    float v[8];
+#pragma unroll
+    for (int e2 = 0; e2 < 4; ++e2) asm("mov.b64 {%0, %1}, %2;" : "=f"(v[2 * e2]), "=f"(v[2 * e2 + 1]) : "l"(acc[e2]));
+    if (a.mask) {
+        const float m = __ldg(a.mask + p);
+#pragma unroll
+        for (int e2 = 0; e2 < 8; ++e2) v[e2] = m * v[e2];
+    }
+    store_vz<8>(a.out + (size_t)p * a.nZ + z0, v, qn);
+}
+
+template <bool FULL>
+__global__ void __launch_bounds__(256, 1) k_backward_tab8(Args a, const int2* __restrict__ tab, const int* __restrict__ cidx,
+                                                       int nA_pad) {
+    k_backward_tab_body<FULL>(a, tab, cidx, nA_pad, blockIdx.x);
+}
+
+// ---------------------------------------------------------------------------
 // 2-D slices (nZ = 1): shared-memory tiles.
 //
 // With one slice there is no contiguous axis to put lanes on: a warp's taps
@@ -1397,7 +1521,7 @@ int fast_vz(int nZ, bool aligned, double min_eff) {
 // same body for many calls inside one persistent launch.  Both paths therefore
 // compute bit-identical results.
 // ---------------------------------------------------------------------------
-enum Kind : int { KF_FAST = 0, KF_GEN, KB_BATCHED, KB_FAST, KB_GEN, KA_TABLE, KA_FAST, KA_GEN, KF_2D, KB_2D };
+enum Kind : int { KF_FAST = 0, KF_GEN, KB_BATCHED, KB_FAST, KB_GEN, KA_TABLE, KA_FAST, KA_GEN, KF_2D, KB_2D, KB_TABLE };
 
 struct Item {
     int kind;
@@ -1417,6 +1541,9 @@ struct Item {
     Args a;
     FastArgs f;
     const float4* table;
+    const int2* btab;  // KB_TABLE: the plan's backprojection bin table, its pixel index and list stride
+    const int* bcidx;
+    int bpad, bpad_;
 };
 static_assert(sizeof(Item) % 8 == 0, "Item is copied to shared memory in 8-byte words");
 
@@ -1502,7 +1629,12 @@ int describe(vam_parallel_plan* plan, Op op, const float* in, float* out, Item& 
         if (op == Op::BackwardRef) {
             // the batched kernel stages cos / sin of every angle in shared memory (16 B per angle)
             const int batch = (size_t)plan->nA * sizeof(double2) <= 48 * 1024 ? plan->tune_bwd_batch : 1;
-            if (batch >= 2) {
+            if (vzf == 8 && !ray && plan->d_bwd_table && plan->tune_bwd_table) {
+                it.kind = KB_TABLE;
+                it.btab = plan->d_bwd_table;
+                it.bcidx = plan->d_bwd_cidx;
+                it.bpad = plan->bwd_table_pad;
+            } else if (batch >= 2) {
                 it.kind = KB_BATCHED;
                 it.batch = vzf == 8 ? 2 : (batch >= 4 ? 4 : 2);
                 it.smem = (unsigned)(sizeof(double2) * plan->nA);
@@ -1587,6 +1719,12 @@ __device__ __forceinline__ void fast_body(const Item& it, unsigned bx, unsigned 
             const Args a = it.a;
             if (it.vz == 8) k_backward_fast_body<8, RAY>(a, bx, by);
             else k_backward_fast_body<4, RAY>(a, bx, by);
+        } else if (it.kind == KB_TABLE) {
+            if constexpr (!RAY) {
+                const Args a = it.a;
+                if (a.nZ % 256 == 0) k_backward_tab_body<true>(a, it.btab, it.bcidx, it.bpad, bx);
+                else k_backward_tab_body<false>(a, it.btab, it.bcidx, it.bpad, bx);
+            }
         }
     }
     if constexpr ((FAM & 4) != 0) {
@@ -1695,6 +1833,9 @@ int launch_item(const Item& it, cudaStream_t st, const char* name) {
         const dim3 block(kWarpsPerBlock * kWarp);
         if (it.vz == 8) k_adjoint_table<8><<<grid, block, 0, st>>>(it.a, it.table);
         else k_adjoint_table<4><<<grid, block, 0, st>>>(it.a, it.table);
+    } else if (it.kind == KB_TABLE) {
+        if (it.a.nZ % 256 == 0) k_backward_tab8<true><<<grid, dim3(kWarpsPerBlock * kWarp), 0, st>>>(it.a, it.btab, it.bcidx, it.bpad);
+        else k_backward_tab8<false><<<grid, dim3(kWarpsPerBlock * kWarp), 0, st>>>(it.a, it.btab, it.bcidx, it.bpad);
     } else if (it.ray) {
         launch_fast<true>(it, grid, st);
     } else {
@@ -1856,6 +1997,7 @@ extern "C" int vam_parallel_plan_create(const vam_parallel_geom* geom, vam_paral
     p->adj_table_abs = -1;
     p->tune_bwd_batch = 2;
     p->tune_adj_table = 1;
+    p->tune_bwd_table = 1;
     // per-angle tables exactly as numpy evaluates them (Projector3DParallel.py:135-143)
     std::vector<double4> trig(p->nA);
     for (int i = 0; i < p->nA; ++i) {
@@ -1927,6 +2069,8 @@ extern "C" int vam_parallel_plan_destroy(vam_parallel_plan* p) {
     cudaFree(p->d_tasks_single);
     cudaFree(p->d_vol_scratch);
     cudaFree(p->d_adj_table);
+    cudaFree(p->d_bwd_table);
+    cudaFree(p->d_bwd_cidx);
     delete p;
     return VAM_OK;
 }
@@ -2057,6 +2201,7 @@ extern "C" int vam_parallel_set_tuning(vam_parallel_plan* p, const vam_parallel_
     p->tune_adj_vz = t->adjoint_vz;
     p->tune_bwd_batch = t->backward_batch == 0 ? 2 : t->backward_batch;
     p->tune_adj_table = t->adjoint_table;
+    p->tune_bwd_table = t->backward_table;
     return VAM_OK;
 }
 
@@ -2068,6 +2213,7 @@ extern "C" int vam_parallel_get_tuning(vam_parallel_plan* p, vam_parallel_tuning
     t->adjoint_vz = p->tune_adj_vz;
     t->backward_batch = p->tune_bwd_batch;
     t->adjoint_table = p->tune_adj_table;
+    t->backward_table = p->tune_bwd_table;
     return VAM_OK;
 }
 
@@ -2085,6 +2231,49 @@ extern "C" int vam_parallel_prepare_adjoint(vam_parallel_plan* p, vam_stream_t s
         k_adj_table<false><<<nb, 256, 0, st>>>(p->d_trig, p->d_adj_table, p->nY, p->nX, p->nA, p->C, 0.f, 0.f);
     VAM_CHECK_LAUNCH("k_adj_table");
     p->adj_table_abs = p->abs_mode;
+    return VAM_OK;
+}
+
+extern "C" int vam_parallel_prepare_backward(vam_parallel_plan* p, vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(p, VAM_ERR_ARG, "vam_parallel_prepare_backward: null plan");
+    VAM_REQUIRE((long long)p->nY * p->nA * p->nZ < (1LL << 31), VAM_ERR_NOTSUP,
+                "vam_parallel_prepare_backward: the table holds 32-bit sinogram offsets (sinogram below 2^31 elements)");
+    DeviceGuard g(p->device);
+    const int n = p->nY * p->nX;
+    // the clip circle exactly as the plan's table (linspace(-1, 1) semantics)
+    std::vector<int> cidx(n, -1), plist;
+    for (int i = 0; i < p->nY; ++i) {
+        const double a = lin_m1_1(i, p->nY);
+        for (int j = 0; j < p->nX; ++j) {
+            const double b = lin_m1_1(j, p->nX);
+            volatile double aa = a * a, bb = b * b;
+            volatile double r2 = aa + bb;
+            if (!(r2 > 1.0)) { cidx[(size_t)i * p->nX + j] = (int)plist.size(); plist.push_back(i * p->nX + j); }
+        }
+    }
+    const int npc = (int)plist.size();
+    const int pad = (p->nA + 1) & ~1;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!p->d_bwd_cidx) VAM_TRY_CUDA(cudaMalloc(&p->d_bwd_cidx, sizeof(int) * n));
+    if (!p->d_bwd_table) VAM_TRY_CUDA(cudaMalloc(&p->d_bwd_table, sizeof(int2) * (size_t)std::max(npc, 1) * pad));
+    int* d_plist = nullptr;
+    VAM_TRY_CUDA(cudaMalloc(&d_plist, sizeof(int) * std::max(npc, 1)));
+    cudaError_t e = cudaMemcpyAsync(p->d_bwd_cidx, cidx.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && npc)
+        e = cudaMemcpyAsync(d_plist, plist.data(), sizeof(int) * npc, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && npc) {
+        const long tot = (long)npc * pad;
+        k_bwd_table<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(p->d_trig, d_plist, p->d_bwd_table, npc, p->nA, pad,
+                                                                   p->nY, p->nX, p->nZ, p->C);
+        e = cudaGetLastError();
+    }
+    // the host vectors and the pixel list are released after the copies and the build complete
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(d_plist);
+    if (e != cudaSuccess)
+        return set_error(VAM_ERR_CUDA, std::string("vam_parallel_prepare_backward: ") + cudaGetErrorString(e));
+    p->bwd_table_pad = pad;
     return VAM_OK;
 }
 
@@ -2235,6 +2424,7 @@ double time_weight(const Item& it) {
         case KF_FAST: return 1.0;
         case KF_GEN: return slice ? 27.0 : 4.0;
         case KB_BATCHED: case KB_FAST: return 1.2;
+        case KB_TABLE: return 1.05;
         case KB_GEN: return slice ? 10.0 : 2.0;
         case KA_TABLE: return 1.5;
         case KA_FAST: return 3.5;

@@ -56,6 +56,12 @@ class ParallelPlan:
         self._adj_ready = False
         # matched-transpose weight table: 16 B per pixel and angle (skipped above this size)
         self.adj_table_limit_bytes = 8 << 30
+        # backprojection bin table (8 B per pixel inside the circle and angle), built here for volumes the
+        # eight-slice kernels serve, so it exists before any capture of a backprojection
+        self.bwd_table_limit_bytes = 8 << 30
+        self.has_backward_table = False
+        if int(n_z) % 8 == 0 and int(n_z) >= 64:
+            self.prepare_backward()
 
     @property
     def handle(self):
@@ -99,7 +105,18 @@ class ParallelPlan:
         self._adj_ready = True
         return True
 
-    _TUNING_FIELDS = ("forward_vz", "backward_vz", "adjoint_vz", "backward_batch", "adjoint_table")
+    def prepare_backward(self):
+        """Build the backprojection bin table (allocates; not during graph capture).  False when it would
+        exceed ``bwd_table_limit_bytes`` or the sinogram is too large for its 32-bit offsets."""
+        ny, nx, nz = self.shape_vol
+        if 8 * ny * nx * (self.angles.size + 1) > self.bwd_table_limit_bytes or ny * self.angles.size * nz >= 2 ** 31:
+            return False
+        with torch.cuda.device(self.device):
+            _lib.call("vam_parallel_prepare_backward", self._h, self._stream())
+        self.has_backward_table = True
+        return True
+
+    _TUNING_FIELDS = ("forward_vz", "backward_vz", "adjoint_vz", "backward_batch", "adjoint_table", "backward_table")
 
     def set_tuning(self, tuning):
         """Set launch shapes: dict with any of forward_vz / backward_vz / adjoint_vz (0 auto, 1 generic,
