@@ -373,3 +373,33 @@ def test_backward_without_clipping_matches_oracle(n):
     assert relL2(got, ref) < TOL
     assert np.abs(got[~O.circle_mask((n, n))]).max() > 0  # pixels outside the circle are not clipped
     assert relL2(A.backward(b.copy()), O.clip_to_circle(ref)) < TOL
+
+
+def test_released_plan_is_reused_reset():
+    """A plan whose ParallelPlan object was released is handed to the next plan of the same geometry with no
+    absorption, no occlusion and the default launch shapes; its results equal a fresh plan's."""
+    import gc
+
+    from vamtoolbox_b200.projector import Projector3DParallel as P3
+
+    P3.clear_plan_pool()
+    shape, ang = (40, 40, 64), np.linspace(0, 360, 24, endpoint=False)
+    rng = np.random.default_rng(12)
+    x, b = rng.uniform(size=shape), rng.uniform(size=(40, 24, 64))
+    p = plan_for(shape, ang)
+    ref_fwd, ref_bwd = p.forward(dev(x)).cpu().numpy(), p.backward_ref(dev(b)).cpu().numpy()
+    first = p.handle.value
+    p.set_absorption("ray", alpha_per_px=0.05, radius_px=15.0)
+    p.set_occlusion(np.zeros(shape))
+    p.set_tuning({"forward_vz": 1, "backward_table": 0})
+    del p
+    gc.collect()
+    q = plan_for(shape, ang)
+    assert q.handle.value == first
+    assert q.get_tuning() == P3._DEFAULT_TUNING
+    assert np.array_equal(q.forward(dev(x)).cpu().numpy(), ref_fwd)
+    assert np.array_equal(q.backward_ref(dev(b)).cpu().numpy(), ref_bwd)
+    other = plan_for((40, 40, 64), ang + 1.0)  # different angles: a new plan
+    assert other.handle.value != first
+    q.close()
+    P3.clear_plan_pool()

@@ -192,8 +192,11 @@ __device__ __forceinline__ void table_interp(const TableRef& t, float d, float& 
 
 // Closed-form response models in float64, in the reference's operation order
 // (response.py:191-218 _map_glf / _dmapdf_glf, :239-250 linear, :252-262 identity).
+// TABLE: the kernel instance for interpolation tables (no closed-form code, whose float64 registers
+// would lower the table instance's occupancy); otherwise the kind is read from t at run time.
+template <bool TABLE>
 __device__ __forceinline__ void response_eval(const TableRef& t, float d, float& out_m, float& out_dm) {
-    if (t.kind == VAM_RESP_TABLE) {
+    if (TABLE || t.kind == VAM_RESP_TABLE) {
         table_interp(t, d, out_m, out_dm);
         return;
     }
@@ -232,10 +235,11 @@ struct DoseStats {
 };
 
 // One voxel of the fused dose pass: response, band error, gradient operand, statistics.
+template <bool TABLE>
 __device__ __forceinline__ void dose_voxel(const TableRef& tab, float d, float tgt, float ep, float w, float p,
                                            float& mp, float& op, DoseStats& S) {
     float dmp;
-    response_eval(tab, d, mp, dmp);
+    response_eval<TABLE>(tab, d, mp, dmp);
     const float e = mp - tgt;
     const float ae = fabsf(e);
     const float eb = ae - ep;
@@ -260,6 +264,7 @@ __device__ __forceinline__ void dose_voxel(const TableRef& tab, float d, float t
 // vec: all arrays 16-byte aligned, so each thread takes four consecutive voxels per
 // iteration with 16-byte loads (four independent loads in flight instead of one
 // dependent chain at a time); the remaining n % 4 voxels go element by element.
+template <bool TABLE>
 __global__ void __launch_bounds__(kThreads) k_bclp_dose(const float* __restrict__ dose, const float* __restrict__ target,
                                                         int64_t n, TableRef tab, float eps, float weight, float p,
                                                         const float* __restrict__ eps_arr,
@@ -276,16 +281,16 @@ __global__ void __launch_bounds__(kThreads) k_bclp_dose(const float* __restrict_
         const float4 w4 = w_arr ? __ldg(reinterpret_cast<const float4*>(w_arr) + i4)
                                 : make_float4(weight, weight, weight, weight);
         float4 m4, o4;
-        dose_voxel(tab, d4.x, g4.x, e4.x, w4.x, p, m4.x, o4.x, S);
-        dose_voxel(tab, d4.y, g4.y, e4.y, w4.y, p, m4.y, o4.y, S);
-        dose_voxel(tab, d4.z, g4.z, e4.z, w4.z, p, m4.z, o4.z, S);
-        dose_voxel(tab, d4.w, g4.w, e4.w, w4.w, p, m4.w, o4.w, S);
+        dose_voxel<TABLE>(tab, d4.x, g4.x, e4.x, w4.x, p, m4.x, o4.x, S);
+        dose_voxel<TABLE>(tab, d4.y, g4.y, e4.y, w4.y, p, m4.y, o4.y, S);
+        dose_voxel<TABLE>(tab, d4.z, g4.z, e4.z, w4.z, p, m4.z, o4.z, S);
+        dose_voxel<TABLE>(tab, d4.w, g4.w, e4.w, w4.w, p, m4.w, o4.w, S);
         if (mapped) reinterpret_cast<float4*>(mapped)[i4] = m4;
         reinterpret_cast<float4*>(operand)[i4] = o4;
     }
     for (int64_t i = 4 * n4 + t0; i < n; i += stride) {
         float mp, op;
-        dose_voxel(tab, dose[i], target[i], eps_arr ? eps_arr[i] : eps, w_arr ? w_arr[i] : weight, p, mp, op, S);
+        dose_voxel<TABLE>(tab, dose[i], target[i], eps_arr ? eps_arr[i] : eps, w_arr ? w_arr[i] : weight, p, mp, op, S);
         if (mapped) mapped[i] = mp;
         operand[i] = op;
     }
@@ -639,7 +644,11 @@ extern "C" int vam_bclp_dose_pass(const float* dose, const float* target, int64_
     cudaStream_t st = (cudaStream_t)stream;
     double* part = (double*)work;
     const bool vec = aligned16({dose, target, prm->eps_dev, prm->weight_dev, mapped, operand});
-    k_bclp_dose<<<nb, kThreads, 0, st>>>(dose, target, n, t, prm->eps, prm->weight, prm->p, prm->eps_dev,
+    if (t.kind == VAM_RESP_TABLE)
+        k_bclp_dose<true><<<nb, kThreads, 0, st>>>(dose, target, n, t, prm->eps, prm->weight, prm->p, prm->eps_dev,
+                                         prm->weight_dev, mapped, operand, part, vec);
+    else
+        k_bclp_dose<false><<<nb, kThreads, 0, st>>>(dose, target, n, t, prm->eps, prm->weight, prm->p, prm->eps_dev,
                                          prm->weight_dev, mapped, operand, part, vec);
     k_bclp_stats_final<<<1, kThreads, 0, st>>>(part, nb, stats);
     VAM_CHECK_LAUNCH("vam_bclp_dose_pass");

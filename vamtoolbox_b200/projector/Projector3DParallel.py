@@ -18,6 +18,7 @@ the host).
 from __future__ import annotations
 
 import ctypes
+import threading
 
 import numpy as np
 import torch
@@ -38,19 +39,63 @@ def _device_of(device):
     return d if d.index is not None else torch.device("cuda", torch.cuda.current_device())
 
 
+# Idle plans of released ParallelPlan objects, by geometry: a plan (per-angle tables, the
+# backprojection bin table, scratch volumes: hundreds of MB at 256^3) is kept when its last Python
+# reference goes away and handed to the next ParallelPlan of the same shape, angles and device, reset
+# to no absorption, no occlusion and the default launch shapes.  Repeated optimize() calls on one
+# geometry then skip the device allocations and frees (cudaMalloc / cudaFree of the tables took
+# 2-140 ms per plan, with the frees synchronising the device).  At most _POOL_MAX idle plans are kept
+# (oldest destroyed first); clear_plan_pool() destroys them all.
+_POOL_MAX = 4
+_pool = []  # [(key, handle, has_backward_table)], oldest first
+_pool_lock = threading.Lock()
+_DEFAULT_TUNING = {"forward_vz": 0, "backward_vz": 0, "adjoint_vz": 0, "backward_batch": 2, "adjoint_table": 1,
+                   "backward_table": 1}
+
+
+def _pool_key(shape_vol, angles, device):
+    return shape_vol, angles.tobytes(), str(device)
+
+
+def _pool_take(key):
+    with _pool_lock:
+        for i, (k, h, tab) in enumerate(_pool):
+            if k == key:
+                del _pool[i]
+                return h, tab
+    return None
+
+
+def _pool_give(key, h, tab):
+    evicted = []
+    with _pool_lock:
+        _pool.append((key, h, tab))
+        while len(_pool) > _POOL_MAX:
+            evicted.append(_pool.pop(0)[1])
+    for e in evicted:
+        _lib.load().vam_parallel_plan_destroy(e)
+
+
+def clear_plan_pool():
+    """Destroy every idle plan kept for reuse (releases their device memory)."""
+    with _pool_lock:
+        items = list(_pool)
+        _pool.clear()
+    for _, h, _ in items:
+        _lib.load().vam_parallel_plan_destroy(h)
+
+
 class ParallelPlan:
-    """Owns a vam_parallel_plan (per-angle tables, circle mask, occlusion, absorption)."""
+    """Owns a vam_parallel_plan (per-angle tables, circle mask, occlusion, absorption).
+
+    When the object is garbage collected its plan is kept for the next ParallelPlan of the same
+    geometry (see ``clear_plan_pool``); ``close()`` destroys it instead."""
 
     def __init__(self, n_y, n_x, n_z, angles_deg, device=None):
         self.device = _device_of(device)
         self.shape_vol = (int(n_y), int(n_x), int(n_z))
         self.angles = np.ascontiguousarray(np.asarray(angles_deg, dtype=np.float64).ravel())
         self.shape_sino = (int(n_y), self.angles.size, int(n_z))
-        geom = _lib.ParallelGeom(n_y, n_x, n_z, self.angles.size,
-                                 self.angles.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), self.device.index)
-        h = ctypes.c_void_p()
-        _lib.call("vam_parallel_plan_create", ctypes.byref(geom), ctypes.byref(h))
-        self._h = h
         self.absorption = None
         self.has_occlusion = False
         self._adj_ready = False
@@ -60,21 +105,46 @@ class ParallelPlan:
         # eight-slice kernels serve, so it exists before any capture of a backprojection
         self.bwd_table_limit_bytes = 8 << 30
         self.has_backward_table = False
+        self._key = _pool_key(self.shape_vol, self.angles, self.device)
+        reused = _pool_take(self._key)
+        if reused is not None:
+            self._h, self.has_backward_table = reused
+            try:
+                self._reset()
+            except Exception:
+                self.close()
+                raise
+            return
+        geom = _lib.ParallelGeom(n_y, n_x, n_z, self.angles.size,
+                                 self.angles.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), self.device.index)
+        h = ctypes.c_void_p()
+        _lib.call("vam_parallel_plan_create", ctypes.byref(geom), ctypes.byref(h))
+        self._h = h
         if int(n_z) % 8 == 0 and int(n_z) >= 64:
             self.prepare_backward()
+
+    def _reset(self):
+        """A reused plan: no absorption, no occlusion, the default launch shapes."""
+        with torch.cuda.device(self.device):
+            _lib.call("vam_parallel_set_absorption", self._h, _lib.ABS_NONE, None, 0.0, 1.0, self._stream())
+            _lib.call("vam_parallel_clear_occlusion", self._h)
+        self.set_tuning(dict(_DEFAULT_TUNING))
 
     @property
     def handle(self):
         return self._h
 
     def close(self):
+        """Destroy the plan now (it is not kept for reuse)."""
         if getattr(self, "_h", None) is not None and self._h.value:
             _lib.load().vam_parallel_plan_destroy(self._h)
             self._h = None
 
     def __del__(self):
         try:
-            self.close()
+            if getattr(self, "_h", None) is not None and self._h.value:
+                h, self._h = self._h, None
+                _pool_give(self._key, h, self.has_backward_table)
         except Exception:
             pass
 
