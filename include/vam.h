@@ -104,6 +104,17 @@ int vam_parallel_clear_occlusion(vam_parallel_plan* plan);
  * occluder) into out_dev.  VAM_ERR_ARG if no occlusion is set. */
 int vam_parallel_get_occlusion_sinogram(vam_parallel_plan* plan, float* out_dev, vam_stream_t stream);
 
+/* Status bits kernels with bounded waits record in their plan. */
+enum vam_status_bits {
+    VAM_STATUS_TIMEOUT = 1  /* a block gave up waiting for its shared-memory copy and left its outputs
+                               unwritten (a stalled copy; not expected in normal operation) */
+};
+/* Reads and clears the plan's status word (synchronises the device).  The 2-D
+ * tile forward stages its image boxes with TMA copies waited on with a bounded
+ * poll; a caller that must know every output was written checks this after
+ * its calls. */
+int vam_parallel_status(vam_parallel_plan* plan, int32_t* status);
+
 /* Builds the plan's backprojection bin table: for every pixel inside the clip
  * circle and every angle, np.interp's bin of t = x cos - y sin (float64, the
  * reference's expression) as a row offset and its float32 weight, 8 bytes per
@@ -153,6 +164,9 @@ typedef struct {
     int32_t adjoint_table;
     int32_t backward_table;  /* 1: the eight-slice backprojection reads its bins from the plan's table
                                 (vam_parallel_prepare_backward) when it is built; 0: computes them */
+    int32_t forward_tma;     /* 1: the 2-D tile forward stages its boxes with TMA tensor copies (an image
+                                whose rows are not 16-byte multiples, or in mask mode, is first copied
+                                into the plan's padded image); 0: with plain loads.  Bit-identical. */
 } vam_parallel_tuning;
 int vam_parallel_set_tuning(vam_parallel_plan* plan, const vam_parallel_tuning* tuning);
 int vam_parallel_get_tuning(vam_parallel_plan* plan, vam_parallel_tuning* tuning);
@@ -164,9 +178,11 @@ int vam_parallel_get_tuning(vam_parallel_plan* plan, vam_parallel_tuning* tuning
  * occupancy).  Each work item is one forward / backward_ref / adjoint
  * call exactly as the single-plan entry points describe it, and produces
  * bit-identical results; items run concurrently, so no item may read another
- * item's output or write another item's input or output.  A fast forward in
- * mask mode uses its plan's scratch volume, so one plan appears at most once
- * per batch with VAM_OP_FORWARD.
+ * item's output or write another item's input or output.  A forward that
+ * stages its input in its plan's scratch (mask mode; a 2-D slice whose width
+ * is not a multiple of four or whose input is not 16-byte aligned) makes that
+ * plan appear at most once per batch with VAM_OP_FORWARD: a list with two
+ * such calls of one plan is refused (VAM_ERR_ARG).
  *
  * The calls' descriptions travel by value in the launch's parameters (48
  * calls per launch; longer lists and further families become further

@@ -134,11 +134,14 @@ def test_batch_large_calls_bitwise():
     fetch their next ticket while a block runs and switch to one ticket at a time near the end."""
     rng = np.random.default_rng(7)
     plans = []
-    for shape, na, mode in [((256, 256, 1), 90, "mask"), ((352, 352, 1), 60, None),
+    for shape, na, mode in [((256, 256, 1), 90, "mask"), ((352, 352, 1), 60, None), ((258, 258, 1), 45, None),
+                            ((363, 363, 1), 36, "mask"), ((228, 228, 1), 40, "plain"),
                             ((96, 96, 160), 40, "mask"), ((64, 64, 96), 120, None)]:
         p = ParallelPlan(shape[0], shape[1], shape[2], np.linspace(0, 360, na, endpoint=False))
         if mode == "mask":
             p.set_absorption("mask", mask=rng.uniform(0.3, 1.0, shape[:2]))
+        elif mode == "plain":  # the 2-D forward with plain-load staging runs in the all-bodies instance
+            p.set_tuning({"forward_tma": 0})
         x = torch.as_tensor(rng.uniform(0, 1, shape), dtype=torch.float32, device="cuda")
         b = torch.as_tensor(rng.uniform(0, 1, p.shape_sino), dtype=torch.float32, device="cuda")
         plans.append((p, x, b))
@@ -171,6 +174,17 @@ def test_batch_rejects_bad_work():
         batch.submit([(p, "forward", b, x)])  # shapes swapped
     h = _lib.load()
     assert h.vam_batch_submit(batch._h, None, 0, None) == _lib.VAM_ERR_ARG
+    # two forwards of one plan that both stage their input (a 2-D slice whose rows are not a multiple of
+    # 16 bytes) would share the plan's padded image: refused, nothing launched
+    q = ParallelPlan(198, 198, 1, np.linspace(0, 180, 30, endpoint=False))
+    x1, x2 = torch.rand(198, 198, 1, device="cuda"), torch.rand(198, 198, 1, device="cuda")
+    o1, o2 = torch.zeros(q.shape_sino, device="cuda"), torch.zeros(q.shape_sino, device="cuda")
+    with pytest.raises(_lib.VamError) as e:
+        batch.submit([(q, "forward", x1, o1), (q, "forward", x2, o2)])
+    assert e.value.code == _lib.VAM_ERR_ARG and "same scratch" in e.value.message
+    batch.submit([(q, "forward", x1, o1)])
+    torch.cuda.synchronize()
+    assert torch.equal(o1, q.forward(x1))
 
 
 @pytest.mark.parametrize("schedule", ["persistent", "streams", "phased", "auto"])

@@ -61,7 +61,8 @@ class RayMedium(ctypes.Structure):
 
 class ParallelTuning(ctypes.Structure):
     _fields_ = [("forward_vz", _c_i32), ("backward_vz", _c_i32), ("adjoint_vz", _c_i32),
-                ("backward_batch", _c_i32), ("adjoint_table", _c_i32), ("backward_table", _c_i32)]
+                ("backward_batch", _c_i32), ("adjoint_table", _c_i32), ("backward_table", _c_i32),
+                ("forward_tma", _c_i32)]
 
 
 OP_FORWARD, OP_BACKWARD_REF, OP_ADJOINT = 0, 1, 2
@@ -115,6 +116,7 @@ _SIGS = {
     "vam_parallel_adjoint": ([_vp, _vp, _vp, _vp], _c_int),
     "vam_parallel_prepare_adjoint": ([_vp, _vp], _c_int),
     "vam_parallel_prepare_backward": ([_vp, _vp], _c_int),
+    "vam_parallel_status": ([_vp, ctypes.POINTER(_c_i32)], _c_int),
     "vam_parallel_set_tuning": ([_vp, ctypes.POINTER(ParallelTuning)], _c_int),
     "vam_parallel_get_tuning": ([_vp, ctypes.POINTER(ParallelTuning)], _c_int),
     "vam_ray_record_count": ([_vp, _vp, _vp], _c_int),

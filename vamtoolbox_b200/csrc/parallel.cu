@@ -24,6 +24,9 @@
 #include <mutex>
 #include <vector>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "vam_internal.cuh"
 
 namespace vam {
@@ -1045,6 +1048,146 @@ __device__ __forceinline__ void k_forward_2d_body(const Args& a, unsigned bx, un
     }
 }
 
+// The same tiles with the footprint box staged by one TMA tensor load per tile.
+//
+// A 2-D tensor map over the image (x = columns, y = rows, float32, zero fill
+// outside) loads a 100 x 96 box into shared memory, signalled on an mbarrier:
+// the box's x coordinate is the footprint's first column rounded down to a
+// multiple of 4 (a tiled copy must start on a 16-byte boundary; the remainder
+// is an offset into the box), its y coordinate the first row (negative and
+// out-of-range coordinates read the fill value: exactly the reference's zero
+// padding).  The samples are the plain tile kernel's, so the sums are
+// bit-identical.  Replacing the block's bounds-checked row loads measured
+// 0.75 -> 0.32 ms at 512^2 x 720, 0.44 -> 0.19 ms at 384^2 x 720 and
+// 0.124 -> 0.049 ms at 256^2 x 360.  Used for images whose rows are a
+// multiple of 16 bytes (nX % 4 == 0) at a 16-byte aligned address.  The wait
+// on the mbarrier is bounded: past the limit the block records
+// VAM_STATUS_TIMEOUT in the plan's status word, waits (bounded) for its copy
+// in flight and leaves its outputs unwritten.
+constexpr int kTmaW = 100, kTmaH = 96;  // box: 100 columns (x, 400 B) x 96 rows
+constexpr long kTmaWaitLimit = 1L << 24;  // try_wait polls before a block gives up
+// dynamic shared memory of the TMA tile body: 128 B of alignment slack, the box, the k-group partial sums
+// and the mbarrier
+constexpr int k2SmemTma = 128 + kTmaH * kTmaW * 4 + 4 * k2J * 4 + 16;
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
+    unsigned done = 0;
+    for (long it = 0; it < kTmaWaitLimit && !done; ++it) {
+        asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+                     : "=r"(done) : "r"(bar), "r"(parity) : "memory");
+    }
+    return done != 0;
+}
+
+// One block (tile of k2J bins x all samples, one angle) of the TMA-staged forward; tmap points to the
+// image's tensor map in parameter space (a __grid_constant__ argument or a batch item).
+template <bool RAY>
+__device__ __forceinline__ void k_forward_2d_tma_body(const Args& a, const CUtensorMap* tmap, int* status,
+                                                      unsigned bx, unsigned by) {
+    extern __shared__ float s_f2[];
+    float* box = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(s_f2) + 127) & ~(uintptr_t)127);
+    float* part = box + kTmaH * kTmaW;
+    unsigned long long* mbar = reinterpret_cast<unsigned long long*>(part + 4 * k2J);
+    const unsigned bar = smem_addr(mbar);
+    const int theta = by;
+    const int tj = threadIdx.x % k2J, tk = threadIdx.x / k2J;
+    const int j0 = bx * k2J, j = j0 + tj;
+    const int j1 = min(j0 + k2J, a.nX) - 1;
+    const double4 tr = a.trig[theta];
+    const double c = tr.x, s = tr.y;
+    const float cf = (float)c, sf = (float)s;
+    const double rowb = fma(-s, (double)j, tr.w), colb = fma(c, (double)j, tr.z);
+    float s_entry = 0.f;
+    bool live = j < a.nX;
+    if (RAY) {
+        const float t = (float)(j - a.C);
+        if (fabsf(t) > a.R) live = false;
+        else s_entry = -sqrtf(a.R * a.R - t * t);
+    }
+    const double rb0 = fma(-s, (double)j0, tr.w), rb1 = fma(-s, (double)j1, tr.w);
+    const double cb0 = fma(c, (double)j0, tr.z), cb1 = fma(c, (double)j1, tr.z);
+    auto to_int = [](double v) { return (int)fmax(fmin(floor(v), 1e9), -1e9); };
+    // the box may hold another body's generic-proxy writes (a persistent batch runs several bodies
+    // in the same shared memory): order them before the tensor copies overwrite it
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    unsigned phase = 0;
+    bool failed = false;
+    float acc = 0.f;
+    for (int k0 = 0; k0 < a.nY; k0 += k2K) {
+        const int k1 = min(k0 + k2K, a.nY) - 1;
+        double rmin = 1e300, rmax = -1e300, cmin = 1e300, cmax = -1e300;
+        for (int q = 0; q < 4; ++q) {
+            const double rb = (q & 1) ? rb1 : rb0, cb = (q & 1) ? cb1 : cb0;
+            const double kk = (q & 2) ? (double)k1 : (double)k0;
+            const double r = fma(c, kk, rb), cl = fma(s, kk, cb);
+            rmin = fmin(rmin, r); rmax = fmax(rmax, r); cmin = fmin(cmin, cl); cmax = fmax(cmax, cl);
+        }
+        const int rlo = to_int(rmin) - 1, rhi = to_int(rmax) + 2;
+        const int clo = to_int(cmin) - 1, chi = to_int(cmax) + 2;
+        // the whole tile samples outside the image: every tap is zero padding (uniform)
+        if (rhi < 0 || rlo > a.nY - 1 || chi < 0 || clo > a.nX - 1) continue;
+        const int H = min(rhi - rlo + 1, k2Box), W = min(chi - clo + 1, k2Box);
+        const int cx = clo & ~3, cofs = clo - cx;  // the box's x on a 16-byte boundary, the remainder an offset
+        if (threadIdx.x == 0) {
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                         "r"((unsigned)(kTmaH * kTmaW * 4)) : "memory");
+            asm volatile(
+                "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+                ::"r"(smem_addr(box)), "l"(tmap), "r"(cx), "r"(rlo), "r"(bar) : "memory");
+        }
+        failed = !mbar_wait(bar, phase);
+        phase ^= 1u;
+        if (failed) break;  // uniform in practice; a block that gives up writes no outputs
+        if (live) {
+            const float rl0 = (float)(fma(c, (double)k0, rowb) - (double)rlo);
+            const float cl0 = (float)(fma(s, (double)k0, colb) - (double)clo);
+            for (int kk = tk; kk <= k1 - k0; kk += 4) {
+                const float row = fmaf(cf, (float)kk, rl0), col = fmaf(sf, (float)kk, cl0);
+                const float fr = floorf(row), fc = floorf(col);
+                const float dr = row - fr, dc = col - fc;
+                // clamped for memory safety only: the margins keep every weighted tap inside the box
+                const int r0 = min(max((int)fr, 0), H - 2), c0 = min(max((int)fc, 0), W - 2);
+                const float* t0 = box + r0 * kTmaW + c0 + cofs;
+                const float w00 = (1.f - dr) * (1.f - dc), w01 = (1.f - dr) * dc;
+                const float w10 = dr * (1.f - dc), w11 = dr * dc;
+                float v = w00 * t0[0];
+                v = fmaf(w01, t0[1], v);
+                v = fmaf(w10, t0[kTmaW], v);
+                v = fmaf(w11, t0[kTmaW + 1], v);
+                if (RAY) v *= ray_factor((float)(k0 + kk - a.C), s_entry, a.alpha);
+                acc += v;
+            }
+        }
+        __syncthreads();  // every read of this box is done before the next copy overwrites it
+    }
+    if (failed) {
+        mbar_wait(bar, phase ^ 1u);  // the copy may still be in flight: wait for it once more (bounded)
+        if (threadIdx.x == 0) atomicOr(status, VAM_STATUS_TIMEOUT);
+    } else {
+        part[tk * k2J + tj] = acc;
+        __syncthreads();
+        if (tk == 0 && j < a.nX) {
+            const float sum = ((part[tj] + part[k2J + tj]) + part[2 * k2J + tj]) + part[3 * k2J + tj];
+            a.out[(size_t)j * a.nA + theta] = sum;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+template <bool RAY>
+__global__ void __launch_bounds__(256) k_forward_2d_tma(Args a, const __grid_constant__ CUtensorMap tmap,
+                                                        int* __restrict__ status) {
+    k_forward_2d_tma_body<RAY>(a, &tmap, status, blockIdx.x, blockIdx.y);
+}
+
 template <bool RAY>
 __global__ void __launch_bounds__(256) k_forward_2d(Args a) {
     k_forward_2d_body<RAY>(a, blockIdx.x, blockIdx.y);
@@ -1154,6 +1297,24 @@ __global__ void k_mask_mul(const float* __restrict__ x, const float* __restrict_
         return;
     }
     for (long i = t0; i < n; i += stride) out[i] = mask[i / nZ] * x[i];
+}
+
+// rows of w floats of x (times mask, when given) into rows of wp >= w floats of out; the columns
+// w .. wp - 1 are not written (the tensor map ends at w)
+__device__ __forceinline__ void stage_rows(const float* __restrict__ x, const float* __restrict__ mask,
+                                           float* __restrict__ out, long long npix, int w, int wp, long long t0,
+                                           long long stride) {
+    for (long long i = t0; i < npix; i += stride) {
+        const long long y = i / w;
+        const float v = mask ? mask[i] * x[i] : x[i];
+        out[y * wp + (i - y * w)] = v;
+    }
+}
+
+__global__ void k_stage_rows(const float* __restrict__ x, const float* __restrict__ mask, float* __restrict__ out,
+                             long long npix, int w, int wp) {
+    stage_rows(x, mask, out, npix, w, wp, (long long)blockIdx.x * blockDim.x + threadIdx.x,
+               (long long)gridDim.x * blockDim.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -1533,19 +1694,27 @@ struct Item {
     long long tstart;  // first ticket (virtual block) of the call inside a batch launch
     long long cost;    // estimated time of the call (batch ordering)
     int family;        // body family (k_batch instances): a bit of the FAM mask
-    // pre-pass of the fast forward in mask mode: pre_out = mask * pre_in
+    // pre-pass of the fast forward in mask mode: pre_out = mask * pre_in; of the 2-D tile forward
+    // (pre_wp > 0): rows of pre_w floats of (mask *) pre_in into rows of pre_wp floats of pre_out
     const float* pre_in;
     const float* pre_mask;
     float* pre_out;
     long long pre_npix;
+    int pre_w, pre_wp;
     Args a;
     FastArgs f;
     const float4* table;
     const int2* btab;  // KB_TABLE: the plan's backprojection bin table, its pixel index and list stride
     const int* bcidx;
     int bpad, bpad_;
+    int* status;       // the plan's status word (kernels with bounded waits record timeouts there)
+    int tma, tma_pad_;  // KF_2D: 1 when tmap describes a.in and the tiles are staged by TMA loads
+    CUtensorMap tmap;   // read from parameter space, as a direct launch's __grid_constant__ argument
 };
 static_assert(sizeof(Item) % 8 == 0, "Item is copied to shared memory in 8-byte words");
+
+bool image_tensor_map(const float* img, int nX, int nY, int row_stride, CUtensorMap& m);
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
 
 int describe(vam_parallel_plan* plan, Op op, const float* in, float* out, Item& it, const char* name,
              bool noclip = false) {
@@ -1576,7 +1745,18 @@ int describe(vam_parallel_plan* plan, Op op, const float* in, float* out, Item& 
         it.ray = ray;
         it.vz = 1;
         if (op == Op::Forward) {
-            if (a.mask) {  // stage the masked image once per call instead of per tile
+            const bool aligned = (((uintptr_t)in) & 15) == 0 && plan->nX % 4 == 0;
+            const bool use_tma = plan->tune_fwd_tma && tensor_map_encoder();
+            const int wp = (plan->nX + 3) & ~3;
+            if (plan->d_img_pad && use_tma && (a.mask || !aligned)) {
+                // TMA rows start on 16-byte boundaries: stage (the masked) image once per call into
+                // rows of a multiple of four floats
+                it.pre_in = in; it.pre_mask = a.mask; it.pre_out = plan->d_img_pad;
+                it.pre_npix = (long long)plan->nY * plan->nX; it.pre_nz = 1;
+                it.pre_w = plan->nX; it.pre_wp = wp;
+                a.in = plan->d_img_pad;
+                a.mask = nullptr;
+            } else if (a.mask) {  // stage the masked image once per call instead of per tile
                 it.pre_in = in; it.pre_mask = plan->d_mask; it.pre_out = plan->d_vol_scratch;
                 it.pre_npix = (long long)plan->nY * plan->nX; it.pre_nz = 1;
                 a.in = plan->d_vol_scratch;
@@ -1584,9 +1764,11 @@ int describe(vam_parallel_plan* plan, Op op, const float* in, float* out, Item& 
             }
             it.kind = KF_2D;
             it.family = 128;
+            it.status = plan->d_status;
+            it.tma = use_tma && image_tensor_map(a.in, a.nX, a.nY, it.pre_wp ? it.pre_wp : a.nX, it.tmap) ? 1 : 0;
             it.gx = (unsigned)((plan->nX + k2J - 1) / k2J);
             it.gy = (unsigned)plan->nA;
-            it.smem = k2Smem;
+            it.smem = it.tma ? k2SmemTma : k2Smem;
         } else {
             it.kind = KB_2D;
             it.gx = (unsigned)(((plan->nX + kB2 - 1) / kB2) * ((plan->nY + kB2 - 1) / kB2));
@@ -1703,7 +1885,8 @@ __device__ __forceinline__ void fast_body(const Item& it, unsigned bx, unsigned 
     if constexpr ((FAM & 128) != 0) {
         if (it.kind == KF_2D) {
             const Args a = it.a;
-            k_forward_2d_body<RAY>(a, bx, by);
+            if (it.tma) k_forward_2d_tma_body<RAY>(a, &it.tmap, it.status, bx, by);
+            else if constexpr (FAM == 255) k_forward_2d_body<RAY>(a, bx, by);
         }
     }
     if constexpr ((FAM & 8) != 0 || ((FAM & 2) != 0 && !RAY)) {
@@ -1790,11 +1973,46 @@ void launch_gen2(const Item& it, dim3 grid, cudaStream_t st) {
     else launch_gen3<VZ, OCC, VAM_ABS_NONE>(it, grid, st);
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against the driver
+// library); null when the driver does not provide it
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static std::once_flag once;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    std::call_once(once, [] {
+        void* fp = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fp, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fp);
+    });
+    return fn;
+}
+
+// The tensor map of a [nY][nX] float32 image with rows row_stride floats apart, for
+// k_forward_2d_tma's boxes: false (plain staging) unless the rows are a multiple of 16 bytes apart and
+// the image starts on a 16-byte boundary.  A host-only call, so a captured launch carries the map in
+// its parameters.
+bool image_tensor_map(const float* img, int nX, int nY, int row_stride, CUtensorMap& m) {
+    if ((((uintptr_t)img) & 15) != 0 || row_stride % 4 != 0 || row_stride < nX) return false;
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)nX, (cuuint64_t)nY};
+    cuuint64_t strides[1] = {(cuuint64_t)row_stride * sizeof(float)};
+    cuuint32_t box[2] = {(cuuint32_t)kTmaW, (cuuint32_t)kTmaH};
+    cuuint32_t es[2] = {1, 1};
+    return enc(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(img), dims, strides, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <bool RAY>
 void launch_fast(const Item& it, dim3 grid, cudaStream_t st) {
     const dim3 block(kWarpsPerBlock * kWarp);
     switch (it.kind) {
-        case KF_2D: k_forward_2d<RAY><<<grid, block, it.smem, st>>>(it.a); break;
+        case KF_2D:
+            if (it.tma) k_forward_2d_tma<RAY><<<grid, block, it.smem, st>>>(it.a, it.tmap, it.status);
+            else k_forward_2d<RAY><<<grid, block, it.smem, st>>>(it.a);
+            break;
         case KB_2D: k_backward_2d<RAY><<<grid, block, it.smem, st>>>(it.a); break;
         case KF_FAST:
             if (it.vz == 8) k_forward_fast<8, RAY><<<grid, block, 0, st>>>(it.f);
@@ -1819,7 +2037,11 @@ void launch_fast(const Item& it, dim3 grid, cudaStream_t st) {
 }
 
 int launch_item(const Item& it, cudaStream_t st, const char* name) {
-    if (it.pre_in) {
+    if (it.pre_in && it.pre_wp) {
+        k_stage_rows<<<(unsigned)std::min<long long>((it.pre_npix + 255) / 256, 148LL * 32), 256, 0, st>>>(
+            it.pre_in, it.pre_mask, it.pre_out, it.pre_npix, it.pre_w, it.pre_wp);
+        VAM_CHECK_LAUNCH("k_stage_rows");
+    } else if (it.pre_in) {
         const long long n = it.pre_npix * it.pre_nz;
         k_mask_mul<<<(unsigned)std::min<long long>((n + 255) / 256, 148LL * 32), 256, 0, st>>>(
             it.pre_in, it.pre_mask, it.pre_out, (long)it.pre_npix, it.pre_nz);
@@ -1955,6 +2177,11 @@ BatchKernel batch_kernel(int fam) {
 __global__ void k_batch_premask(const __grid_constant__ BatchParams P) {
     const Item& it = P.items[blockIdx.y];
     if (!it.pre_in) return;
+    if (it.pre_wp) {
+        stage_rows(it.pre_in, it.pre_mask, it.pre_out, it.pre_npix, it.pre_w, it.pre_wp,
+                   (long long)blockIdx.x * blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
+        return;
+    }
     const long long n = it.pre_npix * it.pre_nz;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         it.pre_out[i] = it.pre_mask[i / it.pre_nz] * it.pre_in[i];
@@ -1998,6 +2225,7 @@ extern "C" int vam_parallel_plan_create(const vam_parallel_geom* geom, vam_paral
     p->tune_bwd_batch = 2;
     p->tune_adj_table = 1;
     p->tune_bwd_table = 1;
+    p->tune_fwd_tma = 1;
     // per-angle tables exactly as numpy evaluates them (Projector3DParallel.py:135-143)
     std::vector<double4> trig(p->nA);
     for (int i = 0; i < p->nA; ++i) {
@@ -2045,6 +2273,10 @@ extern "C" int vam_parallel_plan_create(const vam_parallel_geom* geom, vam_paral
     if (e == cudaSuccess) e = cudaMemcpy(p->d_tasks_paired, paired.data(), sizeof(int2) * paired.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(p->d_tasks_single, single.data(), sizeof(int2) * single.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMalloc(&p->d_circle, circ.size());
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_status, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(p->d_status, 0, sizeof(int));
+    if (e == cudaSuccess && p->nZ == 1)
+        e = cudaMalloc(&p->d_img_pad, sizeof(float) * (size_t)p->nY * (size_t)((p->nX + 3) & ~3));
     if (e == cudaSuccess) e = cudaMemcpy(p->d_trig, trig.data(), sizeof(double4) * p->nA, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(p->d_circle, circ.data(), circ.size(), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
@@ -2071,6 +2303,8 @@ extern "C" int vam_parallel_plan_destroy(vam_parallel_plan* p) {
     cudaFree(p->d_adj_table);
     cudaFree(p->d_bwd_table);
     cudaFree(p->d_bwd_cidx);
+    cudaFree(p->d_status);
+    cudaFree(p->d_img_pad);
     delete p;
     return VAM_OK;
 }
@@ -2202,6 +2436,7 @@ extern "C" int vam_parallel_set_tuning(vam_parallel_plan* p, const vam_parallel_
     p->tune_bwd_batch = t->backward_batch == 0 ? 2 : t->backward_batch;
     p->tune_adj_table = t->adjoint_table;
     p->tune_bwd_table = t->backward_table;
+    p->tune_fwd_tma = t->forward_tma;
     return VAM_OK;
 }
 
@@ -2214,6 +2449,7 @@ extern "C" int vam_parallel_get_tuning(vam_parallel_plan* p, vam_parallel_tuning
     t->backward_batch = p->tune_bwd_batch;
     t->adjoint_table = p->tune_adj_table;
     t->backward_table = p->tune_bwd_table;
+    t->forward_tma = p->tune_fwd_tma;
     return VAM_OK;
 }
 
@@ -2231,6 +2467,17 @@ extern "C" int vam_parallel_prepare_adjoint(vam_parallel_plan* p, vam_stream_t s
         k_adj_table<false><<<nb, 256, 0, st>>>(p->d_trig, p->d_adj_table, p->nY, p->nX, p->nA, p->C, 0.f, 0.f);
     VAM_CHECK_LAUNCH("k_adj_table");
     p->adj_table_abs = p->abs_mode;
+    return VAM_OK;
+}
+
+extern "C" int vam_parallel_status(vam_parallel_plan* p, int32_t* status) {
+    clear_error();
+    VAM_REQUIRE(p && status, VAM_ERR_ARG, "vam_parallel_status: null argument");
+    DeviceGuard g(p->device);
+    int v = 0;
+    VAM_TRY_CUDA(cudaMemcpy(&v, p->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    VAM_TRY_CUDA(cudaMemset(p->d_status, 0, sizeof(int)));
+    *status = v;
     return VAM_OK;
 }
 
@@ -2453,9 +2700,20 @@ int batch_prepare(vam_batch* b, const vam_work* work, int32_t n) {
         if (d.kind == KB_GEN) items[i].family = gen_heavy ? 8 : 64;
         else if (d.family == 2 && d.ray) items[i].family = 8;
         if (d.kind == KF_GEN) items[i].family = gen_heavy ? 16 : 32;
+        // the 2-D forward instance carries the TMA-staged body only; plain staging (no tensor map
+        // encoder) runs in the all-bodies instance
+        if (d.kind == KF_2D && !d.tma) items[i].family = 255;
+
         VAM_REQUIRE((long long)items[i].gx * items[i].gy < (1LL << 31), VAM_ERR_SHAPE, "vam_batch: call grid too large");
         items[i].cost = (long long)std::llround((double)items[i].cost * time_weight(items[i]));
     }
+    // a staged forward writes its plan's scratch: two such calls of one plan would share it
+    std::vector<const float*> staged;
+    for (const Item& it : items)
+        if (it.pre_out) staged.push_back(it.pre_out);
+    std::sort(staged.begin(), staged.end());
+    VAM_REQUIRE(std::adjacent_find(staged.begin(), staged.end()) == staged.end(), VAM_ERR_ARG,
+                "vam_batch: two forwards of one plan stage their input into the same scratch");
     // one launch per body family (each with the narrowest instance and its occupancy), and
     // within a family the largest call first, so the small ones fill the tail of the queue
     std::stable_sort(items.begin(), items.end(), [](const Item& x, const Item& y) {

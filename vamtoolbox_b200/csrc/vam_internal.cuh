@@ -81,6 +81,8 @@ struct vam_parallel_plan {
     int n_tasks_paired;
     int2* d_tasks_single;   // (a, -1) for every angle
     float* d_vol_scratch;   // [nY][nX][nZ] masked copy of the input (VAM_ABS_MASK)
+    int* d_status;          // error bits the kernels record (VAM_STATUS_*), read by vam_parallel_status
+    float* d_img_pad;       // nZ == 1: [nY][nX rounded up to 4] staged image of the TMA-tiled 2-D forward
     // matched-transpose weights: per pixel and angle, the first of <= 3
     // detector rows (as int bits) and their summed forward tap weights
     float4* d_adj_table;    // [nY*nX][nA]
@@ -92,5 +94,5 @@ struct vam_parallel_plan {
     int* d_bwd_cidx;
     int bwd_table_pad;
     // tuning (vam_parallel_set_tuning): vector widths 0 = automatic
-    int tune_fwd_vz, tune_bwd_vz, tune_adj_vz, tune_bwd_batch, tune_adj_table, tune_bwd_table;
+    int tune_fwd_vz, tune_bwd_vz, tune_adj_vz, tune_bwd_batch, tune_adj_table, tune_bwd_table, tune_fwd_tma;
 };

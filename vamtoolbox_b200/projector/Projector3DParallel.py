@@ -50,7 +50,7 @@ _POOL_MAX = 4
 _pool = []  # [(key, handle, has_backward_table)], oldest first
 _pool_lock = threading.Lock()
 _DEFAULT_TUNING = {"forward_vz": 0, "backward_vz": 0, "adjoint_vz": 0, "backward_batch": 2, "adjoint_table": 1,
-                   "backward_table": 1}
+                   "backward_table": 1, "forward_tma": 1}
 
 
 def _pool_key(shape_vol, angles, device):
@@ -186,11 +186,13 @@ class ParallelPlan:
         self.has_backward_table = True
         return True
 
-    _TUNING_FIELDS = ("forward_vz", "backward_vz", "adjoint_vz", "backward_batch", "adjoint_table", "backward_table")
+    _TUNING_FIELDS = ("forward_vz", "backward_vz", "adjoint_vz", "backward_batch", "adjoint_table", "backward_table",
+                      "forward_tma")
 
     def set_tuning(self, tuning):
         """Set launch shapes: dict with any of forward_vz / backward_vz / adjoint_vz (0 auto, 1 generic,
-        4, 8), backward_batch (1, 2, 4) and adjoint_table (0, 1); missing keys keep their value."""
+        4, 8), backward_batch (1, 2, 4), adjoint_table, backward_table and forward_tma (0, 1); missing keys
+        keep their value."""
         cur = self.get_tuning()
         unknown = set(tuning) - set(self._TUNING_FIELDS)
         if unknown:
@@ -218,6 +220,14 @@ class ParallelPlan:
             _lib.call("vam_parallel_set_occlusion", self._h, _lib.ptr(ins), self._stream())
             torch.cuda.current_stream(self.device).synchronize()
         self.has_occlusion = True
+
+    def status(self):
+        """Read and clear the plan's status bits (vam_status_bits; 0 = every launch completed its outputs).
+        Synchronises the device."""
+        v = ctypes.c_int32()
+        with torch.cuda.device(self.device):
+            _lib.call("vam_parallel_status", self._h, ctypes.byref(v))
+        return int(v.value)
 
     def set_occlusion_2d(self, occlusion):
         """The 2-D class's digitised occlusion (Projector2DParallel.py:70-143) from a boolean [nY, nX]
