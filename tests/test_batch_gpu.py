@@ -136,12 +136,15 @@ def test_batch_large_calls_bitwise():
     plans = []
     for shape, na, mode in [((256, 256, 1), 90, "mask"), ((352, 352, 1), 60, None), ((258, 258, 1), 45, None),
                             ((363, 363, 1), 36, "mask"), ((228, 228, 1), 40, "plain"),
-                            ((96, 96, 160), 40, "mask"), ((64, 64, 96), 120, None)]:
+                            ((96, 96, 160), 40, "mask"), ((64, 64, 96), 120, None),
+                            ((64, 64, 256), 72, "table"), ((49, 49, 128), 60, "table")]:
         p = ParallelPlan(shape[0], shape[1], shape[2], np.linspace(0, 360, na, endpoint=False))
         if mode == "mask":
             p.set_absorption("mask", mask=rng.uniform(0.3, 1.0, shape[:2]))
         elif mode == "plain":  # the 2-D forward with plain-load staging runs in the all-bodies instance
             p.set_tuning({"forward_tma": 0})
+        elif mode == "table":  # block-table backprojection (eight and four slices per lane)
+            assert p.prepare_backward()
         x = torch.as_tensor(rng.uniform(0, 1, shape), dtype=torch.float32, device="cuda")
         b = torch.as_tensor(rng.uniform(0, 1, p.shape_sino), dtype=torch.float32, device="cuda")
         plans.append((p, x, b))

@@ -238,6 +238,8 @@ def test_every_launch_shape_matches_oracle(tuning, absn):
         p.set_absorption("ray", alpha_per_px=0.05, radius_px=12.5)
         oabs = ("ray", 0.05, 12.5)
     p.set_tuning(tuning)
+    if tuning["backward_table"]:
+        assert p.prepare_backward()
     got = p.get_tuning()
     assert {k: got[k] for k in tuning} == tuning
     assert relL2(p.forward(dev(x)).cpu().numpy(), O.parallel_forward(x, ang, absorption=oabs)) < TOL
@@ -438,3 +440,29 @@ def test_tma_staged_slice_forward_matches_plain_loads_and_oracle(ny, nx, na, mod
     assert np.array_equal(a, b) and np.array_equal(a, c) and np.array_equal(a, d)
     assert relL2(a, O.parallel_forward(x, ang, absorption=oabs)) < TOL
     assert p.status() == 0
+
+
+@pytest.mark.parametrize("shape,na,mode", [((64, 64, 256), 90, None), ((63, 63, 128), 47, "mask"),
+                                           ((40, 40, 512), 33, None), ((34, 34, 64), 40, None),
+                                           ((37, 37, 200), 25, "mask")])
+def test_backprojection_table_bitwise_and_oracle(shape, na, mode):
+    """The backprojection from the plan's bin table (2 x 2 block table for nZ % 128 == 0: eight slices per
+    lane when nZ % 256 == 0, else four; the per-pixel table otherwise) gives the computed-bin kernel's sums
+    bit for bit, and the oracle's within float32 tolerance: odd widths (partial blocks and tiles), several
+    z chunks, angle counts that are not multiples of 32 (partial entry chunks), mask absorption."""
+    rng = np.random.default_rng(sum(shape) + na)
+    ang = np.linspace(0, 360, na, endpoint=False) + 0.7
+    p = plan_for(shape, ang)
+    oabs = None
+    if mode == "mask":
+        m = rng.uniform(0.2, 1.0, shape[:2])
+        p.set_absorption("mask", mask=m)
+        oabs = ("mask", m)
+    b = rng.uniform(0, 1, (shape[0], na, shape[2]))
+    p.set_tuning({"backward_vz": 8, "backward_table": 0})
+    computed = p.backward_ref(dev(b))
+    assert p.prepare_backward()
+    p.set_tuning({"backward_table": 1})
+    tabled = p.backward_ref(dev(b))
+    assert torch.equal(computed, tabled)
+    assert relL2(tabled.cpu().numpy(), O.parallel_backward_ref(b, ang, absorption=oabs)) < TOL

@@ -934,6 +934,197 @@ __global__ void __launch_bounds__(256, 1) k_backward_tab8(Args a, const int2* __
 }
 
 // ---------------------------------------------------------------------------
+// Block-table backprojection: 2 x 2 pixel blocks share their detector rows.
+//
+// For one angle the four pixels of a 2 x 2 block have t = x cos - y sin within
+// |cos| + |sin| <= sqrt(2) of each other, so their np.interp bins j0 span at
+// most three consecutive values and the block needs at most four detector
+// rows (j_min .. j_max + 1) instead of eight.  k_bwd_btable stores, per block
+// inside the clip circle and angle, 32 bytes: the offset of row j_min
+// (j_min * nA * nZ + angle * nZ, -1 when no pixel of the block contributes),
+// a code (bits 0-1: j_max - j_min; per pixel q three bits at 2 + 3q: bit 0
+// contributes, bits 1-2: j0 - j_min) and the four pixels' float32 weights,
+// each pixel's (j0, weight) exactly as k_bwd_table's entry.  k_backward_blk
+// then loads the block's rows once per warp and runs, per pixel, the same two
+// packed FMAs per slice pair in the same order as k_backward_tab8: the sums
+// are bit-identical to it.  The warp walks the rows in passes d = 0 .. span
+// (rows d and d + 1 live), applying each pixel in the pass of its own j0, so
+// at most three rows are held in registers.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_bwd_btable(const double4* __restrict__ trig, const int* __restrict__ blist,
+                                                    const int* __restrict__ cidx, int4* __restrict__ tab, int nbc,
+                                                    int nA, int nY, int nX, int nZ, int C) {
+    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;  // over (block, angle), angle fastest
+    if (idx >= (long)nbc * nA) return;
+    const int th = (int)(idx % nA);
+    const int blk = blist[idx / nA];
+    const int nbx = (nX + 1) >> 1;
+    const int bi = blk / nbx, bj = blk - bi * nbx;
+    const double4 tr = trig[th];
+    int j0s[4];
+    float ws[4];
+    bool val[4];
+    int jmin = 1 << 30, jmax = -1;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int i = 2 * bi + (q >> 1), j = 2 * bj + (q & 1);
+        val[q] = i < nY && j < nX && cidx[(size_t)i * nX + j] >= 0;
+        j0s[q] = 0;
+        ws[q] = 0.f;
+        if (val[q]) {
+            const double X = (double)(j - C), Y = (double)(i - C);
+            const double t = __dsub_rn(__dmul_rn(X, tr.x), __dmul_rn(Y, tr.y));
+            if (!(t >= (double)(-C) && t <= (double)(nY - 1 - C))) {
+                val[q] = false;
+            } else {
+                const double ft = floor(t);
+                const int j0 = (int)ft + C;
+                if (j0 == nY - 1) { j0s[q] = nY - 2; ws[q] = 1.f; }
+                else { j0s[q] = j0; ws[q] = (float)(t - ft); }
+                jmin = min(jmin, j0s[q]);
+                jmax = max(jmax, j0s[q]);
+            }
+        }
+    }
+    if (jmax < 0) {
+        tab[2 * idx] = make_int4(-1, 0, 0, 0);
+        tab[2 * idx + 1] = make_int4(0, 0, 0, 0);
+        return;
+    }
+    int code = jmax - jmin;  // <= 2
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+        if (val[q]) code |= (1 | ((j0s[q] - jmin) << 1)) << (2 + 3 * q);
+    tab[2 * idx] = make_int4(jmin * nA * nZ + th * nZ, code, __float_as_int(ws[0]), __float_as_int(ws[1]));
+    tab[2 * idx + 1] = make_int4(__float_as_int(ws[2]), __float_as_int(ws[3]), 0, 0);
+}
+
+template <int VZ>
+struct RowV {
+    float4 v[VZ / 4];
+};
+
+template <int VZ>
+__device__ __forceinline__ void load_row(RowV<VZ>& r, const float* __restrict__ p) {
+#pragma unroll
+    for (int q = 0; q < VZ / 4; ++q) r.v[q] = __ldg(reinterpret_cast<const float4*>(p + 128 * q));
+}
+
+// acc (slice pairs) += (1 - w) * r0 then += w * r1: k_backward_tab8's two packed FMAs per pair
+template <int VZ>
+__device__ __forceinline__ void lerp_rows(unsigned long long (&acc)[VZ / 2], float w, const RowV<VZ>& r0,
+                                          const RowV<VZ>& r1) {
+    const unsigned long long w0 = pk_pair(1.f - w, 1.f - w), w1 = pk_pair(w, w);
+#pragma unroll
+    for (int q = 0; q < VZ / 4; ++q) {
+        fma_pair(acc[2 * q], w0, r0.v[q].x, r0.v[q].y);
+        fma_pair(acc[2 * q + 1], w0, r0.v[q].z, r0.v[q].w);
+    }
+#pragma unroll
+    for (int q = 0; q < VZ / 4; ++q) {
+        fma_pair(acc[2 * q], w1, r1.v[q].x, r1.v[q].y);
+        fma_pair(acc[2 * q + 1], w1, r1.v[q].z, r1.v[q].w);
+    }
+}
+
+// one warp per (2 x 2 block, z chunk of 32 VZ slices); nZ a multiple of 32 VZ.  The table entries
+// arrive 32 angles at a time (lane l holds angle k0 + l's 32 bytes, one coalesced 1 KB load per warp,
+// the next 32 in flight) and are broadcast with shuffles, so no angle waits for its entry.
+template <int VZ>
+__device__ __forceinline__ void k_backward_blk_body(const Args& a, const int4* __restrict__ tab,
+                                                    const int* __restrict__ bcidx, unsigned bx) {
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    // a CTA: 4 x 2 blocks (8 x 4 pixels, one block per warp) of one z chunk, so the warps of a CTA
+    // read overlapping detector rows for the same angle at about the same time
+    const int zc = (int)(bx % (unsigned)a.zchunks);
+    const unsigned tile = bx / (unsigned)a.zchunks;
+    const int nbx = (a.nX + 1) >> 1, nby = (a.nY + 1) >> 1;
+    const int ntx = (nbx + 3) >> 2;
+    const int bi = (int)(tile / ntx) * 2 + (wp >> 2), bj = (int)(tile % ntx) * 4 + (wp & 3);
+    if (bi >= nby || bj >= nbx) return;
+    const long blk = (long)bi * nbx + bj;
+    const int z0 = zc * 32 * VZ + 4 * lane;
+    unsigned long long acc[4][VZ / 2];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int e = 0; e < VZ / 2; ++e) acc[q][e] = 0ull;
+    const int pc = bcidx[blk];
+    if (pc >= 0) {
+        const int rs = a.nA * a.nZ;
+        const float* __restrict__ bz = a.in + z0;
+        const int4* __restrict__ e = tab + (size_t)pc * a.nA * 2;
+        const int nA = a.nA;
+        auto chunk = [&](int k0, int4& h0, int4& h1) {
+            const int k = k0 + lane;
+            if (k < nA) { h0 = __ldcs(e + 2 * k); h1 = __ldcs(e + 2 * k + 1); }
+            else { h0 = make_int4(-1, 0, 0, 0); h1 = make_int4(0, 0, 0, 0); }
+        };
+        int4 h0, h1, g0, g1;
+        chunk(0, h0, h1);
+        chunk(32, g0, g1);
+#pragma unroll 1
+        for (int k0 = 0; k0 < nA; k0 += 32) {
+            const int kn = min(32, nA - k0);
+#pragma unroll 1
+            for (int l = 0; l < kn; ++l) {
+                const int off = __shfl_sync(0xffffffffu, h0.x, l);
+                if (off < 0) continue;  // uniform: every lane read lane l's entry
+                const int code = __shfl_sync(0xffffffffu, h0.y, l);
+                const float w[4] = {__int_as_float(__shfl_sync(0xffffffffu, h0.z, l)),
+                                    __int_as_float(__shfl_sync(0xffffffffu, h0.w, l)),
+                                    __int_as_float(__shfl_sync(0xffffffffu, h1.x, l)),
+                                    __int_as_float(__shfl_sync(0xffffffffu, h1.y, l))};
+                const float* pr = bz + off;
+                const int span = code & 3;
+                RowV<VZ> ra, rb, rc;
+                load_row<VZ>(ra, pr);
+                load_row<VZ>(rb, pr + rs);
+                if (span >= 1) load_row<VZ>(rc, pr + 2 * rs);
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if (((code >> (2 + 3 * q)) & 7) == 1) lerp_rows<VZ>(acc[q], w[q], ra, rb);
+                if (span >= 1) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        if (((code >> (2 + 3 * q)) & 7) == 3) lerp_rows<VZ>(acc[q], w[q], rb, rc);
+                    if (span == 2) {
+                        load_row<VZ>(ra, pr + 3 * rs);
+#pragma unroll
+                        for (int q = 0; q < 4; ++q)
+                            if (((code >> (2 + 3 * q)) & 7) == 5) lerp_rows<VZ>(acc[q], w[q], rc, ra);
+                    }
+                }
+            }
+            h0 = g0; h1 = g1;
+            if (k0 + 64 < nA) chunk(k0 + 64, g0, g1);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int i = 2 * bi + (q >> 1), j = 2 * bj + (q & 1);
+        if (i >= a.nY || j >= a.nX) continue;
+        const long p = (long)i * a.nX + j;
+        float v[VZ];
+#pragma unroll
+        for (int e2 = 0; e2 < VZ / 2; ++e2)
+            asm("mov.b64 {%0, %1}, %2;" : "=f"(v[2 * e2]), "=f"(v[2 * e2 + 1]) : "l"(acc[q][e2]));
+        if (a.mask) {
+            const float m = __ldg(a.mask + p);
+#pragma unroll
+            for (int e2 = 0; e2 < VZ; ++e2) v[e2] = m * v[e2];
+        }
+        store_vz<VZ>(a.out + (size_t)p * a.nZ + z0, v, VZ / 4);
+    }
+}
+
+template <int VZ, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_backward_blk(Args a, const int4* __restrict__ tab,
+                                                            const int* __restrict__ bcidx) {
+    k_backward_blk_body<VZ>(a, tab, bcidx, blockIdx.x);
+}
+
+// ---------------------------------------------------------------------------
 // 2-D slices (nZ = 1): shared-memory tiles.
 //
 // With one slice there is no contiguous axis to put lanes on: a warp's taps
@@ -1059,11 +1250,15 @@ __device__ __forceinline__ void k_forward_2d_body(const Args& a, unsigned bx, un
 // padding).  The samples are the plain tile kernel's, so the sums are
 // bit-identical.  Replacing the block's bounds-checked row loads measured
 // 0.75 -> 0.32 ms at 512^2 x 720, 0.44 -> 0.19 ms at 384^2 x 720 and
-// 0.124 -> 0.049 ms at 256^2 x 360.  Used for images whose rows are a
-// multiple of 16 bytes (nX % 4 == 0) at a 16-byte aligned address.  The wait
-// on the mbarrier is bounded: past the limit the block records
-// VAM_STATUS_TIMEOUT in the plan's status word, waits (bounded) for its copy
-// in flight and leaves its outputs unwritten.
+// 0.124 -> 0.049 ms at 256^2 x 360.  The tensor map needs rows a multiple of
+// 16 bytes apart at a 16-byte aligned address: other images (and masked ones)
+// are first copied into the plan's padded image, whose rows are nX rounded up
+// to four floats (the map still ends at nX, so the padding is never read);
+// 0.223 -> 0.105 ms at 363^2 x 360 with that copy.  The wait on the mbarrier
+// is bounded: past the limit the block records VAM_STATUS_TIMEOUT in the
+// plan's status word, waits (bounded) for its copy in flight and leaves its
+// outputs unwritten.  A persistent batch runs the same body from its items'
+// tensor maps (parameter space, like a direct launch's __grid_constant__ map).
 constexpr int kTmaW = 100, kTmaH = 96;  // box: 100 columns (x, 400 B) x 96 rows
 constexpr long kTmaWaitLimit = 1L << 24;  // try_wait polls before a block gives up
 // dynamic shared memory of the TMA tile body: 128 B of alignment slack, the box, the k-group partial sums
@@ -1682,7 +1877,8 @@ int fast_vz(int nZ, bool aligned, double min_eff) {
 // same body for many calls inside one persistent launch.  Both paths therefore
 // compute bit-identical results.
 // ---------------------------------------------------------------------------
-enum Kind : int { KF_FAST = 0, KF_GEN, KB_BATCHED, KB_FAST, KB_GEN, KA_TABLE, KA_FAST, KA_GEN, KF_2D, KB_2D, KB_TABLE };
+enum Kind : int { KF_FAST = 0, KF_GEN, KB_BATCHED, KB_FAST, KB_GEN, KA_TABLE, KA_FAST, KA_GEN, KF_2D, KB_2D, KB_TABLE,
+                  KB_BTABLE };
 
 struct Item {
     int kind;
@@ -1707,6 +1903,7 @@ struct Item {
     const int2* btab;  // KB_TABLE: the plan's backprojection bin table, its pixel index and list stride
     const int* bcidx;
     int bpad, bpad_;
+    const int4* btab4;  // KB_BTABLE: the plan's 2 x 2 block table (bcidx: its block index)
     int* status;       // the plan's status word (kernels with bounded waits record timeouts there)
     int tma, tma_pad_;  // KF_2D: 1 when tmap describes a.in and the tiles are staged by TMA loads
     CUtensorMap tmap;   // read from parameter space, as a direct launch's __grid_constant__ argument
@@ -1717,7 +1914,7 @@ bool image_tensor_map(const float* img, int nX, int nY, int row_stride, CUtensor
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
 
 int describe(vam_parallel_plan* plan, Op op, const float* in, float* out, Item& it, const char* name,
-             bool noclip = false) {
+             bool noclip = false, bool in_batch = false) {
     VAM_REQUIRE(plan && in && out, VAM_ERR_ARG, std::string(name) + ": null argument");
     VAM_REQUIRE(!noclip || plan->d_ones, VAM_ERR_ARG, std::string(name) + ": no all-ones circle table");
     std::memset(&it, 0, sizeof(it));
@@ -1811,7 +2008,17 @@ int describe(vam_parallel_plan* plan, Op op, const float* in, float* out, Item& 
         if (op == Op::BackwardRef) {
             // the batched kernel stages cos / sin of every angle in shared memory (16 B per angle)
             const int batch = (size_t)plan->nA * sizeof(double2) <= 48 * 1024 ? plan->tune_bwd_batch : 1;
-            if (vzf == 8 && !ray && plan->d_bwd_table && plan->tune_bwd_table) {
+            if (!ray && plan->d_bwd_btab && plan->tune_bwd_table && plan->nZ % 128 == 0) {
+                // the 2 x 2 block table: eight slices per lane when nZ % 256 == 0, else four
+                const int bvz = plan->nZ % 256 == 0 ? 8 : 4;
+                it.kind = KB_BTABLE;
+                it.vz = bvz;
+                a.zchunks = plan->nZ / (32 * bvz);
+                const long ntx = ((plan->nX + 1) / 2 + 3) / 4, nty = ((plan->nY + 1) / 2 + 1) / 2;
+                it.gx = (unsigned)(ntx * nty * a.zchunks);
+                it.btab4 = plan->d_bwd_btab;
+                it.bcidx = plan->d_bwd_bcidx;
+            } else if (vzf == 8 && !ray && plan->d_bwd_table && plan->tune_bwd_table) {
                 it.kind = KB_TABLE;
                 it.btab = plan->d_bwd_table;
                 it.bcidx = plan->d_bwd_cidx;
@@ -1886,7 +2093,14 @@ __device__ __forceinline__ void fast_body(const Item& it, unsigned bx, unsigned 
         if (it.kind == KF_2D) {
             const Args a = it.a;
             if (it.tma) k_forward_2d_tma_body<RAY>(a, &it.tmap, it.status, bx, by);
-            else if constexpr (FAM == 255) k_forward_2d_body<RAY>(a, bx, by);
+            else if constexpr (FAM == 511) k_forward_2d_body<RAY>(a, bx, by);
+        }
+    }
+    if constexpr (FAM == 256 && !RAY) {
+        if (it.kind == KB_BTABLE) {
+            const Args a = it.a;
+            if (it.vz == 8) k_backward_blk_body<8>(a, it.btab4, it.bcidx, bx);
+            else k_backward_blk_body<4>(a, it.btab4, it.bcidx, bx);
         }
     }
     if constexpr ((FAM & 8) != 0 || ((FAM & 2) != 0 && !RAY)) {
@@ -1924,7 +2138,8 @@ __device__ __forceinline__ void fast_body(const Item& it, unsigned bx, unsigned 
 // absorption, 4 adjoint, 8 the other backprojections (generic with occlusion
 // or per-ray absorption, fast with per-ray absorption), 16 the generic forward
 // with occlusion or per-ray absorption, 32 / 64 the generic forward /
-// backprojection without either; a batch launches one instance per family
+// backprojection without either, 256 the block-table backprojection (511: all
+// bodies, for calls of mixed families); a batch launches one instance per family
 // present, so no body is compiled around the registers of rarer ones and each
 // keeps about its direct kernel's occupancy.
 template <int FAM>
@@ -2055,6 +2270,9 @@ int launch_item(const Item& it, cudaStream_t st, const char* name) {
         const dim3 block(kWarpsPerBlock * kWarp);
         if (it.vz == 8) k_adjoint_table<8><<<grid, block, 0, st>>>(it.a, it.table);
         else k_adjoint_table<4><<<grid, block, 0, st>>>(it.a, it.table);
+    } else if (it.kind == KB_BTABLE) {
+        if (it.vz == 8) k_backward_blk<8, 2><<<grid, dim3(kWarpsPerBlock * kWarp), 0, st>>>(it.a, it.btab4, it.bcidx);
+        else k_backward_blk<4, 3><<<grid, dim3(kWarpsPerBlock * kWarp), 0, st>>>(it.a, it.btab4, it.bcidx);
     } else if (it.kind == KB_TABLE) {
         if (it.a.nZ % 256 == 0) k_backward_tab8<true><<<grid, dim3(kWarpsPerBlock * kWarp), 0, st>>>(it.a, it.btab, it.bcidx, it.bpad);
         else k_backward_tab8<false><<<grid, dim3(kWarpsPerBlock * kWarp), 0, st>>>(it.a, it.btab, it.bcidx, it.bpad);
@@ -2124,9 +2342,10 @@ static_assert(sizeof(BatchParams) < 32000, "batch parameters must fit the 32 KB 
 // lean generic backprojection fits 40 registers (six CTAs, as its direct
 // kernel: a 160^3 x 720 call ran 1.36x longer at four), the fast and 2-D
 // backprojections and the 2-D forward 48 (five), the fast forward and the
-// lean generic forward 64 (four); the heavy instances keep 80.
+// lean generic forward 64 (four); the heavy instances keep 80, the block-table
+// backprojection 128 (two, as its eight-slice direct kernel).
 template <int FAM>
-__global__ void __launch_bounds__(256, FAM == 64 ? 6 : (FAM == 2 || FAM == 128 ? 5 : (FAM == 1 || FAM == 32 ? 4 : 3)))
+__global__ void __launch_bounds__(256, FAM == 64 ? 6 : (FAM == 2 || FAM == 128 ? 5 : (FAM == 1 || FAM == 32 ? 4 : (FAM == 256 ? 2 : 3))))
     k_batch(const __grid_constant__ BatchParams P) {
     __shared__ unsigned s_t[2];
     __shared__ int s_idx[2];
@@ -2169,7 +2388,8 @@ BatchKernel batch_kernel(int fam) {
         case 32: return k_batch<32>;
         case 64: return k_batch<64>;
         case 128: return k_batch<128>;
-        default: return k_batch<255>;
+        case 256: return k_batch<256>;
+        default: return k_batch<511>;
     }
 }
 
@@ -2305,6 +2525,8 @@ extern "C" int vam_parallel_plan_destroy(vam_parallel_plan* p) {
     cudaFree(p->d_bwd_cidx);
     cudaFree(p->d_status);
     cudaFree(p->d_img_pad);
+    cudaFree(p->d_bwd_btab);
+    cudaFree(p->d_bwd_bcidx);
     delete p;
     return VAM_OK;
 }
@@ -2501,23 +2723,56 @@ extern "C" int vam_parallel_prepare_backward(vam_parallel_plan* p, vam_stream_t 
     }
     const int npc = (int)plist.size();
     const int pad = (p->nA + 1) & ~1;
+    // nZ % 128 == 0: the 2 x 2 block table (k_backward_blk); otherwise the per-pixel table (k_backward_tab8)
+    const bool blocks = p->nZ % 128 == 0;
     cudaStream_t st = (cudaStream_t)stream;
     if (!p->d_bwd_cidx) VAM_TRY_CUDA(cudaMalloc(&p->d_bwd_cidx, sizeof(int) * n));
-    if (!p->d_bwd_table) VAM_TRY_CUDA(cudaMalloc(&p->d_bwd_table, sizeof(int2) * (size_t)std::max(npc, 1) * pad));
+    if (!blocks && !p->d_bwd_table)
+        VAM_TRY_CUDA(cudaMalloc(&p->d_bwd_table, sizeof(int2) * (size_t)std::max(npc, 1) * pad));
     int* d_plist = nullptr;
     VAM_TRY_CUDA(cudaMalloc(&d_plist, sizeof(int) * std::max(npc, 1)));
     cudaError_t e = cudaMemcpyAsync(p->d_bwd_cidx, cidx.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess && npc)
+    if (e == cudaSuccess && npc && !blocks)
         e = cudaMemcpyAsync(d_plist, plist.data(), sizeof(int) * npc, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess && npc) {
+    if (e == cudaSuccess && npc && !blocks) {
         const long tot = (long)npc * pad;
         k_bwd_table<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(p->d_trig, d_plist, p->d_bwd_table, npc, p->nA, pad,
                                                                    p->nY, p->nX, p->nZ, p->C);
         e = cudaGetLastError();
     }
-    // the host vectors and the pixel list are released after the copies and the build complete
+    // 2 x 2 blocks with at least one pixel inside the circle, for the block-table kernel
+    const int nbx = (p->nX + 1) / 2, nby = (p->nY + 1) / 2;
+    std::vector<int> bcidx((size_t)nbx * nby, -1), blist;
+    for (int bi = 0; bi < nby; ++bi)
+        for (int bj = 0; bj < nbx; ++bj) {
+            bool any = false;
+            for (int q = 0; q < 4; ++q) {
+                const int i = 2 * bi + (q >> 1), j = 2 * bj + (q & 1);
+                any |= i < p->nY && j < p->nX && cidx[(size_t)i * p->nX + j] >= 0;
+            }
+            if (any) { bcidx[(size_t)bi * nbx + bj] = (int)blist.size(); blist.push_back(bi * nbx + bj); }
+        }
+    const int nbc = (int)blist.size();
+    int* d_blist = nullptr;
+    if (e == cudaSuccess && blocks && nbc) {
+        if (!p->d_bwd_bcidx) e = cudaMalloc(&p->d_bwd_bcidx, sizeof(int) * bcidx.size());
+        if (e == cudaSuccess && !p->d_bwd_btab) e = cudaMalloc(&p->d_bwd_btab, sizeof(int4) * 2 * (size_t)nbc * p->nA);
+        if (e == cudaSuccess) e = cudaMalloc(&d_blist, sizeof(int) * nbc);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(p->d_bwd_bcidx, bcidx.data(), sizeof(int) * bcidx.size(), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(d_blist, blist.data(), sizeof(int) * nbc, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) {
+            const long tot = (long)nbc * p->nA;
+            k_bwd_btable<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(p->d_trig, d_blist, p->d_bwd_cidx,
+                                                                        p->d_bwd_btab, nbc, p->nA, p->nY, p->nX,
+                                                                        p->nZ, p->C);
+            e = cudaGetLastError();
+        }
+    }
+    // the host vectors and the pixel / block lists are released after the copies and the build complete
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     cudaFree(d_plist);
+    cudaFree(d_blist);
     if (e != cudaSuccess)
         return set_error(VAM_ERR_CUDA, std::string("vam_parallel_prepare_backward: ") + cudaGetErrorString(e));
     p->bwd_table_pad = pad;
@@ -2576,7 +2831,7 @@ struct vam_batch {
     int device;
     unsigned* d_counter;
     int sms;
-    int per_sm[256][4];        // resident CTAs per SM of k_batch<fam> (fam 1 .. 128, 255) per
+    int per_sm[512][4];        // resident CTAs per SM of k_batch<fam> (fam 1 .. 256, 511) per
                                // dynamic shared-memory bucket (kSmemBuckets)
     std::vector<Item> host;    // the described calls of the last list, in queue order
     std::vector<int> group;    // first call of each launch (kBatchMaxItems calls per launch)
@@ -2610,12 +2865,12 @@ extern "C" int vam_batch_create(int32_t device, vam_batch** out) {
     VAM_REQUIRE(g.ok, VAM_ERR_CUDA, "vam_batch_create: cannot select device");
     int sms = 0;
     VAM_TRY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-    int per_sm[256][4] = {};
+    int per_sm[512][4] = {};
     // residency for each dynamic shared-memory bucket up to the largest a call may ask for (48 KB,
     // the batched backprojection's trig table), queried once here, so a list never needs a
     // runtime query (which would not be allowed during graph capture); the opt-in limit is
     // raised first, as 48 KB plus the kernel's static shared memory exceeds the default
-    for (int fam : {1, 2, 4, 8, 16, 32, 64, 128, 255}) {
+    for (int fam : {1, 2, 4, 8, 16, 32, 64, 128, 256, 511}) {
         VAM_TRY_CUDA(cudaFuncSetAttribute(batch_kernel(fam), cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
         for (int k = 0; k < 4; ++k) {
             VAM_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[fam][k], batch_kernel(fam),
@@ -2672,6 +2927,7 @@ double time_weight(const Item& it) {
         case KF_GEN: return slice ? 27.0 : 4.0;
         case KB_BATCHED: case KB_FAST: return 1.2;
         case KB_TABLE: return 1.05;
+        case KB_BTABLE: return 0.7;
         case KB_GEN: return slice ? 10.0 : 2.0;
         case KA_TABLE: return 1.5;
         case KA_FAST: return 3.5;
@@ -2691,7 +2947,7 @@ int batch_prepare(vam_batch* b, const vam_work* work, int32_t n) {
         VAM_REQUIRE(w.plan->device == b->device, VAM_ERR_ARG, "vam_batch: plan on another device than the batch");
         VAM_REQUIRE(w.op >= VAM_OP_FORWARD && w.op <= VAM_OP_ADJOINT, VAM_ERR_ARG, "vam_batch: unknown op");
         const Op op = w.op == VAM_OP_FORWARD ? Op::Forward : (w.op == VAM_OP_BACKWARD_REF ? Op::BackwardRef : Op::Adjoint);
-        const int rc = describe(w.plan, op, w.in, w.out, items[i], "vam_batch");
+        const int rc = describe(w.plan, op, w.in, w.out, items[i], "vam_batch", false, true);
         if (rc != VAM_OK) return rc;
         const Item& d = items[i];
         // generic bodies with occlusion or per-ray absorption, and per-ray fast backprojections, go
@@ -2702,7 +2958,8 @@ int batch_prepare(vam_batch* b, const vam_work* work, int32_t n) {
         if (d.kind == KF_GEN) items[i].family = gen_heavy ? 16 : 32;
         // the 2-D forward instance carries the TMA-staged body only; plain staging (no tensor map
         // encoder) runs in the all-bodies instance
-        if (d.kind == KF_2D && !d.tma) items[i].family = 255;
+        if (d.kind == KF_2D && !d.tma) items[i].family = 511;
+        if (d.kind == KB_BTABLE) items[i].family = 256;
 
         VAM_REQUIRE((long long)items[i].gx * items[i].gy < (1LL << 31), VAM_ERR_SHAPE, "vam_batch: call grid too large");
         items[i].cost = (long long)std::llround((double)items[i].cost * time_weight(items[i]));
@@ -2737,7 +2994,7 @@ int batch_prepare(vam_batch* b, const vam_work* work, int32_t n) {
             b->any_pre |= items[i].pre_in != nullptr;
         }
         b->smem = std::max(b->smem, gsmem);
-        if (fam & (fam - 1)) fam = 255;  // one family per launch; the all-bodies instance otherwise
+        if (fam & (fam - 1)) fam = 511;  // one family per launch; the all-bodies instance otherwise
         // tickets: one per block of each call's grid, the calls one after another
         long long total = 0;
         for (int i = g0; i < g1; ++i) {

@@ -82,6 +82,8 @@ struct vam_parallel_plan {
     int2* d_tasks_single;   // (a, -1) for every angle
     float* d_vol_scratch;   // [nY][nX][nZ] masked copy of the input (VAM_ABS_MASK)
     int* d_status;          // error bits the kernels record (VAM_STATUS_*), read by vam_parallel_status
+    int4* d_bwd_btab;       // [blocks inside][nA][2] 2 x 2 block bin table (k_bwd_btable)
+    int* d_bwd_bcidx;       // [(nY + 1) / 2][(nX + 1) / 2] compact block index, -1 outside the circle
     float* d_img_pad;       // nZ == 1: [nY][nX rounded up to 4] staged image of the TMA-tiled 2-D forward
     // matched-transpose weights: per pixel and angle, the first of <= 3
     // detector rows (as int bits) and their summed forward tap weights
