@@ -999,6 +999,8 @@ __global__ void __launch_bounds__(256) k_bwd_btable(const double4* __restrict__ 
     tab[2 * idx + 1] = make_int4(__float_as_int(ws[2]), __float_as_int(ws[3]), 0, 0);
 }
 
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
 template <int VZ>
 struct RowV {
     float4 v[VZ / 4];
@@ -1028,11 +1030,16 @@ __device__ __forceinline__ void lerp_rows(unsigned long long (&acc)[VZ / 2], flo
 }
 
 // one warp per (2 x 2 block, z chunk of 32 VZ slices); nZ a multiple of 32 VZ.  The table entries
-// arrive 32 angles at a time (lane l holds angle k0 + l's 32 bytes, one coalesced 1 KB load per warp,
-// the next 32 in flight) and are broadcast with shuffles, so no angle waits for its entry.
+// arrive 32 angles at a time (lane l fetches angle k0 + l's 32 bytes, the next chunk in flight while
+// this one is read), so no angle waits for its entry: eight slices per lane by cp.async into the warp's
+// two shared-memory slots (no registers held: the body fits 80 registers, three CTAs per SM; 1.19 ->
+// 0.92 ms at 256^3 x 360 against entries in registers at two CTAs), four slices in registers,
+// broadcast by shuffles (0.21 -> 0.17 ms at 128^3 x 360 against the shared-memory slots).
+constexpr int kBlkEnt = 64;  // int4 per slot: 32 angles x 32 bytes
 template <int VZ>
 __device__ __forceinline__ void k_backward_blk_body(const Args& a, const int4* __restrict__ tab,
                                                     const int* __restrict__ bcidx, unsigned bx) {
+    __shared__ __align__(16) int4 s_ent[VZ == 8 ? kWarpsPerBlock : 1][2][kBlkEnt];
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
     // a CTA: 4 x 2 blocks (8 x 4 pixels, one block per warp) of one z chunk, so the warps of a CTA
     // read overlapping detector rows for the same angle at about the same time
@@ -1055,49 +1062,92 @@ __device__ __forceinline__ void k_backward_blk_body(const Args& a, const int4* _
         const float* __restrict__ bz = a.in + z0;
         const int4* __restrict__ e = tab + (size_t)pc * a.nA * 2;
         const int nA = a.nA;
-        auto chunk = [&](int k0, int4& h0, int4& h1) {
-            const int k = k0 + lane;
-            if (k < nA) { h0 = __ldcs(e + 2 * k); h1 = __ldcs(e + 2 * k + 1); }
-            else { h0 = make_int4(-1, 0, 0, 0); h1 = make_int4(0, 0, 0, 0); }
-        };
-        int4 h0, h1, g0, g1;
-        chunk(0, h0, h1);
-        chunk(32, g0, g1);
-#pragma unroll 1
-        for (int k0 = 0; k0 < nA; k0 += 32) {
-            const int kn = min(32, nA - k0);
-#pragma unroll 1
-            for (int l = 0; l < kn; ++l) {
-                const int off = __shfl_sync(0xffffffffu, h0.x, l);
-                if (off < 0) continue;  // uniform: every lane read lane l's entry
-                const int code = __shfl_sync(0xffffffffu, h0.y, l);
-                const float w[4] = {__int_as_float(__shfl_sync(0xffffffffu, h0.z, l)),
-                                    __int_as_float(__shfl_sync(0xffffffffu, h0.w, l)),
-                                    __int_as_float(__shfl_sync(0xffffffffu, h1.x, l)),
-                                    __int_as_float(__shfl_sync(0xffffffffu, h1.y, l))};
-                const float* pr = bz + off;
-                const int span = code & 3;
-                RowV<VZ> ra, rb, rc;
-                load_row<VZ>(ra, pr);
-                load_row<VZ>(rb, pr + rs);
-                if (span >= 1) load_row<VZ>(rc, pr + 2 * rs);
+        // one angle's rows and FMAs from its entry (e0: row offset, code, w0, w1; e1: w2, w3)
+        auto angle = [&](const int4& e0, const int4& e1) {
+            const int code = e0.y;
+            const float w[4] = {__int_as_float(e0.z), __int_as_float(e0.w), __int_as_float(e1.x),
+                                __int_as_float(e1.y)};
+            const float* pr = bz + e0.x;
+            const int span = code & 3;
+            RowV<VZ> ra, rb, rc;
+            load_row<VZ>(ra, pr);
+            load_row<VZ>(rb, pr + rs);
+            if (span >= 1) load_row<VZ>(rc, pr + 2 * rs);
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (((code >> (2 + 3 * q)) & 7) == 1) lerp_rows<VZ>(acc[q], w[q], ra, rb);
+            if (span >= 1) {
 #pragma unroll
                 for (int q = 0; q < 4; ++q)
-                    if (((code >> (2 + 3 * q)) & 7) == 1) lerp_rows<VZ>(acc[q], w[q], ra, rb);
-                if (span >= 1) {
+                    if (((code >> (2 + 3 * q)) & 7) == 3) lerp_rows<VZ>(acc[q], w[q], rb, rc);
+                if (span == 2) {
+                    load_row<VZ>(ra, pr + 3 * rs);
 #pragma unroll
                     for (int q = 0; q < 4; ++q)
-                        if (((code >> (2 + 3 * q)) & 7) == 3) lerp_rows<VZ>(acc[q], w[q], rb, rc);
-                    if (span == 2) {
-                        load_row<VZ>(ra, pr + 3 * rs);
-#pragma unroll
-                        for (int q = 0; q < 4; ++q)
-                            if (((code >> (2 + 3 * q)) & 7) == 5) lerp_rows<VZ>(acc[q], w[q], rc, ra);
-                    }
+                        if (((code >> (2 + 3 * q)) & 7) == 5) lerp_rows<VZ>(acc[q], w[q], rc, ra);
                 }
             }
-            h0 = g0; h1 = g1;
-            if (k0 + 64 < nA) chunk(k0 + 64, g0, g1);
+        };
+        if constexpr (VZ == 8) {
+            // entries by cp.async into the warp's two shared-memory slots: no registers held for them,
+            // which lets the eight-slice body fit 80 registers (three CTAs per SM)
+            int4* slot = &s_ent[wp][0][0];
+            // chunk of angles k0 .. k0 + 31 into slot sl (one commit group per chunk, empty past the end)
+            auto fetch = [&](int k0, int sl) {
+                const int k = k0 + lane;
+                int4* d = slot + sl * kBlkEnt + 2 * lane;
+                if (k < nA) {
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(d)), "l"(e + 2 * k)
+                                 : "memory");
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(d + 1)),
+                                 "l"(e + 2 * k + 1) : "memory");
+                }
+                asm volatile("cp.async.commit_group;" ::: "memory");
+            };
+            fetch(0, 0);
+            fetch(32, 1);
+#pragma unroll 1
+            for (int k0 = 0, sl = 0; k0 < nA; k0 += 32, sl ^= 1) {
+                const int kn = min(32, nA - k0);
+                asm volatile("cp.async.wait_group 1;" ::: "memory");  // this chunk's copies (the next may fly)
+                __syncwarp();
+                const int4* es = slot + sl * kBlkEnt;
+#pragma unroll 1
+                for (int l = 0; l < kn; ++l) {
+                    const int4 e0 = es[2 * l];
+                    if (e0.x < 0) continue;  // uniform: every lane read the same entry
+                    angle(e0, es[2 * l + 1]);
+                }
+                __syncwarp();  // every lane read the slot before it is refilled
+                fetch(k0 + 64, sl);
+            }
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+            __syncwarp();
+        } else {
+            // entries in registers (lane l: angle k0 + l, the next chunk in flight), broadcast by shuffles
+            auto chunk = [&](int k0, int4& h0, int4& h1) {
+                const int k = k0 + lane;
+                if (k < nA) { h0 = __ldcs(e + 2 * k); h1 = __ldcs(e + 2 * k + 1); }
+                else { h0 = make_int4(-1, 0, 0, 0); h1 = make_int4(0, 0, 0, 0); }
+            };
+            int4 h0, h1, g0, g1;
+            chunk(0, h0, h1);
+            chunk(32, g0, g1);
+#pragma unroll 1
+            for (int k0 = 0; k0 < nA; k0 += 32) {
+                const int kn = min(32, nA - k0);
+#pragma unroll 1
+                for (int l = 0; l < kn; ++l) {
+                    const int off = __shfl_sync(0xffffffffu, h0.x, l);
+                    if (off < 0) continue;  // uniform: every lane read lane l's entry
+                    const int4 e0 = make_int4(off, __shfl_sync(0xffffffffu, h0.y, l), __shfl_sync(0xffffffffu, h0.z, l),
+                                              __shfl_sync(0xffffffffu, h0.w, l));
+                    const int4 e1 = make_int4(__shfl_sync(0xffffffffu, h1.x, l), __shfl_sync(0xffffffffu, h1.y, l), 0, 0);
+                    angle(e0, e1);
+                }
+                h0 = g0; h1 = g1;
+                if (k0 + 64 < nA) chunk(k0 + 64, g0, g1);
+            }
         }
     }
 #pragma unroll
@@ -1265,7 +1315,6 @@ constexpr long kTmaWaitLimit = 1L << 24;  // try_wait polls before a block gives
 // and the mbarrier
 constexpr int k2SmemTma = 128 + kTmaH * kTmaW * 4 + 4 * k2J * 4 + 16;
 
-__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
     unsigned done = 0;
@@ -2271,7 +2320,7 @@ int launch_item(const Item& it, cudaStream_t st, const char* name) {
         if (it.vz == 8) k_adjoint_table<8><<<grid, block, 0, st>>>(it.a, it.table);
         else k_adjoint_table<4><<<grid, block, 0, st>>>(it.a, it.table);
     } else if (it.kind == KB_BTABLE) {
-        if (it.vz == 8) k_backward_blk<8, 2><<<grid, dim3(kWarpsPerBlock * kWarp), 0, st>>>(it.a, it.btab4, it.bcidx);
+        if (it.vz == 8) k_backward_blk<8, 3><<<grid, dim3(kWarpsPerBlock * kWarp), 0, st>>>(it.a, it.btab4, it.bcidx);
         else k_backward_blk<4, 3><<<grid, dim3(kWarpsPerBlock * kWarp), 0, st>>>(it.a, it.btab4, it.bcidx);
     } else if (it.kind == KB_TABLE) {
         if (it.a.nZ % 256 == 0) k_backward_tab8<true><<<grid, dim3(kWarpsPerBlock * kWarp), 0, st>>>(it.a, it.btab, it.bcidx, it.bpad);
@@ -2342,10 +2391,10 @@ static_assert(sizeof(BatchParams) < 32000, "batch parameters must fit the 32 KB 
 // lean generic backprojection fits 40 registers (six CTAs, as its direct
 // kernel: a 160^3 x 720 call ran 1.36x longer at four), the fast and 2-D
 // backprojections and the 2-D forward 48 (five), the fast forward and the
-// lean generic forward 64 (four); the heavy instances keep 80, the block-table
-// backprojection 128 (two, as its eight-slice direct kernel).
+// lean generic forward 64 (four); the heavy instances and the block-table
+// backprojection keep 80 (three).
 template <int FAM>
-__global__ void __launch_bounds__(256, FAM == 64 ? 6 : (FAM == 2 || FAM == 128 ? 5 : (FAM == 1 || FAM == 32 ? 4 : (FAM == 256 ? 2 : 3))))
+__global__ void __launch_bounds__(256, FAM == 64 ? 6 : (FAM == 2 || FAM == 128 ? 5 : (FAM == 1 || FAM == 32 ? 4 : 3)))
     k_batch(const __grid_constant__ BatchParams P) {
     __shared__ unsigned s_t[2];
     __shared__ int s_idx[2];
