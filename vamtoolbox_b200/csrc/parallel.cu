@@ -98,6 +98,16 @@ __device__ __forceinline__ void store_vec(float* p, const float (&d)[VZ]) {
 }
 
 // Per-sample absorption factor of the RAY mode: exp(-a * max(0, s - s_entry)).
+__device__ __forceinline__ unsigned long long pk_pair(float lo, float hi) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+
+__device__ __forceinline__ void fma_pair(unsigned long long& acc, unsigned long long w2, float a, float b) {
+    asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc) : "l"(w2), "l"(pk_pair(a, b)));
+}
+
 __device__ __forceinline__ float ray_factor(float s, float s_entry, float alpha) {
     float d = s - s_entry;
     return d > 0.f ? expf(-alpha * d) : 1.f;
@@ -846,15 +856,6 @@ __global__ void __launch_bounds__(256) k_bwd_table(const double4* __restrict__ t
     else tab[idx] = make_int2(j0 * rs + th * nZ, __float_as_int((float)(t - ft)));
 }
 
-__device__ __forceinline__ unsigned long long pk_pair(float lo, float hi) {
-    unsigned long long r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
-    return r;
-}
-
-__device__ __forceinline__ void fma_pair(unsigned long long& acc, unsigned long long w2, float a, float b) {
-    asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc) : "l"(w2), "l"(pk_pair(a, b)));
-}
 
 // acc (slice pairs) += w0 * row r0 + w1 * row r1, eight slices per lane (q1: the lane's second vector)
 __device__ __forceinline__ void tab_rows(unsigned long long (&acc)[4], const float* __restrict__ p0, int rs, float w,
