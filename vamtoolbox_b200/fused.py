@@ -9,6 +9,7 @@ from __future__ import annotations
 
 import ctypes
 
+import numpy as np
 import torch
 
 from . import _lib
@@ -164,6 +165,38 @@ def to_host_f64(*tensors):
         outs.append(h)
     torch.cuda.current_stream(tensors[0].device).synchronize()
     return [h.numpy() for h in outs]
+
+
+_COPY_POOL = None
+
+
+def _copy_pool():
+    global _COPY_POOL
+    if _COPY_POOL is None:
+        import concurrent.futures
+        import os
+
+        _COPY_POOL = concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1)))
+    return _COPY_POOL
+
+
+def to_device_f64(array, device):
+    """A host array as a float64 device tensor, staged through a page-locked buffer of torch's caching
+    host allocator that several threads fill in slices (numpy releases the GIL for plain copies), then one
+    asynchronous copy on the current stream.  A pageable upload of a 256^3 float64 target ran at about
+    10 GB/s (13 ms); the allocator keeps the staging block alive until the copy has run."""
+    a = np.ascontiguousarray(array, dtype=np.float64)
+    if a.nbytes < (8 << 20):
+        return torch.as_tensor(a).to(device)
+    h = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+    dst, src = h.numpy().reshape(-1), a.reshape(-1)
+    pool = _copy_pool()
+    step = -(-src.size // pool._max_workers)
+    spans = [(lo, min(lo + step, src.size)) for lo in range(0, src.size, step)]
+    list(pool.map(lambda sp: np.copyto(dst[sp[0]:sp[1]], src[sp[0]:sp[1]]), spans))
+    d = torch.empty(a.shape, dtype=torch.float64, device=device)
+    d.copy_(h, non_blocking=True)
+    return d
 
 
 def graph_kernel_nodes(graph):

@@ -26,7 +26,7 @@ import numpy as np
 import torch
 
 from .. import geometry
-from ..fused import Workspace, bclp_params, capture, to_host_f64
+from ..fused import Workspace, bclp_params, capture, to_device_f64, to_host_f64
 from ..projectorconstructor import projectorconstructor
 from ..util import data as udata
 
@@ -129,7 +129,7 @@ class BCLPNorm:
         on the device, and g0 is filtered, scaled and clipped into a float32 device tensor (no host
         round trip of the 3-D arrays)."""
         dev = self.P.device
-        tgt = torch.as_tensor(np.ascontiguousarray(self.target_geo.array, dtype=np.float64)).to(dev)
+        tgt = to_device_f64(self.target_geo.array, dev)
         if self.response_model.checkResponseTarget_t(tgt) is False:
             warnings.warn("Target is either out of range of response function over non-negative real dose input, "
                           "or contains inf/nan.")

@@ -14,7 +14,7 @@ import numpy as np
 import torch
 
 from .. import geometry, metrics
-from ..fused import Workspace, capture, to_host_f64
+from ..fused import Workspace, capture, to_device_f64, to_host_f64
 from ..projectorconstructor import projectorconstructor
 from ..util import data as udata
 
@@ -82,7 +82,7 @@ class OSMODevice:
         self.err_log = torch.full((max(n_iter, 1),), float("nan"), dtype=torch.float32, device=dev)
         self.counter = torch.zeros(1, dtype=torch.int32, device=dev)
         self.ver, self.xmax, self.bmax = ws.scalar(), ws.scalar(), ws.scalar()
-        tgt = torch.as_tensor(np.ascontiguousarray(target_geo.array, dtype=np.float64), device=dev)
+        tgt = to_device_f64(target_geo.array, dev)
         self.xm = udata.filterTargetOSMO_t(tgt, options.filter).to(torch.float32).reshape(vs).contiguous()
         self.b = plan.forward(self.xm).clamp_(min=0)
         self.x = plan.backward_ref(self.b)
