@@ -1094,14 +1094,18 @@ __device__ __forceinline__ void k_backward_blk_body(const Args& a, const int4* _
             // which lets the eight-slice body fit 80 registers (three CTAs per SM)
             int4* slot = &s_ent[wp][0][0];
             // chunk of angles k0 .. k0 + 31 into slot sl (one commit group per chunk, empty past the end)
+            // the table is read once: evict-first in L2, so it does not push out sinogram lines that other
+            // CTAs read again (DRAM 477 -> 459 MB per 256^3 x 360 launch, 0.934 -> 0.922 ms)
+            unsigned long long pol;
+            asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
             auto fetch = [&](int k0, int sl) {
                 const int k = k0 + lane;
                 int4* d = slot + sl * kBlkEnt + 2 * lane;
                 if (k < nA) {
-                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(d)), "l"(e + 2 * k)
-                                 : "memory");
-                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(d + 1)),
-                                 "l"(e + 2 * k + 1) : "memory");
+                    asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(smem_addr(d)),
+                                 "l"(e + 2 * k), "l"(pol) : "memory");
+                    asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(smem_addr(d + 1)),
+                                 "l"(e + 2 * k + 1), "l"(pol) : "memory");
                 }
                 asm volatile("cp.async.commit_group;" ::: "memory");
             };
@@ -1165,7 +1169,12 @@ __device__ __forceinline__ void k_backward_blk_body(const Args& a, const int4* _
 #pragma unroll
             for (int e2 = 0; e2 < VZ; ++e2) v[e2] = m * v[e2];
         }
-        store_vz<VZ>(a.out + (size_t)p * a.nZ + z0, v, VZ / 4);
+        // streaming stores: the volume is not read again by this launch (0.924 -> 0.916 ms, DRAM reads
+        // 399 -> 390 MB per 256^3 x 360 launch)
+#pragma unroll
+        for (int q2 = 0; q2 < VZ / 4; ++q2)
+            __stcs(reinterpret_cast<float4*>(a.out + (size_t)p * a.nZ + z0 + 128 * q2),
+                   make_float4(v[4 * q2], v[4 * q2 + 1], v[4 * q2 + 2], v[4 * q2 + 3]));
     }
 }
 
