@@ -115,13 +115,16 @@ enum vam_status_bits {
  * its calls. */
 int vam_parallel_status(vam_parallel_plan* plan, int32_t* status);
 
-/* Builds the plan's backprojection bin table: for every pixel inside the clip
- * circle and every angle, np.interp's bin of t = x cos - y sin (float64, the
- * reference's expression) as a row offset and its float32 weight, 8 bytes per
- * pixel and angle (147 MB at 256^3 x 360).  Later eight-slice backprojections
- * read the table instead of evaluating the float64 bins (identical results).
+/* Builds the plan's backprojection bin table: for every 2 x 2 block of pixels
+ * with a pixel inside the clip circle and every angle, np.interp's bin of
+ * t = x cos - y sin (float64, the reference's expression) of each of the four
+ * pixels as the offset of the block's least bin row, a code of the pixels' bin
+ * offsets and their float32 weights, 32 bytes per block and angle (148.5 MB at
+ * 256^3 x 360).  Later backprojections (nZ % 4 == 0, no per-ray absorption)
+ * read the table and share each block's at most four detector rows among its
+ * pixels instead of evaluating the float64 bins (identical results).
  * Allocates: call before any stream capture.  VAM_ERR_NOTSUP when the plan's
- * sinogram has 2^31 elements or more. */
+ * sinogram has 2^31 elements or more, or nZ % 4 != 0. */
 int vam_parallel_prepare_backward(vam_parallel_plan* plan, vam_stream_t stream);
 
 /* R1 forward: rotate-and-sum Radon transform with bilinear sampling, zero
@@ -162,8 +165,9 @@ typedef struct {
     int32_t forward_vz, backward_vz, adjoint_vz;
     int32_t backward_batch;
     int32_t adjoint_table;
-    int32_t backward_table;  /* 1: the eight-slice backprojection reads its bins from the plan's table
-                                (vam_parallel_prepare_backward) when it is built; 0: computes them */
+    int32_t backward_table;  /* 1: the backprojection reads its bins from the plan's table
+                                (vam_parallel_prepare_backward) when it is built, with backward_vz 4
+                                or 8 slices per lane (0: 8 from 160 slices up); 0: computes them */
     int32_t forward_tma;     /* 1: the 2-D tile forward stages its boxes with TMA tensor copies (an image
                                 whose rows are not 16-byte multiples, or in mask mode, is first copied
                                 into the plan's padded image); 0: with plain loads.  Bit-identical. */

@@ -444,12 +444,12 @@ def test_tma_staged_slice_forward_matches_plain_loads_and_oracle(ny, nx, na, mod
 
 @pytest.mark.parametrize("shape,na,mode", [((64, 64, 256), 90, None), ((63, 63, 128), 47, "mask"),
                                            ((40, 40, 512), 33, None), ((34, 34, 64), 40, None),
-                                           ((37, 37, 200), 25, "mask")])
+                                           ((37, 37, 200), 25, "mask"), ((30, 30, 12), 19, None)])
 def test_backprojection_table_bitwise_and_oracle(shape, na, mode):
-    """The backprojection from the plan's bin table (2 x 2 block table for nZ % 128 == 0: eight slices per
-    lane when nZ % 256 == 0, else four; the per-pixel table otherwise) gives the computed-bin kernel's sums
-    bit for bit, and the oracle's within float32 tolerance: odd widths (partial blocks and tiles), several
-    z chunks, angle counts that are not multiples of 32 (partial entry chunks), mask absorption."""
+    """The backprojection from the plan's 2 x 2 block bin table, with four and with eight slices per lane,
+    gives the computed-bin kernel's sums bit for bit, and the oracle's within float32 tolerance: odd widths
+    (partial blocks and tiles), several z chunks and partial ones (nZ not a multiple of 128 or 256), angle
+    counts that are not multiples of 32 (partial entry chunks), mask absorption."""
     rng = np.random.default_rng(sum(shape) + na)
     ang = np.linspace(0, 360, na, endpoint=False) + 0.7
     p = plan_for(shape, ang)
@@ -462,7 +462,9 @@ def test_backprojection_table_bitwise_and_oracle(shape, na, mode):
     p.set_tuning({"backward_vz": 8, "backward_table": 0})
     computed = p.backward_ref(dev(b))
     assert p.prepare_backward()
-    p.set_tuning({"backward_table": 1})
-    tabled = p.backward_ref(dev(b))
-    assert torch.equal(computed, tabled)
+    for vz in (4, 8):
+        p.set_tuning({"backward_table": 1, "backward_vz": vz})
+        tabled = p.backward_ref(dev(b))
+        assert torch.equal(computed, tabled), vz
     assert relL2(tabled.cpu().numpy(), O.parallel_backward_ref(b, ang, absorption=oabs)) < TOL
+    assert p.status() == 0

@@ -23,8 +23,8 @@ from . import _lib
 
 # slices per lane: 1 = the generic kernel, 4 / 8 = the fast kernels (nZ % 4 == 0)
 FORWARD_VZ = (1, 4, 8)
-# (slices per lane, angles per batch, bin table): the table serves eight slices per lane
-BACKWARD = ((1, 1, 0), (4, 1, 0), (8, 1, 0), (4, 2, 0), (8, 2, 0), (4, 4, 0), (8, 2, 1))
+# (slices per lane, angles per batch, bin table): the block table serves four or eight slices per lane
+BACKWARD = ((1, 1, 0), (4, 1, 0), (8, 1, 0), (4, 2, 0), (8, 2, 0), (4, 4, 0), (4, 2, 1), (8, 2, 1))
 ADJOINT = ((1, 0), (4, 1), (8, 1), (4, 0), (8, 0))           # (slices per lane, weight table on)
 
 _lock = threading.Lock()

@@ -820,137 +820,30 @@ __global__ void __launch_bounds__(256, 6) k_backward_batched8(Args a) {
 }
 
 // ---------------------------------------------------------------------------
-// R2 backprojection from the plan's bin table.
+// R2 backprojection from the plan's bin table: 2 x 2 pixel blocks share their
+// detector rows.
 //
-// k_bwd_table evaluates, once per plan, for every pixel inside the clip circle
-// and every angle the same float64 t = x cos - y sin, floor and float32 weight
-// as the batched kernel, stored as (j0 * nA * nZ + angle * nZ, weight bits),
-// or (-1, 0) where t falls outside the detector (np.interp left = right = 0:
-// no contribution).  At the detector's last bin (t == xp[-1], weight 0) the
-// entry is (row nY - 2, weight 1), which adds the same single row with the
-// same rounding.  k_backward_tab8 then runs, per pixel and z chunk, one table
-// entry per angle (streamed: the table is read once per call), two 16-byte
-// loads per detector row and packed f32x2 FMAs (two fmaf roundings each), so
-// its sums are bit-identical to k_backward_batched8's for finite data.  One
-// angle per step with the next entry prefetched, 48 registers, five CTAs per
-// SM: 1.52 -> 1.32 ms at 256^3 x 360 (A/B in one process; two angles in flight
-// at 64 registers 1.43 ms, a six- or eight-CTA register cap 1.41 / 1.44 ms).
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_bwd_table(const double4* __restrict__ trig, const int* __restrict__ plist,
-                                                   int2* __restrict__ tab, int npc, int nA, int nA_pad, int nY,
-                                                   int nX, int nZ, int C) {
-    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;  // over (in-circle pixel, angle), angle fastest
-    if (idx >= (long)npc * nA_pad) return;
-    const int th = (int)(idx % nA_pad);
-    const int pc = (int)(idx / nA_pad);
-    if (th >= nA) { tab[idx] = make_int2(-1, 0); return; }
-    const int p = plist[pc];
-    const double X = (double)(p % nX - C), Y = (double)(p / nX - C);
-    const double4 tr = trig[th];
-    const double t = __dsub_rn(__dmul_rn(X, tr.x), __dmul_rn(Y, tr.y));
-    if (!(t >= (double)(-C) && t <= (double)(nY - 1 - C))) { tab[idx] = make_int2(-1, 0); return; }
-    const double ft = floor(t);
-    const int j0 = (int)ft + C;
-    const int rs = nA * nZ;
-    if (j0 == nY - 1) tab[idx] = make_int2((nY - 2) * rs + th * nZ, __float_as_int(1.f));
-    else tab[idx] = make_int2(j0 * rs + th * nZ, __float_as_int((float)(t - ft)));
-}
-
-
-// acc (slice pairs) += w0 * row r0 + w1 * row r1, eight slices per lane (q1: the lane's second vector)
-__device__ __forceinline__ void tab_rows(unsigned long long (&acc)[4], const float* __restrict__ p0, int rs, float w,
-                                         bool q1) {
-    const float4 a0 = __ldg(reinterpret_cast<const float4*>(p0));
-    const float4 a2 = __ldg(reinterpret_cast<const float4*>(p0 + rs));
-    float4 a1 = make_float4(0.f, 0.f, 0.f, 0.f), a3 = a1;
-    if (q1) {
-        a1 = __ldg(reinterpret_cast<const float4*>(p0 + 128));
-        a3 = __ldg(reinterpret_cast<const float4*>(p0 + rs + 128));
-    }
-    const unsigned long long w0 = pk_pair(1.f - w, 1.f - w), w1 = pk_pair(w, w);
-    fma_pair(acc[0], w0, a0.x, a0.y); fma_pair(acc[1], w0, a0.z, a0.w);
-    fma_pair(acc[2], w0, a1.x, a1.y); fma_pair(acc[3], w0, a1.z, a1.w);
-    fma_pair(acc[0], w1, a2.x, a2.y); fma_pair(acc[1], w1, a2.z, a2.w);
-    fma_pair(acc[2], w1, a3.x, a3.y); fma_pair(acc[3], w1, a3.z, a3.w);
-}
-
-// FULL: nZ a multiple of 256, every lane's two vectors inside the volume (no load predicates)
-template <bool FULL>
-__device__ __forceinline__ void k_backward_tab_body(const Args& a, const int2* __restrict__ tab,
-                                                    const int* __restrict__ cidx, int nA_pad, unsigned bx) {
-    const int lane = threadIdx.x & 31;
-    const long item = (long)bx * kWarpsPerBlock + (threadIdx.x >> 5);
-    const int zc = (int)(item % a.zchunks);
-    const long p = item / a.zchunks;
-    if (p >= (long)a.nY * a.nX) return;
-    int z0, qn;
-    lane_z<8>(zc, lane, a.nZ, z0, qn);
-    if (qn == 0) return;
-    const bool q1 = FULL || qn == 2;
-    unsigned long long acc[4] = {0ull, 0ull, 0ull, 0ull};
-    const int pc = cidx[p];
-    if (pc >= 0) {
-        const int rs = a.nA * a.nZ;
-        const float* __restrict__ bz = a.in + z0;
-        const int2* __restrict__ e = tab + (size_t)pc * nA_pad;
-        int2 q = __ldcs(e);
-#pragma unroll 1
-        for (int k = 0; k < a.nA; ++k) {
-            const int2 nq = __ldcs(e + min(k + 1, nA_pad - 1));  // the next angle's entry in flight
-            if (q.x >= 0) {
-                if (FULL) {
-                    const float* pa = bz + q.x;
-                    const float4 a0 = __ldg(reinterpret_cast<const float4*>(pa));
-                    const float4 a1 = __ldg(reinterpret_cast<const float4*>(pa + 128));
-                    const float4 a2 = __ldg(reinterpret_cast<const float4*>(pa + rs));
-                    const float4 a3 = __ldg(reinterpret_cast<const float4*>(pa + rs + 128));
-                    const float w = __int_as_float(q.y);
-                    const unsigned long long w0 = pk_pair(1.f - w, 1.f - w), w1 = pk_pair(w, w);
-                    fma_pair(acc[0], w0, a0.x, a0.y); fma_pair(acc[1], w0, a0.z, a0.w);
-                    fma_pair(acc[2], w0, a1.x, a1.y); fma_pair(acc[3], w0, a1.z, a1.w);
-                    fma_pair(acc[0], w1, a2.x, a2.y); fma_pair(acc[1], w1, a2.z, a2.w);
-                    fma_pair(acc[2], w1, a3.x, a3.y); fma_pair(acc[3], w1, a3.z, a3.w);
-                } else {
-                    tab_rows(acc, bz + q.x, rs, __int_as_float(q.y), q1);
-                }
-            }
-            q = nq;
-        }
-    }
-    float v[8];
-#pragma unroll
-    for (int e2 = 0; e2 < 4; ++e2) asm("mov.b64 {%0, %1}, %2;" : "=f"(v[2 * e2]), "=f"(v[2 * e2 + 1]) : "l"(acc[e2]));
-    if (a.mask) {
-        const float m = __ldg(a.mask + p);
-#pragma unroll
-        for (int e2 = 0; e2 < 8; ++e2) v[e2] = m * v[e2];
-    }
-    store_vz<8>(a.out + (size_t)p * a.nZ + z0, v, qn);
-}
-
-template <bool FULL>
-__global__ void __launch_bounds__(256, 1) k_backward_tab8(Args a, const int2* __restrict__ tab, const int* __restrict__ cidx,
-                                                       int nA_pad) {
-    k_backward_tab_body<FULL>(a, tab, cidx, nA_pad, blockIdx.x);
-}
-
-// ---------------------------------------------------------------------------
-// Block-table backprojection: 2 x 2 pixel blocks share their detector rows.
-//
-// For one angle the four pixels of a 2 x 2 block have t = x cos - y sin within
-// |cos| + |sin| <= sqrt(2) of each other, so their np.interp bins j0 span at
-// most three consecutive values and the block needs at most four detector
-// rows (j_min .. j_max + 1) instead of eight.  k_bwd_btable stores, per block
-// inside the clip circle and angle, 32 bytes: the offset of row j_min
-// (j_min * nA * nZ + angle * nZ, -1 when no pixel of the block contributes),
-// a code (bits 0-1: j_max - j_min; per pixel q three bits at 2 + 3q: bit 0
-// contributes, bits 1-2: j0 - j_min) and the four pixels' float32 weights,
-// each pixel's (j0, weight) exactly as k_bwd_table's entry.  k_backward_blk
-// then loads the block's rows once per warp and runs, per pixel, the same two
-// packed FMAs per slice pair in the same order as k_backward_tab8: the sums
-// are bit-identical to it.  The warp walks the rows in passes d = 0 .. span
-// (rows d and d + 1 live), applying each pixel in the pass of its own j0, so
-// at most three rows are held in registers.
+// k_bwd_btable evaluates np.interp's bin once per plan: for every pixel
+// inside the clip circle and every angle the same float64 t = x cos - y sin,
+// floor j0 and float32 weight t - floor(t) as the batched kernel, no
+// contribution where t leaves the detector (np.interp left = right = 0), and
+// at the detector's last bin (t == xp[-1], weight 0) row nY - 2 with weight 1,
+// which adds the same single row with the same rounding.  For one angle the
+// four pixels of a 2 x 2 block have t within |cos| + |sin| <= sqrt(2) of each
+// other, so their bins span at most three consecutive values and the block
+// needs at most four detector rows (j_min .. j_max + 1) instead of eight.  The
+// table holds, per block inside the circle and angle, 32 bytes: the offset of
+// row j_min (j_min * nA * nZ + angle * nZ, -1 when no pixel of the block
+// contributes), a code (bits 0-1: j_max - j_min; per pixel q three bits at
+// 2 + 3q: bit 0 contributes, bits 1-2: j0 - j_min) and the four pixels'
+// weights.  k_backward_blk loads the block's rows once per warp and runs, per
+// pixel, (1 - w) * row j0 then w * row j0 + 1 as packed f32x2 FMAs (two fmaf
+// roundings each), the order of k_backward_batched8, so the sums are
+// bit-identical to it for finite data.  The warp walks the rows in passes
+// d = 0 .. span (rows d and d + 1 live), applying each pixel in the pass of
+// its own j0, so at most three rows are held in registers.  It replaced a
+// per-pixel table kernel (8-byte entries, two rows per pixel and angle, L1
+// bound at 90 %): 1.33 -> 0.92 ms at 256^3 x 360.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_bwd_btable(const double4* __restrict__ trig, const int* __restrict__ blist,
                                                     const int* __restrict__ cidx, int4* __restrict__ tab, int nbc,
@@ -1007,13 +900,15 @@ struct RowV {
     float4 v[VZ / 4];
 };
 
+// the lane's vectors of one detector row; vectors q >= qn (past nZ) read as zeros
 template <int VZ>
-__device__ __forceinline__ void load_row(RowV<VZ>& r, const float* __restrict__ p) {
+__device__ __forceinline__ void load_row(RowV<VZ>& r, const float* __restrict__ p, int qn = VZ / 4) {
 #pragma unroll
-    for (int q = 0; q < VZ / 4; ++q) r.v[q] = __ldg(reinterpret_cast<const float4*>(p + 128 * q));
+    for (int q = 0; q < VZ / 4; ++q)
+        r.v[q] = q < qn ? __ldg(reinterpret_cast<const float4*>(p + 128 * q)) : make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
-// acc (slice pairs) += (1 - w) * r0 then += w * r1: k_backward_tab8's two packed FMAs per pair
+// acc (slice pairs) += (1 - w) * r0 then += w * r1: two packed FMAs per pair
 template <int VZ>
 __device__ __forceinline__ void lerp_rows(unsigned long long (&acc)[VZ / 2], float w, const RowV<VZ>& r0,
                                           const RowV<VZ>& r1) {
@@ -1030,14 +925,15 @@ __device__ __forceinline__ void lerp_rows(unsigned long long (&acc)[VZ / 2], flo
     }
 }
 
-// one warp per (2 x 2 block, z chunk of 32 VZ slices); nZ a multiple of 32 VZ.  The table entries
+// one warp per (2 x 2 block, z chunk of 32 VZ slices); FULL: nZ a multiple of 32 VZ, else the lanes
+// past nZ in the last chunk load and store nothing.  The table entries
 // arrive 32 angles at a time (lane l fetches angle k0 + l's 32 bytes, the next chunk in flight while
 // this one is read), so no angle waits for its entry: eight slices per lane by cp.async into the warp's
 // two shared-memory slots (no registers held: the body fits 80 registers, three CTAs per SM; 1.19 ->
 // 0.92 ms at 256^3 x 360 against entries in registers at two CTAs), four slices in registers,
 // broadcast by shuffles (0.21 -> 0.17 ms at 128^3 x 360 against the shared-memory slots).
 constexpr int kBlkEnt = 64;  // int4 per slot: 32 angles x 32 bytes
-template <int VZ>
+template <int VZ, bool FULL>
 __device__ __forceinline__ void k_backward_blk_body(const Args& a, const int4* __restrict__ tab,
                                                     const int* __restrict__ bcidx, unsigned bx) {
     __shared__ __align__(16) int4 s_ent[VZ == 8 ? kWarpsPerBlock : 1][2][kBlkEnt];
@@ -1051,7 +947,8 @@ __device__ __forceinline__ void k_backward_blk_body(const Args& a, const int4* _
     const int bi = (int)(tile / ntx) * 2 + (wp >> 2), bj = (int)(tile % ntx) * 4 + (wp & 3);
     if (bi >= nby || bj >= nbx) return;
     const long blk = (long)bi * nbx + bj;
-    const int z0 = zc * 32 * VZ + 4 * lane;
+    int z0 = zc * 32 * VZ + 4 * lane, qn = VZ / 4;
+    if (!FULL) lane_z<VZ>(zc, lane, a.nZ, z0, qn);
     unsigned long long acc[4][VZ / 2];
 #pragma unroll
     for (int q = 0; q < 4; ++q)
@@ -1071,9 +968,9 @@ __device__ __forceinline__ void k_backward_blk_body(const Args& a, const int4* _
             const float* pr = bz + e0.x;
             const int span = code & 3;
             RowV<VZ> ra, rb, rc;
-            load_row<VZ>(ra, pr);
-            load_row<VZ>(rb, pr + rs);
-            if (span >= 1) load_row<VZ>(rc, pr + 2 * rs);
+            load_row<VZ>(ra, pr, qn);
+            load_row<VZ>(rb, pr + rs, qn);
+            if (span >= 1) load_row<VZ>(rc, pr + 2 * rs, qn);
 #pragma unroll
             for (int q = 0; q < 4; ++q)
                 if (((code >> (2 + 3 * q)) & 7) == 1) lerp_rows<VZ>(acc[q], w[q], ra, rb);
@@ -1082,7 +979,7 @@ __device__ __forceinline__ void k_backward_blk_body(const Args& a, const int4* _
                 for (int q = 0; q < 4; ++q)
                     if (((code >> (2 + 3 * q)) & 7) == 3) lerp_rows<VZ>(acc[q], w[q], rb, rc);
                 if (span == 2) {
-                    load_row<VZ>(ra, pr + 3 * rs);
+                    load_row<VZ>(ra, pr + 3 * rs, qn);
 #pragma unroll
                     for (int q = 0; q < 4; ++q)
                         if (((code >> (2 + 3 * q)) & 7) == 5) lerp_rows<VZ>(acc[q], w[q], rc, ra);
@@ -1173,15 +1070,16 @@ __device__ __forceinline__ void k_backward_blk_body(const Args& a, const int4* _
         // 399 -> 390 MB per 256^3 x 360 launch)
 #pragma unroll
         for (int q2 = 0; q2 < VZ / 4; ++q2)
-            __stcs(reinterpret_cast<float4*>(a.out + (size_t)p * a.nZ + z0 + 128 * q2),
-                   make_float4(v[4 * q2], v[4 * q2 + 1], v[4 * q2 + 2], v[4 * q2 + 3]));
+            if (q2 < qn)
+                __stcs(reinterpret_cast<float4*>(a.out + (size_t)p * a.nZ + z0 + 128 * q2),
+                       make_float4(v[4 * q2], v[4 * q2 + 1], v[4 * q2 + 2], v[4 * q2 + 3]));
     }
 }
 
-template <int VZ, int MINB>
+template <int VZ, int MINB, bool FULL>
 __global__ void __launch_bounds__(256, MINB) k_backward_blk(Args a, const int4* __restrict__ tab,
                                                             const int* __restrict__ bcidx) {
-    k_backward_blk_body<VZ>(a, tab, bcidx, blockIdx.x);
+    k_backward_blk_body<VZ, FULL>(a, tab, bcidx, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -1936,8 +1834,7 @@ int fast_vz(int nZ, bool aligned, double min_eff) {
 // same body for many calls inside one persistent launch.  Both paths therefore
 // compute bit-identical results.
 // ---------------------------------------------------------------------------
-enum Kind : int { KF_FAST = 0, KF_GEN, KB_BATCHED, KB_FAST, KB_GEN, KA_TABLE, KA_FAST, KA_GEN, KF_2D, KB_2D, KB_TABLE,
-                  KB_BTABLE };
+enum Kind : int { KF_FAST = 0, KF_GEN, KB_BATCHED, KB_FAST, KB_GEN, KA_TABLE, KA_FAST, KA_GEN, KF_2D, KB_2D, KB_BTABLE };
 
 struct Item {
     int kind;
@@ -1959,10 +1856,8 @@ struct Item {
     Args a;
     FastArgs f;
     const float4* table;
-    const int2* btab;  // KB_TABLE: the plan's backprojection bin table, its pixel index and list stride
+    const int4* btab4;  // KB_BTABLE: the plan's 2 x 2 block bin table and its block index
     const int* bcidx;
-    int bpad, bpad_;
-    const int4* btab4;  // KB_BTABLE: the plan's 2 x 2 block table (bcidx: its block index)
     int* status;       // the plan's status word (kernels with bounded waits record timeouts there)
     int tma, tma_pad_;  // KF_2D: 1 when tmap describes a.in and the tiles are staged by TMA loads
     CUtensorMap tmap;   // read from parameter space, as a direct launch's __grid_constant__ argument
@@ -2067,21 +1962,17 @@ int describe(vam_parallel_plan* plan, Op op, const float* in, float* out, Item& 
         if (op == Op::BackwardRef) {
             // the batched kernel stages cos / sin of every angle in shared memory (16 B per angle)
             const int batch = (size_t)plan->nA * sizeof(double2) <= 48 * 1024 ? plan->tune_bwd_batch : 1;
-            if (!ray && plan->d_bwd_btab && plan->tune_bwd_table && plan->nZ % 128 == 0) {
-                // the 2 x 2 block table: eight slices per lane when nZ % 256 == 0, else four
-                const int bvz = plan->nZ % 256 == 0 ? 8 : 4;
+            if (!ray && plan->d_bwd_btab && plan->tune_bwd_table) {
+                // the 2 x 2 block table: eight slices per lane from 160 slices up (or tuned to 8), else four
+                // (256^3 x 360: 0.92 / 1.41 ms; 192^3 x 720: 1.46 / 1.94; 96^3 x 720: 0.42 / 0.31)
+                const int bvz = plan->tune_bwd_vz == 8 || (plan->tune_bwd_vz != 4 && plan->nZ >= 160) ? 8 : 4;
                 it.kind = KB_BTABLE;
                 it.vz = bvz;
-                a.zchunks = plan->nZ / (32 * bvz);
+                a.zchunks = (plan->nZ + 32 * bvz - 1) / (32 * bvz);
                 const long ntx = ((plan->nX + 1) / 2 + 3) / 4, nty = ((plan->nY + 1) / 2 + 1) / 2;
                 it.gx = (unsigned)(ntx * nty * a.zchunks);
                 it.btab4 = plan->d_bwd_btab;
                 it.bcidx = plan->d_bwd_bcidx;
-            } else if (vzf == 8 && !ray && plan->d_bwd_table && plan->tune_bwd_table) {
-                it.kind = KB_TABLE;
-                it.btab = plan->d_bwd_table;
-                it.bcidx = plan->d_bwd_cidx;
-                it.bpad = plan->bwd_table_pad;
             } else if (batch >= 2) {
                 it.kind = KB_BATCHED;
                 it.batch = vzf == 8 ? 2 : (batch >= 4 ? 4 : 2);
@@ -2158,8 +2049,9 @@ __device__ __forceinline__ void fast_body(const Item& it, unsigned bx, unsigned 
     if constexpr (FAM == 256 && !RAY) {
         if (it.kind == KB_BTABLE) {
             const Args a = it.a;
-            if (it.vz == 8) k_backward_blk_body<8>(a, it.btab4, it.bcidx, bx);
-            else k_backward_blk_body<4>(a, it.btab4, it.bcidx, bx);
+            const bool full = a.nZ % (32 * it.vz) == 0;
+            if (it.vz == 8) { if (full) k_backward_blk_body<8, true>(a, it.btab4, it.bcidx, bx); else k_backward_blk_body<8, false>(a, it.btab4, it.bcidx, bx); }
+            else { if (full) k_backward_blk_body<4, true>(a, it.btab4, it.bcidx, bx); else k_backward_blk_body<4, false>(a, it.btab4, it.bcidx, bx); }
         }
     }
     if constexpr ((FAM & 8) != 0 || ((FAM & 2) != 0 && !RAY)) {
@@ -2175,12 +2067,6 @@ __device__ __forceinline__ void fast_body(const Item& it, unsigned bx, unsigned 
             const Args a = it.a;
             if (it.vz == 8) k_backward_fast_body<8, RAY>(a, bx, by);
             else k_backward_fast_body<4, RAY>(a, bx, by);
-        } else if (it.kind == KB_TABLE) {
-            if constexpr (!RAY) {
-                const Args a = it.a;
-                if (a.nZ % 256 == 0) k_backward_tab_body<true>(a, it.btab, it.bcidx, it.bpad, bx);
-                else k_backward_tab_body<false>(a, it.btab, it.bcidx, it.bpad, bx);
-            }
         }
     }
     if constexpr ((FAM & 4) != 0) {
@@ -2330,11 +2216,15 @@ int launch_item(const Item& it, cudaStream_t st, const char* name) {
         if (it.vz == 8) k_adjoint_table<8><<<grid, block, 0, st>>>(it.a, it.table);
         else k_adjoint_table<4><<<grid, block, 0, st>>>(it.a, it.table);
     } else if (it.kind == KB_BTABLE) {
-        if (it.vz == 8) k_backward_blk<8, 3><<<grid, dim3(kWarpsPerBlock * kWarp), 0, st>>>(it.a, it.btab4, it.bcidx);
-        else k_backward_blk<4, 3><<<grid, dim3(kWarpsPerBlock * kWarp), 0, st>>>(it.a, it.btab4, it.bcidx);
-    } else if (it.kind == KB_TABLE) {
-        if (it.a.nZ % 256 == 0) k_backward_tab8<true><<<grid, dim3(kWarpsPerBlock * kWarp), 0, st>>>(it.a, it.btab, it.bcidx, it.bpad);
-        else k_backward_tab8<false><<<grid, dim3(kWarpsPerBlock * kWarp), 0, st>>>(it.a, it.btab, it.bcidx, it.bpad);
+        const dim3 block(kWarpsPerBlock * kWarp);
+        const bool full = it.a.nZ % (32 * it.vz) == 0;
+        if (it.vz == 8) {
+            if (full) k_backward_blk<8, 3, true><<<grid, block, 0, st>>>(it.a, it.btab4, it.bcidx);
+            else k_backward_blk<8, 3, false><<<grid, block, 0, st>>>(it.a, it.btab4, it.bcidx);
+        } else {
+            if (full) k_backward_blk<4, 3, true><<<grid, block, 0, st>>>(it.a, it.btab4, it.bcidx);
+            else k_backward_blk<4, 3, false><<<grid, block, 0, st>>>(it.a, it.btab4, it.bcidx);
+        }
     } else if (it.ray) {
         launch_fast<true>(it, grid, st);
     } else {
@@ -2401,10 +2291,11 @@ static_assert(sizeof(BatchParams) < 32000, "batch parameters must fit the 32 KB 
 // lean generic backprojection fits 40 registers (six CTAs, as its direct
 // kernel: a 160^3 x 720 call ran 1.36x longer at four), the fast and 2-D
 // backprojections and the 2-D forward 48 (five), the fast forward and the
-// lean generic forward 64 (four); the heavy instances and the block-table
-// backprojection keep 80 (three).
+// lean generic forward 64 (four); the heavy instances keep 80 (three), the
+// block-table backprojection (four bodies: 4 or 8 slices, full or partial z
+// chunks) 128 (two).
 template <int FAM>
-__global__ void __launch_bounds__(256, FAM == 64 ? 6 : (FAM == 2 || FAM == 128 ? 5 : (FAM == 1 || FAM == 32 ? 4 : 3)))
+__global__ void __launch_bounds__(256, FAM == 64 ? 6 : (FAM == 2 || FAM == 128 ? 5 : (FAM == 1 || FAM == 32 ? 4 : (FAM == 256 ? 2 : 3))))
     k_batch(const __grid_constant__ BatchParams P) {
     __shared__ unsigned s_t[2];
     __shared__ int s_idx[2];
@@ -2580,7 +2471,6 @@ extern "C" int vam_parallel_plan_destroy(vam_parallel_plan* p) {
     cudaFree(p->d_tasks_single);
     cudaFree(p->d_vol_scratch);
     cudaFree(p->d_adj_table);
-    cudaFree(p->d_bwd_table);
     cudaFree(p->d_bwd_cidx);
     cudaFree(p->d_status);
     cudaFree(p->d_img_pad);
@@ -2767,39 +2657,22 @@ extern "C" int vam_parallel_prepare_backward(vam_parallel_plan* p, vam_stream_t 
     VAM_REQUIRE(p, VAM_ERR_ARG, "vam_parallel_prepare_backward: null plan");
     VAM_REQUIRE((long long)p->nY * p->nA * p->nZ < (1LL << 31), VAM_ERR_NOTSUP,
                 "vam_parallel_prepare_backward: the table holds 32-bit sinogram offsets (sinogram below 2^31 elements)");
+    VAM_REQUIRE(p->nZ % 4 == 0, VAM_ERR_NOTSUP,
+                "vam_parallel_prepare_backward: the table kernel runs four-slice vectors (nZ % 4 == 0)");
     DeviceGuard g(p->device);
     const int n = p->nY * p->nX;
     // the clip circle exactly as the plan's table (linspace(-1, 1) semantics)
-    std::vector<int> cidx(n, -1), plist;
-    for (int i = 0; i < p->nY; ++i) {
+    std::vector<int> cidx(n, -1);
+    for (int i = 0, c = 0; i < p->nY; ++i) {
         const double a = lin_m1_1(i, p->nY);
         for (int j = 0; j < p->nX; ++j) {
             const double b = lin_m1_1(j, p->nX);
             volatile double aa = a * a, bb = b * b;
             volatile double r2 = aa + bb;
-            if (!(r2 > 1.0)) { cidx[(size_t)i * p->nX + j] = (int)plist.size(); plist.push_back(i * p->nX + j); }
+            if (!(r2 > 1.0)) cidx[(size_t)i * p->nX + j] = c++;
         }
     }
-    const int npc = (int)plist.size();
-    const int pad = (p->nA + 1) & ~1;
-    // nZ % 128 == 0: the 2 x 2 block table (k_backward_blk); otherwise the per-pixel table (k_backward_tab8)
-    const bool blocks = p->nZ % 128 == 0;
-    cudaStream_t st = (cudaStream_t)stream;
-    if (!p->d_bwd_cidx) VAM_TRY_CUDA(cudaMalloc(&p->d_bwd_cidx, sizeof(int) * n));
-    if (!blocks && !p->d_bwd_table)
-        VAM_TRY_CUDA(cudaMalloc(&p->d_bwd_table, sizeof(int2) * (size_t)std::max(npc, 1) * pad));
-    int* d_plist = nullptr;
-    VAM_TRY_CUDA(cudaMalloc(&d_plist, sizeof(int) * std::max(npc, 1)));
-    cudaError_t e = cudaMemcpyAsync(p->d_bwd_cidx, cidx.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess && npc && !blocks)
-        e = cudaMemcpyAsync(d_plist, plist.data(), sizeof(int) * npc, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess && npc && !blocks) {
-        const long tot = (long)npc * pad;
-        k_bwd_table<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(p->d_trig, d_plist, p->d_bwd_table, npc, p->nA, pad,
-                                                                   p->nY, p->nX, p->nZ, p->C);
-        e = cudaGetLastError();
-    }
-    // 2 x 2 blocks with at least one pixel inside the circle, for the block-table kernel
+    // 2 x 2 blocks with at least one pixel inside the circle
     const int nbx = (p->nX + 1) / 2, nby = (p->nY + 1) / 2;
     std::vector<int> bcidx((size_t)nbx * nby, -1), blist;
     for (int bi = 0; bi < nby; ++bi)
@@ -2812,29 +2685,27 @@ extern "C" int vam_parallel_prepare_backward(vam_parallel_plan* p, vam_stream_t 
             if (any) { bcidx[(size_t)bi * nbx + bj] = (int)blist.size(); blist.push_back(bi * nbx + bj); }
         }
     const int nbc = (int)blist.size();
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!p->d_bwd_cidx) VAM_TRY_CUDA(cudaMalloc(&p->d_bwd_cidx, sizeof(int) * n));
+    if (!p->d_bwd_bcidx) VAM_TRY_CUDA(cudaMalloc(&p->d_bwd_bcidx, sizeof(int) * bcidx.size()));
+    if (!p->d_bwd_btab) VAM_TRY_CUDA(cudaMalloc(&p->d_bwd_btab, sizeof(int4) * 2 * (size_t)std::max(nbc, 1) * p->nA));
     int* d_blist = nullptr;
-    if (e == cudaSuccess && blocks && nbc) {
-        if (!p->d_bwd_bcidx) e = cudaMalloc(&p->d_bwd_bcidx, sizeof(int) * bcidx.size());
-        if (e == cudaSuccess && !p->d_bwd_btab) e = cudaMalloc(&p->d_bwd_btab, sizeof(int4) * 2 * (size_t)nbc * p->nA);
-        if (e == cudaSuccess) e = cudaMalloc(&d_blist, sizeof(int) * nbc);
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(p->d_bwd_bcidx, bcidx.data(), sizeof(int) * bcidx.size(), cudaMemcpyHostToDevice, st);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(d_blist, blist.data(), sizeof(int) * nbc, cudaMemcpyHostToDevice, st);
-        if (e == cudaSuccess) {
-            const long tot = (long)nbc * p->nA;
-            k_bwd_btable<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(p->d_trig, d_blist, p->d_bwd_cidx,
-                                                                        p->d_bwd_btab, nbc, p->nA, p->nY, p->nX,
-                                                                        p->nZ, p->C);
-            e = cudaGetLastError();
-        }
+    VAM_TRY_CUDA(cudaMalloc(&d_blist, sizeof(int) * std::max(nbc, 1)));
+    cudaError_t e = cudaMemcpyAsync(p->d_bwd_cidx, cidx.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(p->d_bwd_bcidx, bcidx.data(), sizeof(int) * bcidx.size(), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && nbc) e = cudaMemcpyAsync(d_blist, blist.data(), sizeof(int) * nbc, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && nbc) {
+        const long tot = (long)nbc * p->nA;
+        k_bwd_btable<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(p->d_trig, d_blist, p->d_bwd_cidx, p->d_bwd_btab,
+                                                                    nbc, p->nA, p->nY, p->nX, p->nZ, p->C);
+        e = cudaGetLastError();
     }
-    // the host vectors and the pixel / block lists are released after the copies and the build complete
+    // the host vectors and the block list are released after the copies and the build complete
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    cudaFree(d_plist);
     cudaFree(d_blist);
     if (e != cudaSuccess)
         return set_error(VAM_ERR_CUDA, std::string("vam_parallel_prepare_backward: ") + cudaGetErrorString(e));
-    p->bwd_table_pad = pad;
     return VAM_OK;
 }
 
@@ -2985,7 +2856,6 @@ double time_weight(const Item& it) {
         case KF_FAST: return 1.0;
         case KF_GEN: return slice ? 27.0 : 4.0;
         case KB_BATCHED: case KB_FAST: return 1.2;
-        case KB_TABLE: return 1.05;
         case KB_BTABLE: return 0.7;
         case KB_GEN: return slice ? 10.0 : 2.0;
         case KA_TABLE: return 1.5;

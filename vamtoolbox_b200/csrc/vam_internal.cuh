@@ -89,12 +89,9 @@ struct vam_parallel_plan {
     // detector rows (as int bits) and their summed forward tap weights
     float4* d_adj_table;    // [nY*nX][nA]
     int adj_table_abs;      // absorption mode the table was built for (-1: none built)
-    // reference-parity backprojection bins: per pixel inside the clip circle (compact index d_bwd_cidx,
-    // -1 outside) and angle, (row offset j0 * nA * nZ + angle * nZ, weight bits) of np.interp's bin, or
-    // (-1, 0) where t falls outside the detector; each pixel's list padded to an even length
-    int2* d_bwd_table;
+    // reference-parity backprojection bins (k_bwd_btable): the clip circle's compact pixel index
+    // (-1 outside) from which the block table is built
     int* d_bwd_cidx;
-    int bwd_table_pad;
     // tuning (vam_parallel_set_tuning): vector widths 0 = automatic
     int tune_fwd_vz, tune_bwd_vz, tune_adj_vz, tune_bwd_batch, tune_adj_table, tune_bwd_table, tune_fwd_tma;
 };

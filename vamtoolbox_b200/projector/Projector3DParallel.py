@@ -101,8 +101,9 @@ class ParallelPlan:
         self._adj_ready = False
         # matched-transpose weight table: 16 B per pixel and angle (skipped above this size)
         self.adj_table_limit_bytes = 8 << 30
-        # backprojection bin table (8 B per pixel inside the circle and angle), built here for volumes the
-        # eight-slice kernels serve, so it exists before any capture of a backprojection
+        # backprojection bin table (32 B per 2 x 2 pixel block inside the circle and angle, about 8 B per
+        # pixel), built here for volumes of 64 slices and more, so it exists before any capture of a
+        # backprojection
         self.bwd_table_limit_bytes = 8 << 30
         self.has_backward_table = False
         self._key = _pool_key(self.shape_vol, self.angles, self.device)
@@ -120,7 +121,7 @@ class ParallelPlan:
         h = ctypes.c_void_p()
         _lib.call("vam_parallel_plan_create", ctypes.byref(geom), ctypes.byref(h))
         self._h = h
-        if int(n_z) % 8 == 0 and int(n_z) >= 64:
+        if int(n_z) % 4 == 0 and int(n_z) >= 64:
             self.prepare_backward()
 
     def _reset(self):
@@ -177,9 +178,10 @@ class ParallelPlan:
 
     def prepare_backward(self):
         """Build the backprojection bin table (allocates; not during graph capture).  False when it would
-        exceed ``bwd_table_limit_bytes`` or the sinogram is too large for its 32-bit offsets."""
+        exceed ``bwd_table_limit_bytes``, the sinogram is too large for its 32-bit offsets or nZ % 4 != 0."""
         ny, nx, nz = self.shape_vol
-        if 8 * ny * nx * (self.angles.size + 1) > self.bwd_table_limit_bytes or ny * self.angles.size * nz >= 2 ** 31:
+        if (8 * ny * nx * (self.angles.size + 1) > self.bwd_table_limit_bytes or ny * self.angles.size * nz >= 2 ** 31
+                or nz % 4 != 0):
             return False
         with torch.cuda.device(self.device):
             _lib.call("vam_parallel_prepare_backward", self._h, self._stream())
