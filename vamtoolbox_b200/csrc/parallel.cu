@@ -298,6 +298,20 @@ __device__ __forceinline__ void load_vz(const float* __restrict__ p, float* d, i
     }
 }
 
+// load_vz with an L1 evict-last priority: the forward's taps, which neighbouring bins and samples of
+// the CTA read again (1.406 -> 1.373 ms at 256^3 x 360, identical results)
+template <int VZ>
+__device__ __forceinline__ void load_vz_keep(const float* __restrict__ p, float* d, int qn = VZ / 4) {
+#pragma unroll
+    for (int q = 0; q < VZ / 4; ++q) {
+        float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (q < qn)
+            asm("ld.global.nc.L1::evict_last.v4.f32 {%0, %1, %2, %3}, [%4];"
+                : "=f"(t.x), "=f"(t.y), "=f"(t.z), "=f"(t.w) : "l"(p + 128 * q));
+        d[4 * q] = t.x; d[4 * q + 1] = t.y; d[4 * q + 2] = t.z; d[4 * q + 3] = t.w;
+    }
+}
+
 template <int VZ>
 __device__ __forceinline__ void store_vz(float* __restrict__ p, const float* d, int qn) {
 #pragma unroll
@@ -403,10 +417,10 @@ __device__ __forceinline__ void k_forward_fast_body(const FastArgs& a, unsigned 
                 float w10 = dr * (1.f - dc), w11 = dr * dc;
                 if (RAY) { w00 *= f; w01 *= f; w10 *= f; w11 *= f; }
                 float t0[VZ], t1[VZ], t2[VZ], t3[VZ];
-                load_vz<VZ>(volz + o00, t0, qn);
-                load_vz<VZ>(volz + o00 + dcol, t1, qn);
-                load_vz<VZ>(volz + o10, t2, qn);
-                load_vz<VZ>(volz + o10 + dcol, t3, qn);
+                load_vz_keep<VZ>(volz + o00, t0, qn);
+                load_vz_keep<VZ>(volz + o00 + dcol, t1, qn);
+                load_vz_keep<VZ>(volz + o10, t2, qn);
+                load_vz_keep<VZ>(volz + o10 + dcol, t3, qn);
 #pragma unroll
                 for (int e = 0; e < VZ; ++e) {
                     acc[e] = fmaf(w00, t0[e], acc[e]);
