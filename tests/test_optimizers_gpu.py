@@ -216,3 +216,38 @@ def test_device_metrics_match_reference(golden):
     n = np.sum(tg.gel_inds) + np.sum(tg.void_inds)
     assert abs(metrics.calcVER(tg, d) - G["m_ver"]) * n <= 1.0 + 1e-9
     assert abs(metrics.calcIPDR(tg, d) - G["m_ipdr"]) <= 1e-6 * abs(G["m_ipdr"])
+
+
+def test_zslab_bclp_one_rank_equals_optimize():
+    """vamtoolbox_b200.distributed.optimize_bclp_zslab on a one-rank NCCL group runs the same kernels as
+    optimize() (eagerly, the loss sums passed through the all-reduce): the same sinogram, dose and loss."""
+    import socket
+
+    import torch
+    import torch.distributed as dist
+
+    from vamtoolbox_b200 import geometry, optimize as vopt
+    from vamtoolbox_b200.distributed import optimize_bclp_zslab
+
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            device_id=torch.device("cuda", 0))
+    try:
+        rng = np.random.default_rng(4)
+        t = np.zeros((48, 48, 16))
+        t[14:34, 12:36, 3:13] = 1.0
+        t[20:26, 20:26, :] = rng.uniform(0.3, 0.7)
+        pg = geometry.ProjectionGeometry(np.linspace(0, 360, 60, endpoint=False), "parallel", CUDA=True,
+                                         projector_pixel_size=0.01, absorption_coeff=2.0, container_radius=0.3)
+        opts = vopt.Options(method="BCLP", n_iter=6, p=2, q=1, eps=0.1, learning_rate=1e-5)
+        ref = vopt.optimize(geometry.TargetGeometry(target=t.copy()), pg, opts)
+        opts2 = vopt.Options(method="BCLP", n_iter=6, p=2, q=1, eps=0.1, learning_rate=1e-5)
+        got = optimize_bclp_zslab(geometry.TargetGeometry(target=t.copy()), pg, opts2)
+        assert np.array_equal(ref[0].array, got[0].array)
+        assert np.array_equal(ref[1].array, got[1].array)
+        assert np.array_equal(np.asarray(ref[2]), np.asarray(got[2]))
+    finally:
+        dist.destroy_process_group()

@@ -100,3 +100,69 @@ def target_shards(costs, world: int):
         load[r] += float(costs[i])
         out[r].append(i)
     return [sorted(o) for o in out]
+
+
+def gather_zslabs(local, nz_total: int, group=None):
+    """The whole [..., nz_total] array from every rank's z-slab [..., z0:z1] (slab_range): the slabs, padded to
+    the largest slab, are all-gathered and concatenated in rank order on every rank."""
+    import torch
+    import torch.distributed as dist
+
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    z0, z1 = slab_range(nz_total, world, rank)
+    if local.shape[-1] != z1 - z0:
+        raise ValueError(f"rank {rank}: slab of {local.shape[-1]} slices, expected {z1 - z0}")
+    zmax = max(b - a for a, b in (slab_range(nz_total, world, r) for r in range(world)))
+    pad = torch.zeros(local.shape[:-1] + (zmax,), dtype=local.dtype, device=local.device)
+    pad[..., : z1 - z0] = local
+    parts = [torch.empty_like(pad) for _ in range(world)]
+    dist.all_gather(parts, pad.contiguous(), group=group)
+    return torch.cat([parts[r][..., : b - a] for r, (a, b) in
+                      enumerate(slab_range(nz_total, world, r) for r in range(world))], dim=-1)
+
+
+def optimize_bclp_zslab(target_geo, proj_geo, options, group=None, gather=True):
+    """optimize(target_geo, proj_geo, options) for BCLP (vamtoolbox/optimize.py:174-217 ->
+    vamtoolbox/optimizer/BCLP.py) over z-slabs, one per rank of ``group`` (one process per GPU, NCCL).
+
+    Parallel beam without inclination treats slices independently in every projection, so each rank
+    builds its own projector on slices [z0, z1) of the target (slab_range) and runs the device engine
+    there; the 9 loss / norm sums are all-reduced every iteration, so every rank takes the whole volume's
+    loss, gradient scale and convergence decision, as one process would (float32 sums combined in another
+    order).  Returns (Sinogram, Reconstruction, loss) of the whole volume on every rank when ``gather``
+    (the slabs all-gathered), else this rank's slabs (sinogram [nR, nA, z1 - z0], dose [nY, nX, z1 - z0]).
+    The caller's geometry objects are not modified."""
+    import copy
+
+    import torch
+    import torch.distributed as dist
+
+    from . import geometry
+    from .optimizer.BCLP import BCLPNorm
+
+    if options.method != "BCLP":
+        raise ValueError("optimize_bclp_zslab runs BCLP")
+    world, rank = dist.get_world_size(group), dist.get_rank(group)
+    arr = np.atleast_3d(np.asarray(target_geo.array))
+    nz = arr.shape[2]
+    z0, z1 = slab_range(nz, world, rank)
+    if z1 <= z0:
+        raise ValueError(f"{world} ranks for {nz} slices: rank {rank} has no slice")
+    tg, pg = copy.copy(target_geo), copy.copy(proj_geo)
+    tg.array = np.ascontiguousarray(arr[:, :, z0:z1])
+    if options.units != "normalized" or pg.absorption_coeff is not None:
+        pg.calcAbsorptionMask(tg)
+    bclp = BCLPNorm(tg, pg, options)
+    if not bclp._device_init_ok():
+        raise ValueError("optimize_bclp_zslab needs the device engine on a parallel-beam projector")
+    g = bclp.checkSinogramShape(bclp.gradientDescentDevice(graph=False,
+                                                           reduce_stats=lambda s: bclp_stats_allreduce(s, group)),
+                                "cylindrical")
+    if not gather:
+        return g, bclp.dose, bclp.logs.loss
+    dev = bclp.P.device
+    g_all = gather_zslabs(torch.as_tensor(g, device=dev), nz, group).cpu().numpy()
+    d_all = gather_zslabs(torch.as_tensor(bclp.dose, device=dev), nz, group).cpu().numpy()
+    return (geometry.Sinogram(g_all, proj_geo, options), geometry.Reconstruction(d_all, proj_geo, options),
+            bclp.logs.loss)

@@ -250,15 +250,17 @@ class BCLPNorm:
         """A :class:`DeviceIteration` holding this problem's device state (g = g0)."""
         return DeviceIteration(self, reduce_stats=reduce_stats)
 
-    def gradientDescentDevice(self, graph=True):
-        it = self.device_iteration()
+    def gradientDescentDevice(self, graph=True, reduce_stats=None):
+        """The device engine's loop; ``reduce_stats`` (see DeviceIteration) runs it eagerly with the loss /
+        norm sums combined across ranks every iteration (vamtoolbox_b200.distributed.optimize_bclp_zslab)."""
+        it = self.device_iteration(reduce_stats=reduce_stats)
         n_iter = self.logs.options.n_iter
         q, p = self.q, self.p
         dev = it.device
         st = torch.cuda.current_stream(dev)
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(n_iter + 1)]
         ev[0].record(st)
-        eager = (not graph) or self.bit_depth is not None or self.exit_param is not None
+        eager = (not graph) or self.bit_depth is not None or self.exit_param is not None or reduce_stats is not None
         done = n_iter
         if eager:
             for k in range(n_iter):
