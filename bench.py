@@ -498,11 +498,35 @@ def run_ray_bclp(dev, n=128, n_angles=360, steps=5, warmup=2, cpu=True):
     plan = bclp.P.plan
     rays = int(plan.num_rays)
     cap = int(plan.max_num_step) if hasattr(plan, "max_num_step") else 3 * n
+    cache = None
+    if getattr(plan, "has_trajectories", False):
+        # the same kernels tracing every call (the cache dropped), and the one-time trace that fills it
+        active_cached = int(plan.active_at_cap())
+        plan.drop_trajectories()
+        traced = {}
+        for name, fn in (("deposit", lambda: it.back(it.g, it.dose)), ("integrate", lambda: it.fwd(it.operand, it.grad))):
+            fn()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            fn()
+            b.record(st)
+            torch.cuda.synchronize(dev)
+            traced[name] = round(a.elapsed_time(b), 3)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        plan.prepare_trajectories()
+        torch.cuda.synchronize(dev)
+        cache = {"bytes": int(plan.trajectory_bytes()), "prepare_ms": round((time.perf_counter() - t0) * 1e3, 2),
+                 "kernel_ms_traced": traced, "rays_active_at_cap_cached": active_cached,
+                 "what": "ray paths traced once per medium (position and attenuance per step, 16 B per ray-step); "
+                         "integrate / deposit stream them (integrate bit-identical, deposit equal up to atomic "
+                         "order)"}
     out = {"workload": f"BCLP iteration through the ray tracer, {n}^3 graded-index medium, {n_angles} angles, "
                        f"{rays} rays, step cap {cap}",
            "bclp_iter_s": round(1000.0 / ms, 3), "ms_per_iteration": round(ms, 3), "kernel_ms": kt,
            "ray_steps_per_s": round(rays * cap / (kt["integrate"] * 1e-3), 1),
-           "rays_active_at_cap": int(plan.active_at_cap()), "launches_per_iteration": launches}
+           "rays_active_at_cap": int(plan.active_at_cap()), "launches_per_iteration": launches,
+           "trajectory_cache": cache}
     if cpu:
         try:
             out["cpu_baseline"] = ray_cpu_sample(cv, nx, ax, n_angles)

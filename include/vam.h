@@ -307,6 +307,22 @@ int vam_ray_grad_alpha(vam_ray_plan* plan, const float* f_dev, const float* w_de
  * pyTorchRayTrace.py:464-467).  Synchronises the device. */
 int vam_ray_active_at_cap(vam_ray_plan* plan, int64_t* out_count);
 
+/* Trajectory cache of a plan on a 3-D grid medium with the physical path
+ * length and the symplectic Euler solver: the rays are traced once (the same
+ * steps and exit checks as vam_ray_integrate) and each executed step's
+ * position x_ip1 and attenuance are kept, 16 bytes per ray and step
+ * (max_num_step x num_rays x 16 B: 36 GB at 128^3 x 360 rays x 384 steps).
+ * While it is valid, vam_ray_integrate and vam_ray_deposit stream the records
+ * instead of re-tracing (bit-identical results); vam_ray_set_medium
+ * invalidates it (prepare again to refresh it).  VAM_ERR_NOTSUP when the
+ * configuration has no padded path or the cache would exceed limit_bytes,
+ * VAM_ERR_NOMEM when the device cannot hold it (the plan then traces as
+ * before).  Allocates: call before any stream capture.
+ * vam_ray_drop_trajectories frees it.  The reference re-traces every call
+ * (pyTorchRayTrace.py:378-571). */
+int vam_ray_prepare_trajectories(vam_ray_plan* plan, int64_t limit_bytes, vam_stream_t stream);
+int vam_ray_drop_trajectories(vam_ray_plan* plan);
+
 /* The propagation matrix of vam_ray_integrate, one CSR row per ray, replacing
  * PyTorchRayTracingPropagator.buildPropagationMatrix / recordEnergyUntilExit
  * (vamtoolbox/projector/pyTorchRayTrace.py:169-197, 573-690, 901-937,

@@ -135,3 +135,44 @@ def test_integrate_is_bitwise_repeatable(golden):
         assert torch.equal(P.forward_t(f), first)
     P.backward_t(torch.ones(P.plan.num_rays, device="cuda"))
     assert torch.equal(P.forward_t(f), first)
+
+
+def test_trajectory_cache_bitwise_and_invalidated(golden):
+    """With the trajectory cache (rays traced once, each step's position and attenuance kept) integrate
+    and deposit stream the records instead of re-tracing: the integrate gives the tracing kernel's bits,
+    the deposit its sums up to the order of its float32 atomics, the same count of rays active at the
+    cap; a new medium invalidates the cache, and a cache over its byte limit is refused without changing
+    the results."""
+    R = golden["raytrace"]
+    P = make_prop(R, "r3")
+    plan = P.plan
+    rng = np.random.default_rng(11)
+    f = torch.as_tensor(rng.uniform(size=plan.grid_shape), device="cuda", dtype=torch.float32)
+    w = torch.as_tensor(rng.uniform(size=plan.num_rays), device="cuda", dtype=torch.float32)
+    w[::7] = 0.0  # rays with no energy deposit nothing
+    g0, d0 = plan.integrate(f).clone(), plan.deposit(w).clone()
+    cap0 = plan.active_at_cap()
+    assert not plan.prepare_trajectories(limit_bytes=plan.trajectory_bytes() - 1)
+    assert torch.equal(plan.integrate(f), g0)
+    assert plan.prepare_trajectories()
+    assert plan.has_trajectories
+    for _ in range(2):
+        assert torch.equal(plan.integrate(f), g0)
+        assert plan.active_at_cap() == cap0
+        assert relL2(plan.deposit(w).cpu().numpy(), d0.cpu().numpy()) < 1e-5
+        assert plan.active_at_cap() == cap0
+    # a changed medium: the cache is dropped from use and the results follow the new medium
+    P2 = make_prop(R, "r3")
+    am_scale = 1.7
+    from vamtoolbox_b200 import medium
+
+    cv = P2.target_geo.constructCoordVec() if hasattr(P2, "target_geo") else None
+    im = medium.IndexModel(cv, type="interpolation", form="freeform", n_x=torch.as_tensor(R["r3_n"]))
+    am = medium.AttenuationModel(cv, type="interpolation", form="freeform",
+                                 alpha_x=torch.as_tensor(R["r3_alpha"] * am_scale))
+    plan.bind_medium(im, am, am)
+    P2.plan.bind_medium(im, am, am)
+    assert not plan.has_trajectories
+    assert torch.equal(plan.integrate(f), P2.plan.integrate(f))
+    assert relL2(plan.deposit(w).cpu().numpy(), P2.plan.deposit(w).cpu().numpy()) < 1e-5
+    plan.drop_trajectories()

@@ -134,6 +134,8 @@ _SIGS = {
     "vam_ray_deposit": ([_vp, _vp, _vp, _vp], _c_int),
     "vam_ray_grad_alpha": ([_vp, _vp, _vp, _vp, _vp, _vp], _c_int),
     "vam_ray_active_at_cap": ([_vp, ctypes.POINTER(_c_i64)], _c_int),
+    "vam_ray_prepare_trajectories": ([_vp, _c_i64, _vp], _c_int),
+    "vam_ray_drop_trajectories": ([_vp], _c_int),
     "vam_reduce_workspace_bytes": ([_c_i64], ctypes.c_size_t),
     "vam_reduce": ([_vp, _c_i64, _c_int, _vp, _vp, ctypes.c_size_t, _vp], _c_int),
     "vam_reduce_noalloc": ([_vp, _c_i64, _c_int, _vp, _vp], _c_int),

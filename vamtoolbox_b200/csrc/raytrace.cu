@@ -21,6 +21,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <string>
 
 #include "vam_internal.cuh"
 
@@ -42,6 +43,14 @@ struct vam_ray_plan {
     unsigned long long* d_active;  // rays active at the cap (last call)
     vam_ray_medium med;  // kinds and analytic parameters (pointers unused after bind)
     int has_medium;
+    // trajectory cache of the padded path (vam_ray_prepare_trajectories): per executed step of every ray its
+    // position x_ip1 and attenuance, [max_num_step][num_rays] float4 (step-major: a warp's rays are
+    // consecutive), the executed steps per ray and the rays active at the cap; valid until the medium changes
+    float4* d_traj;
+    int* d_traj_len;
+    unsigned long long* d_traj_active;
+    size_t traj_bytes;
+    int traj_valid;
 };
 
 namespace vam {
@@ -750,6 +759,138 @@ __global__ void __launch_bounds__(kRayThreads) k_ray_deposit_pad(RayArgs a, PadA
     if (st.active) atomicAdd(a.active, 1ULL);
 }
 
+// ---------------------------------------------------------------------------
+// Trajectory cache.  The rays' paths depend on the medium only, not on f or g, so
+// the padded path can trace them once (k_ray_record_pad: the same ray_step_pad
+// sequence and exit checks as the integrate / deposit kernels) and keep, per
+// executed step, x_ip1 and the attenuance; k_ray_integrate_traj and
+// k_ray_deposit_traj then stream those records and run only the corner work of a
+// step: the same corners_at / pad_corners on the same float32 values, the energy
+// E0 * exp(-attenuance) as ray_step_pad forms it, the same accumulation order, so
+// their results are bit-identical to the tracing kernels'.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kRayThreads) k_ray_record_pad(RayArgs a, PadArgs q, float4* __restrict__ traj,
+                                                                int* __restrict__ len,
+                                                                unsigned long long* __restrict__ active) {
+    const int64_t r = (int64_t)blockIdx.x * kRayThreads + threadIdx.x;
+    if (r >= a.nr) return;
+    RayState st;
+    ray_init<kCfgGridSymplectic>(a, r, 1.f, st);
+    int until_check = 0, n = 0;
+    for (int step = 0; step < a.max_steps; ++step) {
+        float ds;
+        ray_step_pad(a, q, st, ds);
+        __stcs(traj + (size_t)step * a.nr + r, make_float4(st.xp[0], st.xp[1], st.xp[2], st.att));
+        n = step + 1;
+        if (until_check == 0) {
+            until_check = a.check;
+            if (exited(a, st)) { st.active = false; break; }
+        }
+        --until_check;
+    }
+    len[r] = n;
+    if (st.active) atomicAdd(active, 1ULL);
+}
+
+__global__ void __launch_bounds__(kRayThreads) k_ray_integrate_traj(RayArgs a, PadArgs q, const float4* __restrict__ traj,
+                                                                    const int* __restrict__ len,
+                                                                    const float* __restrict__ fpad, float* __restrict__ g) {
+    const int64_t r = (int64_t)blockIdx.x * kRayThreads + threadIdx.x;
+    if (r >= a.nr) return;
+    const float E0 = a.energy0;
+    const int n = len[r];
+    float integral = 0.f;
+    float4 t = n > 0 ? __ldcs(traj + r) : make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int step = 0; step < n; ++step) {
+        // the next record in flight while this step's corners are gathered
+        const float4 tn = step + 1 < n ? __ldcs(traj + (size_t)(step + 1) * a.nr + r) : t;
+        const float xp[3] = {t.x, t.y, t.z};
+        const float E = E0 * __expf(-t.w);
+        Corners c;
+        corners_at(a, xp, c);
+        int o, dx, dy, dz;
+        float w[8];
+        if (pad_corners(a, q, c, a.h_idx * E, o, dx, dy, dz, w)) {
+            const float* f0 = fpad + o;
+            const float* f1 = f0 + dx;
+            integral = fmaf(__ldg(f0), w[0], integral);
+            integral = fmaf(__ldg(f1), w[1], integral);
+            integral = fmaf(__ldg(f0 + dy), w[2], integral);
+            integral = fmaf(__ldg(f1 + dy), w[3], integral);
+            integral = fmaf(__ldg(f0 + dz), w[4], integral);
+            integral = fmaf(__ldg(f1 + dz), w[5], integral);
+            integral = fmaf(__ldg(f0 + dy + dz), w[6], integral);
+            integral = fmaf(__ldg(f1 + dy + dz), w[7], integral);
+        }
+        t = tn;
+    }
+    g[r] = integral;
+}
+
+// The deposit from the records.  A warp's rays are consecutive z rows of one detector column and angle,
+// so at one step lane l's upper-z corners are, as a rule, lane l + 1's lower-z corners (same x / y cells,
+// z cell one higher): lane l + 1 then adds lane l's four upper weights to its own lower ones before its
+// atomics and lane l issues only its lower four, about halving the atomics (the deposit's bound once the
+// tracing is gone).  The sums are the tracing kernel's up to the order of float32 additions, which atomics
+// leave open anyway.  Lanes walk to the warp's longest record, inactive ones with no corners.
+__global__ void __launch_bounds__(kRayThreads) k_ray_deposit_traj(RayArgs a, PadArgs q, const float4* __restrict__ traj,
+                                                                  const int* __restrict__ len,
+                                                                  const float* __restrict__ gin, float* __restrict__ spad) {
+    const int64_t r = (int64_t)blockIdx.x * kRayThreads + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const bool in = r < a.nr;
+    const float E0 = in ? gin[r] : 0.f;
+    const int n = in && E0 != 0.f ? len[r] : 0;
+    const int nmax = __reduce_max_sync(0xffffffffu, n);
+    float4 t = n > 0 ? __ldcs(traj + r) : make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int step = 0; step < nmax; ++step) {
+        const bool live = step < n;
+        const float4 tn = step + 1 < n ? __ldcs(traj + (size_t)(step + 1) * a.nr + r) : t;
+        int o = 0, dx = 0, dy = 0, dz = 0;
+        float w[8];
+        bool ok = false;
+        if (live) {
+            const float xp[3] = {t.x, t.y, t.z};
+            const float E = E0 * __expf(-t.w);
+            Corners c;
+            corners_at(a, xp, c);
+            ok = pad_corners(a, q, c, a.h_idx * E, o, dx, dy, dz, w);
+        }
+        if (!ok) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) w[k] = 0.f;
+        }
+        // lane l - 1's upper corners onto this lane's lower ones
+        const int op = __shfl_up_sync(0xffffffffu, o, 1), dxp = __shfl_up_sync(0xffffffffu, dx, 1);
+        const int dyp = __shfl_up_sync(0xffffffffu, dy, 1), dzp = __shfl_up_sync(0xffffffffu, dz, 1);
+        const bool okp = __shfl_up_sync(0xffffffffu, ok, 1);
+        float up[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) up[k] = __shfl_up_sync(0xffffffffu, w[4 + k], 1);
+        const bool recv = lane > 0 && ok && okp && o == op + dzp && dx == dxp && dy == dyp;
+        const bool sent = __shfl_down_sync(0xffffffffu, recv, 1) && lane < 31;
+        if (ok) {
+            if (recv) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) w[k] += up[k];
+            }
+            float* s0 = spad + o;
+            float* s1 = s0 + dx;
+            atomicAdd(s0, w[0]);
+            atomicAdd(s1, w[1]);
+            atomicAdd(s0 + dy, w[2]);
+            atomicAdd(s1 + dy, w[3]);
+            if (!sent) {
+                atomicAdd(s0 + dz, w[4]);
+                atomicAdd(s1 + dz, w[5]);
+                atomicAdd(s0 + dy + dz, w[6]);
+                atomicAdd(s1 + dy + dz, w[7]);
+            }
+        }
+        t = tn;
+    }
+}
+
 // padded [nx+1][ny+1][nz+1] texels: the last plane of each axis repeated (border padding)
 __global__ void k_pad_n(const float4* __restrict__ src, float4* __restrict__ dst, int nx, int ny, int nz) {
     const int64_t n = (int64_t)(nx + 1) * (ny + 1) * (nz + 1);
@@ -940,6 +1081,9 @@ extern "C" int vam_ray_plan_destroy(vam_ray_plan* p) {
     cudaFree(p->d_apad);
     cudaFree(p->d_spad);
     cudaFree(p->d_active);
+    cudaFree(p->d_traj);
+    cudaFree(p->d_traj_len);
+    cudaFree(p->d_traj_active);
     delete p;
     return VAM_OK;
 }
@@ -983,6 +1127,7 @@ extern "C" int vam_ray_set_medium(vam_ray_plan* p, const vam_ray_medium* m, vam_
     p->med = *m;
     p->med.n_grid_dev = p->med.grad_n_grid_dev = p->med.atten_grid_dev = p->med.absorb_at_grid_dev = nullptr;
     p->has_medium = 1;
+    p->traj_valid = 0;  // the paths follow the medium: a cached trajectory set is stale now
     return VAM_OK;
 }
 
@@ -1000,6 +1145,13 @@ extern "C" int vam_ray_integrate(vam_ray_plan* p, const float* f, float* g, vam_
         // a deposit leaves values in the border of d_spad: zero it, then write the interior
         VAM_TRY_CUDA(cudaMemsetAsync(p->d_spad, 0, sizeof(float) * padded_voxels(p->g), st));
         k_pad_mul<<<ew_blocks(nv), 256, 0, st>>>(f, p->d_absorb, p->d_spad, p->g.n_x, p->g.n_y, p->g.n_z);
+        if (p->traj_valid) {
+            VAM_TRY_CUDA(cudaMemcpyAsync(p->d_active, p->d_traj_active, sizeof(unsigned long long),
+                                         cudaMemcpyDeviceToDevice, st));
+            k_ray_integrate_traj<<<nb, kRayThreads, 0, st>>>(a, make_pad_args(p), p->d_traj, p->d_traj_len, p->d_spad, g);
+            VAM_CHECK_LAUNCH("k_ray_integrate_traj");
+            return VAM_OK;
+        }
         k_ray_integrate_pad<<<nb, kRayThreads, 0, st>>>(a, make_pad_args(p), p->d_spad, g);
         VAM_CHECK_LAUNCH("k_ray_integrate_pad");
         return VAM_OK;
@@ -1024,8 +1176,15 @@ extern "C" int vam_ray_deposit(vam_ray_plan* p, const float* gin, float* dose, v
         // deposits of corners outside the grid land in the zero border and are not copied out; the
         // border is zeroed again by the next call's memset
         VAM_TRY_CUDA(cudaMemsetAsync(p->d_spad, 0, sizeof(float) * padded_voxels(p->g), st));
-        k_ray_deposit_pad<<<nb, kRayThreads, 0, st>>>(a, make_pad_args(p), gin, p->d_spad);
-        VAM_CHECK_LAUNCH("k_ray_deposit_pad");
+        if (p->traj_valid) {
+            VAM_TRY_CUDA(cudaMemcpyAsync(p->d_active, p->d_traj_active, sizeof(unsigned long long),
+                                         cudaMemcpyDeviceToDevice, st));
+            k_ray_deposit_traj<<<nb, kRayThreads, 0, st>>>(a, make_pad_args(p), p->d_traj, p->d_traj_len, gin, p->d_spad);
+            VAM_CHECK_LAUNCH("k_ray_deposit_traj");
+        } else {
+            k_ray_deposit_pad<<<nb, kRayThreads, 0, st>>>(a, make_pad_args(p), gin, p->d_spad);
+            VAM_CHECK_LAUNCH("k_ray_deposit_pad");
+        }
         k_unpad_mul<<<ew_blocks(nv), 256, 0, st>>>(p->d_spad, p->d_absorb, dose, p->g.n_x, p->g.n_y, p->g.n_z);
         VAM_CHECK_LAUNCH("k_unpad_mul");
         return VAM_OK;
@@ -1075,6 +1234,61 @@ extern "C" int vam_ray_active_at_cap(vam_ray_plan* p, int64_t* out) {
     unsigned long long v = 0;
     VAM_TRY_CUDA(cudaMemcpy(&v, p->d_active, sizeof(v), cudaMemcpyDeviceToHost));
     *out = (int64_t)v;
+    return VAM_OK;
+}
+
+extern "C" int vam_ray_prepare_trajectories(vam_ray_plan* p, int64_t limit_bytes, vam_stream_t stream) {
+    clear_error();
+    VAM_REQUIRE(p, VAM_ERR_ARG, "vam_ray_prepare_trajectories: null plan");
+    VAM_REQUIRE(p->has_medium, VAM_ERR_ARG, "vam_ray_prepare_trajectories: no medium bound (vam_ray_set_medium)");
+    DeviceGuard dg(p->g.device);
+    RayArgs a = make_args(p);
+    VAM_REQUIRE(padded_path(p, a), VAM_ERR_NOTSUP,
+                "vam_ray_prepare_trajectories: serves 3-D grid media with the physical path length and the "
+                "symplectic Euler solver");
+    const size_t steps = (size_t)std::max(a.max_steps, 1);
+    const size_t bytes = sizeof(float4) * steps * (size_t)p->g.num_rays + sizeof(int) * (size_t)p->g.num_rays;
+    VAM_REQUIRE(limit_bytes >= 0 && bytes <= (size_t)limit_bytes, VAM_ERR_NOTSUP,
+                "vam_ray_prepare_trajectories: the cache needs " + std::to_string(bytes) + " bytes, over the limit");
+    if (p->traj_bytes != bytes) {
+        cudaFree(p->d_traj);
+        cudaFree(p->d_traj_len);
+        p->d_traj = nullptr;
+        p->d_traj_len = nullptr;
+        p->traj_bytes = 0;
+        p->traj_valid = 0;
+        cudaError_t e = cudaMalloc(&p->d_traj, sizeof(float4) * steps * (size_t)p->g.num_rays);
+        if (e == cudaSuccess) e = cudaMalloc(&p->d_traj_len, sizeof(int) * (size_t)p->g.num_rays);
+        if (e != cudaSuccess) {
+            cudaFree(p->d_traj);
+            cudaFree(p->d_traj_len);
+            p->d_traj = nullptr;
+            p->d_traj_len = nullptr;
+            cudaGetLastError();
+            return set_error(VAM_ERR_NOMEM, std::string("vam_ray_prepare_trajectories: ") + cudaGetErrorString(e));
+        }
+        p->traj_bytes = bytes;
+    }
+    if (!p->d_traj_active) VAM_TRY_CUDA(cudaMalloc(&p->d_traj_active, sizeof(unsigned long long)));
+    cudaStream_t st = (cudaStream_t)stream;
+    VAM_TRY_CUDA(cudaMemsetAsync(p->d_traj_active, 0, sizeof(unsigned long long), st));
+    const unsigned nb = (unsigned)((p->g.num_rays + kRayThreads - 1) / kRayThreads);
+    k_ray_record_pad<<<nb, kRayThreads, 0, st>>>(a, make_pad_args(p), p->d_traj, p->d_traj_len, p->d_traj_active);
+    VAM_CHECK_LAUNCH("k_ray_record_pad");
+    p->traj_valid = 1;
+    return VAM_OK;
+}
+
+extern "C" int vam_ray_drop_trajectories(vam_ray_plan* p) {
+    clear_error();
+    VAM_REQUIRE(p, VAM_ERR_ARG, "vam_ray_drop_trajectories: null plan");
+    DeviceGuard dg(p->g.device);
+    cudaFree(p->d_traj);
+    cudaFree(p->d_traj_len);
+    p->d_traj = nullptr;
+    p->d_traj_len = nullptr;
+    p->traj_bytes = 0;
+    p->traj_valid = 0;
     return VAM_OK;
 }
 

@@ -235,6 +235,10 @@ class BCLPNorm:
             return (lambda g, out: plan.backward_ref(g, out), lambda x, out: plan.forward(x, out),
                     plan.shape_vol, plan.shape_sino, P.device)
         if plan is not None and hasattr(plan, "deposit"):
+            # the ray paths depend on the medium only: trace them once for the whole run when the cache
+            # fits (half of the free device memory), before any capture
+            if self.logs.options.n_iter > 1 and not getattr(plan, "has_trajectories", True):
+                plan.prepare_trajectories()
             return (lambda g, out: plan.deposit(g, out), lambda x, out: plan.integrate(x, out),
                     plan.grid_shape, (plan.num_rays,), P.device)
         if plan is not None and hasattr(P, "backward_t") and hasattr(P, "forward_t"):

@@ -145,6 +145,39 @@ class RayPlan:
             _lib.call("vam_ray_set_medium", self._h, ctypes.byref(m), _lib.stream_ptr(torch.cuda.current_stream(self.device)))
             torch.cuda.current_stream(self.device).synchronize()
         self._medium_keep = keep
+        self.has_trajectories = False  # a new medium makes the cached paths stale
+
+    def trajectory_bytes(self):
+        """Device bytes of the trajectory cache: 16 per ray and step of the cap, 4 per ray."""
+        return 16 * max(self.max_num_step, 1) * self.num_rays + 4 * self.num_rays
+
+    def prepare_trajectories(self, limit_bytes=None):
+        """Trace the rays once and keep every step's position and attenuance (vam_ray_prepare_trajectories),
+        so later integrate / deposit calls stream them instead of re-tracing (bit-identical results).  The
+        paths depend on the medium only.  ``limit_bytes`` defaults to half of the device's free memory.
+        Allocates: not during a graph capture.  False when the configuration has no cached path (it serves
+        3-D grid media, physical path length, symplectic Euler) or the cache exceeds the limit or the
+        device; the plan then keeps tracing."""
+        if limit_bytes is None:
+            free, _ = torch.cuda.mem_get_info(self.device)
+            limit_bytes = free // 2
+        try:
+            with torch.cuda.device(self.device):
+                _lib.call("vam_ray_prepare_trajectories", self._h, int(limit_bytes), self._s())
+                torch.cuda.current_stream(self.device).synchronize()
+        except _lib.VamError as exc:
+            if exc.code in (_lib.VAM_ERR_NOTSUP, _lib.VAM_ERR_NOMEM):
+                self.has_trajectories = False
+                return False
+            raise
+        self.has_trajectories = True
+        return True
+
+    def drop_trajectories(self):
+        """Free the trajectory cache (later calls trace again)."""
+        with torch.cuda.device(self.device):
+            _lib.call("vam_ray_drop_trajectories", self._h)
+        self.has_trajectories = False
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
