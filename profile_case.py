@@ -11,7 +11,8 @@
 adjoint (after building its weight table) on a random N x N x N volume with
 ``angles`` equally spaced over 360 degrees; ``ray`` runs integrate and deposit
 of the curved-ray tracer through a graded-index, attenuating N^3 medium
-(physical path length, forward symplectic Euler), ``angles`` angles;
+(physical path length, forward symplectic Euler), ``angles`` angles (with
+``--traj`` from the trajectory cache, filled once first);
 ``formats`` turns an N x angles x N float64 sinogram into 1920 x 1080 uint8
 projector frames (99.5th-percentile normalisation: select, then the frame
 kernel) and rebins it for a 300 px fan-beam vial; ``vec`` runs the
@@ -55,7 +56,7 @@ def run_parallel(n, na, calls, tuning, nz=None):
     return f"parallel {n}^2 x {nz} x {na}: tuning {p.get_tuning()}"
 
 
-def run_ray(n, na, calls):
+def run_ray(n, na, calls, traj=False):
     from vamtoolbox_b200 import geometry, medium, synthetic
     from vamtoolbox_b200.projector.pyTorchRayTrace import PyTorchRayTracingPropagator
 
@@ -74,11 +75,14 @@ def run_ray(n, na, calls):
     g = torch.Generator(device="cuda").manual_seed(0)
     f = torch.rand((n, n, n), device="cuda", generator=g)
     w = torch.rand(P.plan.num_rays, device="cuda", generator=g)
+    if traj and not P.plan.prepare_trajectories():
+        raise SystemExit("the trajectory cache does not fit")
     for _ in range(calls):
         P.forward_t(f)
         P.backward_t(w)
     torch.cuda.synchronize()
-    return f"ray {n}^3 x {na}: {P.plan.num_rays} rays, {P.plan.active_at_cap()} active at the step cap"
+    return (f"ray {n}^3 x {na}: {P.plan.num_rays} rays, {P.plan.active_at_cap()} active at the step cap"
+            + (f", trajectory cache {P.plan.trajectory_bytes()} B" if traj else ""))
 
 
 def summarize_launches(path):
@@ -187,6 +191,7 @@ def main(argv=None):
     ap.add_argument("--incline", type=float, default=15.0, help="vec case: ray inclination in degrees")
     ap.add_argument("--tuning", default="", help="comma list key=value of launch shapes (parallel case)")
     ap.add_argument("--direct", action="store_true", help="batch case: also run every call on its own")
+    ap.add_argument("--traj", action="store_true", help="ray case: trace once into the trajectory cache first")
     a = ap.parse_args(argv)
     if a.case == "summarize":
         print(summarize_launches(a.csv))
@@ -202,7 +207,7 @@ def main(argv=None):
     elif a.case == "formats":
         print(run_formats(a.size or 256, a.angles or 120, a.calls))
     else:
-        print(run_ray(a.size or 96, a.angles or 120, a.calls))
+        print(run_ray(a.size or 96, a.angles or 120, a.calls, a.traj))
 
 
 if __name__ == "__main__":
