@@ -44,7 +44,7 @@ struct vam_ray_plan {
     vam_ray_medium med;  // kinds and analytic parameters (pointers unused after bind)
     int has_medium;
     // trajectory cache of the padded path (vam_ray_prepare_trajectories): per executed step of every ray its
-    // position x_ip1 and attenuance, [max_num_step][num_rays] float4 (step-major: a warp's rays are
+    // position x_ip1 and exp(-attenuance), [max_num_step][num_rays] float4 (step-major: a warp's rays are
     // consecutive), the executed steps per ray and the rays active at the cap; valid until the medium changes
     float4* d_traj;
     int* d_traj_len;
@@ -763,11 +763,12 @@ __global__ void __launch_bounds__(kRayThreads) k_ray_deposit_pad(RayArgs a, PadA
 // Trajectory cache.  The rays' paths depend on the medium only, not on f or g, so
 // the padded path can trace them once (k_ray_record_pad: the same ray_step_pad
 // sequence and exit checks as the integrate / deposit kernels) and keep, per
-// executed step, x_ip1 and the attenuance; k_ray_integrate_traj and
+// executed step, x_ip1 and exp(-attenuance); k_ray_integrate_traj and
 // k_ray_deposit_traj then stream those records and run only the corner work of a
 // step: the same corners_at / pad_corners on the same float32 values, the energy
-// E0 * exp(-attenuance) as ray_step_pad forms it, the same accumulation order, so
-// their results are bit-identical to the tracing kernels'.
+// E0 * exp(-attenuance) as ray_step_pad forms it (the same exponential, recorded),
+// the same accumulation order, so their results are bit-identical to the tracing
+// kernels'.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kRayThreads) k_ray_record_pad(RayArgs a, PadArgs q, float4* __restrict__ traj,
                                                                 int* __restrict__ len,
@@ -780,7 +781,7 @@ __global__ void __launch_bounds__(kRayThreads) k_ray_record_pad(RayArgs a, PadAr
     for (int step = 0; step < a.max_steps; ++step) {
         float ds;
         ray_step_pad(a, q, st, ds);
-        __stcs(traj + (size_t)step * a.nr + r, make_float4(st.xp[0], st.xp[1], st.xp[2], st.att));
+        __stcs(traj + (size_t)step * a.nr + r, make_float4(st.xp[0], st.xp[1], st.xp[2], __expf(-st.att)));
         n = step + 1;
         if (until_check == 0) {
             until_check = a.check;
@@ -805,7 +806,7 @@ __global__ void __launch_bounds__(kRayThreads) k_ray_integrate_traj(RayArgs a, P
         // the next record in flight while this step's corners are gathered
         const float4 tn = step + 1 < n ? __ldcs(traj + (size_t)(step + 1) * a.nr + r) : t;
         const float xp[3] = {t.x, t.y, t.z};
-        const float E = E0 * __expf(-t.w);
+        const float E = E0 * t.w;
         Corners c;
         corners_at(a, xp, c);
         int o, dx, dy, dz;
@@ -851,7 +852,7 @@ __global__ void __launch_bounds__(kRayThreads) k_ray_deposit_traj(RayArgs a, Pad
         bool ok = false;
         if (live) {
             const float xp[3] = {t.x, t.y, t.z};
-            const float E = E0 * __expf(-t.w);
+            const float E = E0 * t.w;
             Corners c;
             corners_at(a, xp, c);
             ok = pad_corners(a, q, c, a.h_idx * E, o, dx, dy, dz, w);
