@@ -468,3 +468,39 @@ def test_backprojection_table_bitwise_and_oracle(shape, na, mode):
         assert torch.equal(computed, tabled), vz
     assert relL2(tabled.cpu().numpy(), O.parallel_backward_ref(b, ang, absorption=oabs)) < TOL
     assert p.status() == 0
+
+
+@pytest.mark.parametrize("shape,na,absn", [((33, 33, 192), 29, None), ((24, 24, 384), 36, "ray"),
+                                           ((30, 30, 192), 40, "mask")])
+def test_six_slice_lanes_bitwise(shape, na, absn):
+    """Six slices per lane (a float4 and a float2 per lane: 192-slice chunks fill every lane where
+    256-slice ones would not) give the eight-slice kernels' sums bit for bit: the forward (paired and
+    unpaired angles, per-ray and mask absorption) and the block-table backprojection, and the oracle's."""
+    rng = np.random.default_rng(sum(shape) + na)
+    ang = np.linspace(0, 360, na, endpoint=False) + 0.9
+    x = rng.uniform(0, 1, shape)
+    b = rng.uniform(0, 1, (shape[0], na, shape[2]))
+    p = plan_for(shape, ang)
+    oabs = None
+    if absn == "ray":
+        p.set_absorption("ray", alpha_per_px=0.04, radius_px=shape[0] / 2 - 1.0)
+        oabs = ("ray", 0.04, shape[0] / 2 - 1.0)
+    elif absn == "mask":
+        m = rng.uniform(0.2, 1.0, shape[:2])
+        p.set_absorption("mask", mask=m)
+        oabs = ("mask", m)
+    p.set_tuning({"forward_vz": 8})
+    f8 = p.forward(dev(x))
+    p.set_tuning({"forward_vz": 6})
+    f6 = p.forward(dev(x))
+    p.set_tuning({"forward_vz": 0})
+    f0 = p.forward(dev(x))
+    assert torch.equal(f6, f8) and torch.equal(f0, f8)
+    assert relL2(f6.cpu().numpy(), O.parallel_forward(x, ang, absorption=oabs)) < TOL
+    if absn != "ray":
+        p.set_tuning({"backward_vz": 8, "backward_table": 0})
+        computed = p.backward_ref(dev(b))
+        assert p.prepare_backward()
+        p.set_tuning({"backward_vz": 0, "backward_table": 1})  # automatic: six slices on 192-slice chunks
+        assert torch.equal(p.backward_ref(dev(b)), computed)
+    assert p.status() == 0
