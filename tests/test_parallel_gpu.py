@@ -470,12 +470,14 @@ def test_backprojection_table_bitwise_and_oracle(shape, na, mode):
     assert p.status() == 0
 
 
-@pytest.mark.parametrize("shape,na,absn", [((33, 33, 192), 29, None), ((24, 24, 384), 36, "ray"),
-                                           ((30, 30, 192), 40, "mask")])
-def test_six_slice_lanes_bitwise(shape, na, absn):
-    """Six slices per lane (a float4 and a float2 per lane: 192-slice chunks fill every lane where
-    256-slice ones would not) give the eight-slice kernels' sums bit for bit: the forward (paired and
-    unpaired angles, per-ray and mask absorption) and the block-table backprojection, and the oracle's."""
+@pytest.mark.parametrize("shape,na,absn,vz", [((33, 33, 192), 29, None, 6), ((24, 24, 384), 36, "ray", 6),
+                                              ((30, 30, 192), 40, "mask", 6), ((28, 28, 160), 31, None, 5),
+                                              ((26, 26, 320), 24, "mask", 5), ((22, 22, 160), 30, "ray", 5)])
+def test_six_slice_lanes_bitwise(shape, na, absn, vz):
+    """Six / five slices per lane (a float4 and a float2 / a float per lane: 192- / 160-slice chunks fill
+    every lane where 256-slice ones would not) give the eight-slice kernels' sums bit for bit: the forward
+    (paired and unpaired angles, per-ray and mask absorption) and the block-table backprojection, and the
+    oracle's."""
     rng = np.random.default_rng(sum(shape) + na)
     ang = np.linspace(0, 360, na, endpoint=False) + 0.9
     x = rng.uniform(0, 1, shape)
@@ -491,7 +493,7 @@ def test_six_slice_lanes_bitwise(shape, na, absn):
         oabs = ("mask", m)
     p.set_tuning({"forward_vz": 8})
     f8 = p.forward(dev(x))
-    p.set_tuning({"forward_vz": 6})
+    p.set_tuning({"forward_vz": vz})
     f6 = p.forward(dev(x))
     p.set_tuning({"forward_vz": 0})
     f0 = p.forward(dev(x))
@@ -501,6 +503,6 @@ def test_six_slice_lanes_bitwise(shape, na, absn):
         p.set_tuning({"backward_vz": 8, "backward_table": 0})
         computed = p.backward_ref(dev(b))
         assert p.prepare_backward()
-        p.set_tuning({"backward_vz": 0, "backward_table": 1})  # automatic: six slices on 192-slice chunks
+        p.set_tuning({"backward_vz": 0, "backward_table": 1})  # automatic: six / five slices per lane
         assert torch.equal(p.backward_ref(dev(b)), computed)
     assert p.status() == 0

@@ -21,11 +21,11 @@ import torch
 
 from . import _lib
 
-# slices per lane: 1 = the generic kernel, 4 / 8 = the fast kernels (nZ % 4 == 0), 6 = the fast forward
-# on 192-slice chunks (nZ % 192 == 0)
-FORWARD_VZ = (1, 4, 6, 8)
+# slices per lane: 1 = the generic kernel, 4 / 8 = the fast kernels (nZ % 4 == 0), 6 / 5 = the fast forward
+# on 192- / 160-slice chunks (nZ % 192 == 0 / nZ % 160 == 0)
+FORWARD_VZ = (1, 4, 5, 6, 8)
 # (slices per lane, angles per batch, bin table): the block table serves four or eight slices per lane,
-# and 0 (automatic) adds six on 192-slice chunks
+# and 0 (automatic) adds six / five on 192- / 160-slice chunks
 BACKWARD = ((1, 1, 0), (4, 1, 0), (8, 1, 0), (4, 2, 0), (8, 2, 0), (4, 4, 0), (4, 2, 1), (8, 2, 1), (0, 2, 1))
 ADJOINT = ((1, 0), (4, 1), (8, 1), (4, 0), (8, 0))           # (slices per lane, weight table on)
 
@@ -92,7 +92,7 @@ def measure(plan, reps=3, warm=1, ops=("forward", "backward", "adjoint")):
         times = {"forward": {}, "backward": {}, "adjoint": {}}
         base = plan.get_tuning()
         for vz in FORWARD_VZ if "forward" in ops else ():
-            if vz == 6 and plan.shape_vol[2] % 192:
+            if (vz == 6 and plan.shape_vol[2] % 192) or (vz == 5 and plan.shape_vol[2] % 160):
                 continue
             plan.set_tuning(dict(base, forward_vz=vz))
             times["forward"][str(vz)] = _time(lambda: plan.forward(x, ob), reps, warm)

@@ -288,14 +288,20 @@ struct Acc {
 // a warp owns slices zbase + 4l + 128q + (0..3), q < Q, so every float4 load
 // of the warp covers 512 contiguous bytes (four 128-byte lines).  p points at
 // the lane's first slice; qn is the number of its vectors inside the volume.
-// Six slices per lane (192-slice chunks, full chunks only): a float4 at
-// zbase + 4l and a float2 at zbase + 128 + 2l (a 256-byte run per warp).
+// Six / five slices per lane (192- / 160-slice chunks, full chunks only): a
+// float4 at zbase + 4l and a float2 at zbase + 128 + 2l or a float at
+// zbase + 128 + l (a 256- / 128-byte run per warp).
 template <int VZ>
 __device__ __forceinline__ void load_vz(const float* __restrict__ p, float* d, int qn = VZ / 4) {
-    if constexpr (VZ == 6) {
+    if constexpr (VZ == 6 || VZ == 5) {
         const float4 t = __ldg(reinterpret_cast<const float4*>(p));
-        const float2 u = __ldg(reinterpret_cast<const float2*>(p + 128 - 2 * (int)(threadIdx.x & 31)));
-        d[0] = t.x; d[1] = t.y; d[2] = t.z; d[3] = t.w; d[4] = u.x; d[5] = u.y;
+        d[0] = t.x; d[1] = t.y; d[2] = t.z; d[3] = t.w;
+        if constexpr (VZ == 6) {
+            const float2 u = __ldg(reinterpret_cast<const float2*>(p + 128 - 2 * (int)(threadIdx.x & 31)));
+            d[4] = u.x; d[5] = u.y;
+        } else {
+            d[4] = __ldg(p + 128 - 3 * (int)(threadIdx.x & 31));
+        }
         return;
     }
 #pragma unroll
@@ -310,14 +316,19 @@ __device__ __forceinline__ void load_vz(const float* __restrict__ p, float* d, i
 // the CTA read again (1.406 -> 1.373 ms at 256^3 x 360, identical results)
 template <int VZ>
 __device__ __forceinline__ void load_vz_keep(const float* __restrict__ p, float* d, int qn = VZ / 4) {
-    if constexpr (VZ == 6) {
+    if constexpr (VZ == 6 || VZ == 5) {
         float4 t;
-        float2 u;
         asm("ld.global.nc.L1::evict_last.v4.f32 {%0, %1, %2, %3}, [%4];"
             : "=f"(t.x), "=f"(t.y), "=f"(t.z), "=f"(t.w) : "l"(p));
-        asm("ld.global.nc.L1::evict_last.v2.f32 {%0, %1}, [%2];"
-            : "=f"(u.x), "=f"(u.y) : "l"(p + 128 - 2 * (int)(threadIdx.x & 31)));
-        d[0] = t.x; d[1] = t.y; d[2] = t.z; d[3] = t.w; d[4] = u.x; d[5] = u.y;
+        d[0] = t.x; d[1] = t.y; d[2] = t.z; d[3] = t.w;
+        if constexpr (VZ == 6) {
+            float2 u;
+            asm("ld.global.nc.L1::evict_last.v2.f32 {%0, %1}, [%2];"
+                : "=f"(u.x), "=f"(u.y) : "l"(p + 128 - 2 * (int)(threadIdx.x & 31)));
+            d[4] = u.x; d[5] = u.y;
+        } else {
+            asm("ld.global.nc.L1::evict_last.f32 %0, [%1];" : "=f"(d[4]) : "l"(p + 128 - 3 * (int)(threadIdx.x & 31)));
+        }
         return;
     }
 #pragma unroll
@@ -332,9 +343,10 @@ __device__ __forceinline__ void load_vz_keep(const float* __restrict__ p, float*
 
 template <int VZ>
 __device__ __forceinline__ void store_vz(float* __restrict__ p, const float* d, int qn) {
-    if constexpr (VZ == 6) {
+    if constexpr (VZ == 6 || VZ == 5) {
         *reinterpret_cast<float4*>(p) = make_float4(d[0], d[1], d[2], d[3]);
-        *reinterpret_cast<float2*>(p + 128 - 2 * (int)(threadIdx.x & 31)) = make_float2(d[4], d[5]);
+        if constexpr (VZ == 6) *reinterpret_cast<float2*>(p + 128 - 2 * (int)(threadIdx.x & 31)) = make_float2(d[4], d[5]);
+        else p[128 - 3 * (int)(threadIdx.x & 31)] = d[4];
         return;
     }
 #pragma unroll
@@ -342,12 +354,12 @@ __device__ __forceinline__ void store_vz(float* __restrict__ p, const float* d, 
         if (q < qn) *reinterpret_cast<float4*>(p + 128 * q) = make_float4(d[4 * q], d[4 * q + 1], d[4 * q + 2], d[4 * q + 3]);
 }
 
-// First slice and number of in-range vectors of a lane in z-chunk zc (six slices per lane: full chunks,
-// qn = 2 vectors).
+// First slice and number of in-range vectors of a lane in z-chunk zc (six / five slices per lane: full
+// chunks, qn = 2 vectors).
 template <int VZ>
 __device__ __forceinline__ void lane_z(int zc, int lane, int nZ, int& z0, int& qn) {
     const int base = zc * 32 * VZ + 4 * lane;
-    if constexpr (VZ == 6) {
+    if constexpr (VZ == 6 || VZ == 5) {
         z0 = base;
         qn = 2;
         return;
@@ -938,12 +950,13 @@ __global__ void __launch_bounds__(256) k_bwd_btable(const double4* __restrict__ 
 
 __device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
-// A lane's slices of one detector row: VZ / 4 float4 vectors at 4 l + 128 q (VZ = 4, 8), or, for six
-// slices per lane (192-slice chunks), a float4 at 4 l and a float2 at 128 + 2 l.
+// A lane's slices of one detector row: VZ / 4 float4 vectors at 4 l + 128 q (VZ = 4, 8), or a float4
+// at 4 l and a float2 at 128 + 2 l (VZ = 6, 192-slice chunks) or a float at 128 + l (VZ = 5, 160-slice
+// chunks).  The slice pairs of the packed FMAs: (VZ + 1) / 2, the fifth slice paired with a zero.
 template <int VZ>
 struct RowV {
     float4 v[VZ / 4];
-    float2 t;  // VZ == 6 only
+    float2 t;  // VZ == 6, 5 (t.y = 0 for VZ == 5)
 };
 
 // the lane's vectors of one detector row (p: the row at the lane's first slice); vectors q >= qn (past
@@ -953,6 +966,9 @@ __device__ __forceinline__ void load_row(RowV<VZ>& r, const float* __restrict__ 
     if constexpr (VZ == 6) {
         r.v[0] = __ldg(reinterpret_cast<const float4*>(p));
         r.t = __ldg(reinterpret_cast<const float2*>(p + 128 - 2 * (int)(threadIdx.x & 31)));
+    } else if constexpr (VZ == 5) {
+        r.v[0] = __ldg(reinterpret_cast<const float4*>(p));
+        r.t = make_float2(__ldg(p + 128 - 3 * (int)(threadIdx.x & 31)), 0.f);
     } else {
 #pragma unroll
         for (int q = 0; q < VZ / 4; ++q)
@@ -962,7 +978,7 @@ __device__ __forceinline__ void load_row(RowV<VZ>& r, const float* __restrict__ 
 
 // acc (slice pairs) += (1 - w) * r0 then += w * r1: two packed FMAs per pair
 template <int VZ>
-__device__ __forceinline__ void lerp_rows(unsigned long long (&acc)[VZ / 2], float w, const RowV<VZ>& r0,
+__device__ __forceinline__ void lerp_rows(unsigned long long (&acc)[(VZ + 1) / 2], float w, const RowV<VZ>& r0,
                                           const RowV<VZ>& r1) {
     const unsigned long long w0 = pk_pair(1.f - w, 1.f - w), w1 = pk_pair(w, w);
 #pragma unroll
@@ -970,13 +986,13 @@ __device__ __forceinline__ void lerp_rows(unsigned long long (&acc)[VZ / 2], flo
         fma_pair(acc[2 * q], w0, r0.v[q].x, r0.v[q].y);
         fma_pair(acc[2 * q + 1], w0, r0.v[q].z, r0.v[q].w);
     }
-    if constexpr (VZ == 6) fma_pair(acc[2], w0, r0.t.x, r0.t.y);
+    if constexpr (VZ == 6 || VZ == 5) fma_pair(acc[2], w0, r0.t.x, r0.t.y);
 #pragma unroll
     for (int q = 0; q < VZ / 4; ++q) {
         fma_pair(acc[2 * q], w1, r1.v[q].x, r1.v[q].y);
         fma_pair(acc[2 * q + 1], w1, r1.v[q].z, r1.v[q].w);
     }
-    if constexpr (VZ == 6) fma_pair(acc[2], w1, r1.t.x, r1.t.y);
+    if constexpr (VZ == 6 || VZ == 5) fma_pair(acc[2], w1, r1.t.x, r1.t.y);
 }
 
 // one warp per (2 x 2 block, z chunk of 32 VZ slices); FULL: nZ a multiple of 32 VZ, else the lanes
@@ -1002,13 +1018,14 @@ __device__ __forceinline__ void k_backward_blk_body(const Args& a, const int4* _
     if (bi >= nby || bj >= nbx) return;
     const long blk = (long)bi * nbx + bj;
     int z0 = zc * 32 * VZ + 4 * lane, qn = VZ / 4;
-    static_assert(VZ != 6 || FULL, "six slices per lane: full 192-slice chunks only");
+    static_assert((VZ != 6 && VZ != 5) || FULL, "six / five slices per lane: full chunks only");
     if constexpr (!FULL) lane_z<VZ>(zc, lane, a.nZ, z0, qn);
-    unsigned long long acc[4][VZ / 2];
+    constexpr int NP = (VZ + 1) / 2;  // slice pairs
+    unsigned long long acc[4][NP];
 #pragma unroll
     for (int q = 0; q < 4; ++q)
 #pragma unroll
-        for (int e = 0; e < VZ / 2; ++e) acc[q][e] = 0ull;
+        for (int e = 0; e < NP; ++e) acc[q][e] = 0ull;
     const int pc = bcidx[blk];
     if (pc >= 0) {
         const int rs = a.nA * a.nZ;
@@ -1112,9 +1129,9 @@ __device__ __forceinline__ void k_backward_blk_body(const Args& a, const int4* _
         const int i = 2 * bi + (q >> 1), j = 2 * bj + (q & 1);
         if (i >= a.nY || j >= a.nX) continue;
         const long p = (long)i * a.nX + j;
-        float v[VZ];
+        float v[2 * NP];
 #pragma unroll
-        for (int e2 = 0; e2 < VZ / 2; ++e2)
+        for (int e2 = 0; e2 < NP; ++e2)
             asm("mov.b64 {%0, %1}, %2;" : "=f"(v[2 * e2]), "=f"(v[2 * e2 + 1]) : "l"(acc[q][e2]));
         if (a.mask) {
             const float m = __ldg(a.mask + p);
@@ -1127,6 +1144,9 @@ __device__ __forceinline__ void k_backward_blk_body(const Args& a, const int4* _
         if constexpr (VZ == 6) {
             __stcs(reinterpret_cast<float4*>(dst), make_float4(v[0], v[1], v[2], v[3]));
             __stcs(reinterpret_cast<float2*>(dst + 128 - 2 * lane), make_float2(v[4], v[5]));
+        } else if constexpr (VZ == 5) {
+            __stcs(reinterpret_cast<float4*>(dst), make_float4(v[0], v[1], v[2], v[3]));
+            __stcs(dst + 128 - 3 * lane, v[4]);
         } else {
 #pragma unroll
             for (int q2 = 0; q2 < VZ / 4; ++q2)
@@ -1988,9 +2008,11 @@ int describe(vam_parallel_plan* plan, Op op, const float* in, float* out, Item& 
         }
         return VAM_OK;
     }
-    // the forward's slices per lane: also six where 192-slice chunks fill every lane (tuned to 6, or
-    // automatic when 256-slice chunks would not)
-    const int fvz = fast_ok && plan->nZ % 192 == 0 && (want == 6 || (want == 0 && plan->nZ % 256 != 0)) ? 6 : vzf;
+    // the forward's slices per lane: also six / five where 192- / 160-slice chunks fill every lane
+    // (tuned to 6 / 5, or automatic when 256-slice chunks would not)
+    int fvz = vzf;
+    if (fast_ok && plan->nZ % 192 == 0 && (want == 6 || (want == 0 && plan->nZ % 256 != 0))) fvz = 6;
+    else if (fast_ok && plan->nZ % 160 == 0 && (want == 5 || (want == 0 && plan->nZ % 256 != 0))) fvz = 5;
     if (op == Op::Forward && !plan->has_occ && (long)plan->nY * plan->nX * plan->nZ < (1L << 31) && fvz) {
         FastArgs& a = it.f;
         a.vol = in;
@@ -2012,13 +2034,17 @@ int describe(vam_parallel_plan* plan, Op op, const float* in, float* out, Item& 
         it.gy = (unsigned)(ray ? plan->nA : plan->n_tasks_paired);
         return VAM_OK;
     }
-    if (op != Op::Forward && !plan->has_occ && vzf && !noclip &&
+    // the block-table backprojection serves every nZ % 4 == 0, also where the automatic width of the
+    // computed-bin kernels would fall back to the generic kernel (too many idle lanes)
+    const bool blk_ok = op == Op::BackwardRef && fast_ok && !ray && plan->d_bwd_btab && plan->tune_bwd_table;
+    if (op != Op::Forward && !plan->has_occ && (vzf || blk_ok) && !noclip &&
         (long long)plan->nY * plan->nA * plan->nZ < (1LL << 31)) {
         Args& a = it.a;
         a.in = in; a.out = out; a.trig = plan->d_trig; a.circle = plan->d_circle;
         a.mask = plan->abs_mode == VAM_ABS_MASK ? plan->d_mask : nullptr;
         a.nY = plan->nY; a.nX = plan->nX; a.nZ = plan->nZ; a.nA = plan->nA; a.C = plan->C;
-        a.zchunks = (plan->nZ + 32 * vzf - 1) / (32 * vzf);
+        const int vzc = vzf ? vzf : 4;  // vzf == 0 only where the block table serves the call (blk_ok)
+        a.zchunks = (plan->nZ + 32 * vzc - 1) / (32 * vzc);
         a.alpha = plan->abs_alpha; a.R = plan->abs_R;
         const long items = (long)plan->nY * plan->nX * a.zchunks;
         it.gx = (unsigned)((items + kWarpsPerBlock - 1) / kWarpsPerBlock);
@@ -2026,14 +2052,15 @@ int describe(vam_parallel_plan* plan, Op op, const float* in, float* out, Item& 
         if (op == Op::BackwardRef) {
             // the batched kernel stages cos / sin of every angle in shared memory (16 B per angle)
             const int batch = (size_t)plan->nA * sizeof(double2) <= 48 * 1024 ? plan->tune_bwd_batch : 1;
-            if (!ray && plan->d_bwd_btab && plan->tune_bwd_table) {
+            if (blk_ok) {
                 // the 2 x 2 block table: slices per lane as tuned (4 or 8), else eight for full 256-slice
-                // chunks, six for full 192-slice chunks, eight from 160 slices up, four below
+                // chunks, six / five for full 192- / 160-slice chunks, eight from 160 slices up, four below
                 // (256^3 x 360: 0.92 / 1.41 ms with 8 / 4; 192^3 x 720: 1.46 / 1.94; 96^3 x 720: 0.42 / 0.31)
                 int bvz = 4;
                 if (plan->tune_bwd_vz == 8 || plan->tune_bwd_vz == 4) bvz = plan->tune_bwd_vz;
                 else if (plan->nZ % 256 == 0) bvz = 8;
                 else if (plan->nZ % 192 == 0) bvz = 6;
+                else if (plan->nZ % 160 == 0) bvz = 5;
                 else if (plan->nZ >= 160) bvz = 8;
                 it.kind = KB_BTABLE;
                 it.vz = bvz;
@@ -2106,6 +2133,7 @@ __device__ __forceinline__ void fast_body(const Item& it, unsigned bx, unsigned 
             const FastArgs f = it.f;
             if (it.vz == 8) k_forward_fast_body<8, RAY>(f, bx, by);
             else if (it.vz == 6) k_forward_fast_body<6, RAY>(f, bx, by);
+            else if (it.vz == 5) k_forward_fast_body<5, RAY>(f, bx, by);
             else k_forward_fast_body<4, RAY>(f, bx, by);
         }
     }
@@ -2122,6 +2150,7 @@ __device__ __forceinline__ void fast_body(const Item& it, unsigned bx, unsigned 
             const bool full = a.nZ % (32 * it.vz) == 0;
             if (it.vz == 8) { if (full) k_backward_blk_body<8, true>(a, it.btab4, it.bcidx, bx); else k_backward_blk_body<8, false>(a, it.btab4, it.bcidx, bx); }
             else if (it.vz == 6) k_backward_blk_body<6, true>(a, it.btab4, it.bcidx, bx);
+            else if (it.vz == 5) k_backward_blk_body<5, true>(a, it.btab4, it.bcidx, bx);
             else { if (full) k_backward_blk_body<4, true>(a, it.btab4, it.bcidx, bx); else k_backward_blk_body<4, false>(a, it.btab4, it.bcidx, bx); }
         }
     }
@@ -2248,6 +2277,7 @@ void launch_fast(const Item& it, dim3 grid, cudaStream_t st) {
         case KF_FAST:
             if (it.vz == 8) k_forward_fast<8, RAY><<<grid, block, 0, st>>>(it.f);
             else if (it.vz == 6) k_forward_fast<6, RAY><<<grid, block, 0, st>>>(it.f);
+            else if (it.vz == 5) k_forward_fast<5, RAY><<<grid, block, 0, st>>>(it.f);
             else k_forward_fast<4, RAY><<<grid, block, 0, st>>>(it.f);
             break;
         case KB_BATCHED:
@@ -2295,6 +2325,8 @@ int launch_item(const Item& it, cudaStream_t st, const char* name) {
             else k_backward_blk<8, 3, false><<<grid, block, 0, st>>>(it.a, it.btab4, it.bcidx);
         } else if (it.vz == 6) {
             k_backward_blk<6, 3, true><<<grid, block, 0, st>>>(it.a, it.btab4, it.bcidx);
+        } else if (it.vz == 5) {
+            k_backward_blk<5, 3, true><<<grid, block, 0, st>>>(it.a, it.btab4, it.bcidx);
         } else {
             if (full) k_backward_blk<4, 3, true><<<grid, block, 0, st>>>(it.a, it.btab4, it.bcidx);
             else k_backward_blk<4, 3, false><<<grid, block, 0, st>>>(it.a, it.btab4, it.bcidx);
@@ -2671,9 +2703,10 @@ extern "C" int vam_parallel_set_tuning(vam_parallel_plan* p, const vam_parallel_
     clear_error();
     VAM_REQUIRE(p && t, VAM_ERR_ARG, "vam_parallel_set_tuning: null argument");
     auto vz_ok = [](int v) { return v == 0 || v == 1 || v == 4 || v == 8; };
-    VAM_REQUIRE((vz_ok(t->forward_vz) || t->forward_vz == 6) && vz_ok(t->backward_vz) && vz_ok(t->adjoint_vz),
+    VAM_REQUIRE((vz_ok(t->forward_vz) || t->forward_vz == 6 || t->forward_vz == 5) && vz_ok(t->backward_vz) &&
+                    vz_ok(t->adjoint_vz),
                 VAM_ERR_ARG, "vam_parallel_set_tuning: vector widths must be 0 (auto), 1 (generic kernel), 4 or 8 "
-                "(the forward also 6)");
+                "(the forward also 6 or 5)");
     VAM_REQUIRE(t->backward_batch == 0 || t->backward_batch == 1 || t->backward_batch == 2 || t->backward_batch == 4,
                 VAM_ERR_ARG, "vam_parallel_set_tuning: backward_batch must be 0 (auto), 1, 2 or 4");
     p->tune_fwd_vz = t->forward_vz;
