@@ -182,20 +182,25 @@ def _copy_pool():
 
 def to_device_f64(array, device):
     """A host array as a float64 device tensor, staged through a page-locked buffer of torch's caching
-    host allocator that several threads fill in slices (numpy releases the GIL for plain copies), then one
-    asynchronous copy on the current stream.  A pageable upload of a 256^3 float64 target ran at about
-    10 GB/s (13 ms); the allocator keeps the staging block alive until the copy has run."""
+    host allocator that several threads fill in chunks (numpy releases the GIL for plain copies); each
+    chunk's asynchronous copy on the current stream is issued as soon as that chunk is staged, so the
+    host copy and the transfer overlap.  A pageable upload of a 256^3 float64 target ran at about
+    10 GB/s (13 ms), staged then copied whole about 7 ms; the allocator keeps the staging block alive
+    until the copies have run."""
     a = np.ascontiguousarray(array, dtype=np.float64)
     if a.nbytes < (8 << 20):
         return torch.as_tensor(a).to(device)
     h = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+    d = torch.empty(a.shape, dtype=torch.float64, device=device)
+    hf, df = h.view(-1), d.view(-1)
     dst, src = h.numpy().reshape(-1), a.reshape(-1)
     pool = _copy_pool()
-    step = -(-src.size // pool._max_workers)
+    step = -(-src.size // (4 * pool._max_workers))
     spans = [(lo, min(lo + step, src.size)) for lo in range(0, src.size, step)]
-    list(pool.map(lambda sp: np.copyto(dst[sp[0]:sp[1]], src[sp[0]:sp[1]]), spans))
-    d = torch.empty(a.shape, dtype=torch.float64, device=device)
-    d.copy_(h, non_blocking=True)
+    staged = [pool.submit(np.copyto, dst[lo:hi], src[lo:hi]) for lo, hi in spans]
+    for (lo, hi), f in zip(spans, staged):
+        f.result()
+        df[lo:hi].copy_(hf[lo:hi], non_blocking=True)
     return d
 
 
