@@ -376,11 +376,11 @@ int vam_spectrum_scale(void* spectrum_dev, const double* filter_dev, int64_t n_f
 int vam_filter_epilogue(const double* y_dev, int64_t n_rows, int64_t m, double scale, int has_lo, double lo,
                         int has_hi, double hi, float* out_dev, vam_stream_t stream);
 
-/* Same reduction as vam_reduce for callers that cannot allocate device memory
- * (code running between cudaStreamBeginCapture and EndCapture in global
- * capture mode, where cudaMalloc is not permitted, or a host that reserves
- * all device memory up front and must not trigger cudaMalloc's implicit
- * synchronisation while a print is exposing).  No counterpart in the
+/* Same reduction as vam_reduce for callers that cannot allocate device memory:
+ * a printer host that reserves all device memory for its projection buffers
+ * before a print starts, so cudaMalloc would fail, and that must not trigger
+ * cudaMalloc's implicit device synchronisation while a layer is exposing; or
+ * a plug-in that is handed fixed buffers and has no allocator of its own.  No counterpart in the
  * reference.  Its scratch is one static device array of 4096 doubles (32 KiB)
  * inside the library, held on every GPU that loads it until process exit; one
  * partial per 2048 inputs, so n is limited to 8388608 elements (larger n:

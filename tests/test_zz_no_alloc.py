@@ -1,9 +1,9 @@
 """vam_reduce_noalloc: the reduction for callers that cannot allocate device memory.
 
-Some callers can't call cudaMalloc: code inside a CUDA graph capture in global
-mode (allocation is not permitted there) and hosts that reserve all device
-memory before a print starts and must not trigger cudaMalloc's implicit
-synchronisation during exposure.  This entry point keeps its scratch in a
+Some callers can't call cudaMalloc: printer hosts that reserve all device
+memory for their projection buffers before a print starts (an allocation
+would fail) and must not trigger cudaMalloc's implicit synchronisation during
+exposure, and plug-ins that are handed fixed buffers and have no allocator.  This entry point keeps its scratch in a
 static device array inside the library instead of a caller workspace.  The
 test calls it through the C ABI and checks it against the workspace-based
 vam_reduce and against a float64 numpy reduction of the same data, twice in
