@@ -76,6 +76,36 @@ __device__ __forceinline__ float bilerp(const float* __restrict__ base, float f0
     return fmaf(t0, r1 - r0, r0);
 }
 
+// bilerp where all four taps are known to lie inside the plane: the same arithmetic and loads, no
+// bounds tests
+__device__ __forceinline__ float bilerp_in(const float* __restrict__ base, float f0, float f1, int s0, int s1) {
+    const float g0 = floorf(f0), g1 = floorf(f1);
+    const int o = (int)g0 * s0 + (int)g1 * s1;
+    const float t0 = f0 - g0, t1 = f1 - g1;
+    const float x00 = __ldg(base + o), x01 = __ldg(base + o + s1);
+    const float x10 = __ldg(base + o + s0), x11 = __ldg(base + o + s0 + s1);
+    const float r0 = fmaf(t1, x01 - x00, x00), r1 = fmaf(t1, x11 - x10, x10);
+    return fmaf(t0, r1 - r0, r0);
+}
+
+// Planes s in [lo, hi) on which f = f0 + m s stays inside [eps, n - 1 - eps] (so floor(f) and
+// floor(f) + 1 are both valid indices), narrowed by one plane at each end against the rounding of
+// the bound; the margin eps = 1e-3 in index units is far above the rounding of fmaf(m, s, f0).
+__device__ __forceinline__ void inside_planes(float f0, float m, int n, int np, int& lo, int& hi) {
+    const float a = 1e-3f, b = (float)(n - 1) - 1e-3f;
+    if (!(b > a) || !isfinite(f0) || !isfinite(m)) { lo = 0; hi = 0; return; }
+    if (fabsf(m) < 1e-20f) {
+        if (f0 >= a && f0 <= b) { lo = 0; hi = np; } else { lo = 0; hi = 0; }
+        return;
+    }
+    float s0 = (a - f0) / m, s1 = (b - f0) / m;
+    if (m < 0.f) { const float t = s0; s0 = s1; s1 = t; }
+    const float l = fmaxf(ceilf(s0) + 1.f, 0.f), h = fminf(floorf(s1) - 1.f, (float)(np - 1));
+    if (!(h >= l)) { lo = 0; hi = 0; return; }
+    lo = (int)l;
+    hi = (int)h + 1;
+}
+
 // Linear sample along one axis (slice-exact geometries: the other in-plane
 // coordinate is an integer voxel index on every sample).
 __device__ __forceinline__ float lerp1(const float* __restrict__ base, float f, int n, int s) {
@@ -108,19 +138,51 @@ __global__ void __launch_bounds__(kThreads) k_vec_forward(const float* __restric
         // HU: the horizontal coordinate has no row term, so it is the same for
         // every lane of the warp (computed from block indices and s only)
         const float h0 = affine(g.p0, fc, HU ? 0.f : fr, 0.f), k0 = affine(g.p1, fc, fr, 0.f);
+        if (FLAT) {
 #pragma unroll 4
-        for (int s = 0; s < np; ++s) {
-            const float fh = fmaf(g.p0[3], (float)s, h0);
-            const float* pl = vol + s * plane;
-            if (FLAT)
-                acc += lerp1(pl + r, fh, nh, hs);
-            else
-                acc += bilerp(pl, fh, fmaf(g.p1[3], (float)s, k0), nh, nZ, hs, 1);
+            for (int s = 0; s < np; ++s) acc += lerp1(vol + s * plane + r, fmaf(g.p0[3], (float)s, h0), nh, hs);
+        } else {
+            // the planes where every lane's four taps are inside run without bounds tests; the sum keeps
+            // its order, so the result is bit-identical
+            int lo, hi, lo1, hi1;
+            inside_planes(h0, g.p0[3], nh, np, lo, hi);
+            inside_planes(k0, g.p1[3], nZ, np, lo1, hi1);
+            lo = max(lo, lo1);
+            hi = min(hi, hi1);
+            const unsigned act = __activemask();
+            lo = __reduce_max_sync(act, lo);
+            hi = __reduce_min_sync(act, hi);
+            if (hi < lo) hi = lo;
+            auto checked = [&](int s) {
+                return bilerp(vol + s * plane, fmaf(g.p0[3], (float)s, h0), fmaf(g.p1[3], (float)s, k0), nh, nZ, hs, 1);
+            };
+#pragma unroll 4
+            for (int s = 0; s < lo; ++s) acc += checked(s);
+#pragma unroll 4
+            for (int s = lo; s < hi; ++s)
+                acc += bilerp_in(vol + s * plane, fmaf(g.p0[3], (float)s, h0), fmaf(g.p1[3], (float)s, k0), hs, 1);
+#pragma unroll 4
+            for (int s = hi; s < np; ++s) acc += checked(s);
         }
     } else {                      // planes across k; in-plane (i, j)
         const float i0 = affine(g.p0, fc, fr, 0.f), j0 = affine(g.p1, fc, fr, 0.f);
+        int lo, hi, lo1, hi1;
+        inside_planes(i0, g.p0[3], nY, nZ, lo, hi);
+        inside_planes(j0, g.p1[3], nX, nZ, lo1, hi1);
+        lo = max(lo, lo1);
+        hi = min(hi, hi1);
+        const unsigned act = __activemask();
+        lo = __reduce_max_sync(act, lo);
+        hi = __reduce_min_sync(act, hi);
+        if (hi < lo) hi = lo;
 #pragma unroll 4
-        for (int s = 0; s < nZ; ++s)
+        for (int s = 0; s < lo; ++s)
+            acc += bilerp(vol + s, fmaf(g.p0[3], (float)s, i0), fmaf(g.p1[3], (float)s, j0), nY, nX, sI, sJ);
+#pragma unroll 4
+        for (int s = lo; s < hi; ++s)
+            acc += bilerp_in(vol + s, fmaf(g.p0[3], (float)s, i0), fmaf(g.p1[3], (float)s, j0), sI, sJ);
+#pragma unroll 4
+        for (int s = hi; s < nZ; ++s)
             acc += bilerp(vol + s, fmaf(g.p0[3], (float)s, i0), fmaf(g.p1[3], (float)s, j0), nY, nX, sI, sJ);
     }
     sino[(c * nA + a) * nV + r] = acc * g.scale;
