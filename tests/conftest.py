@@ -38,4 +38,4 @@ def golden():
 
     d = ROOT / "tests" / "golden"
     return {k: np.load(d / f"{k}.npz") for k in ("parallel", "raytrace", "optim", "ray_autograd", "algebraic", "formats", "vecgeom",
-                                                 "occ2d", "options", "analytic_bclp")}
+                                                 "occ2d", "options", "analytic_bclp", "datafilters")}

@@ -557,6 +557,23 @@ GROUPS = {"parallel": parallel_cases, "ray": ray_cases, "algebraic": algebraic_c
           "analytic_bclp": analytic_response_cases}
 
 
+def data_filter_cases(vam):
+    """util.data's target filters (filterTarget, filterTargetBCLP) for every filter name and a 2-D and
+    a 3-D input, and histogramEqualization, on seeded inputs."""
+    D = vam.util.data
+    rng = np.random.default_rng(77)
+    out = {"x2": rng.uniform(0, 1, (24, 24)), "x3": rng.uniform(0, 1, (17, 17, 2)), "h": rng.normal(0, 1, (20, 12))}
+    for name in ("ram-lak", "shepp-logan", "cosine", "hamming", "hanning"):
+        for tag in ("x2", "x3"):
+            out[f"bclp_{name}_{tag}"] = D.filterTargetBCLP(out[tag].copy(), name)
+            out[f"target_{name}_{tag}"] = D.filterTarget(out[tag].copy(), name)
+    out["histeq"] = D.histogramEqualization(out["h"].copy(), 8)
+    np.savez_compressed(OUT / "datafilters.npz", **out)
+
+
+GROUPS["datafilters"] = data_filter_cases
+
+
 def main():
     import argparse
 

@@ -89,6 +89,69 @@ def filterTargetOSMO_t(x, filter_name):
     return out.to(x.dtype).contiguous()
 
 
+def filterTargetBCLP(real_space_array, filter_name):
+    """Radial Fourier filter of each z slice for BCLP targets (util/data.py:116-196): |f| on the
+    fftfreq grid, centred, with the window of the named filter; the Shepp-Logan and cosine windows are
+    evaluated on the uncentred frequencies and multiplied into the centred filter, as the reference
+    does.  The first two axes must have equal length."""
+    filter_types = ("ram-lak", "shepp-logan", "cosine", "hamming", "hanning", None)
+    if filter_name not in filter_types:
+        raise ValueError("Unknown filter: %s" % filter_name)
+    if filter_name is None or filter_name.lower() == "none":
+        return real_space_array
+    n_x, n_y = real_space_array.shape[0], real_space_array.shape[1]
+    assert n_x == n_y, "The first two dimensions of the real space array must have the same number of elements."
+    f_x, f_y = np.meshgrid(scipy.fft.fftfreq(n_x), scipy.fft.fftfreq(n_y), indexing="ij")
+    f_radial = np.sqrt(f_x ** 2 + f_y ** 2)
+    filt = scipy.fft.fftshift(f_radial)
+    if filter_name == "shepp-logan":
+        omega = np.pi / 2 * f_radial
+        nz = omega != 0
+        filt[nz] *= np.sin(omega[nz]) / omega[nz]
+    elif filter_name == "cosine":
+        filt *= np.cos(np.pi / 2 * f_radial)
+    elif filter_name in ("hamming", "hanning"):
+        w = np.abs(np.hamming(n_x) if filter_name == "hamming" else np.hanning(n_x))
+        filt *= np.abs(np.sqrt(np.outer(w, w)))
+    X = scipy.fft.fftshift(fft2(real_space_array, axes=(0, 1)), axes=(0, 1))
+    f = filt if real_space_array.ndim == 2 else filt[:, :, np.newaxis]
+    return np.real(ifft2(scipy.fft.ifftshift(X * f, axes=(0, 1)), axes=(0, 1))).astype(float)
+
+
+def filterTarget(real_space_array, filter_name):
+    """Each z slice filtered with the 2-D radial extension of the 1-D sinogram filter
+    (util/data.py:199-300): the slices zero-padded in x / y (centred) to the next power of two, at least
+    64; the 1-D filter of that length (_get_fourier_filter) interpolated linearly at every radial
+    frequency |f| (zero beyond its last frequency); the product with the slices' 2-D FFT transformed
+    back and cropped to the input size."""
+    n_x, n_y = real_space_array.shape[0], real_space_array.shape[1]
+    assert n_x == n_y, "The first two dimensions of the real space array must have the same number of elements."
+    n_p = max(64, int(2 ** np.ceil(np.log2(n_x))))
+    before, after = int(np.ceil((n_p - n_x) / 2)), int(np.floor((n_p - n_x) / 2))
+    pad = ((before, after), (before, after)) + (() if real_space_array.ndim == 2 else ((0, 0),))
+    padded = np.pad(real_space_array, pad, mode="constant", constant_values=0)
+    f1 = np.squeeze(_get_fourier_filter(n_p, filter_name))
+    freq = scipy.fft.fftfreq(n_p)
+    order = freq.argsort()
+    f_x, f_y = np.meshgrid(freq, freq, indexing="ij")
+    filt = np.interp(np.sqrt(f_x ** 2 + f_y ** 2), np.sort(freq), f1[order], left=0, right=0)
+    if real_space_array.ndim > 2:
+        filt = filt[:, :, np.newaxis]
+    out = np.real(ifft2(fft2(padded, axes=(0, 1)) * filt, axes=(0, 1))).astype(float)
+    return out[before:, before:] if after == 0 else out[before:-after, before:-after]
+
+
+def histogramEqualization(x, bit_depth, output_dtype=float):
+    """Contrast stretch of util/data.py:471-492: x scaled by max / (99th - 1st percentile), then values
+    at or above the 99th percentile set to 1 and at or below the 1st to 0 (bit_depth and output_dtype
+    are accepted and unused, as in the reference)."""
+    mx = np.amax(x)
+    p01, p99 = np.percentile(x, 1), np.percentile(x, 99)
+    y = x * (mx / (p99 - p01))
+    y = np.where(y >= p99, 1, y)
+    return np.where(y <= p01, 0, y)
+
+
 def _get_fourier_filter(size, filter_name):
     """Ram-Lak family filter built from its spatial form (util/data.py:373-438; Kak & Slaney ch. 3 eq. 61)."""
     n = np.concatenate((np.arange(1, size / 2 + 1, 2, dtype=int), np.arange(size / 2 - 1, 0, -2, dtype=int)))
