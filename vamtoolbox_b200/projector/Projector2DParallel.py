@@ -70,3 +70,9 @@ class Projector2DParallel:
 def _inside(ny, nx):
     cy, cx = np.meshgrid(np.linspace(-1, 1, ny), np.linspace(-1, 1, nx))
     return ~(cx ** 2 + cy ** 2 > 1)
+
+
+# The reference's names for the same dispatch slots (projectorconstructor.py:74-160).  The
+# ASTRA-model CUDA class (the 2-D line projector) is projector/Projector2DParallelCUDA.py.
+Projector2DParallelPython = Projector2DParallel
+Projector2DParallelAstra = Projector2DParallel

@@ -326,3 +326,13 @@ class PyTorchRayTracingPropagator:
         if self.output_torch_tensor:
             return torch.as_tensor(g0, device=self.device)
         return g0
+
+    # placeholders of the reference's interface with no body there either (pyTorchRayTrace.py:199-209)
+    def perAngleTrace(self):
+        pass
+
+    def perZTrace(self):
+        pass
+
+    def perRayTrace(self):
+        pass
