@@ -81,6 +81,38 @@ def test_bclp_matches_reference(golden, engine):
     assert np.allclose(norms[5:], O["bclp_norms"][5:], rtol=1e-3, atol=1e-5)
 
 
+def test_bclp_step_interface_matches_reference(golden):
+    """The reference's step interface of BCLPNorm (getLossGrad / getLoss / callback / updateVariables /
+    evaluateNormMetrics: the calls an external optimizer makes), driven the way the reference's own
+    gradientDescent drives it, reproduces the reference's BCLP run; the state is computed once per
+    iteration index, so a second getLoss at the same index does not project again."""
+    from vamtoolbox_b200.optimizer.BCLP import BCLPNorm
+    from vamtoolbox_b200.response import ResponseModel
+
+    O = golden["optim"]
+    tg, pg = geo(O["bclp_target"], O["angles"])
+    b = BCLPNorm(tg, pg, opts(method="BCLP", n_iter=4, p=2, q=1, eps=0.05, learning_rate=0.002,
+                              response_model=ResponseModel(B=12, M=0.6), filter="ram-lak"))
+    g = b.checkSinogramShape(b.host_g0(), desired_shape="flattened")
+    for _ in range(4):
+        g = b.imposeSinogramConstraints(g - b.learning_rate * b.getLossGrad(g))
+        dose_before = b.dose
+        b.getLoss(g)
+        assert b.dose is dose_before  # same iteration index: nothing recomputed
+        b.callback(g)
+    b.updateVariables(g)
+    b.evaluateNormMetrics()
+    assert relL2(b.checkSinogramShape(g, desired_shape="cylindrical"), O["bclp_sino"]) < 1e-4
+    assert relL2(b.dose, O["bclp_dose"]) < 1e-4
+    assert relL2(b.mapped_dose, O["bclp_mapped"]) < 1e-4
+    L = b.logs
+    assert np.allclose(L.loss, O["bclp_loss"], rtol=1e-4)
+    norms = np.stack([L.l0, L.l1, L.l2, L.lf, L.l0_eps0, L.l1_eps0, L.l2_eps0, L.lf_eps0])
+    assert np.all(np.abs(norms[0] - O["bclp_norms"][0]) <= 1)  # voxel counts
+    assert np.allclose(norms[1:4], O["bclp_norms"][1:4], rtol=1e-3, atol=1e-5)
+    assert np.allclose(norms[5:], O["bclp_norms"][5:], rtol=1e-3, atol=1e-5)
+
+
 def test_pm_runs_and_tracks_reference(golden):
     from vamtoolbox_b200.optimize import optimize
 

@@ -93,6 +93,13 @@ class BCLPNorm:
         self.dose = None
         self._mapped_dose = None
         self.mapped_t = None
+        # state of the reference's step interface (updateVariables: each quantity computed once per
+        # iteration index, BCLP.py:203-216)
+        self.v = self.loss = self.loss_grad = None
+        self.mapped_dose_error_from_f_T = self.mapped_dose_error_from_band = None
+        self.dose_iter = self.mapped_dose_iter = self.mapped_dose_error_from_f_T_iter = -1
+        self.mapped_dose_error_from_band_iter = self.v_iter = self.weight_iter = -1
+        self.loss_iter = self.loss_grad_iter = -1
         self.g0_t = self.fT_t = None
         self.P = projectorconstructor(self.target_geo, self.proj_geo)
         if self._device_init_ok():
@@ -184,6 +191,93 @@ class BCLPNorm:
             ch = np.abs(np.diff(self.logs.loss[it - 5:it + 1]))
             conv = bool(np.mean(ch) <= self.exit_param * self.logs.loss[it])
         return conv or zero
+
+    # -- the reference's step interface (BCLP.py:277-475) -----------------------------
+    # The same quantities as the host engine below, held as attributes and refreshed once per iteration
+    # index (logs.curr_iter), so a caller can drive the problem with its own optimizer (for example
+    # scipy.optimize.minimize(fun=getLoss, jac=getLossGrad, callback=callback)) as with the reference.
+    def updateVariables(self, g_iter):
+        """Bring dose, mapped dose, its errors from the target and from the tolerance band, the violation
+        set, the loss and its gradient up to date for g_iter, each computed once per iteration index and
+        in that order (BCLP.py:277-330)."""
+        it = self.logs.curr_iter
+        if self.dose_iter != it:
+            g = self.checkSinogramShape(np.asarray(g_iter), desired_shape="cylindrical")
+            self.dose = np.asarray(self.P.backward(g)).reshape(self.target_geo.array.shape)
+            self.dose_iter = it
+        if self.mapped_dose_iter != it:
+            self.mapped_dose = self.response_model.map(self.dose)
+            self.mapped_dose_iter = it
+        if self.mapped_dose_error_from_f_T_iter != it:
+            self.mapped_dose_error_from_f_T = self.mapped_dose - self.target_geo.array
+            self.mapped_dose_error_from_f_T_iter = it
+        if self.mapped_dose_error_from_band_iter != it:
+            # positive exactly where the band constraint is violated
+            self.mapped_dose_error_from_band = np.abs(self.mapped_dose_error_from_f_T) - self.eps
+            self.mapped_dose_error_from_band_iter = it
+        if self.v_iter != it:
+            self.v = self.mapped_dose_error_from_band > 0
+            self.v_iter = it
+        if self.test_alternate_handling and self.weight_iter != it:
+            inside = self.target_geo.array > 0
+            self.weight = (inside if it % 2 == 0 else ~inside).astype(float)
+            self.weight_iter = it
+        if self.loss_iter != it:
+            self.loss = self.computeLoss()
+            self.loss_iter = it
+        if self.loss_grad_iter != it:
+            self.loss_grad = self.computeLossGradient()
+            self.loss_grad_iter = it
+
+    def computeLoss(self):
+        """(sum over violating voxels of weight * |band error|^p * dvol)^(q/p), logged at the current
+        iteration (BCLP.py:332-351)."""
+        integrand = self.v * self.weight * np.abs(self.mapped_dose_error_from_band) ** self.p
+        loss = (np.sum(integrand) * self.dvol) ** (self.q / self.p)
+        self.logs.loss[self.logs.curr_iter] = loss
+        return loss
+
+    def computeLossGradient(self):
+        """The loss gradient with respect to the sinogram, flattened: q loss^((q-p)/q) times the forward
+        projection of v * weight * |band error|^(p-1) * sign(error) * dmap/df(dose); the forward alone
+        when the loss is zero, where the factor is not finite (BCLP.py:353-386)."""
+        operand = (self.v * self.weight * (np.abs(self.mapped_dose_error_from_band) ** (self.p - 1))
+                   * np.sign(self.mapped_dose_error_from_f_T) * self.response_model.dmapdf(self.dose))
+        fwd = np.asarray(self.P.forward(operand))
+        grad = (self.q * self.loss ** ((self.q - self.p) / self.q)) * fwd if self.loss != 0.0 else fwd
+        return self.checkSinogramShape(grad, desired_shape="flattened")
+
+    def getLoss(self, g_iter):
+        self.updateVariables(g_iter)
+        return self.loss
+
+    def getLossGrad(self, g_iter):
+        self.updateVariables(g_iter)
+        return self.loss_grad
+
+    def evaluateNormMetrics(self):
+        """l0 / l1 / l2 / l-infinity norms of the band violation and of the error itself (eps = 0), times
+        dvol, logged at the current iteration (BCLP.py:396-437)."""
+        i, L = self.logs.curr_iter, self.logs
+        e, eb, v = self.mapped_dose_error_from_f_T, self.mapped_dose_error_from_band, self.v
+        v0 = np.abs(e) > 0
+        L.l0[i], L.l0_eps0[i] = np.sum(v) * self.dvol, np.sum(v0) * self.dvol
+        L.l1[i], L.l1_eps0[i] = np.sum(v * np.abs(eb)) * self.dvol, np.sum(np.abs(e)) * self.dvol
+        L.l2[i] = np.sqrt(np.sum(v * eb ** 2) * self.dvol)
+        L.l2_eps0[i] = np.sqrt(np.sum(e ** 2) * self.dvol)
+        L.lf[i], L.lf_eps0[i] = np.amax(v * np.abs(eb)), np.amax(v0 * np.abs(e))
+
+    def callback(self, g_iter):
+        """Norms and iteration time of the current iteration, then the next iteration index
+        (BCLP.py:439-475; the live plots of verbose='plot' are not drawn here)."""
+        self.updateVariables(g_iter)
+        self.evaluateNormMetrics()
+        self.logs.recordIterTime()
+        if self.verbose in ("time", "plot", "plot_demo"):
+            self.logger.info(f"Iteration {self.logs.curr_iter: 4.0f} at time: "
+                             f"{self.logs.iter_times[self.logs.curr_iter]: 6.1f} s. "
+                             f"Loss = {self.logs.loss[self.logs.curr_iter]}")
+        self.logs.curr_iter += 1
 
     # -- host engine: the reference's numpy loop (BCLP.py:277-526) ---------------
     def _host_state(self, g):
