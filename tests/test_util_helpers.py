@@ -1,0 +1,49 @@
+"""The reference's small util modules: thresholding.threshold, timing.timing, matlab.saveMatData
+(vamtoolbox/util/thresholding.py, timing.py, matlab.py) on the host, and build_sparse_matrix.buildMatrix
+(vamtoolbox/util/build_sparse_matrix.py) on the device: its rows are the projector's backprojections of
+unit sinograms, so P^T b equals the backprojection of b."""
+import numpy as np
+import pytest
+import scipy.io
+
+
+def test_threshold_timing_and_matlab(tmp_path, capsys):
+    from vamtoolbox_b200 import geometry
+    from vamtoolbox_b200.util import matlab, thresholding, timing
+
+    x = np.array([[0.2, 0.5], [0.7, 0.49]])
+    t = thresholding.threshold(x, 0.5)
+    assert t.dtype == np.bool_ and t.tolist() == [[False, True], [True, False]]
+
+    @timing.timing
+    def twice(v):
+        return 2 * v
+
+    assert twice(3) == 6 and "twice function took" in capsys.readouterr().out
+    tg = geometry.TargetGeometry(target=x.copy())
+    sino = geometry.Sinogram(np.arange(6.0).reshape(3, 2), geometry.ProjectionGeometry(np.array([0.0, 90.0]), "parallel"))
+    f = tmp_path / "out.mat"
+    matlab.saveMatData(str(f), target_geo=tg, sinogram=sino)
+    d = scipy.io.loadmat(str(f))
+    assert np.array_equal(d["target"], tg.array)
+    assert np.array_equal(d["opt_proj"], sino.array)
+    with pytest.raises(Exception):
+        matlab.saveMatData(str(f), sinogram=np.zeros(3))
+
+
+@pytest.mark.gpu
+def test_build_matrix_rows_are_unit_backprojections():
+    from vamtoolbox_b200 import geometry
+    from vamtoolbox_b200.projectorconstructor import projectorconstructor
+    from vamtoolbox_b200.util.build_sparse_matrix import buildMatrix
+
+    rng = np.random.default_rng(5)
+    tg = geometry.TargetGeometry(target=rng.uniform(0, 1, (12, 12)))
+    pg = geometry.ProjectionGeometry(np.linspace(0, 180, 7, endpoint=False), "parallel", CUDA=True)
+    P = buildMatrix(tg, pg)
+    A = projectorconstructor(tg, pg)
+    b = rng.uniform(0, 1, np.asarray(A.forward(np.zeros_like(tg.array))).shape)
+    want = np.asarray(A.backward(b.copy())).ravel()
+    got = P.T @ b.ravel()
+    assert np.linalg.norm(got - want) <= 1e-5 * np.linalg.norm(want)
+    assert P.format == "csr" and P.shape == (b.size, tg.array.size)

@@ -1,2 +1,2 @@
 """Array helpers (vamtoolbox.util counterpart)."""
-from . import data
+from . import build_sparse_matrix, data, matlab, thresholding, timing
