@@ -289,7 +289,7 @@ def oracle_bclp_iteration(tg, pg, opts, g):
 
     rm = opts.response_model
     tables = (rm.interp_f_0, rm.interp_map_0, rm.interp_dmapdf_0)
-    mask = np.asarray(pg.absorption_mask)[:, :, 0] if pg.absorption_mask is not None else None
+    mask = np.atleast_3d(np.asarray(pg.absorption_mask))[:, :, 0] if pg.absorption_mask is not None else None
     t0 = time.perf_counter()
     ref = OI.bclp_iteration(g, np.asarray(tg.array, np.float64), np.asarray(pg.angles, np.float64), mask, tables,
                             opts.eps, opts.weight, opts.p, opts.q, opts.learning_rate, opts.blb, opts.bub)
@@ -352,7 +352,7 @@ def multi_target_problems(seed=5, n_iter=25):
     return probs, desc
 
 
-def run_multi_target(dev, n_iter=25):
+def run_multi_target(dev, n_iter=25, parity=True):
     """Aggregate BCLP iter/s of 16 uneven targets, four ways, each a captured graph replayed n_iter
     times after 3 warm-up replays: all targets per iteration in two persistent work-queue batches
     (vam_batch_submit; all backprojections, then all forwards), the same with the targets in two halves
@@ -404,6 +404,49 @@ def run_multi_target(dev, n_iter=25):
     for sched in ("persistent", "streams", "phased"):
         out[f"speedup_{sched}"] = round(out[f"{sched}_iter_s"] / out["one_at_a_time_iter_s"], 3)
     out["launches_per_iteration"] = launches
+    if parity:
+        out["parity"] = multi_target_parity(multi, probs, desc)
+    return out
+
+
+def multi_target_parity(multi, probs, desc, n_check=2):
+    """Every schedule's sinograms after n_check captured iterations from one saved start against each
+    target's own graph replayed alone (bit for bit), and one iteration of the largest slice and of the
+    smallest volume against the float64 oracle from the same sinogram (whole target, all angles)."""
+    import torch
+
+    saved = [it.g.clone() for it in multi.its]
+    got = {}
+    for sched in ("persistent", "streams", "phased"):
+        multi.schedule = sched
+        multi.reset(saved)
+        g = multi.capture()
+        for _ in range(n_check):
+            g.replay()
+        torch.cuda.synchronize(multi.device)
+        del g
+        got[sched] = [it.g.clone() for it in multi.its]
+    multi.reset(saved)
+    graphs = [it.capture() for it in multi.its]
+    for gr in graphs:
+        for _ in range(n_check):
+            gr.replay()
+    torch.cuda.synchronize(multi.device)
+    del graphs
+    alone = [it.g.clone() for it in multi.its]
+    out = {"bitwise_equal_to_one_at_a_time": {s: all(torch.equal(a, b) for a, b in zip(v, alone))
+                                              for s, v in got.items()},
+           "iterations_compared": n_check}
+    cost = [float(np.asarray(tg.array).size) * pg.n_angles for tg, pg, _ in probs]
+    two_d = [k for k, d in enumerate(desc) if "^2x" in d]
+    three_d = [k for k, d in enumerate(desc) if "^3x" in d]
+    picks = [max(two_d, key=lambda k: cost[k]), min(three_d, key=lambda k: cost[k])]
+    for k in picks:
+        tg, pg, opts = probs[k]
+        dev_out = device_bclp_step(multi.its[k])
+        ref, t = oracle_bclp_iteration(tg, pg, opts, dev_out["g"])
+        out[desc[k]] = {"oracle_s": round(t, 2), "relL2": bclp_parity(dev_out, ref)}
+    out["reference"] = "float64 oracle, one BCLP iteration from the same g, whole target"
     return out
 
 
