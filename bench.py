@@ -1320,7 +1320,7 @@ def run_ours(args):
             ray = {"error": f"{type(exc).__name__}: {exc}"}
 
     cpu, parity = None, None
-    if rank == 0 and not args.no_cpu:
+    if ws_ == 1 and not args.no_cpu:  # the CPU baseline (and the parity pass beside it) at N = 1 only
         try:
             # a fresh iteration state (g = g0) with no cross-rank hook: only rank 0 runs it
             cpu, parity = cpu_baseline_and_parity(bclp.device_iteration(), tg, pg, opts)
