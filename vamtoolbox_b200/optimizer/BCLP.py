@@ -194,8 +194,9 @@ class BCLPNorm:
 
     # -- the reference's step interface (BCLP.py:277-475) -----------------------------
     # The same quantities as the host engine below, held as attributes and refreshed once per iteration
-    # index (logs.curr_iter), so a caller can drive the problem with its own optimizer (for example
-    # scipy.optimize.minimize(fun=getLoss, jac=getLossGrad, callback=callback)) as with the reference.
+    # index (logs.curr_iter), so a caller can drive the problem with its own iteration loop as with the
+    # reference: every getLoss / getLossGrad between two callback calls sees the state of the first
+    # sinogram queried at that index (callback advances the index).
     def updateVariables(self, g_iter):
         """Bring dose, mapped dose, its errors from the target and from the tolerance band, the violation
         set, the loss and its gradient up to date for g_iter, each computed once per iteration index and
