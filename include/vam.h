@@ -314,8 +314,11 @@ int vam_ray_active_at_cap(vam_ray_plan* plan, int64_t* out_count);
  * (max_num_step x num_rays x 16 B: 36 GB at 128^3 x 360 rays x 384 steps).
  * While it is valid, vam_ray_integrate and vam_ray_deposit stream the records
  * instead of re-tracing (bit-identical results); vam_ray_set_medium
- * invalidates it (prepare again to refresh it).  VAM_ERR_NOTSUP when the
- * configuration has no padded path or the cache would exceed limit_bytes,
+ * invalidates it (prepare again to refresh it).  When not every ray fits in
+ * limit_bytes (16 B per step of the cap plus 4 B per ray), the cache holds
+ * rays 0 .. m - 1 for the largest multiple of 32 rays m that fits and the
+ * remaining rays are traced every call (same results).  VAM_ERR_NOTSUP when
+ * the configuration has no padded path or not even 32 rays fit,
  * VAM_ERR_NOMEM when the device cannot hold it (the plan then traces as
  * before).  Allocates: call before any stream capture.
  * vam_ray_drop_trajectories frees it.  The reference re-traces every call

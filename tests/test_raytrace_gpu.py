@@ -152,9 +152,20 @@ def test_trajectory_cache_bitwise_and_invalidated(golden):
     w[::7] = 0.0  # rays with no energy deposit nothing
     g0, d0 = plan.integrate(f).clone(), plan.deposit(w).clone()
     cap0 = plan.active_at_cap()
-    assert not plan.prepare_trajectories(limit_bytes=plan.trajectory_bytes() - 1)
+    # not even one warp of rays fits: refused, the plan keeps tracing
+    assert not plan.prepare_trajectories(limit_bytes=plan.trajectory_bytes(32) - 1)
     assert torch.equal(plan.integrate(f), g0)
+    # a prefix of the rays (a multiple of 32) cached, the rest traced: the same results
+    assert plan.num_rays > 96
+    assert plan.prepare_trajectories(limit_bytes=plan.trajectory_bytes(plan.num_rays // 2))
+    m = plan.cached_rays
+    assert 0 < m < plan.num_rays and m % 32 == 0
+    assert torch.equal(plan.integrate(f), g0)
+    assert plan.active_at_cap() == cap0
+    assert relL2(plan.deposit(w).cpu().numpy(), d0.cpu().numpy()) < 1e-5
+    assert plan.active_at_cap() == cap0
     assert plan.prepare_trajectories()
+    assert plan.cached_rays == plan.num_rays
     assert plan.has_trajectories
     for _ in range(2):
         assert torch.equal(plan.integrate(f), g0)

@@ -50,6 +50,7 @@ struct vam_ray_plan {
     int* d_traj_len;
     unsigned long long* d_traj_active;
     size_t traj_bytes;
+    int64_t traj_rays;  // rays 0 .. traj_rays - 1 are cached (all, or a multiple of 32); the rest are traced
     int traj_valid;
 };
 
@@ -684,9 +685,10 @@ __device__ __forceinline__ bool pad_corners(const RayArgs& a, const PadArgs& q, 
     return true;
 }
 
+// r0: the first ray this launch traces (the rays before it come from the trajectory cache)
 __global__ void __launch_bounds__(kRayThreads) k_ray_integrate_pad(RayArgs a, PadArgs q, const float* __restrict__ fpad,
-                                                                   float* __restrict__ g) {
-    const int64_t r = (int64_t)blockIdx.x * kRayThreads + threadIdx.x;
+                                                                   float* __restrict__ g, int64_t r0) {
+    const int64_t r = r0 + (int64_t)blockIdx.x * kRayThreads + threadIdx.x;
     if (r >= a.nr) return;
     RayState st;
     ray_init<kCfgGridSymplectic>(a, r, a.energy0, st);
@@ -722,8 +724,8 @@ __global__ void __launch_bounds__(kRayThreads) k_ray_integrate_pad(RayArgs a, Pa
 }
 
 __global__ void __launch_bounds__(kRayThreads) k_ray_deposit_pad(RayArgs a, PadArgs q, const float* __restrict__ gin,
-                                                                 float* __restrict__ spad) {
-    const int64_t r = (int64_t)blockIdx.x * kRayThreads + threadIdx.x;
+                                                                 float* __restrict__ spad, int64_t r0) {
+    const int64_t r = r0 + (int64_t)blockIdx.x * kRayThreads + threadIdx.x;
     if (r >= a.nr) return;
     RayState st;
     ray_init<kCfgGridSymplectic>(a, r, gin[r], st);
@@ -770,18 +772,19 @@ __global__ void __launch_bounds__(kRayThreads) k_ray_deposit_pad(RayArgs a, PadA
 // the same accumulation order, so their results are bit-identical to the tracing
 // kernels'.
 // ---------------------------------------------------------------------------
+// rays 0 .. m - 1 (m: the cached rays), records step-major with stride m
 __global__ void __launch_bounds__(kRayThreads) k_ray_record_pad(RayArgs a, PadArgs q, float4* __restrict__ traj,
                                                                 int* __restrict__ len,
-                                                                unsigned long long* __restrict__ active) {
+                                                                unsigned long long* __restrict__ active, int64_t m) {
     const int64_t r = (int64_t)blockIdx.x * kRayThreads + threadIdx.x;
-    if (r >= a.nr) return;
+    if (r >= m) return;
     RayState st;
     ray_init<kCfgGridSymplectic>(a, r, 1.f, st);
     int until_check = 0, n = 0;
     for (int step = 0; step < a.max_steps; ++step) {
         float ds;
         ray_step_pad(a, q, st, ds);
-        __stcs(traj + (size_t)step * a.nr + r, make_float4(st.xp[0], st.xp[1], st.xp[2], __expf(-st.att)));
+        __stcs(traj + (size_t)step * m + r, make_float4(st.xp[0], st.xp[1], st.xp[2], __expf(-st.att)));
         n = step + 1;
         if (until_check == 0) {
             until_check = a.check;
@@ -795,16 +798,17 @@ __global__ void __launch_bounds__(kRayThreads) k_ray_record_pad(RayArgs a, PadAr
 
 __global__ void __launch_bounds__(kRayThreads) k_ray_integrate_traj(RayArgs a, PadArgs q, const float4* __restrict__ traj,
                                                                     const int* __restrict__ len,
-                                                                    const float* __restrict__ fpad, float* __restrict__ g) {
+                                                                    const float* __restrict__ fpad, float* __restrict__ g,
+                                                                    int64_t m) {
     const int64_t r = (int64_t)blockIdx.x * kRayThreads + threadIdx.x;
-    if (r >= a.nr) return;
+    if (r >= m) return;
     const float E0 = a.energy0;
     const int n = len[r];
     float integral = 0.f;
     float4 t = n > 0 ? __ldcs(traj + r) : make_float4(0.f, 0.f, 0.f, 0.f);
     for (int step = 0; step < n; ++step) {
         // the next record in flight while this step's corners are gathered
-        const float4 tn = step + 1 < n ? __ldcs(traj + (size_t)(step + 1) * a.nr + r) : t;
+        const float4 tn = step + 1 < n ? __ldcs(traj + (size_t)(step + 1) * m + r) : t;
         const float xp[3] = {t.x, t.y, t.z};
         const float E = E0 * t.w;
         Corners c;
@@ -834,19 +838,21 @@ __global__ void __launch_bounds__(kRayThreads) k_ray_integrate_traj(RayArgs a, P
 // atomics and lane l issues only its lower four, about halving the atomics (the deposit's bound once the
 // tracing is gone).  The sums are the tracing kernel's up to the order of float32 additions, which atomics
 // leave open anyway.  Lanes walk to the warp's longest record, inactive ones with no corners.
+// rays 0 .. m - 1; m is the ray count or a multiple of 32, so a warp's rays are all cached or none
 __global__ void __launch_bounds__(kRayThreads) k_ray_deposit_traj(RayArgs a, PadArgs q, const float4* __restrict__ traj,
                                                                   const int* __restrict__ len,
-                                                                  const float* __restrict__ gin, float* __restrict__ spad) {
+                                                                  const float* __restrict__ gin, float* __restrict__ spad,
+                                                                  int64_t m) {
     const int64_t r = (int64_t)blockIdx.x * kRayThreads + threadIdx.x;
     const int lane = threadIdx.x & 31;
-    const bool in = r < a.nr;
+    const bool in = r < m;
     const float E0 = in ? gin[r] : 0.f;
     const int n = in && E0 != 0.f ? len[r] : 0;
     const int nmax = __reduce_max_sync(0xffffffffu, n);
     float4 t = n > 0 ? __ldcs(traj + r) : make_float4(0.f, 0.f, 0.f, 0.f);
     for (int step = 0; step < nmax; ++step) {
         const bool live = step < n;
-        const float4 tn = step + 1 < n ? __ldcs(traj + (size_t)(step + 1) * a.nr + r) : t;
+        const float4 tn = step + 1 < n ? __ldcs(traj + (size_t)(step + 1) * m + r) : t;
         int o = 0, dx = 0, dy = 0, dz = 0;
         float w[8];
         bool ok = false;
@@ -1146,15 +1152,21 @@ extern "C" int vam_ray_integrate(vam_ray_plan* p, const float* f, float* g, vam_
         // a deposit leaves values in the border of d_spad: zero it, then write the interior
         VAM_TRY_CUDA(cudaMemsetAsync(p->d_spad, 0, sizeof(float) * padded_voxels(p->g), st));
         k_pad_mul<<<ew_blocks(nv), 256, 0, st>>>(f, p->d_absorb, p->d_spad, p->g.n_x, p->g.n_y, p->g.n_z);
-        if (p->traj_valid) {
+        // the cached rays (0 .. traj_rays - 1) stream their records, the rest are traced; the count of
+        // rays active at the cap starts from the cached rays' recorded count
+        const int64_t m = p->traj_valid ? p->traj_rays : 0;
+        if (m > 0) {
             VAM_TRY_CUDA(cudaMemcpyAsync(p->d_active, p->d_traj_active, sizeof(unsigned long long),
                                          cudaMemcpyDeviceToDevice, st));
-            k_ray_integrate_traj<<<nb, kRayThreads, 0, st>>>(a, make_pad_args(p), p->d_traj, p->d_traj_len, p->d_spad, g);
+            k_ray_integrate_traj<<<(unsigned)((m + kRayThreads - 1) / kRayThreads), kRayThreads, 0, st>>>(
+                a, make_pad_args(p), p->d_traj, p->d_traj_len, p->d_spad, g, m);
             VAM_CHECK_LAUNCH("k_ray_integrate_traj");
-            return VAM_OK;
         }
-        k_ray_integrate_pad<<<nb, kRayThreads, 0, st>>>(a, make_pad_args(p), p->d_spad, g);
-        VAM_CHECK_LAUNCH("k_ray_integrate_pad");
+        if (m < p->g.num_rays) {
+            k_ray_integrate_pad<<<(unsigned)((p->g.num_rays - m + kRayThreads - 1) / kRayThreads), kRayThreads, 0, st>>>(
+                a, make_pad_args(p), p->d_spad, g, m);
+            VAM_CHECK_LAUNCH("k_ray_integrate_pad");
+        }
         return VAM_OK;
     }
     k_mul<<<ew_blocks(nv), 256, 0, st>>>(f, p->d_absorb, p->d_scratch, nv);
@@ -1177,13 +1189,17 @@ extern "C" int vam_ray_deposit(vam_ray_plan* p, const float* gin, float* dose, v
         // deposits of corners outside the grid land in the zero border and are not copied out; the
         // border is zeroed again by the next call's memset
         VAM_TRY_CUDA(cudaMemsetAsync(p->d_spad, 0, sizeof(float) * padded_voxels(p->g), st));
-        if (p->traj_valid) {
+        const int64_t m = p->traj_valid ? p->traj_rays : 0;
+        if (m > 0) {
             VAM_TRY_CUDA(cudaMemcpyAsync(p->d_active, p->d_traj_active, sizeof(unsigned long long),
                                          cudaMemcpyDeviceToDevice, st));
-            k_ray_deposit_traj<<<nb, kRayThreads, 0, st>>>(a, make_pad_args(p), p->d_traj, p->d_traj_len, gin, p->d_spad);
+            k_ray_deposit_traj<<<(unsigned)((m + kRayThreads - 1) / kRayThreads), kRayThreads, 0, st>>>(
+                a, make_pad_args(p), p->d_traj, p->d_traj_len, gin, p->d_spad, m);
             VAM_CHECK_LAUNCH("k_ray_deposit_traj");
-        } else {
-            k_ray_deposit_pad<<<nb, kRayThreads, 0, st>>>(a, make_pad_args(p), gin, p->d_spad);
+        }
+        if (m < p->g.num_rays) {
+            k_ray_deposit_pad<<<(unsigned)((p->g.num_rays - m + kRayThreads - 1) / kRayThreads), kRayThreads, 0, st>>>(
+                a, make_pad_args(p), gin, p->d_spad, m);
             VAM_CHECK_LAUNCH("k_ray_deposit_pad");
         }
         k_unpad_mul<<<ew_blocks(nv), 256, 0, st>>>(p->d_spad, p->d_absorb, dose, p->g.n_x, p->g.n_y, p->g.n_z);
@@ -1248,9 +1264,16 @@ extern "C" int vam_ray_prepare_trajectories(vam_ray_plan* p, int64_t limit_bytes
                 "vam_ray_prepare_trajectories: serves 3-D grid media with the physical path length and the "
                 "symplectic Euler solver");
     const size_t steps = (size_t)std::max(a.max_steps, 1);
-    const size_t bytes = sizeof(float4) * steps * (size_t)p->g.num_rays + sizeof(int) * (size_t)p->g.num_rays;
-    VAM_REQUIRE(limit_bytes >= 0 && bytes <= (size_t)limit_bytes, VAM_ERR_NOTSUP,
-                "vam_ray_prepare_trajectories: the cache needs " + std::to_string(bytes) + " bytes, over the limit");
+    const size_t per_ray = sizeof(float4) * steps + sizeof(int);
+    VAM_REQUIRE(limit_bytes >= 0, VAM_ERR_ARG, "vam_ray_prepare_trajectories: negative byte limit");
+    // every ray when they all fit, else the largest multiple of 32 rays (whole warps) from ray 0
+    int64_t m = (int64_t)std::min<size_t>((size_t)p->g.num_rays, (size_t)limit_bytes / per_ray);
+    if (m < p->g.num_rays) m -= m % 32;
+    VAM_REQUIRE(m > 0, VAM_ERR_NOTSUP,
+                "vam_ray_prepare_trajectories: one warp of rays needs " + std::to_string(per_ray * 32) +
+                    " bytes, over the limit");
+    const size_t bytes = per_ray * (size_t)m;
+    p->traj_valid = 0;
     if (p->traj_bytes != bytes) {
         cudaFree(p->d_traj);
         cudaFree(p->d_traj_len);
@@ -1258,8 +1281,8 @@ extern "C" int vam_ray_prepare_trajectories(vam_ray_plan* p, int64_t limit_bytes
         p->d_traj_len = nullptr;
         p->traj_bytes = 0;
         p->traj_valid = 0;
-        cudaError_t e = cudaMalloc(&p->d_traj, sizeof(float4) * steps * (size_t)p->g.num_rays);
-        if (e == cudaSuccess) e = cudaMalloc(&p->d_traj_len, sizeof(int) * (size_t)p->g.num_rays);
+        cudaError_t e = cudaMalloc(&p->d_traj, sizeof(float4) * steps * (size_t)m);
+        if (e == cudaSuccess) e = cudaMalloc(&p->d_traj_len, sizeof(int) * (size_t)m);
         if (e != cudaSuccess) {
             cudaFree(p->d_traj);
             cudaFree(p->d_traj_len);
@@ -1273,9 +1296,10 @@ extern "C" int vam_ray_prepare_trajectories(vam_ray_plan* p, int64_t limit_bytes
     if (!p->d_traj_active) VAM_TRY_CUDA(cudaMalloc(&p->d_traj_active, sizeof(unsigned long long)));
     cudaStream_t st = (cudaStream_t)stream;
     VAM_TRY_CUDA(cudaMemsetAsync(p->d_traj_active, 0, sizeof(unsigned long long), st));
-    const unsigned nb = (unsigned)((p->g.num_rays + kRayThreads - 1) / kRayThreads);
-    k_ray_record_pad<<<nb, kRayThreads, 0, st>>>(a, make_pad_args(p), p->d_traj, p->d_traj_len, p->d_traj_active);
+    const unsigned nb = (unsigned)((m + kRayThreads - 1) / kRayThreads);
+    k_ray_record_pad<<<nb, kRayThreads, 0, st>>>(a, make_pad_args(p), p->d_traj, p->d_traj_len, p->d_traj_active, m);
     VAM_CHECK_LAUNCH("k_ray_record_pad");
+    p->traj_rays = m;
     p->traj_valid = 1;
     return VAM_OK;
 }
@@ -1289,6 +1313,7 @@ extern "C" int vam_ray_drop_trajectories(vam_ray_plan* p) {
     p->d_traj = nullptr;
     p->d_traj_len = nullptr;
     p->traj_bytes = 0;
+    p->traj_rays = 0;
     p->traj_valid = 0;
     return VAM_OK;
 }

@@ -146,21 +146,32 @@ class RayPlan:
             torch.cuda.current_stream(self.device).synchronize()
         self._medium_keep = keep
         self.has_trajectories = False  # a new medium makes the cached paths stale
+        self.cached_rays = 0
 
-    def trajectory_bytes(self):
-        """Device bytes of the trajectory cache: 16 per ray and step of the cap, 4 per ray."""
-        return 16 * max(self.max_num_step, 1) * self.num_rays + 4 * self.num_rays
+    def trajectory_bytes(self, rays=None):
+        """Device bytes of the trajectory cache of ``rays`` rays (default: every ray): 16 per ray and step
+        of the cap, 4 per ray."""
+        rays = self.num_rays if rays is None else int(rays)
+        return (16 * max(self.max_num_step, 1) + 4) * rays
+
+    def _cacheable_rays(self, limit_bytes):
+        """The rays vam_ray_prepare_trajectories caches under limit_bytes: every ray when they fit, else the
+        largest multiple of 32 (rays 0 .. m - 1; the rest are traced every call)."""
+        m = min(self.num_rays, int(limit_bytes) // (16 * max(self.max_num_step, 1) + 4))
+        return m if m == self.num_rays else m - m % 32
 
     def prepare_trajectories(self, limit_bytes=None):
         """Trace the rays once and keep every step's position and attenuance (vam_ray_prepare_trajectories),
         so later integrate / deposit calls stream them instead of re-tracing (bit-identical results).  The
-        paths depend on the medium only.  ``limit_bytes`` defaults to half of the device's free memory.
-        Allocates: not during a graph capture.  False when the configuration has no cached path (it serves
-        3-D grid media, physical path length, symplectic Euler) or the cache exceeds the limit or the
-        device; the plan then keeps tracing."""
+        paths depend on the medium only.  ``limit_bytes`` defaults to half of the device's free memory;
+        when not every ray fits, the first ``cached_rays`` rays (a multiple of 32) are cached and the rest
+        traced every call.  Allocates: not during a graph capture.  False when the configuration has no
+        cached path (it serves 3-D grid media, physical path length, symplectic Euler) or not even 32 rays
+        fit the limit or the device; the plan then keeps tracing."""
         if limit_bytes is None:
             free, _ = torch.cuda.mem_get_info(self.device)
             limit_bytes = free // 2
+        self.cached_rays = 0
         try:
             with torch.cuda.device(self.device):
                 _lib.call("vam_ray_prepare_trajectories", self._h, int(limit_bytes), self._s())
@@ -171,6 +182,7 @@ class RayPlan:
                 return False
             raise
         self.has_trajectories = True
+        self.cached_rays = self._cacheable_rays(limit_bytes)
         return True
 
     def drop_trajectories(self):
@@ -178,6 +190,7 @@ class RayPlan:
         with torch.cuda.device(self.device):
             _lib.call("vam_ray_drop_trajectories", self._h)
         self.has_trajectories = False
+        self.cached_rays = 0
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
