@@ -559,7 +559,8 @@ def run_ray_bclp(dev, n=128, n_angles=360, steps=5, warmup=2, cpu=True):
         t0 = time.perf_counter()
         plan.prepare_trajectories()
         torch.cuda.synchronize(dev)
-        cache = {"bytes": int(plan.trajectory_bytes()), "prepare_ms": round((time.perf_counter() - t0) * 1e3, 2),
+        cache = {"bytes": int(plan.trajectory_bytes(plan.cached_rays)), "rays_cached": int(plan.cached_rays),
+                 "prepare_ms": round((time.perf_counter() - t0) * 1e3, 2),
                  "kernel_ms_traced": traced, "rays_active_at_cap_cached": active_cached,
                  "what": "ray paths traced once per medium (position and attenuance per step, 16 B per ray-step); "
                          "integrate / deposit stream them (integrate bit-identical, deposit equal up to atomic "
