@@ -67,6 +67,9 @@ def parse():
     ap.add_argument("--no-vec", action="store_true", help="skip the vector-geometry (inclined rays) projector leg")
     ap.add_argument("--ray-size", type=int, default=128)
     ap.add_argument("--e2e-iters", type=int, default=40, help="iterations of the timed optimize() call (e2e)")
+    ap.add_argument("--dist-backend", default="nccl", choices=["nccl", "gloo"],
+                    help="process-group backend of a multi-rank run (gloo: host collectives, e.g. to run the "
+                         "multi-rank control flow with several ranks on one device)")
     return ap.parse_args()
 
 
@@ -1059,6 +1062,7 @@ def run_ours(args):
     import torch
 
     ws_, rank, local = dist_env()
+    local = local % max(torch.cuda.device_count(), 1)  # one rank per device; ranks share devices only if asked
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     dist = None
@@ -1067,7 +1071,10 @@ def run_ours(args):
 
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+        if args.dist_backend == "nccl":
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
     from vamtoolbox_b200 import _lib
     from vamtoolbox_b200.optimizer.BCLP import BCLPNorm
 
