@@ -47,3 +47,34 @@ def test_build_matrix_rows_are_unit_backprojections():
     got = P.T @ b.ravel()
     assert np.linalg.norm(got - want) <= 1e-5 * np.linalg.norm(want)
     assert P.format == "csr" and P.shape == (b.size, tg.array.size)
+
+
+def test_package_namespace_and_resources(tmp_path, monkeypatch):
+    """The reference's examples use vam.optimize / vam.response / vam.imagesequence / vam.resources right
+    after `import vamtoolbox as vam`; resources.load resolves the reference's names in a resource folder."""
+    from argparse import ArgumentError
+
+    import vamtoolbox_b200 as vam
+
+    for name in ("optimize", "response", "metrics", "imagesequence", "resources", "projector", "optimizer",
+                 "projectorconstructor", "geometry", "medium", "util"):
+        assert hasattr(vam, name), name
+    assert callable(vam.optimize.optimize) and callable(vam.optimize.Options)
+    monkeypatch.setenv("VAMTOOLBOX_RESOURCES", str(tmp_path))
+    assert vam.resources.load("Flower.png") == str(tmp_path / "flower.png")
+    with pytest.raises(ArgumentError):
+        vam.resources.load("teapot.stl")
+
+
+def test_show_is_headless(caplog):
+    """The reference's examples end with .show() on targets, sinograms, reconstructions and loss logs; here
+    those calls log that nothing is drawn and return, so the scripts finish on a headless machine."""
+    from vamtoolbox_b200 import geometry
+    from vamtoolbox_b200.optimize import Options
+    from vamtoolbox_b200.optimizer.BCLP import LogPerf
+
+    tg = geometry.TargetGeometry(target=np.ones((8, 8)))
+    with caplog.at_level("WARNING"):
+        assert tg.show() is None
+        assert LogPerf(Options(method="BCLP", n_iter=2)).show() is None
+    assert "no display" in caplog.text

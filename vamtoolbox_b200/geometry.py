@@ -101,6 +101,15 @@ class Volume:
                 self.nR, self.nTheta, self.nZ = shape
                 self.resolution = self.nZ
 
+    def show(self, *args, **kwargs):
+        """The reference draws the volume with matplotlib / vedo (geometry.py show()); this package has no
+        display: it logs that nothing is drawn and returns, so a script that shows its results still runs
+        to the end headless (the data is ``self.array``)."""
+        import logging
+
+        logging.getLogger(__name__).warning("%s.show(): no display in this package; the data is .array",
+                                            type(self).__name__)
+
     def segmentZ(self, slices):
         if isinstance(slices, int) or (isinstance(slices, list) and len(slices) == 1):
             self.array = self.array[:, :, slices]

@@ -50,6 +50,11 @@ class LogPerf:
     def recordIterTime(self):
         self.iter_times[self.curr_iter] = time.perf_counter() - self.t0
 
+    def show(self, *args, **kwargs):
+        """The reference plots the loss and norm histories (BCLP.py:94-135); this package has no display:
+        it logs that nothing is drawn and returns (the histories are the arrays on this object)."""
+        logging.getLogger(__name__).warning("LogPerf.show(): no display in this package; see .loss, .l0 ... .lf_eps0")
+
     def save(self, filename):
         np.savetxt(filename, np.column_stack([range(self.options.n_iter + 1), self.iter_times, self.loss, self.l0,
                                               self.l1, self.l2, self.lf, self.l0_eps0, self.l1_eps0, self.l2_eps0,
