@@ -393,9 +393,13 @@ class ImageSeq:
             dill.dump(self, fh)
 
     def preview(self):
-        """The reference previews through its pyglet DLP player (vamtoolbox/dlp/players.py),
-        a windowing stack that is not part of this package."""
-        raise NotImplementedError("ImageSeq.preview needs the DLP player window, which this package does not provide")
+        """The reference previews through its pyglet DLP player (vamtoolbox/dlp/players.py), a windowing
+        stack that is not part of this package: like ``show()`` on volumes, this logs that nothing is shown
+        and returns, so a script runs to the end headless (the frames are ``self.images``; saveAsImages /
+        saveAsVideo write them)."""
+        import logging
+
+        logging.getLogger(__name__).warning("ImageSeq.preview(): no display in this package; see .images")
 
     def saveAsVideo(self, save_path, rot_vel, num_loops=1, mode="conventional", angle_increment_per_image=None,
                     preview=False):
