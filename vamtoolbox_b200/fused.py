@@ -8,6 +8,7 @@ graph with :func:`capture` and replayed.
 from __future__ import annotations
 
 import ctypes
+import gc
 
 import numpy as np
 import torch
@@ -130,12 +131,20 @@ def capture(fn, device):
     # garbage collection and empties the allocator cache on entry (tens of ms per capture), which the
     # captured launches here do not need (they allocate nothing)
     s.wait_stream(torch.cuda.current_stream(device))
-    with torch.cuda.stream(s):
-        g.capture_begin(capture_error_mode="global")
-        try:
-            fn()
-        finally:
-            g.capture_end()
+    # no garbage collection while capturing: a collected object that owns device memory (a plan released
+    # earlier) would free it inside the capture, which invalidates the graph
+    gc_on = gc.isenabled()
+    gc.disable()
+    try:
+        with torch.cuda.stream(s):
+            g.capture_begin(capture_error_mode="global")
+            try:
+                fn()
+            finally:
+                g.capture_end()
+    finally:
+        if gc_on:
+            gc.enable()
     torch.cuda.current_stream(device).wait_stream(s)
     g.instantiate()
     return g
