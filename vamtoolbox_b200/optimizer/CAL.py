@@ -100,7 +100,10 @@ class CALDevice:
         # initial sinogram: forward, filter (cuFFT), clip
         b = plan.forward(self.tgt)
         self.b = udata.filterSinogram_t(b, options.filter, lo=0.0)
-        self.x = plan.backward_ref(self.b)
+        # the zero-dose entries of b are set to 0 before every backprojection, as the reference's
+        # projector does (a no-op without a zero-dose region; the mask is built here, before any capture)
+        self.zd = getattr(A, "zero_dose_", lambda t: t)
+        self.x = plan.backward_ref(self.zd(self.b))
         ws.max(self.x, self.xmax)
         ws.ver(self.x, self.mask, self.ver)
         ws.append(self.ver, self.err_log, self.counter)
@@ -114,7 +117,7 @@ class CALDevice:
         ws.cal_threshold(self.x, self.xmax, self.tgt, o.d_h, o.sigmoid, self.xt)
         plan.forward(self.xt, self.db)
         ws.cal_update(self.b, self.db, self.db_prev if self.m != 0 else None, self.lr, self.m, it)
-        plan.backward_ref(self.b, self.x)
+        plan.backward_ref(self.zd(self.b), self.x)
         ws.max(self.x, self.xmax)
         ws.ver(self.x, self.mask, self.ver)
         ws.append(self.ver, self.err_log, self.counter)
@@ -156,7 +159,7 @@ def minimizeCAL(target_geo, proj_geo, options):
     b.clamp_(min=0)
     ws.max(b, bmax)
     ws.scale(b, bmax)
-    x_opt = plan.backward_ref(b)
+    x_opt = plan.backward_ref(c.zd(b))
     ws.max(x_opt, xmax)
     ws.scale(x_opt, xmax)
     err = c.err_log.double().cpu().numpy()

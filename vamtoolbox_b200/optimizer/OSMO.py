@@ -85,7 +85,10 @@ class OSMODevice:
         tgt = to_device_f64(target_geo.array, dev)
         self.xm = udata.filterTargetOSMO_t(tgt, options.filter).to(torch.float32).reshape(vs).contiguous()
         self.b = plan.forward(self.xm).clamp_(min=0)
-        self.x = plan.backward_ref(self.b)
+        # the zero-dose entries of b are set to 0 before every backprojection, as the reference's
+        # projector does (a no-op without a zero-dose region; the mask is built here, before any capture)
+        self.zd = getattr(A, "zero_dose_", lambda t: t)
+        self.x = plan.backward_ref(self.zd(self.b))
         ws.max(self.x, self.xmax)
         ws.scale(self.x, self.xmax)
         ws.ver(self.x, self.mask, self.ver)
@@ -98,7 +101,7 @@ class OSMODevice:
         plan.forward(self.xm, self.b)
         ws.max(self.b, self.bmax)
         ws.scale(self.b, self.bmax, floor=self.inh)
-        plan.backward_ref(self.b, self.x)
+        plan.backward_ref(self.zd(self.b), self.x)
         ws.max(self.x, self.xmax)
         ws.scale(self.x, self.xmax, floor=0.0)
 

@@ -82,7 +82,17 @@ class MultiTargetBCLP:
     # -- persistent schedule: phases over all targets
     # (the per-target passes between the batched launches run on the targets' own streams, so
     # the small ones overlap instead of queueing one after another)
+    @staticmethod
+    def _zero_dose(its):
+        # the targets' zero-dose sinogram entries set to 0 before their batched backprojections, as each
+        # target's own projector does (nothing is launched for a target without a zero-dose region)
+        for it in its:
+            zd = getattr(it.bclp.P, "zero_dose_", None)
+            if zd is not None:
+                zd(it.g)
+
     def state(self):
+        self._zero_dose(self.its)
         self.back.submit(self.back_work)
         self._fork_join(self._dose)
 
@@ -140,9 +150,11 @@ class MultiTargetBCLP:
             self.state()
             self.update()
         elif self.schedule == "phased":
+            self._zero_dose(self.half_a)
             self.phase1.submit(self.phase1_work)
             self._fork_join_over(self.half_a, self._dose)
             self._fork_join_over(self.half_b, self._update)
+            self._zero_dose(self.half_b)
             self.phase2.submit(self.phase2_work)
             self._fork_join_over(self.half_a, self._update)
             self._fork_join_over(self.half_b, self._dose)

@@ -357,16 +357,49 @@ class Projector3DParallel:
             self.plan.set_absorption("ray", alpha_per_px=float(proj_geo.absorption_coeff) * px,
                                      radius_px=float(proj_geo.container_radius) / px)
         self.absorption = absorption
+        self._zd_src, self._zd_mask = None, None
         if getattr(proj_geo, "attenuation_field", None) is not None:
             att = np.atleast_3d(np.asarray(proj_geo.attenuation_field))
             self.plan.set_occlusion(np.where(att > 0, 1.0, 0.0))
+
+    # -- zero-dose sinogram (geometry.ProjectionGeometry.calcZeroDoseSinogram) ----------------
+    def _zero_dose_applies(self):
+        # the reference's backward zeroes the entries in its ASTRA classes and 2-D classes
+        # (Projector3DParallel.py:43-44, Projector3DParallelCUDA.py:57-58, Projector2DParallel.py:206-207),
+        # not in the 3-D Python class it dispatches to when an attenuation field is set
+        zd = getattr(self.proj_geo, "zero_dose_sino", None)
+        return zd is not None and not (self.nZ > 1 and getattr(self.proj_geo, "attenuation_field", None) is not None)
+
+    def zero_dose_mask(self):
+        """The zero-dose entries as a device bool tensor of the sinogram's shape (built once per zero-dose
+        array, so call it before any graph capture), or None when no zero-dose region applies."""
+        if not self._zero_dose_applies():
+            return None
+        zd = self.proj_geo.zero_dose_sino
+        if self._zd_src is not zd:
+            self._zd_mask = torch.as_tensor(np.asarray(zd, dtype=bool), device=self.device).reshape(self.plan.shape_sino)
+            self._zd_src = zd
+        return self._zd_mask
+
+    def zero_dose_(self, b):
+        """b with its zero-dose entries set to 0 in place, as the reference's backward does before it
+        projects (a numpy array or a device tensor; b itself is returned); nothing without a zero-dose
+        region."""
+        if not self._zero_dose_applies():
+            return b
+        if isinstance(b, torch.Tensor):
+            m = self.zero_dose_mask()
+            b.view(self.plan.shape_sino).masked_fill_(m if m.device == b.device else m.to(b.device), 0.0)
+        else:
+            b[np.asarray(self.proj_geo.zero_dose_sino, dtype=bool).reshape(np.shape(b))] = 0.0
+        return b
 
     # -- device API ---------------------------------------------------------
     def forward_t(self, x, out=None):
         return self.plan.forward(_to_device(x, self.device, self.plan.shape_vol), out)
 
     def backward_t(self, b, out=None):
-        return self.plan.backward_ref(_to_device(b, self.device, self.plan.shape_sino), out)
+        return self.plan.backward_ref(self.zero_dose_(_to_device(b, self.device, self.plan.shape_sino)), out)
 
     def adjoint_t(self, b, out=None):
         return self.plan.adjoint(_to_device(b, self.device, self.plan.shape_sino), out)
@@ -379,7 +412,9 @@ class Projector3DParallel:
         return self.forward_t(x).double().cpu().numpy()
 
     def backward(self, b):
-        """Reference-parity backprojection (R2, Projector3DParallel.py:158-207)."""
+        """Reference-parity backprojection (R2, Projector3DParallel.py:158-207); the zero-dose entries of b
+        are set to 0 in place first, as the reference's backward does."""
+        self.zero_dose_(b)
         if isinstance(b, torch.Tensor) and b.is_cuda:
             return self.backward_t(b)
         return self.backward_t(b).double().cpu().numpy()
