@@ -332,7 +332,12 @@ class BCLPNorm:
         P = self.P
         plan = getattr(P, "plan", None)
         if plan is not None and hasattr(plan, "backward_ref"):
-            return (lambda g, out: plan.backward_ref(g, out), lambda x, out: plan.forward(x, out),
+            # the zero-dose entries of g are set to 0 before every backprojection, as the reference's
+            # projector does (no-op without a zero-dose region; the mask is built now, before any capture)
+            zd = getattr(P, "zero_dose_", lambda t: t)
+            if hasattr(P, "zero_dose_mask"):
+                P.zero_dose_mask()
+            return (lambda g, out: plan.backward_ref(zd(g), out), lambda x, out: plan.forward(x, out),
                     plan.shape_vol, plan.shape_sino, P.device)
         if plan is not None and hasattr(plan, "deposit"):
             # the ray paths depend on the medium only: trace them once for the whole run when the cache
@@ -406,8 +411,18 @@ class BCLPNorm:
         self.dose, g = to_host_f64(self.dose_t, it.g)
         return g.reshape(-1)
 
+    def _device_engine_ok(self):
+        """The fused engine serves this problem: a projector of this package with device entry points
+        (parallel-beam plan, ray plan, vector geometry) and a device form of the response model."""
+        P, plan = self.P, getattr(self.P, "plan", None)
+        proj_ok = plan is not None and (hasattr(plan, "backward_ref") or hasattr(plan, "deposit")
+                                        or (hasattr(P, "backward_t") and hasattr(P, "forward_t")))
+        return proj_ok and self._device_response_ok()
+
     def gradientDescent(self):
-        if getattr(self.options, "engine", "device") == "host":
+        """The fused device engine where it serves the problem, else the reference's host loop (the
+        algebraic propagator, response models without a device form, or engine="host")."""
+        if getattr(self.options, "engine", "device") == "host" or not self._device_engine_ok():
             return self.gradientDescentHost()
         return self.gradientDescentDevice()
 
