@@ -73,8 +73,16 @@ def test_show_is_headless(caplog):
     from vamtoolbox_b200.optimize import Options
     from vamtoolbox_b200.optimizer.BCLP import LogPerf
 
+    from vamtoolbox_b200 import medium
+    from vamtoolbox_b200.response import ResponseModel
+
     tg = geometry.TargetGeometry(target=np.ones((8, 8)))
+    cv = tg.constructCoordVec()
     with caplog.at_level("WARNING"):
         assert tg.show() is None
         assert LogPerf(Options(method="BCLP", n_iter=2)).show() is None
-    assert "no display" in caplog.text
+        im = medium.IndexModel(cv, type="analytical", form="homogeneous")
+        am = medium.AttenuationModel(cv, type="analytical", form="homogeneous_cylinder", R=1, alpha_internal=0.2)
+        assert im.plotIndex(block=False) is None and am.plotAlpha(block=True) is None
+        assert ResponseModel(form="gen_log_fun", B=10).plotMap(None, None, label="B=10") is None
+    assert caplog.text.count("no display") >= 5

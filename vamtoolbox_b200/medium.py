@@ -93,6 +93,12 @@ class MediumModel:
         return R * (min(spans[0], spans[1]) if self.coord_vec[2].size == 1 else min(spans))
 
 
+def _no_display(obj, name):
+    """The reference draws these with matplotlib; this package has no display: log that nothing is drawn
+    and return, so a script runs to the end headless (the fields are the model's presampled arrays)."""
+    logging.getLogger(__name__).warning("%s.%s(): no display in this package", type(obj).__name__, name)
+
+
 class IndexModel(MediumModel):
     """Refractive index n(x) and its gradient (medium.py:276-473)."""
 
@@ -246,6 +252,22 @@ class AttenuationModel(MediumModel):
         if self.type == "interpolation":
             return self.presampled_scalar_field_3D.to(dtype=torch.float32).contiguous()
         return self.alpha(self.getPositionVectorsAtGridPoints()).reshape(self.shape).to(torch.float32).contiguous()
+
+
+def _headless(name):
+    def method(self, *args, **kwargs):
+        _no_display(self, name)
+
+    method.__name__ = name
+    method.__doc__ = "The reference's plot of the field (medium.py); headless here: logs and returns."
+    return method
+
+
+# the reference's plotting methods (medium.py:570-751, 918-990), headless
+for _cls, _names in ((IndexModel, ("plotIndex", "plotGradNMag", "plotRandomlySampledIndex", "plotIndexAtPosition")),
+                     (AttenuationModel, ("plotAlpha", "plotRandomlySampledAlpha", "plotAlphaAtPosition"))):
+    for _n in _names:
+        setattr(_cls, _n, _headless(_n))
 
 
 class AbsorptionModel(AttenuationModel):

@@ -215,6 +215,24 @@ class ResponseModel:
                                  float(np.float32(f[0])), float((f.size - 1) / (f[-1] - f[0])))
         return self._tables[key]
 
+    def _no_display(self, name):
+        import logging
+
+        logging.getLogger(__name__).warning("ResponseModel.%s(): no display in this package", name)
+
+    def plotMap(self, *args, **kwargs):
+        """The reference plots the response curve with matplotlib (response.py:294-339); headless here:
+        logs and returns (the curve is ``map`` over a dose range)."""
+        self._no_display("plotMap")
+
+    def plotDmapDf(self, *args, **kwargs):
+        """Headless counterpart of the reference's derivative plot: logs and returns."""
+        self._no_display("plotDmapDf")
+
+    def plotMapInv(self, *args, **kwargs):
+        """Headless counterpart of the reference's inverse-map plot (response.py:340-): logs and returns."""
+        self._no_display("plotMapInv")
+
     def __repr__(self):
         return str(self.params)
 
