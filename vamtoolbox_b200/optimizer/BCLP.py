@@ -350,7 +350,16 @@ class BCLPNorm:
             # vector-geometry (ASTRA-model) projector: its wrappers carry the circle clip and mask
             return (lambda g, out: P.backward_t(g, out), lambda x, out: P.forward_t(x, out),
                     plan.shape_vol, plan.shape_sino, P.device)
+        if self._algebraic():
+            # algebraic propagator: its CSR products (z-tiled) into the iteration's buffers
+            return (lambda g, out: P.backward_t(g, out), lambda x, out: P.forward_t(x, out),
+                    tuple(np.shape(self.target_geo.array)), (P.n_row_eff,), P.device)
         raise TypeError("the device engine needs a vamtoolbox_b200 projector")
+
+    def _algebraic(self):
+        from ..projector.pyTorchAlgebraicPropagation import PyTorchAlgebraicPropagator
+
+        return isinstance(self.P, PyTorchAlgebraicPropagator)
 
     def _device_response_ok(self):
         return getattr(self.response_model, "has_device_form", lambda: False)()
@@ -413,15 +422,16 @@ class BCLPNorm:
 
     def _device_engine_ok(self):
         """The fused engine serves this problem: a projector of this package with device entry points
-        (parallel-beam plan, ray plan, vector geometry) and a device form of the response model."""
+        (parallel-beam plan, ray plan, vector geometry, algebraic propagator) and a device form of the
+        response model."""
         P, plan = self.P, getattr(self.P, "plan", None)
         proj_ok = plan is not None and (hasattr(plan, "backward_ref") or hasattr(plan, "deposit")
                                         or (hasattr(P, "backward_t") and hasattr(P, "forward_t")))
-        return proj_ok and self._device_response_ok()
+        return (proj_ok or self._algebraic()) and self._device_response_ok()
 
     def gradientDescent(self):
-        """The fused device engine where it serves the problem, else the reference's host loop (the
-        algebraic propagator, response models without a device form, or engine="host")."""
+        """The fused device engine where it serves the problem, else the reference's host loop (response
+        models without a device form, or engine="host")."""
         if getattr(self.options, "engine", "device") == "host" or not self._device_engine_ok():
             return self.gradientDescentHost()
         return self.gradientDescentDevice()

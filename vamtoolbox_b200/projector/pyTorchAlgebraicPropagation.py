@@ -99,6 +99,21 @@ class PyTorchAlgebraicPropagator:
         y = y.flatten().to(self.dtype)
         return y if self.output_torch_tensor else y.cpu().numpy()
 
+    def _spmm_into(self, csr, n_out_rows, x, out):
+        row_ptr, cols, vals = csr
+        _lib.call("vam_csr_spmm", n_out_rows, _lib.ptr(row_ptr), _lib.ptr(cols), _lib.ptr(vals), _lib.ptr(x),
+                  self.z_tiling, _lib.ptr(out), _lib.stream_ptr(torch.cuda.current_stream(self.device)))
+        return out
+
+    def forward_t(self, x, out):
+        """b = P x into ``out`` on the current stream: x and out contiguous float32 tensors on the device
+        with n_col_eff and n_row_eff elements.  Allocates nothing (the fused BCLP engine captures it)."""
+        return self._spmm_into(self._A, self.n_row_internal, x, out)
+
+    def backward_t(self, b, out):
+        """x = P^T b into ``out`` on the current stream (as forward_t)."""
+        return self._spmm_into(self._AT, self.n_col_internal, b, out)
+
     def forward(self, x):
         """b = P x, x of n_col_eff voxels (z tiled), b of n_row_eff elements (pyTorchAlgebraicPropagation.py:146-163)."""
         return self._apply(self._A, self.n_row_internal, x)
