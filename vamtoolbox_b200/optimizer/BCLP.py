@@ -329,37 +329,12 @@ class BCLPNorm:
 
     # -- device engine ---------------------------------------------------------
     def _device_projector_ops(self):
-        P = self.P
-        plan = getattr(P, "plan", None)
-        if plan is not None and hasattr(plan, "backward_ref"):
-            # the zero-dose entries of g are set to 0 before every backprojection, as the reference's
-            # projector does (no-op without a zero-dose region; the mask is built now, before any capture)
-            zd = getattr(P, "zero_dose_", lambda t: t)
-            if hasattr(P, "zero_dose_mask"):
-                P.zero_dose_mask()
-            return (lambda g, out: plan.backward_ref(zd(g), out), lambda x, out: plan.forward(x, out),
-                    plan.shape_vol, plan.shape_sino, P.device)
-        if plan is not None and hasattr(plan, "deposit"):
-            # the ray paths depend on the medium only: trace them once for the whole run when the cache
-            # fits (half of the free device memory), before any capture
-            if self.logs.options.n_iter > 1 and not getattr(plan, "has_trajectories", True):
-                plan.prepare_trajectories()
-            return (lambda g, out: plan.deposit(g, out), lambda x, out: plan.integrate(x, out),
-                    plan.grid_shape, (plan.num_rays,), P.device)
-        if plan is not None and hasattr(P, "backward_t") and hasattr(P, "forward_t"):
-            # vector-geometry (ASTRA-model) projector: its wrappers carry the circle clip and mask
-            return (lambda g, out: P.backward_t(g, out), lambda x, out: P.forward_t(x, out),
-                    plan.shape_vol, plan.shape_sino, P.device)
-        if self._algebraic():
-            # algebraic propagator: its CSR products (z-tiled) into the iteration's buffers
-            return (lambda g, out: P.backward_t(g, out), lambda x, out: P.forward_t(x, out),
-                    tuple(np.shape(self.target_geo.array)), (P.n_row_eff,), P.device)
-        raise TypeError("the device engine needs a vamtoolbox_b200 projector")
+        from ._device_ops import device_ops
 
-    def _algebraic(self):
-        from ..projector.pyTorchAlgebraicPropagation import PyTorchAlgebraicPropagator
-
-        return isinstance(self.P, PyTorchAlgebraicPropagator)
+        ops = device_ops(self.P, self.target_geo, self.logs.options.n_iter)
+        if ops is None:
+            raise TypeError("the device engine needs a vamtoolbox_b200 projector")
+        return ops
 
     def _device_response_ok(self):
         return getattr(self.response_model, "has_device_form", lambda: False)()
@@ -425,9 +400,12 @@ class BCLPNorm:
         (parallel-beam plan, ray plan, vector geometry, algebraic propagator) and a device form of the
         response model."""
         P, plan = self.P, getattr(self.P, "plan", None)
-        proj_ok = plan is not None and (hasattr(plan, "backward_ref") or hasattr(plan, "deposit")
-                                        or (hasattr(P, "backward_t") and hasattr(P, "forward_t")))
-        return (proj_ok or self._algebraic()) and self._device_response_ok()
+        from ..projector.pyTorchAlgebraicPropagation import PyTorchAlgebraicPropagator
+
+        proj_ok = (plan is not None and (hasattr(plan, "backward_ref") or hasattr(plan, "deposit")
+                                         or (hasattr(P, "backward_t") and hasattr(P, "forward_t")))
+                   or isinstance(P, PyTorchAlgebraicPropagator))
+        return proj_ok and self._device_response_ok()
 
     def gradientDescent(self):
         """The fused device engine where it serves the problem, else the reference's host loop (response

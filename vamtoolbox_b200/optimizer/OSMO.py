@@ -70,13 +70,16 @@ class OSMODevice:
     records a step once as a CUDA graph.
     """
 
-    def __init__(self, target_geo, proj_geo, options, A):
+    def __init__(self, target_geo, proj_geo, options, A, ops=None):
+        from ._device_ops import device_ops
+
         self.options = options
         self.A = A
-        dev = self.device = A.device
-        plan = self.plan = A.plan
+        # the projector's device entry points: back(b, out), fwd(x, out) (parallel beam, vector geometry,
+        # ray tracer, algebraic propagator)
+        self.back, self.fwd, vs, ss, dev = ops if ops is not None else device_ops(A, target_geo, options.n_iter)
+        self.device = dev
         ws = self.ws = Workspace(dev)
-        vs = plan.shape_vol
         self.mask = torch.as_tensor(metrics.region_mask(target_geo).reshape(vs), device=dev)
         n_iter = options.n_iter
         self.err_log = torch.full((max(n_iter, 1),), float("nan"), dtype=torch.float32, device=dev)
@@ -84,11 +87,11 @@ class OSMODevice:
         self.ver, self.xmax, self.bmax = ws.scalar(), ws.scalar(), ws.scalar()
         tgt = to_device_f64(target_geo.array, dev)
         self.xm = udata.filterTargetOSMO_t(tgt, options.filter).to(torch.float32).reshape(vs).contiguous()
-        self.b = plan.forward(self.xm).clamp_(min=0)
-        # the zero-dose entries of b are set to 0 before every backprojection, as the reference's
-        # projector does (a no-op without a zero-dose region; the mask is built here, before any capture)
-        self.zd = getattr(A, "zero_dose_", lambda t: t)
-        self.x = plan.backward_ref(self.zd(self.b))
+        self.b = torch.empty(ss, dtype=torch.float32, device=dev)
+        self.x = torch.empty(vs, dtype=torch.float32, device=dev)
+        self.fwd(self.xm, self.b)
+        self.b.clamp_(min=0)
+        self.back(self.b, self.x)
         ws.max(self.x, self.xmax)
         ws.scale(self.x, self.xmax)
         ws.ver(self.x, self.mask, self.ver)
@@ -96,12 +99,12 @@ class OSMODevice:
         self.inh = float(options.inhibition)
 
     def half(self, gel):
-        o, ws, plan = self.options, self.ws, self.plan
+        o, ws = self.options, self.ws
         ws.osmo_model(self.xm, self.x, None, self.mask, gel, o.d_h if gel else o.d_l)
-        plan.forward(self.xm, self.b)
+        self.fwd(self.xm, self.b)
         ws.max(self.b, self.bmax)
         ws.scale(self.b, self.bmax, floor=self.inh)
-        plan.backward_ref(self.zd(self.b), self.x)
+        self.back(self.b, self.x)
         ws.max(self.x, self.xmax)
         ws.scale(self.x, self.xmax, floor=0.0)
 
@@ -116,13 +119,15 @@ class OSMODevice:
 
 
 def minimizeOSMO(target_geo, proj_geo, options):
-    from ..projector.Projector3DParallel import Projector3DParallel
+    from ._device_ops import device_ops
 
     A = projectorconstructor(target_geo, proj_geo)
-    if (getattr(options, "engine", "device") == "host" or not isinstance(A, Projector3DParallel)
-            or options.bit_depth is not None):
+    ops = None
+    if getattr(options, "engine", "device") != "host" and options.bit_depth is None:
+        ops = device_ops(A, target_geo, options.n_iter)
+    if ops is None:
         return _osmo_host(target_geo, proj_geo, options, A)
-    it = OSMODevice(target_geo, proj_geo, options, A)
+    it = OSMODevice(target_geo, proj_geo, options, A, ops)
     dev, n_iter = it.device, options.n_iter
     st = torch.cuda.current_stream(dev)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
