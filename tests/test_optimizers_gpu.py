@@ -316,10 +316,11 @@ def test_zero_dose_region_device_engine_matches_host_engine(method):
     assert relL2(out["device"], out["host"]) < 1e-4
 
 
-def test_osmo_device_engine_on_vector_geometry_matches_host_engine():
-    """OSMO with inclined rays (the vector-geometry projector) runs on the fused device engine -- the
-    projector's forward / backprojection into the engine's buffers, captured with the model update and
-    normalisations -- and gives the reference's host loop result."""
+@pytest.mark.parametrize("method", ["OSMO", "CAL"])
+def test_device_engine_on_vector_geometry_matches_host_engine(method):
+    """OSMO and CAL with inclined rays (the vector-geometry projector) run on the fused device engines --
+    the projector's forward / backprojection into the engine's buffers, captured with the updates and
+    normalisations -- and give the reference's host loop results."""
     from vamtoolbox_b200 import geometry
     from vamtoolbox_b200.optimize import optimize
 
@@ -331,8 +332,9 @@ def test_osmo_device_engine_on_vector_geometry_matches_host_engine():
         tg = geometry.TargetGeometry(target=t.copy())
         pg = geometry.ProjectionGeometry(np.linspace(0, 360, 30, endpoint=False), "parallel", CUDA=True,
                                          inclination_angle=15.0)
-        sino, recon, err = optimize(tg, pg, opts(method="OSMO", n_iter=4, d_h=0.85, d_l=0.6, filter="hamming",
-                                                 engine=engine))
+        kw = (dict(n_iter=4, d_h=0.85, d_l=0.6, filter="hamming") if method == "OSMO"
+              else dict(n_iter=4, learning_rate=0.4, d_h=0.5, sigmoid=0.01))
+        sino, recon, err = optimize(tg, pg, opts(method=method, engine=engine, **kw))
         out[engine] = (np.asarray(sino.array), np.asarray(recon.array), np.asarray(err))
     assert relL2(out["device"][0], out["host"][0]) < 1e-4
     assert relL2(out["device"][1], out["host"][1]) < 1e-4

@@ -84,12 +84,14 @@ class CALDevice:
     graph when the momentum is zero.
     """
 
-    def __init__(self, target_geo, proj_geo, options, A):
+    def __init__(self, target_geo, proj_geo, options, A, ops=None):
+        from ._device_ops import device_ops
+
         self.options = options
-        dev = self.device = A.device
+        # the projector's device entry points: back(b, out), fwd(x, out) (parallel beam, vector geometry)
+        self.back, self.fwd, vs, ss, dev = ops if ops is not None else device_ops(A, target_geo, options.n_iter)
+        self.device = dev
         ws = self.ws = Workspace(dev)
-        plan = self.plan = A.plan
-        vs, ss = plan.shape_vol, plan.shape_sino
         self.tgt = torch.as_tensor(np.ascontiguousarray(np.atleast_3d(target_geo.array), dtype=np.float32),
                                    device=dev)
         self.mask = torch.as_tensor(metrics.region_mask(target_geo).reshape(vs), device=dev)
@@ -98,12 +100,11 @@ class CALDevice:
         self.counter = torch.zeros(1, dtype=torch.int32, device=dev)
         self.ver, self.xmax = ws.scalar(), ws.scalar()
         # initial sinogram: forward, filter (cuFFT), clip
-        b = plan.forward(self.tgt)
+        b = torch.empty(ss, dtype=torch.float32, device=dev)
+        self.fwd(self.tgt, b)
         self.b = udata.filterSinogram_t(b, options.filter, lo=0.0)
-        # the zero-dose entries of b are set to 0 before every backprojection, as the reference's
-        # projector does (a no-op without a zero-dose region; the mask is built here, before any capture)
-        self.zd = getattr(A, "zero_dose_", lambda t: t)
-        self.x = plan.backward_ref(self.zd(self.b))
+        self.x = torch.empty(vs, dtype=torch.float32, device=dev)
+        self.back(self.b, self.x)
         ws.max(self.x, self.xmax)
         ws.ver(self.x, self.mask, self.ver)
         ws.append(self.ver, self.err_log, self.counter)
@@ -113,25 +114,30 @@ class CALDevice:
         self.m, self.lr = float(options.momentum), float(options.learning_rate)
 
     def step(self, it):
-        o, ws, plan = self.options, self.ws, self.plan
+        o, ws = self.options, self.ws
         ws.cal_threshold(self.x, self.xmax, self.tgt, o.d_h, o.sigmoid, self.xt)
-        plan.forward(self.xt, self.db)
+        self.fwd(self.xt, self.db)
         ws.cal_update(self.b, self.db, self.db_prev if self.m != 0 else None, self.lr, self.m, it)
-        plan.backward_ref(self.zd(self.b), self.x)
+        self.back(self.b, self.x)
         ws.max(self.x, self.xmax)
         ws.ver(self.x, self.mask, self.ver)
         ws.append(self.ver, self.err_log, self.counter)
 
 
 def minimizeCAL(target_geo, proj_geo, options):
-    from ..projector.Projector3DParallel import Projector3DParallel
+    from ._device_ops import device_ops
 
     A = projectorconstructor(target_geo, proj_geo)
-    if (getattr(options, "engine", "device") == "host" or options.d_h is None or options.bit_depth is not None
-            or not isinstance(A, Projector3DParallel)):
+    ops = None
+    if getattr(options, "engine", "device") != "host" and options.d_h is not None and options.bit_depth is None:
+        ops = device_ops(A, target_geo, options.n_iter)
+    # the set-up filters the sinogram along its detector axis: projectors with a (detector, angle, z)
+    # sinogram (parallel beam, vector geometry); the ray tracer's and algebraic propagator's flat ones
+    # take the host loop
+    if ops is None or len(ops[3]) != 3:
         return _cal_host(target_geo, proj_geo, options, A)
-    c = CALDevice(target_geo, proj_geo, options, A)
-    dev, ws, plan, n_iter, m = c.device, c.ws, c.plan, options.n_iter, c.m
+    c = CALDevice(target_geo, proj_geo, options, A, ops)
+    dev, ws, n_iter, m = c.device, c.ws, options.n_iter, c.m
     st = torch.cuda.current_stream(dev)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     done = 0
@@ -159,7 +165,8 @@ def minimizeCAL(target_geo, proj_geo, options):
     b.clamp_(min=0)
     ws.max(b, bmax)
     ws.scale(b, bmax)
-    x_opt = plan.backward_ref(c.zd(b))
+    x_opt = torch.empty_like(c.x)
+    c.back(b, x_opt)
     ws.max(x_opt, xmax)
     ws.scale(x_opt, xmax)
     err = c.err_log.double().cpu().numpy()
