@@ -80,6 +80,11 @@ def test_ray_traced_and_algebraic_example_flows(image_file, tmp_path):
                                         response_model=vam.response.ResponseModel(B=25), eps=0.1)
     sino, recon, resp, logs = vam.optimize.optimize(tg, pg, opts(), output="full")
     assert np.isfinite(recon.array).all() and np.isfinite(logs.loss[:4]).all()
+    # OSMO through the ray tracer on the fused engine (deposit / integrate into the engine's buffers)
+    s_o, r_o, e_o = vam.optimize.optimize(tg, pg, vam.optimize.Options(method="OSMO", n_iter=3, d_h=0.85, d_l=0.6,
+                                                                      filter="hamming"))
+    assert np.isfinite(np.asarray(s_o.array)).all() and np.isfinite(np.asarray(r_o.array)).all()
+    assert np.asarray(r_o.array).size == np.asarray(tg.array).size and np.isfinite(e_o[:3]).all()
     P = vam.projector.pyTorchRayTrace.PyTorchRayTracingPropagator(tg, pg, output_torch_tensor=False)
     M = P.buildPropagationMatrix()
     path = str(tmp_path / "P.npz")
